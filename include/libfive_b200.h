@@ -1,0 +1,124 @@
+/*
+ *  Additional entry points of the B200 implementation (additive: nothing in
+ *  libfive.h changes).  They expose what the reference keeps behind C++
+ *  classes — reusable evaluators, batched evaluation of many points, the
+ *  gradient with respect to free variables — as plain C calls over flat
+ *  float arrays, so that the GPU can be fed large batches.
+ *
+ *  Pointer arguments are host pointers unless LFB_DEVICE_PTRS is set in
+ *  `flags`, in which case they are CUDA device pointers and `stream` (a
+ *  cudaStream_t, or NULL for the legacy default stream) orders the work.
+ *  Every call returns 0 on success or a negative LFB_E* code; the message of
+ *  the last failure on the calling thread is read with lfb_last_error.
+ */
+#pragma once
+#include "libfive.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    LFB_OK = 0,
+    LFB_E_INVALID = -1,      /* bad argument / invalid tree */
+    LFB_E_UNSUPPORTED = -2,  /* opcode or feature the device path lacks */
+    LFB_E_CUDA = -3,         /* CUDA error or no CUDA device */
+    LFB_E_CAPACITY = -4,     /* a device buffer was too small (retried
+                                internally; reported only if retries fail) */
+    LFB_E_CANCELLED = -5,
+};
+
+#define LFB_DEVICE_PTRS 1u
+
+/* Message and code of the last failure on this thread. */
+int lfb_last_error(char* buf, uint32_t len);
+
+/*  A device tape: the tree flattened once (Deck, deck.cpp:19-94) and kept
+ *  resident on the GPU, with values for its free variables (unlisted
+ *  variables read as zero).  Replaces constructing a libfive::Evaluator
+ *  (libfive/include/libfive/eval/evaluator.hpp:16-50). */
+typedef struct lfb_tape_* lfb_tape;
+lfb_tape lfb_tape_new(libfive_tree t, libfive_vars vars);
+void lfb_tape_delete(lfb_tape t);
+/* Evaluator::updateVars (evaluator.hpp:35-44); returns 1 if any changed. */
+int lfb_tape_set_vars(lfb_tape t, libfive_vars vars);
+/* counts[0..5] = clauses, registers, constants, free variables, min/max
+ * clauses, reference slot count (Deck::num_clauses). */
+int lfb_tape_info(lfb_tape t, uint32_t counts[6]);
+/* Variable order used by the gradient calls: var_ids[i] receives the
+ * libfive_tree_id of variable i (ascending reference slot order, as
+ * JacobianEvaluator::gradient, eval_jacobian.cpp:77-90). */
+int lfb_tape_var_ids(lfb_tape t, const void** var_ids, uint32_t len);
+
+/* ArrayEvaluator::values (eval_array.cpp:106-118) over n points. */
+int lfb_eval_values(lfb_tape t, uint64_t n, const float* x, const float* y,
+                    const float* z, float* out, void* stream, uint32_t flags);
+
+/* DerivArrayEvaluator::derivs (eval_deriv_array.cpp:101-117): value and
+ * d/dx, d/dy, d/dz (any of dx/dy/dz may be NULL). */
+int lfb_eval_derivs(lfb_tape t, uint64_t n, const float* x, const float* y,
+                    const float* z, float* v, float* dx, float* dy, float* dz,
+                    void* stream, uint32_t flags);
+
+/* IntervalEvaluator::eval (eval_interval.cpp:68-93) over n boxes; out_nan
+ * receives the "may be NaN" flag (0/1). */
+int lfb_eval_intervals(lfb_tape t, uint64_t n,
+                       const float* xlo, const float* xhi,
+                       const float* ylo, const float* yhi,
+                       const float* zlo, const float* zhi,
+                       float* out_lo, float* out_hi, uint8_t* out_nan,
+                       void* stream, uint32_t flags);
+
+/* JacobianEvaluator::gradient (eval_jacobian.cpp:49-115) for n points:
+ * out[i * n_vars + k] = df(p_i)/dvar_k (CONST_VAR blocks the gradient). */
+int lfb_eval_jacobian(lfb_tape t, uint64_t n, const float* x,
+                      const float* y, const float* z, float* out,
+                      void* stream, uint32_t flags);
+
+/*  Reverse-mode gradient (new; the reference has forward mode only).
+ *  For each point i: f[i] = f(p_i); with seed s_i (1 when seed is NULL):
+ *    gx/gy/gz[i] = s_i * df/dp_i            (any of them may be NULL)
+ *    gvars[k]   += sum_i s_i * df(p_i)/dvar_k   (if gvars is not NULL;
+ *                  accumulated, so zero it first)
+ *  Subgradient choices at min / max / abs match the forward rules of
+ *  DerivArrayEvaluator (eval_deriv_array.cpp:139-146, 219-222). */
+int lfb_eval_grad(lfb_tape t, uint64_t n, const float* x, const float* y,
+                  const float* z, const float* seed, float* f, float* gx,
+                  float* gy, float* gz, float* gvars, void* stream,
+                  uint32_t flags);
+
+/*  Mesh settings (BRepSettings, settings.hpp:27-74, minus the CPU-thread
+ *  fields).  min_feature: subdivide until cells are smaller; max_err: QEF
+ *  error below which cells collapse (negative disables collapsing). */
+typedef struct lfb_mesh_settings {
+    double min_feature;
+    double max_err;
+} lfb_mesh_settings;
+
+typedef struct lfb_mesh_stats {
+    uint32_t levels;           /* octree depth (Region::withResolution) */
+    uint64_t cells_evaluated;  /* interval-evaluated cells, all levels */
+    uint64_t leaf_groups;      /* sibling groups evaluated at the finest level */
+    uint64_t leaves_ambiguous;
+    uint64_t clause_evals;     /* point clause evaluations in leaf kernels */
+    double ms_total;           /* device time of the whole pipeline */
+} lfb_mesh_stats;
+
+/* Mesh::render with DUAL_CONTOURING (mesh.cpp:35-125) on the GPU.  The
+ * result is freed with libfive_mesh_delete; NULL on failure. */
+libfive_mesh* lfb_render_mesh(lfb_tape t, libfive_region3 R,
+                              lfb_mesh_settings settings,
+                              lfb_mesh_stats* stats);
+
+/* The reference-layout tape of a tree (Deck, deck.cpp:19-94), for
+ * checking slot numbering and for CPU cross-checks.  counts[0..7] =
+ * num_clauses, tape length, constants, variables, X, Y, Z, root slot.
+ * clauses holds 4 int32 per clause (op, id, a, b) root first; any array may
+ * be NULL (call once with NULLs to size them). */
+int lfb_tree_slot_tape(libfive_tree t, uint32_t counts[8], int32_t* clauses,
+                       uint32_t* const_slots, float* const_values,
+                       uint32_t* var_slots, const void** var_ids);
+
+#ifdef __cplusplus
+}
+#endif

@@ -1,0 +1,613 @@
+// libfive.h and libfive_b200.h entry points.
+//
+// Tree construction follows libfive/src/libfive.cpp:75-190; evaluation and
+// meshing run on the GPU through the device tapes in runtime.cpp and the
+// kernels in eval_kernels.cu / dc_mesher.cu.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+
+#include "libfive.h"
+#include "libfive_b200.h"
+#include "mesher.hpp"
+#include "eval_api.hpp"
+#include "runtime.hpp"
+#include "tree.hpp"
+
+using namespace lfb;
+
+static const Node* N(libfive_tree t) { return reinterpret_cast<const Node*>(t); }
+static libfive_tree H(const Node* n)
+{
+    return reinterpret_cast<libfive_tree>(const_cast<Node*>(n));
+}
+
+struct lfb_tape_ {
+    std::shared_ptr<GpuTape> g;
+};
+
+struct libfive_evaluator_ {
+    std::shared_ptr<GpuTape> g;
+};
+
+extern "C" {
+
+////////////////////////////////////////////////////////////////////////////////
+// Deleters (libfive.cpp:31-71)
+
+void libfive_contours_delete(libfive_contours* cs)
+{
+    if (!cs) return;
+    for (unsigned i = 0; i < cs->count; ++i) delete[] cs->cs[i].pts;
+    delete[] cs->cs;
+    delete cs;
+}
+
+void libfive_contours3_delete(libfive_contours3* cs)
+{
+    if (!cs) return;
+    for (unsigned i = 0; i < cs->count; ++i) delete[] cs->cs[i].pts;
+    delete[] cs->cs;
+    delete cs;
+}
+
+void libfive_mesh_delete(libfive_mesh* m)
+{
+    if (!m) return;
+    delete[] m->verts;
+    delete[] m->tris;
+    delete m;
+}
+
+void libfive_mesh_coords_delete(libfive_mesh_coords* m)
+{
+    if (!m) return;
+    delete[] m->verts;
+    delete[] m->coord_indices;
+    delete m;
+}
+
+void libfive_pixels_delete(libfive_pixels* m)
+{
+    if (!m) return;
+    delete[] m->pixels;
+    delete m;
+}
+
+void libfive_vars_delete(libfive_vars* vs)
+{
+    if (!vs) return;
+    delete[] vs->vars;
+    delete[] vs->values;
+    delete vs;
+}
+
+int libfive_opcode_enum(const char* name)
+{
+    if (!name) return -1;
+    const int o = op::from_scm_name(name);
+    return (o == op::INVALID || o == op::LAST_OP) ? -1 : o;
+}
+
+int libfive_opcode_args(int o)
+{
+    return (o >= 0 && o < op::LAST_OP) ? op::arity(o) : -1;
+}
+
+////////////////////////////////////////////////////////////////////////////////
+// Trees (libfive.cpp:75-190)
+
+libfive_tree libfive_tree_x(void) { return H(Tree::X().release()); }
+libfive_tree libfive_tree_y(void) { return H(Tree::Y().release()); }
+libfive_tree libfive_tree_z(void) { return H(Tree::Z().release()); }
+libfive_tree libfive_tree_var(void) { return H(Tree::var().release()); }
+libfive_tree libfive_tree_const(float f) { return H(Tree::constant(f).release()); }
+
+bool libfive_tree_is_var(libfive_tree t)
+{
+    return t && Tree(N(t)).op() == op::VAR_FREE;
+}
+
+float libfive_tree_get_const(libfive_tree t, bool* success)
+{
+    if (t && N(t)->kind == Kind::Constant) {
+        if (success) *success = true;
+        return N(t)->value;
+    }
+    if (success) *success = false;
+    return 0;
+}
+
+static bool opcode_ok(int o, int args)
+{
+    return o >= 0 && o < op::LAST_OP && op::arity(o) == args;
+}
+
+libfive_tree libfive_tree_nullary(int o)
+{
+    return opcode_ok(o, 0) ? H(Tree::nullary(o).release()) : nullptr;
+}
+
+libfive_tree libfive_tree_unary(int o, libfive_tree a)
+{
+    return (opcode_ok(o, 1) && a) ? H(Tree::unary(o, Tree(N(a))).release())
+                                  : nullptr;
+}
+
+libfive_tree libfive_tree_binary(int o, libfive_tree a, libfive_tree b)
+{
+    return (opcode_ok(o, 2) && a && b)
+        ? H(Tree::binary(o, Tree(N(a)), Tree(N(b))).release())
+        : nullptr;
+}
+
+const void* libfive_tree_id(libfive_tree t)
+{
+    return static_cast<const void*>(t);
+}
+
+void libfive_tree_delete(libfive_tree ptr)
+{
+    if (!ptr) return;
+    invalidate_cached(N(ptr));
+    Tree::reclaim(N(ptr));
+}
+
+bool libfive_tree_save(libfive_tree, const char*)
+{
+    std::fprintf(stderr, "libfive_tree_save: tree serialization is not "
+                         "provided by libfive_b200\n");
+    return false;
+}
+
+libfive_tree libfive_tree_load(const char*)
+{
+    std::fprintf(stderr, "libfive_tree_load: tree serialization is not "
+                         "provided by libfive_b200\n");
+    return nullptr;
+}
+
+libfive_tree libfive_tree_remap(libfive_tree p, libfive_tree x,
+                                libfive_tree y, libfive_tree z)
+{
+    if (!p || !x || !y || !z) return nullptr;
+    return H(Tree(N(p)).remap(Tree(N(x)), Tree(N(y)), Tree(N(z))).release());
+}
+
+libfive_tree libfive_tree_optimized(libfive_tree t)
+{
+    if (!t) return nullptr;
+    return H(Tree(N(t)).optimized().release());
+}
+
+char* libfive_tree_print(libfive_tree t)
+{
+    std::stringstream ss;
+    if (t) Tree(N(t)).print(ss);
+    const std::string s = ss.str();
+    char* out = static_cast<char*>(std::malloc(s.size() + 1));
+    std::memcpy(out, s.c_str(), s.size() + 1);
+    return out;
+}
+
+void libfive_free_str(char* ptr) { std::free(ptr); }
+
+////////////////////////////////////////////////////////////////////////////////
+// Single-point evaluation (libfive.cpp:195-214), served by cached device tapes
+
+float libfive_tree_eval_f(libfive_tree t, libfive_vec3 p)
+{
+    if (!t) return NAN;
+    auto g = cached_tape(N(t));
+    float out = NAN;
+    if (!g || eval_values_host(*g, 1, &p.x, &p.y, &p.z, &out) != 0) {
+        std::string msg;
+        last_error(&msg);
+        std::fprintf(stderr, "libfive_tree_eval_f: %s\n", msg.c_str());
+        return NAN;
+    }
+    return out;
+}
+
+libfive_interval libfive_tree_eval_r(libfive_tree t, libfive_region3 r)
+{
+    libfive_interval out{NAN, NAN};
+    if (!t) return out;
+    auto g = cached_tape(N(t));
+    uint8_t nan_flag = 0;
+    if (!g || eval_intervals_host(*g, 1, &r.X.lower, &r.X.upper, &r.Y.lower,
+                                  &r.Y.upper, &r.Z.lower, &r.Z.upper,
+                                  &out.lower, &out.upper, &nan_flag) != 0) {
+        std::string msg;
+        last_error(&msg);
+        std::fprintf(stderr, "libfive_tree_eval_r: %s\n", msg.c_str());
+        return {NAN, NAN};
+    }
+    return out;
+}
+
+libfive_vec3 libfive_tree_eval_d(libfive_tree t, libfive_vec3 p)
+{
+    libfive_vec3 out{NAN, NAN, NAN};
+    if (!t) return out;
+    auto g = cached_tape(N(t));
+    float v = 0;
+    if (!g || eval_derivs_host(*g, 1, &p.x, &p.y, &p.z, &v, &out.x, &out.y,
+                               &out.z) != 0) {
+        std::string msg;
+        last_error(&msg);
+        std::fprintf(stderr, "libfive_tree_eval_d: %s\n", msg.c_str());
+        return {NAN, NAN, NAN};
+    }
+    return out;
+}
+
+////////////////////////////////////////////////////////////////////////////////
+// Outside the evaluate-and-mesh path
+
+libfive_contours* libfive_tree_render_slice(libfive_tree, libfive_region2,
+                                            float, float)
+{
+    std::fprintf(stderr, "libfive_tree_render_slice: 2D contouring is not "
+                         "provided by libfive_b200\n");
+    return nullptr;
+}
+
+libfive_contours3* libfive_tree_render_slice3(libfive_tree, libfive_region2,
+                                              float, float)
+{
+    std::fprintf(stderr, "libfive_tree_render_slice3: 2D contouring is not "
+                         "provided by libfive_b200\n");
+    return nullptr;
+}
+
+void libfive_tree_save_slice(libfive_tree, libfive_region2, float, float,
+                             const char*)
+{
+    std::fprintf(stderr, "libfive_tree_save_slice: 2D contouring is not "
+                         "provided by libfive_b200\n");
+}
+
+libfive_pixels* libfive_tree_render_pixels(libfive_tree, libfive_region2,
+                                           float, float)
+{
+    std::fprintf(stderr, "libfive_tree_render_pixels: pixel rendering is "
+                         "not provided by libfive_b200\n");
+    return nullptr;
+}
+
+////////////////////////////////////////////////////////////////////////////////
+// Meshing (libfive.cpp:306-440)
+
+static libfive_mesh* render_with(const std::shared_ptr<GpuTape>& g,
+                                 libfive_region3 R, double min_feature,
+                                 double max_err, const char* who)
+{
+    if (!g) {
+        std::string msg;
+        last_error(&msg);
+        std::fprintf(stderr, "%s: %s\n", who, msg.c_str());
+        return nullptr;
+    }
+    MeshOut mesh;
+    if (render_dc_mesh(*g, R, min_feature, max_err, mesh, nullptr) != 0) {
+        std::string msg;
+        last_error(&msg);
+        std::fprintf(stderr, "%s: %s\n", who, msg.c_str());
+        return nullptr;
+    }
+    auto out = new libfive_mesh;
+    out->vert_count = static_cast<uint32_t>(mesh.verts.size() / 3);
+    out->tri_count = static_cast<uint32_t>(mesh.tris.size() / 3);
+    out->verts = new libfive_vec3[out->vert_count];
+    out->tris = new libfive_tri[out->tri_count];
+    std::memcpy(out->verts, mesh.verts.data(), mesh.verts.size() * sizeof(float));
+    std::memcpy(out->tris, mesh.tris.data(), mesh.tris.size() * sizeof(uint32_t));
+    return out;
+}
+
+libfive_mesh* libfive_tree_render_mesh(libfive_tree tree, libfive_region3 R,
+                                       float res)
+{
+    if (!tree) return nullptr;
+    return render_with(cached_tape(N(tree)), R, 1.0 / res, 1e-8,
+                       "libfive_tree_render_mesh");
+}
+
+libfive_mesh* libfive_tree_render_mesh_st(libfive_tree tree,
+                                          libfive_region3 R, float res)
+{
+    if (!tree) return nullptr;
+    return render_with(cached_tape(N(tree)), R, 1.0 / res, 1e-8,
+                       "libfive_tree_render_mesh_st");
+}
+
+libfive_mesh_coords* libfive_tree_render_mesh_coords(libfive_tree tree,
+                                                     libfive_region3 R,
+                                                     float res)
+{
+    libfive_mesh* m = libfive_tree_render_mesh(tree, R, res);
+    if (!m) return nullptr;
+    auto out = new libfive_mesh_coords;
+    out->vert_count = m->vert_count;
+    out->verts = m->verts;
+    out->coord_index_count = 4 * m->tri_count;
+    out->coord_indices = new int32_t[out->coord_index_count];
+    for (uint32_t i = 0; i < m->tri_count; ++i) {
+        out->coord_indices[4 * i + 0] = static_cast<int32_t>(m->tris[i].a);
+        out->coord_indices[4 * i + 1] = static_cast<int32_t>(m->tris[i].b);
+        out->coord_indices[4 * i + 2] = static_cast<int32_t>(m->tris[i].c);
+        out->coord_indices[4 * i + 3] = -1;
+    }
+    delete[] m->tris;
+    delete m;
+    return out;
+}
+
+bool libfive_tree_save_mesh(libfive_tree tree, libfive_region3 R, float res,
+                            const char* f)
+{
+    libfive_mesh* m = libfive_tree_render_mesh(tree, R, res);
+    if (!m) return false;
+    const bool ok = save_stl(f, {m});
+    libfive_mesh_delete(m);
+    return ok;
+}
+
+bool libfive_tree_save_meshes(libfive_tree trees[], libfive_region3 R,
+                              float res, float quality, const char* f)
+{
+    std::vector<libfive_mesh*> ms;
+    bool ok = true;
+    const double max_err = std::pow(10.0, -quality);
+    for (unsigned i = 0; trees && trees[i] != nullptr; ++i) {
+        auto m = render_with(cached_tape(N(trees[i])), R, 1.0 / res, max_err,
+                             "libfive_tree_save_meshes");
+        if (!m) {
+            ok = false;
+            break;
+        }
+        ms.push_back(m);
+    }
+    if (ok) ok = save_stl(f, ms);
+    for (auto m : ms) libfive_mesh_delete(m);
+    return ok;
+}
+
+bool libfive_evaluator_save_mesh(libfive_evaluator ev, libfive_region3 R,
+                                 const char* f)
+{
+    if (!ev) return false;
+    // BRepSettings defaults (settings.hpp:34-43): min_feature 0.1, max_err 1e-8
+    auto m = render_with(ev->g, R, 0.1, 1e-8, "libfive_evaluator_save_mesh");
+    if (!m) return false;
+    const bool ok = save_stl(f, {m});
+    libfive_mesh_delete(m);
+    return ok;
+}
+
+////////////////////////////////////////////////////////////////////////////////
+// Evaluators (libfive.cpp:467-502)
+
+libfive_evaluator libfive_tree_evaluator(libfive_tree tree, libfive_vars vars)
+{
+    if (!tree) return nullptr;
+    auto g = make_tape(Tree(N(tree)));
+    if (!g) return nullptr;
+    g->set_vars(vars.vars, vars.values, vars.size);
+    if (!g->upload_cpool()) return nullptr;
+    auto e = new libfive_evaluator_;
+    e->g = g;
+    return e;
+}
+
+bool libfive_evaluator_update_vars(libfive_evaluator ev, libfive_vars vars)
+{
+    if (!ev) return false;
+    const bool changed = ev->g->set_vars(vars.vars, vars.values, vars.size);
+    ev->g->upload_cpool();
+    return changed;
+}
+
+void libfive_evaluator_delete(libfive_evaluator ptr)
+{
+    delete ptr;
+}
+
+const char* libfive_git_version(void) { return "libfive_b200"; }
+const char* libfive_git_revision(void) { return "b200"; }
+const char* libfive_git_branch(void) { return "main"; }
+
+////////////////////////////////////////////////////////////////////////////////
+// libfive_b200.h
+
+int lfb_last_error(char* buf, uint32_t len)
+{
+    std::string msg;
+    const int code = last_error(&msg);
+    if (buf && len) {
+        std::snprintf(buf, len, "%s", msg.c_str());
+    }
+    return code;
+}
+
+lfb_tape lfb_tape_new(libfive_tree t, libfive_vars vars)
+{
+    clear_error();
+    if (!t) {
+        set_error(LFB_E_INVALID, "null tree");
+        return nullptr;
+    }
+    auto g = make_tape(Tree(N(t)));
+    if (!g) return nullptr;
+    if (vars.size) {
+        g->set_vars(vars.vars, vars.values, vars.size);
+        if (!g->upload_cpool()) return nullptr;
+    }
+    auto out = new lfb_tape_;
+    out->g = g;
+    return out;
+}
+
+void lfb_tape_delete(lfb_tape t) { delete t; }
+
+int lfb_tape_set_vars(lfb_tape t, libfive_vars vars)
+{
+    if (!t) return set_error(LFB_E_INVALID, "null tape");
+    std::lock_guard<std::mutex> lock(t->g->mu);
+    const bool changed = t->g->set_vars(vars.vars, vars.values, vars.size);
+    if (!t->g->upload_cpool()) return LFB_E_CUDA;
+    return changed ? 1 : 0;
+}
+
+int lfb_tape_info(lfb_tape t, uint32_t counts[6])
+{
+    if (!t || !counts) return set_error(LFB_E_INVALID, "null argument");
+    const auto& r = t->g->reg;
+    counts[0] = static_cast<uint32_t>(r.clauses.size());
+    counts[1] = r.n_regs;
+    counts[2] = r.n_const;
+    counts[3] = r.n_vars;
+    counts[4] = r.n_choices;
+    counts[5] = t->g->slot.num_clauses;
+    return 0;
+}
+
+int lfb_tape_var_ids(lfb_tape t, const void** ids, uint32_t len)
+{
+    if (!t) return set_error(LFB_E_INVALID, "null tape");
+    const auto& r = t->g->reg;
+    for (uint32_t i = 0; i < r.n_vars && i < len; ++i) {
+        ids[i] = r.var_nodes[i];
+    }
+    return 0;
+}
+
+int lfb_eval_values(lfb_tape t, uint64_t n, const float* x, const float* y,
+                    const float* z, float* out, void* stream, uint32_t flags)
+{
+    clear_error();
+    if (!t) return set_error(LFB_E_INVALID, "null tape");
+    if (flags & LFB_DEVICE_PTRS) {
+        return eval_values_device(*t->g, n, x, y, z, out,
+                                  static_cast<cudaStream_t>(stream));
+    }
+    return eval_values_host(*t->g, n, x, y, z, out);
+}
+
+int lfb_eval_derivs(lfb_tape t, uint64_t n, const float* x, const float* y,
+                    const float* z, float* v, float* dx, float* dy, float* dz,
+                    void* stream, uint32_t flags)
+{
+    clear_error();
+    if (!t) return set_error(LFB_E_INVALID, "null tape");
+    if (flags & LFB_DEVICE_PTRS) {
+        return eval_derivs_device(*t->g, n, x, y, z, v, dx, dy, dz,
+                                  static_cast<cudaStream_t>(stream));
+    }
+    return eval_derivs_host(*t->g, n, x, y, z, v, dx, dy, dz);
+}
+
+int lfb_eval_intervals(lfb_tape t, uint64_t n, const float* xlo,
+                       const float* xhi, const float* ylo, const float* yhi,
+                       const float* zlo, const float* zhi, float* out_lo,
+                       float* out_hi, uint8_t* out_nan, void* stream,
+                       uint32_t flags)
+{
+    clear_error();
+    if (!t) return set_error(LFB_E_INVALID, "null tape");
+    if (flags & LFB_DEVICE_PTRS) {
+        return eval_intervals_device(*t->g, n, xlo, xhi, ylo, yhi, zlo, zhi,
+                                     out_lo, out_hi, out_nan,
+                                     static_cast<cudaStream_t>(stream));
+    }
+    return eval_intervals_host(*t->g, n, xlo, xhi, ylo, yhi, zlo, zhi,
+                               out_lo, out_hi, out_nan);
+}
+
+int lfb_eval_jacobian(lfb_tape t, uint64_t n, const float* x, const float* y,
+                      const float* z, float* out, void* stream, uint32_t flags)
+{
+    clear_error();
+    if (!t) return set_error(LFB_E_INVALID, "null tape");
+    return eval_jacobian(*t->g, n, x, y, z, out,
+                         static_cast<cudaStream_t>(stream),
+                         (flags & LFB_DEVICE_PTRS) != 0);
+}
+
+int lfb_eval_grad(lfb_tape t, uint64_t n, const float* x, const float* y,
+                  const float* z, const float* seed, float* f, float* gx,
+                  float* gy, float* gz, float* gvars, void* stream,
+                  uint32_t flags)
+{
+    clear_error();
+    if (!t) return set_error(LFB_E_INVALID, "null tape");
+    return eval_grad(*t->g, n, x, y, z, seed, f, gx, gy, gz, gvars,
+                     static_cast<cudaStream_t>(stream),
+                     (flags & LFB_DEVICE_PTRS) != 0);
+}
+
+libfive_mesh* lfb_render_mesh(lfb_tape t, libfive_region3 R,
+                              lfb_mesh_settings s, lfb_mesh_stats* stats)
+{
+    clear_error();
+    if (!t) {
+        set_error(LFB_E_INVALID, "null tape");
+        return nullptr;
+    }
+    MeshOut mesh;
+    if (render_dc_mesh(*t->g, R, s.min_feature, s.max_err, mesh, stats) != 0) {
+        return nullptr;
+    }
+    auto out = new libfive_mesh;
+    out->vert_count = static_cast<uint32_t>(mesh.verts.size() / 3);
+    out->tri_count = static_cast<uint32_t>(mesh.tris.size() / 3);
+    out->verts = new libfive_vec3[out->vert_count];
+    out->tris = new libfive_tri[out->tri_count];
+    std::memcpy(out->verts, mesh.verts.data(), mesh.verts.size() * sizeof(float));
+    std::memcpy(out->tris, mesh.tris.data(), mesh.tris.size() * sizeof(uint32_t));
+    return out;
+}
+
+int lfb_tree_slot_tape(libfive_tree t, uint32_t counts[8], int32_t* clauses,
+                       uint32_t* const_slots, float* const_values,
+                       uint32_t* var_slots, const void** var_ids)
+{
+    clear_error();
+    if (!t || !counts) return set_error(LFB_E_INVALID, "null argument");
+    SlotTape st;
+    std::string err;
+    if (!build_slot_tape(Tree(N(t)), st, &err)) {
+        return set_error(LFB_E_UNSUPPORTED, err);
+    }
+    counts[0] = st.num_clauses;
+    counts[1] = static_cast<uint32_t>(st.clauses.size());
+    counts[2] = static_cast<uint32_t>(st.constants.size());
+    counts[3] = static_cast<uint32_t>(st.vars.size());
+    counts[4] = st.X;
+    counts[5] = st.Y;
+    counts[6] = st.Z;
+    counts[7] = st.root;
+    if (clauses) {
+        for (size_t i = 0; i < st.clauses.size(); ++i) {
+            clauses[4 * i + 0] = st.clauses[i].op;
+            clauses[4 * i + 1] = static_cast<int32_t>(st.clauses[i].id);
+            clauses[4 * i + 2] = static_cast<int32_t>(st.clauses[i].a);
+            clauses[4 * i + 3] = static_cast<int32_t>(st.clauses[i].b);
+        }
+    }
+    for (size_t i = 0; i < st.constants.size(); ++i) {
+        if (const_slots) const_slots[i] = st.constants[i].first;
+        if (const_values) const_values[i] = st.constants[i].second;
+    }
+    for (size_t i = 0; i < st.vars.size(); ++i) {
+        if (var_slots) var_slots[i] = st.vars[i].first;
+        if (var_ids) var_ids[i] = st.vars[i].second;
+    }
+    return 0;
+}
+
+}  // extern "C"

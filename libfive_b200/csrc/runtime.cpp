@@ -1,0 +1,197 @@
+#include "runtime.hpp"
+
+#include <cstdio>
+
+#include "libfive_b200.h"
+
+namespace lfb {
+
+static thread_local int t_code = 0;
+static thread_local std::string t_msg;
+
+int set_error(int code, const std::string& msg)
+{
+    t_code = code;
+    t_msg = msg;
+    return code;
+}
+
+void clear_error()
+{
+    t_code = 0;
+    t_msg.clear();
+}
+
+int last_error(std::string* msg)
+{
+    if (msg) *msg = t_msg;
+    return t_code;
+}
+
+bool cuda_ok(cudaError_t e, const char* what)
+{
+    if (e == cudaSuccess) {
+        return true;
+    }
+    set_error(LFB_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return false;
+}
+
+bool require_device()
+{
+    static int state = -1;   // -1 unknown, 0 none, 1 ok
+    if (state < 0) {
+        int n = 0;
+        const cudaError_t e = cudaGetDeviceCount(&n);
+        state = (e == cudaSuccess && n > 0) ? 1 : 0;
+        if (!state) {
+            cudaGetLastError();
+        }
+    }
+    if (!state) {
+        set_error(LFB_E_CUDA,
+                  "no CUDA device: libfive_b200 evaluates on the GPU only");
+        return false;
+    }
+    return true;
+}
+
+std::mutex& global_mutex()
+{
+    static std::mutex m;
+    return m;
+}
+
+GpuTape::~GpuTape()
+{
+    if (d_clauses) cudaFree(d_clauses);
+    if (d_cpool) cudaFree(d_cpool);
+}
+
+DevTape GpuTape::dev() const
+{
+    DevTape d;
+    d.clauses = d_clauses;
+    d.n = static_cast<uint32_t>(reg.clauses.size());
+    d.cpool = d_cpool;
+    d.n_cpool = static_cast<uint32_t>(reg.cpool.size());
+    d.n_const = reg.n_const;
+    d.n_regs = reg.n_regs;
+    d.n_choices = reg.n_choices;
+    d.root_kind = reg.root_kind;
+    d.root = reg.root;
+    return d;
+}
+
+bool GpuTape::upload_cpool()
+{
+    if (reg.cpool.empty()) return true;
+    return cuda_ok(cudaMemcpy(d_cpool, reg.cpool.data(),
+                              reg.cpool.size() * sizeof(float),
+                              cudaMemcpyHostToDevice),
+                   "upload constants");
+}
+
+bool GpuTape::set_vars(const void* const* ids, const float* values,
+                       uint32_t n)
+{
+    bool changed = false;
+    for (uint32_t i = 0; i < n; ++i) {
+        for (uint32_t k = 0; k < reg.n_vars; ++k) {
+            if (reg.var_nodes[k] == ids[i]) {
+                float& slot = reg.cpool[reg.n_const + k];
+                if (slot != values[i]) {
+                    changed = true;
+                }
+                slot = values[i];
+            }
+        }
+    }
+    return changed;
+}
+
+std::shared_ptr<GpuTape> make_tape(const Tree& t)
+{
+    if (!require_device()) {
+        return nullptr;
+    }
+    if (!t.is_valid()) {
+        set_error(LFB_E_INVALID, "invalid tree");
+        return nullptr;
+    }
+    auto g = std::make_shared<GpuTape>();
+    g->tree = t;
+    std::string err;
+    if (!build_slot_tape(t, g->slot, &err) ||
+        !build_reg_tape(g->slot, g->reg, &err)) {
+        set_error(LFB_E_UNSUPPORTED, err);
+        return nullptr;
+    }
+    const size_t nc = std::max<size_t>(1, g->reg.clauses.size());
+    const size_t np = std::max<size_t>(1, g->reg.cpool.size());
+    if (!cuda_ok(cudaMalloc(&g->d_clauses, nc * sizeof(RegClause)), "tape alloc") ||
+        !cuda_ok(cudaMalloc(&g->d_cpool, np * sizeof(float)), "tape alloc")) {
+        return nullptr;
+    }
+    if (!g->reg.clauses.empty() &&
+        !cuda_ok(cudaMemcpy(g->d_clauses, g->reg.clauses.data(),
+                            g->reg.clauses.size() * sizeof(RegClause),
+                            cudaMemcpyHostToDevice),
+                 "tape upload")) {
+        return nullptr;
+    }
+    if (!g->upload_cpool()) {
+        return nullptr;
+    }
+    return g;
+}
+
+static std::mutex g_cache_mu;
+static std::unordered_map<const Node*, std::shared_ptr<GpuTape>> g_cache;
+
+std::shared_ptr<GpuTape> cached_tape(const Node* root)
+{
+    {
+        std::lock_guard<std::mutex> lock(g_cache_mu);
+        auto it = g_cache.find(root);
+        if (it != g_cache.end()) {
+            return it->second;
+        }
+    }
+    auto g = make_tape(Tree(root));
+    if (g) {
+        std::lock_guard<std::mutex> lock(g_cache_mu);
+        if (g_cache.size() > 4096) {
+            g_cache.clear();
+        }
+        g_cache[root] = g;
+    }
+    return g;
+}
+
+void invalidate_cached(const Node* root)
+{
+    std::lock_guard<std::mutex> lock(g_cache_mu);
+    g_cache.erase(root);
+}
+
+DevBuf::~DevBuf()
+{
+    if (ptr) cudaFree(ptr);
+}
+
+bool DevBuf::reserve(size_t n)
+{
+    if (n <= bytes) return true;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    const size_t want = std::max<size_t>(n, 256);
+    if (!cuda_ok(cudaMalloc(&ptr, want), "scratch alloc")) {
+        return false;
+    }
+    bytes = want;
+    return true;
+}
+
+}  // namespace lfb

@@ -1,0 +1,63 @@
+// Host runtime: device tapes, error state, scratch buffers.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "dev_tape.h"
+#include "tape.hpp"
+#include "tree.hpp"
+
+namespace lfb {
+
+/// Records the failure for lfb_last_error and returns `code`.
+int set_error(int code, const std::string& msg);
+void clear_error();
+int last_error(std::string* msg);
+
+/// Fails with LFB_E_CUDA unless a CUDA device is usable.  There is no CPU
+/// path: every evaluation in this library runs on the GPU.
+bool require_device();
+
+/// Converts a CUDA status into an error record; returns true on success.
+bool cuda_ok(cudaError_t e, const char* what);
+
+/// A tree flattened into both tape layouts, resident on the device.
+struct GpuTape {
+    Tree tree;
+    SlotTape slot;
+    RegTape reg;
+    RegClause* d_clauses = nullptr;
+    float* d_cpool = nullptr;
+    std::mutex mu;   // guards cpool updates
+
+    ~GpuTape();
+    DevTape dev() const;
+    /// Sets variable values by tree id; returns true if any value changed.
+    bool set_vars(const void* const* ids, const float* values, uint32_t n);
+    bool upload_cpool();
+};
+
+std::shared_ptr<GpuTape> make_tape(const Tree& t);
+
+/// Cached device tape for a C API tree handle (free variables at zero).
+std::shared_ptr<GpuTape> cached_tape(const Node* root);
+void invalidate_cached(const Node* root);
+
+/// Growable device buffer.
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    ~DevBuf();
+    bool reserve(size_t n);
+    template <class T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+/// Serialises use of the library's default stream and scratch buffers.
+std::mutex& global_mutex();
+
+}  // namespace lfb

@@ -1,0 +1,182 @@
+#include "tape.hpp"
+
+#include <algorithm>
+#include <queue>
+#include <unordered_map>
+
+namespace lfb {
+
+bool build_slot_tape(const Tree& root_, SlotTape& out, std::string* err)
+{
+    const Tree root = root_.optimized();
+    const auto flat = root.walk();
+
+    // Slot ids count down from flat.size() so that the root lands on 1
+    // (deck.cpp:24-58); slot 0 is the reference's placeholder.
+    std::unordered_map<const Node*, uint32_t> slot;
+    slot[nullptr] = 0;
+    uint32_t id = static_cast<uint32_t>(flat.size());
+    std::vector<SlotClause> rev;
+    rev.reserve(flat.size());
+    for (const Node* m : flat) {
+        switch (m->kind) {
+            case Kind::Constant:
+                out.constants.push_back({id, m->value});
+                break;
+            case Kind::Nullary:
+                if (m->op == op::VAR_FREE) {
+                    out.vars.push_back({id, m});
+                } else if (m->op != op::VAR_X && m->op != op::VAR_Y &&
+                           m->op != op::VAR_Z) {
+                    if (err) *err = "unsupported nullary opcode";
+                    return false;
+                }
+                break;
+            case Kind::Unary:
+                rev.push_back({m->op, id, slot.at(m->kid[0]), 0});
+                break;
+            case Kind::Binary:
+                rev.push_back({m->op, id, slot.at(m->kid[0]),
+                               slot.at(m->kid[1])});
+                break;
+            default:
+                if (err) *err = "tree contains an unsupported node";
+                return false;
+        }
+        slot[m] = id--;
+    }
+    out.clauses.assign(rev.rbegin(), rev.rend());
+
+    const Node* axes[3] = {Tree::X().get(), Tree::Y().get(), Tree::Z().get()};
+    for (auto a : axes) {
+        if (slot.find(a) == slot.end()) {
+            const uint32_t next = static_cast<uint32_t>(slot.size());
+            slot[a] = next;
+        }
+    }
+    out.num_clauses = static_cast<uint32_t>(slot.size() - 1);
+    out.X = slot.at(axes[0]);
+    out.Y = slot.at(axes[1]);
+    out.Z = slot.at(axes[2]);
+    std::sort(out.vars.begin(), out.vars.end(),
+              [](const auto& a, const auto& b) { return a.first < b.first; });
+    out.root = slot.at(root.get());
+    return true;
+}
+
+bool build_reg_tape(const SlotTape& st, RegTape& out, std::string* err)
+{
+    out = RegTape();
+    const uint32_t n_slots = st.num_clauses + 1;
+
+    // Operand descriptor for every slot: kind + index.
+    std::vector<uint8_t> kind(n_slots, 0xff);
+    std::vector<uint32_t> index(n_slots, 0);
+    kind[st.X] = OPND_REG; index[st.X] = 0;
+    kind[st.Y] = OPND_REG; index[st.Y] = 1;
+    kind[st.Z] = OPND_REG; index[st.Z] = 2;
+    for (const auto& c : st.constants) {
+        kind[c.first] = OPND_CONST;
+        index[c.first] = static_cast<uint32_t>(out.cpool.size());
+        out.cpool.push_back(c.second);
+    }
+    out.n_const = static_cast<uint32_t>(out.cpool.size());
+    for (const auto& v : st.vars) {
+        kind[v.first] = OPND_VAR;
+        index[v.first] = static_cast<uint32_t>(out.cpool.size());
+        out.cpool.push_back(0.0f);
+        out.var_nodes.push_back(v.second);
+        out.var_slots.push_back(v.first);
+    }
+    out.n_vars = static_cast<uint32_t>(st.vars.size());
+    if (out.cpool.size() > 0xffff) {
+        if (err) *err = "too many constants and variables for a device tape";
+        return false;
+    }
+
+    // Evaluation order is the slot tape reversed.
+    const size_t n = st.clauses.size();
+    std::vector<const SlotClause*> order(n);
+    for (size_t i = 0; i < n; ++i) {
+        order[i] = &st.clauses[n - 1 - i];
+    }
+
+    // Last position at which each slot is read (the root stays live to the
+    // end of the tape).
+    std::vector<int64_t> last_use(n_slots, -1);
+    for (size_t i = 0; i < n; ++i) {
+        const auto* c = order[i];
+        const int ar = op::arity(c->op);
+        if (ar >= 1) last_use[c->a] = static_cast<int64_t>(i);
+        if (ar >= 2) last_use[c->b] = static_cast<int64_t>(i);
+    }
+    last_use[st.root] = static_cast<int64_t>(n);
+
+    std::priority_queue<uint32_t, std::vector<uint32_t>, std::greater<uint32_t>>
+        free_regs;
+    uint32_t next_reg = 3;
+    out.clauses.reserve(n);
+    for (size_t i = 0; i < n; ++i) {
+        const auto* c = order[i];
+        const int ar = op::arity(c->op);
+        if (ar < 1) {
+            if (err) *err = "unsupported opcode in tape";
+            return false;
+        }
+        RegClause rc{};
+        rc.op = static_cast<uint8_t>(c->op);
+        auto operand = [&](uint32_t s, uint16_t& idx, int shift) {
+            if (kind[s] == 0xff) {
+                return false;
+            }
+            idx = static_cast<uint16_t>(index[s]);
+            rc.kinds |= static_cast<uint8_t>(kind[s] << shift);
+            return true;
+        };
+        if (!operand(c->a, rc.a, 0) ||
+            (ar == 2 && !operand(c->b, rc.b, 2))) {
+            if (err) *err = "tape refers to an undefined slot";
+            return false;
+        }
+        // Release operand registers whose last use is this clause (before
+        // allocating the output, which may then reuse one of them).
+        auto release = [&](uint32_t s) {
+            if (kind[s] == OPND_REG && index[s] >= 3 &&
+                last_use[s] == static_cast<int64_t>(i)) {
+                free_regs.push(index[s]);
+                last_use[s] = -2;   // released once even if read twice
+            }
+        };
+        release(c->a);
+        if (ar == 2) release(c->b);
+
+        uint32_t r;
+        if (!free_regs.empty()) {
+            r = free_regs.top();
+            free_regs.pop();
+        } else {
+            r = next_reg++;
+        }
+        if (r > 0xffff) {
+            if (err) *err = "register file overflow";
+            return false;
+        }
+        rc.out = static_cast<uint16_t>(r);
+        kind[c->id] = OPND_REG;
+        index[c->id] = r;
+        if (c->op == op::MIN || c->op == op::MAX) {
+            out.n_choices++;
+        }
+        out.clauses.push_back(rc);
+    }
+    out.n_regs = next_reg;
+    if (kind[st.root] == 0xff) {
+        if (err) *err = "root slot undefined";
+        return false;
+    }
+    out.root_kind = kind[st.root];
+    out.root = static_cast<uint16_t>(index[st.root]);
+    return true;
+}
+
+}  // namespace lfb

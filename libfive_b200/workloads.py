@@ -1,0 +1,160 @@
+"""Seeded synthetic shapes for the benchmark and parity workloads.
+
+All randomness comes from SplitMix64 (Steele et al., 2014), so a seed names
+a shape exactly.  Primitives follow libfive's stdlib formulas
+(libfive/stdlib/stdlib_impl.cpp): sphere 227-230, union/intersection/
+difference 51-65 (min / max / max(a, -b)), blend_expt_unit 79-85 (the Python
+`blend`), with a box as the max of three slab distances and a z-cylinder as
+max(radial distance, |z - cz| - h).
+"""
+import numpy as np
+
+from .shape import Shape, X, Y, Z
+
+MASK = (1 << 64) - 1
+
+
+class SplitMix64:
+    def __init__(self, seed):
+        self.s = seed & MASK
+
+    def next(self):
+        self.s = (self.s + 0x9E3779B97F4A7C15) & MASK
+        z = self.s
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & MASK
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & MASK
+        return z ^ (z >> 31)
+
+    def uniform(self, lo=0.0, hi=1.0):
+        return lo + (hi - lo) * ((self.next() >> 11) * (1.0 / (1 << 53)))
+
+    def below(self, n):
+        return self.next() % n
+
+
+def sphere(c, r):
+    x, y, z = X(), Y(), Z()
+    return ((x - c[0]).square() + (y - c[1]).square() + (z - c[2]).square()).sqrt() - r
+
+
+def box(c, s):
+    x, y, z = X(), Y(), Z()
+    return ((x - c[0]).abs() - s).max(((y - c[1]).abs() - s).max((z - c[2]).abs() - s))
+
+
+def zcylinder(c, r, h):
+    x, y, z = X(), Y(), Z()
+    radial = ((x - c[0]).square() + (y - c[1]).square()).sqrt() - r
+    return radial.max((z - c[2]).abs() - h)
+
+
+def union(a, b):
+    return a.min(b)
+
+
+def intersection(a, b):
+    return a.max(b)
+
+
+def difference(a, b):
+    return a.max(-b)
+
+
+def blend(a, b, m=0.05):
+    """blend_expt_unit(a, b, m) = -log(exp(-k a) + exp(-k b)) / k,
+    k = 2.75 / m^2, built with the same tree operations as the stdlib."""
+    mt = Shape.constant(m)
+    k = Shape.constant(2.75) / (mt ** Shape.constant(2))
+    ea = ((-k) * a).exp()
+    eb = ((-k) * b).exp()
+    return -((ea + eb).log()) / k
+
+
+def spheres_union(n=64, seed=1):
+    """Union (min) of n spheres, centres U[-1,1]^3, radii U[0.1,0.35]."""
+    rng = SplitMix64(seed)
+    out = None
+    for _ in range(n):
+        c = [rng.uniform(-1, 1) for _ in range(3)]
+        r = rng.uniform(0.1, 0.35)
+        s = sphere(c, r)
+        out = s if out is None else out.min(s)
+    return out
+
+
+# Operator weights for the random CSG tree: (union, blend, difference,
+# intersection).  Unions dominate so that the combined surface stays large.
+CSG_WEIGHTS = (0.63, 0.07, 0.20, 0.10)
+
+
+def random_csg(n_prims=2000, seed=2, size=(0.02, 0.2)):
+    """Random binary CSG tree over n primitives (spheres, boxes, z-cylinders
+    in rotation), centres U[-1,1]^3, sizes U[size]."""
+    rng = SplitMix64(seed)
+    prims = []
+    for i in range(n_prims):
+        c = [rng.uniform(-1, 1) for _ in range(3)]
+        s = rng.uniform(*size)
+        kind = i % 3
+        if kind == 0:
+            prims.append(sphere(c, s))
+        elif kind == 1:
+            prims.append(box(c, s))
+        else:
+            prims.append(zcylinder(c, s, rng.uniform(*size)))
+    level = prims
+    while len(level) > 1:
+        nxt = []
+        for i in range(0, len(level) - 1, 2):
+            u = rng.uniform()
+            a, b = level[i], level[i + 1]
+            w = CSG_WEIGHTS
+            if u < w[0]:
+                nxt.append(union(a, b))
+            elif u < w[0] + w[1]:
+                nxt.append(blend(a, b))
+            elif u < w[0] + w[1] + w[2]:
+                nxt.append(difference(a, b))
+            else:
+                nxt.append(intersection(a, b))
+        if len(level) % 2:
+            nxt.append(level[-1])
+        level = nxt
+    return level[0]
+
+
+def blended_spheres_vars(n=256, seed=4, m=0.05):
+    """n spheres whose centres and radii are free variables, combined by a
+    balanced binary tree of blends.  Returns (shape, {var: value})."""
+    rng = SplitMix64(seed)
+    values = {}
+    leaves = []
+    x, y, z = X(), Y(), Z()
+    for _ in range(n):
+        cx, cy, cz, r = Shape.var(), Shape.var(), Shape.var(), Shape.var()
+        values[cx] = rng.uniform(-1, 1)
+        values[cy] = rng.uniform(-1, 1)
+        values[cz] = rng.uniform(-1, 1)
+        values[r] = rng.uniform(0.1, 0.35)
+        leaves.append(((x - cx).square() + (y - cy).square() + (z - cz).square()).sqrt() - r)
+    level = leaves
+    while len(level) > 1:
+        nxt = [blend(level[i], level[i + 1], m) for i in range(0, len(level) - 1, 2)]
+        if len(level) % 2:
+            nxt.append(level[-1])
+        level = nxt
+    return level[0], values
+
+
+def lattice(n=128, lo=-1.5, hi=1.5):
+    """n^3 inclusive lattice as flat float32 x, y, z arrays."""
+    t = (lo + (hi - lo) * np.arange(n, dtype=np.float64) / (n - 1)).astype(np.float32)
+    zz, yy, xx = np.meshgrid(t, t, t, indexing="ij")
+    return (np.ascontiguousarray(xx.ravel()), np.ascontiguousarray(yy.ravel()),
+            np.ascontiguousarray(zz.ravel()))
+
+
+def uniform_points(n, seed=3, lo=-1.5, hi=1.5):
+    r = np.random.Generator(np.random.PCG64(seed))
+    p = r.uniform(lo, hi, size=(3, n)).astype(np.float32)
+    return p[0].copy(), p[1].copy(), p[2].copy()

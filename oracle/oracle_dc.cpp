@@ -1,0 +1,1 @@
+// CPU oracle dual-contouring mesher (TEST INFRASTRUCTURE ONLY).

@@ -1,0 +1,115 @@
+"""ctypes access to the CPU oracle (oracle/lib/liboracle.so), for tests only."""
+import ctypes
+import os
+
+import numpy as np
+
+from libfive_b200.shape import slot_tape
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is None:
+        _lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "lib", "liboracle.so"))
+        vp = ctypes.c_void_p
+        _lib.ora_tape_new.restype = vp
+        _lib.ora_tape_new.argtypes = [ctypes.c_uint32, ctypes.c_uint32, vp, ctypes.c_uint32,
+                                      vp, vp, ctypes.c_uint32, vp, vp, ctypes.c_uint32,
+                                      ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]
+        _lib.ora_tape_delete.argtypes = [vp]
+        _lib.ora_values.argtypes = [vp, ctypes.c_uint64, vp, vp, vp, vp, ctypes.c_int]
+        _lib.ora_derivs.argtypes = [vp, ctypes.c_uint64, vp, vp, vp, vp, vp, vp, vp, ctypes.c_int]
+        _lib.ora_ambiguous.argtypes = [vp, ctypes.c_uint64, vp, vp, vp, vp]
+        _lib.ora_intervals.argtypes = [vp, ctypes.c_uint64] + [vp] * 9 + [ctypes.c_int]
+        _lib.ora_pushed_size.restype = ctypes.c_uint32
+        _lib.ora_pushed_size.argtypes = [vp] + [ctypes.c_float] * 6
+        _lib.ora_jacobian.argtypes = [vp, ctypes.c_uint64, vp, vp, vp, vp, ctypes.c_int]
+        _lib.ora_is_inside.restype = ctypes.c_int
+        _lib.ora_is_inside.argtypes = [vp, ctypes.c_float, ctypes.c_float, ctypes.c_float]
+        _lib.ora_features.restype = ctypes.c_int
+        _lib.ora_features.argtypes = [vp, ctypes.c_float, ctypes.c_float, ctypes.c_float, vp, ctypes.c_int]
+        if hasattr(_lib, "ora_render_mesh"):
+            _lib.ora_render_mesh.restype = ctypes.c_int
+            _lib.ora_render_mesh.argtypes = [vp] + [ctypes.c_float] * 6 + [
+                ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.POINTER(vp),
+                ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(vp),
+                ctypes.POINTER(ctypes.c_uint32)]
+            _lib.ora_free.argtypes = [vp]
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data
+
+
+class OracleTape:
+    """The reference-layout tape of a shape, evaluated on the CPU."""
+
+    def __init__(self, shape, var_values=None):
+        lib = load()
+        st = slot_tape(shape)
+        self.st = st
+        cl = np.array(st["clauses"], np.int32).reshape(-1, 4) if st["clauses"] else np.zeros((0, 4), np.int32)
+        cl = np.ascontiguousarray(cl)
+        cs = np.array([c[0] for c in st["constants"]], np.uint32)
+        cv = np.array([c[1] for c in st["constants"]], np.float32)
+        vs = np.array([v[0] for v in st["vars"]], np.uint32)
+        vals = {}
+        if var_values:
+            for k, v in var_values.items():
+                vals[k.id() if hasattr(k, "id") else k] = v
+        vv = np.array([vals.get(v[1], 0.0) for v in st["vars"]], np.float32)
+        self._keep = (cl, cs, cv, vs, vv)
+        self.n_vars = len(st["vars"])
+        self.h = lib.ora_tape_new(st["num_clauses"], len(cl), _p(cl), len(cs), _p(cs), _p(cv),
+                                  len(vs), _p(vs), _p(vv), st["X"], st["Y"], st["Z"], st["root"])
+
+    def __del__(self):
+        try:
+            load().ora_tape_delete(self.h)
+        except Exception:
+            pass
+
+    def values(self, x, y, z, threads=1):
+        out = np.empty(len(x), np.float32)
+        load().ora_values(self.h, len(x), _p(x), _p(y), _p(z), _p(out), threads)
+        return out
+
+    def derivs(self, x, y, z, threads=1):
+        outs = [np.empty(len(x), np.float32) for _ in range(4)]
+        load().ora_derivs(self.h, len(x), _p(x), _p(y), _p(z), *[_p(o) for o in outs], threads)
+        return outs
+
+    def ambiguous(self, x, y, z):
+        out = np.empty(len(x), np.uint8)
+        load().ora_ambiguous(self.h, len(x), _p(x), _p(y), _p(z), _p(out))
+        return out.astype(bool)
+
+    def intervals(self, lo, hi, threads=1):
+        lo = np.ascontiguousarray(lo, np.float32)
+        hi = np.ascontiguousarray(hi, np.float32)
+        n = lo.shape[1]
+        olo, ohi = np.empty(n, np.float32), np.empty(n, np.float32)
+        onan = np.empty(n, np.uint8)
+        load().ora_intervals(self.h, n, _p(lo[0]), _p(hi[0]), _p(lo[1]), _p(hi[1]),
+                             _p(lo[2]), _p(hi[2]), _p(olo), _p(ohi), _p(onan), threads)
+        return olo, ohi, onan.astype(bool)
+
+    def pushed_size(self, lo, hi):
+        return load().ora_pushed_size(self.h, *lo, *hi)
+
+    def jacobian(self, x, y, z, threads=1):
+        out = np.zeros((len(x), self.n_vars), np.float32)
+        load().ora_jacobian(self.h, len(x), _p(x), _p(y), _p(z), _p(out), threads)
+        return out
+
+    def is_inside(self, p):
+        return bool(load().ora_is_inside(self.h, *p))
+
+    def features(self, p, max_n=16):
+        out = np.zeros((max_n, 3), np.float32)
+        n = load().ora_features(self.h, *p, _p(out), max_n)
+        return out[:min(n, max_n)]

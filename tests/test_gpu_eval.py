@@ -1,0 +1,199 @@
+"""GPU point / box evaluation through the C ABI, checked against the CPU
+oracle on the same reference-layout tape and against the reference's known
+answers.  Exactly rounded opcodes must agree bit for bit; library-call
+opcodes (sin, exp, pow, ...) within the per-opcode ULP bounds below."""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from libfive_b200 import workloads
+from libfive_b200.shape import Shape, Tape
+from oracle_ffi import OracleTape
+from sexpr import parse
+
+pytestmark = pytest.mark.gpu
+
+KATS = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "eval_kats.json")))
+
+# Largest allowed difference, in float32 ULPs, between CUDA's and the host C
+# library's result for ops that call a math library function.
+ULP_BOUND = {"sin": 4, "cos": 4, "tan": 8, "asin": 4, "acos": 4, "atan": 4,
+             "exp": 4, "log": 4, "pow": 8, "nth-root": 8, "atan2": 8}
+
+
+def ulp_diff(a, b):
+    a = np.asarray(a, np.float32)
+    b = np.asarray(b, np.float32)
+    both_nan = np.isnan(a) & np.isnan(b)
+    ai = a.view(np.int32).astype(np.int64)
+    bi = b.view(np.int32).astype(np.int64)
+    ai = np.where(ai < 0, -(ai & 0x7fffffff), ai)
+    bi = np.where(bi < 0, -(bi & 0x7fffffff), bi)
+    d = np.abs(ai - bi)
+    d[both_nan] = 0
+    d[np.isnan(a) ^ np.isnan(b)] = 1 << 40
+    return d
+
+
+def _f(v):
+    return {"inf": math.inf, "-inf": -math.inf}.get(v, v) if isinstance(v, str) else v
+
+
+def build(e):
+    vars_ = {}
+    t = parse(e["expr"], vars_)
+    return t, {vars_[k]: v for k, v in e.get("vars", {}).items()}
+
+
+def pts(p):
+    return [np.array([float(_f(v))], np.float32) for v in p]
+
+
+@pytest.mark.parametrize("e", KATS["values"], ids=lambda e: e["src"])
+def test_value_kats(gpu, e):
+    t, vals = build(e)
+    got = Tape(t, vals).values(*pts(e["p"]))[0]
+    assert abs(got - e["want"]) <= e["tol"]
+    assert ulp_diff(got, OracleTape(t, vals).values(*pts(e["p"]))[0]) <= 8
+
+
+@pytest.mark.parametrize("e", KATS["derivs"], ids=lambda e: e["src"])
+def test_deriv_kats(gpu, e):
+    t, vals = build(e)
+    v, dx, dy, dz = Tape(t, vals).derivs(*pts(e["p"]))
+    got = [dx[0], dy[0], dz[0], v[0]]
+    for g, w in zip(got, e["want"]):
+        w = _f(w)
+        if math.isinf(w):
+            assert math.isinf(g) and (g > 0) == (w > 0)
+        else:
+            assert abs(g - w) <= e["tol"]
+
+
+@pytest.mark.parametrize("e", KATS["intervals"], ids=lambda e: e["src"])
+def test_interval_kats(gpu, e):
+    t, vals = build(e)
+    lo = np.array([[_f(v)] for v in e["lo"]], np.float32)
+    hi = np.array([[_f(v)] for v in e["hi"]], np.float32)
+    l, h, _ = Tape(t, vals).intervals(lo, hi)
+    assert l[0] == _f(e["want"][0]) and h[0] == _f(e["want"][1])
+
+
+@pytest.mark.parametrize("e", KATS["interval_nan"], ids=lambda e: e["src"])
+def test_interval_nan_kats(gpu, e):
+    t, vals = build(e)
+    lo = np.array([[_f(v)] for v in e["lo"]], np.float32)
+    hi = np.array([[_f(v)] for v in e["hi"]], np.float32)
+    _, _, n = Tape(t, vals).intervals(lo, hi)
+    assert (not n[0]) == e["safe"]
+
+
+def test_capi_single_point(gpu, lib):
+    # api.cpp:44-73 through libfive_tree_eval_f / _r / _d
+    x, y = Shape.X(), Shape.Y()
+    c = x / y
+    assert c(1, 2, 3) == 0.5 and c(1, 4, 3) == 0.25 and c(1, -1, 3) == -1
+    assert (x - y).eval_interval((1, 2, 0), (2, 3, 0)) == (-2.0, 0.0)
+    assert (x * x + y).eval_deriv(3, 1, 0) == (6.0, 1.0, 0.0)
+
+
+UNARY = ["square", "sqrt", "neg", "sin", "cos", "tan", "asin", "acos", "atan",
+         "exp", "log", "abs", "recip", "const-var"]
+BINARY = ["add", "mul", "min", "max", "sub", "div", "atan2", "mod", "nanfill",
+          "compare"]
+
+
+def _points(n, seed, lo=-3, hi=3):
+    r = np.random.default_rng(seed)
+    p = r.uniform(lo, hi, (3, n)).astype(np.float32)
+    # exact ties, zeros and integers exercise select / sign rules
+    p[:, : n // 8] = np.round(p[:, : n // 8])
+    p[1, n // 8: n // 4] = p[0, n // 8: n // 4]
+    return [np.ascontiguousarray(q) for q in p]
+
+
+@pytest.mark.parametrize("op", UNARY + BINARY)
+def test_every_opcode_matches_oracle(gpu, op):
+    x, y = Shape.X(), Shape.Y()
+    t = Shape.new(op, x * 1.5 + 0.25) if op in UNARY else Shape.new(op, x, y + 0.5)
+    P = _points(4096, 7)
+    g = Tape(t)
+    o = OracleTape(t)
+    bound = ULP_BOUND.get(op, 0)
+    assert ulp_diff(g.values(*P), o.values(*P)).max() <= bound
+    gv, gdx, gdy, gdz = g.derivs(*P)
+    ov, odx, ody, odz = o.derivs(*P)
+    dbound = max(bound, 0) * 2
+    for a, b in ((gv, ov), (gdx, odx), (gdy, ody), (gdz, odz)):
+        assert ulp_diff(a, b).max() <= dbound, op
+
+
+@pytest.mark.parametrize("op", UNARY + BINARY)
+def test_every_opcode_interval_encloses_oracle(gpu, op):
+    x, y = Shape.X(), Shape.Y()
+    t = Shape.new(op, x * 1.5 + 0.25) if op in UNARY else Shape.new(op, x, y + 0.5)
+    r = np.random.default_rng(11)
+    c = r.uniform(-3, 3, (3, 2048)).astype(np.float32)
+    w = r.uniform(0, 1.5, (3, 2048)).astype(np.float32) * (r.uniform(0, 1, (1, 2048)) < 0.9)
+    lo, hi = c - w, c + w
+    gl, gh, gn = Tape(t).intervals(lo, hi)
+    ol, oh, on = OracleTape(t).intervals(lo, hi)
+    valid = ~(np.isnan(ol) | np.isnan(oh))
+    exact = op not in ULP_BOUND
+    if exact:
+        # directed-rounding arithmetic: bit-identical bounds
+        assert np.array_equal(gl[valid], ol[valid]) and np.array_equal(gh[valid], oh[valid]), op
+    else:
+        assert np.all(gl[valid] <= ol[valid]) and np.all(gh[valid] >= oh[valid]), op
+    assert np.all(gn >= on), op   # maybe-NaN flag is a superset
+
+
+def test_spheres_lattice_parity(gpu):
+    """64-sphere union on a 48^3 lattice: values and derivatives bit-exact."""
+    t = workloads.spheres_union(64, seed=1)
+    P = workloads.lattice(48)
+    g, o = Tape(t), OracleTape(t)
+    assert np.array_equal(g.values(*P), o.values(*P, threads=8))
+    gd = g.derivs(*P)
+    od = o.derivs(*P, threads=8)
+    for a, b in zip(gd, od):
+        assert np.array_equal(a, b)
+
+
+def test_random_csg_parity(gpu):
+    """Random CSG with blends: exact ops bit-exact, exp/log within bounds."""
+    t = workloads.random_csg(200, seed=5)
+    P = workloads.uniform_points(20000, seed=9)
+    g, o = Tape(t), OracleTape(t)
+    d = ulp_diff(g.values(*P), o.values(*P, threads=8))
+    assert np.percentile(d, 99) == 0 and d.max() <= 64
+
+
+def test_vars_and_update(gpu):
+    # eval_array.cpp:185-197 setVar sequence through lfb_tape_set_vars
+    vars_ = {}
+    t = parse("(+ (* a 1) (* b 2) (* c 3))", vars_)
+    a, b, c = vars_["a"], vars_["b"], vars_["c"]
+    tape = Tape(t, {a: 3, c: 7, b: 5})
+    z = np.zeros(1, np.float32)
+    assert tape.values(z, z, z)[0] == 34
+    tape.set_vars({a: 5})
+    assert tape.values(z, z, z)[0] == 36
+    tape.set_vars({b: 0})
+    assert tape.values(z, z, z)[0] == 26
+    tape.set_vars({c: 10})
+    assert tape.values(z, z, z)[0] == 35
+
+
+def test_device_pointers_with_torch(gpu):
+    import torch
+    t = workloads.spheres_union(16, seed=3)
+    P = workloads.uniform_points(100000, seed=2)
+    dev = [torch.from_numpy(p).cuda() for p in P]
+    out = torch.empty_like(dev[0])
+    Tape(t).values(*dev, out=out)
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy(), OracleTape(t).values(*P, threads=8))

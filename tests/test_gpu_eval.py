@@ -25,8 +25,8 @@ ULP_BOUND = {"sin": 4, "cos": 4, "tan": 8, "asin": 4, "acos": 4, "atan": 4,
 
 
 def ulp_diff(a, b):
-    a = np.asarray(a, np.float32)
-    b = np.asarray(b, np.float32)
+    a = np.atleast_1d(np.asarray(a, np.float32))
+    b = np.atleast_1d(np.asarray(b, np.float32))
     both_nan = np.isnan(a) & np.isnan(b)
     ai = a.view(np.int32).astype(np.int64)
     bi = b.view(np.int32).astype(np.int64)

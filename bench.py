@@ -1,0 +1,362 @@
+"""Benchmark: dual-contouring meshes per second on a 2000-primitive CSG.
+
+Workload (the single-GPU configuration of the benchmark plan): a random
+binary CSG tree of 2000 primitives (spheres, boxes, z-cylinders; centres
+U[-1,1]^3, sizes U[0.02,0.2]; unions / smooth blends / differences /
+intersections), region [-1.5,1.5]^3 meshed to octree depth 10 (1024^3
+cells) with max_err 1e-8.  One step = one complete mesh.  Inputs are
+synthetic and seeded (libfive_b200/workloads.py); rank r meshes seed 2 + r.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  `value` is meshes/s with the tape resident on
+the device (lfb_render_mesh, mesh downloaded to the host each step); `e2e`
+builds the device tape from the host tree (flatten + upload) and downloads
+the mesh every step.  L2 is flushed (a 512 MiB write) before every timed
+step, outside the per-step event pair.
+"""
+import argparse
+import concurrent.futures
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SEED_BASE = 2
+N_PRIMS = 2000
+REGION = ((-1.5, -1.5, -1.5), (1.5, 1.5, 1.5))
+MIN_FEATURE = 3.0 / 1000.0      # Region::withResolution -> depth 10
+MAX_ERR = 1e-8
+SUBDIV = 8                       # CPU sample: sub-boxes of a 8x8x8 split
+
+# FP32 lane-ops per clause evaluation (value mode / value+gradient mode),
+# fixed per opcode; library calls count as 20.
+W_VALUE = {"copy": 0, "add": 1, "sub": 1, "neg": 1, "mul": 1, "min": 1, "max": 1,
+           "square": 1, "abs": 1, "sqrt": 1, "div": 3, "recip": 3, "exp": 3, "log": 3,
+           "const-var": 0}
+W_GRAD = {"copy": 0, "add": 4, "sub": 4, "neg": 4, "mul": 7, "min": 5, "max": 5,
+          "square": 5, "abs": 5, "sqrt": 7, "div": 11, "recip": 8, "exp": 6, "log": 7,
+          "const-var": 0}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--cpu-sample", type=int, default=24,
+                   help="sub-boxes meshed per CPU baseline step")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def build_shape(seed):
+    from libfive_b200 import workloads
+    return workloads.random_csg(N_PRIMS, seed=seed)
+
+
+def tape_weights(shape):
+    """Average FP32 lane-ops per clause of the unpruned tape, value / grad."""
+    from libfive_b200 import ffi
+    from libfive_b200.shape import slot_tape
+    lib = ffi.load()
+    st = slot_tape(shape)
+    names = {}
+    for op, _, _, _ in st["clauses"]:
+        n = names.setdefault(op, None)
+        if n is None:
+            for cand in list(W_VALUE) + ["atan2", "pow", "sin", "cos"]:
+                if lib.libfive_opcode_enum(cand.encode()) == op:
+                    names[op] = cand
+                    break
+    wv = [W_VALUE.get(names.get(op), 20) for op, _, _, _ in st["clauses"]]
+    wg = [W_GRAD.get(names.get(op), 20) for op, _, _, _ in st["clauses"]]
+    n = max(1, len(wv))
+    return sum(wv) / n, sum(wg) / n, len(st["clauses"])
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_sample_boxes(step_seed, count):
+    """`count` distinct sub-boxes of the SUBDIV^3 split of the region."""
+    import numpy as np
+    rng = np.random.default_rng(step_seed)
+    ids = rng.choice(SUBDIV ** 3, size=count, replace=False)
+    lo, hi = REGION
+    w = [(hi[a] - lo[a]) / SUBDIV for a in range(3)]
+    boxes = []
+    for i in ids:
+        c = (int(i) % SUBDIV, (int(i) // SUBDIV) % SUBDIV, int(i) // (SUBDIV * SUBDIV))
+        blo = tuple(lo[a] + c[a] * w[a] for a in range(3))
+        bhi = tuple(lo[a] + (c[a] + 1) * w[a] for a in range(3))
+        boxes.append((blo, bhi))
+    return boxes
+
+
+def cpu_mesh_rate(shape, count, step_seed, cores):
+    """CPU oracle (restatement of the reference mesher) on `count` sub-boxes
+    at the benchmark's cell size, one box per thread; returns extrapolated
+    meshes/s for the whole region and the wall time of the sample."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_ffi import OracleTape, load
+    lib = load()
+    ora = OracleTape(shape)
+    boxes = cpu_sample_boxes(step_seed, count)
+
+    def one(box):
+        vp, tp = ctypes.c_void_p(), ctypes.c_void_p()
+        nv, nt = ctypes.c_uint32(), ctypes.c_uint32()
+        lib.ora_render_mesh(ora.h, *box[0], *box[1], MIN_FEATURE, MAX_ERR, 1,
+                            ctypes.byref(vp), ctypes.byref(nv), ctypes.byref(tp),
+                            ctypes.byref(nt))
+        lib.ora_free(vp)
+        lib.ora_free(tp)
+        return nt.value
+
+    t0 = time.perf_counter()
+    with concurrent.futures.ThreadPoolExecutor(max_workers=cores) as ex:
+        list(ex.map(one, boxes))
+    wall = time.perf_counter() - t0
+    full = wall * (SUBDIV ** 3) / count
+    return 1.0 / full, wall
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    shape = build_shape(SEED_BASE)
+    for w in range(args.warmup):
+        cpu_mesh_rate(shape, max(1, args.cpu_sample // 4), 1000 + w, cores)
+    rates, walls = [], []
+    for k in range(args.steps):
+        r, wall = cpu_mesh_rate(shape, args.cpu_sample, 2000 + k, cores)
+        rates.append(r)
+        walls.append(wall)
+    value = len(rates) / sum(1.0 / r for r in rates)
+    sample = (f"{args.cpu_sample} random sub-boxes of a {SUBDIV}^3 split of the region per "
+              f"step (same cell size, depth 7 each), one box per thread, extrapolated "
+              f"x{SUBDIV ** 3 // args.cpu_sample} to the whole region")
+    print(json.dumps({
+        "impl": "reference",
+        "metric": "DC meshes/s", "value": value, "unit": "meshes/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "csg2000-depth10-dc", "primitives": N_PRIMS,
+                   "octree_depth": 10, "region": "[-1.5,1.5]^3", "max_err": MAX_ERR},
+        "cpu_baseline": {"value": value, "unit": "meshes/s", "cores": cores,
+                         "kind": "port", "sample": sample,
+                         "sample_wall_s": sum(walls)},
+        "e2e": {"value": value, "unit": "meshes/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }))
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+
+    from libfive_b200 import ffi
+    from libfive_b200.shape import Tape
+    lib = ffi.load()
+    shape = build_shape(SEED_BASE + rank)
+    tape = Tape(shape)
+    wv, wg, n_clauses = tape_weights(shape)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    region = ffi.Region3(*[ffi.Interval(a, b) for a, b in zip(*REGION)])
+    settings = ffi.MeshSettings(MIN_FEATURE, MAX_ERR)
+
+    def mesh_once(t):
+        st = ffi.MeshStats()
+        m = lib.lfb_render_mesh(t.ptr, region, settings, ctypes.byref(st))
+        if not m:
+            raise RuntimeError("lfb_render_mesh failed: " + ffi.last_error()[1])
+        lib.libfive_mesh_delete(m)
+        return st
+
+    for _ in range(args.warmup):
+        mesh_once(tape)
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    launches0 = lib.lfb_kernel_launches()
+    total_ms, leaf_ms, evals_v, evals_g = 0.0, 0.0, 0, 0
+    stats = None
+    for _ in range(args.steps):
+        flush.fill_(1)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        stats = mesh_once(tape)
+        b.record()
+        b.synchronize()
+        total_ms += a.elapsed_time(b)
+        leaf_ms += stats.ms_leaf
+        evals_v += stats.clause_evals
+        evals_g += stats.clause_evals_grad
+    torch.cuda.synchronize()
+    launches = lib.lfb_kernel_launches() - launches0
+    if pg:
+        pg.barrier()
+    clk = clocks.stop()
+
+    # End to end through the public API: flatten + upload the tape, mesh,
+    # download and copy into a libfive_mesh, every step.
+    e2e_ms, h2d, d2h = 0.0, 0, 0
+    for _ in range(args.steps):
+        flush.fill_(1)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        t = Tape(shape)
+        st = mesh_once(t)
+        b.record()
+        b.synchronize()
+        e2e_ms += a.elapsed_time(b)
+        h2d = t.n_clauses * 8 + (t.n_const + t.n_vars) * 4
+        d2h = (st.vertices + 1) * 12 + st.triangles * 12
+        del t
+
+    times = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device="cuda")
+    if pg:
+        pg.all_reduce(times, op=pg.ReduceOp.MAX)
+    total_ms, e2e_ms = times.tolist()
+    value = world * args.steps / (total_ms / 1000.0)
+    e2e_value = world * args.steps / (e2e_ms / 1000.0)
+
+    if rank == 0:
+        sm_mhz = clk.get("sm_mhz") or 1965.0
+        sms = torch.cuda.get_device_properties(0).multi_processor_count
+        peak = sms * 128 * sm_mhz * 1e6 / 1e9          # G lane-ops/s
+        ops = (evals_v * wv + evals_g * wg) / args.steps
+        achieved = ops / (leaf_ms / args.steps / 1000.0) / 1e9
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "leaf_kernel_traffic.json")
+        if os.path.exists(tpath):
+            traffic = json.load(open(tpath)).get("dram_bytes_per_launch")
+        line = {
+            "metric": "DC meshes/s", "value": value, "unit": "meshes/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded CSG, seed 2 + rank)",
+            "config": {"workload": "csg2000-depth10-dc", "primitives": N_PRIMS,
+                       "tape_clauses": n_clauses, "octree_depth": stats.levels,
+                       "region": "[-1.5,1.5]^3", "max_err": MAX_ERR,
+                       "triangles": stats.triangles, "vertices": stats.vertices,
+                       "leaf_records": stats.leaves_ambiguous,
+                       "l2": "flushed (512 MiB write) before every timed step"},
+            "roofline": {
+                "kernel": "k_leaf_groups",
+                "bound": "fp32",
+                "achieved": achieved, "peak": peak, "unit": "G lane-ops/s",
+                "frac": achieved / peak,
+                "peak_source": f"derived: {sms} SMs x 128 FP32 lanes x {sm_mhz:.0f} MHz "
+                               "(sampled median SM clock); no measured FP32 figure exists",
+                "algorithmic_ops_per_launch": ops,
+                "clause_evals_per_launch": (evals_v + evals_g) / args.steps,
+                "kernel_ms_per_launch": leaf_ms / args.steps,
+                "traffic": traffic,
+            },
+            "stages_ms": {"interval": stats.ms_interval, "leaf": stats.ms_leaf,
+                          "collapse": stats.ms_collapse, "dual": stats.ms_dual},
+            "e2e": {"value": e2e_value, "unit": "meshes/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+        }
+        if not args.no_cpu_baseline and world == 1:
+            cores = os.cpu_count() or 1
+            rate, wall = cpu_mesh_rate(shape, args.cpu_sample, 2000, cores)
+            line["cpu_baseline"] = {
+                "value": rate, "unit": "meshes/s", "cores": cores, "kind": "port",
+                "sample": f"{args.cpu_sample} random sub-boxes of a {SUBDIV}^3 split "
+                          f"(same cell size), one per thread, extrapolated to the "
+                          f"whole region; {wall:.1f} s wall"}
+        print(json.dumps(line))
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+    else:
+        run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

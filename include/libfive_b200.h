@@ -96,13 +96,25 @@ typedef struct lfb_mesh_settings {
 } lfb_mesh_settings;
 
 typedef struct lfb_mesh_stats {
-    uint32_t levels;           /* octree depth (Region::withResolution) */
-    uint64_t cells_evaluated;  /* interval-evaluated cells, all levels */
-    uint64_t leaf_groups;      /* sibling groups evaluated at the finest level */
-    uint64_t leaves_ambiguous;
-    uint64_t clause_evals;     /* point clause evaluations in leaf kernels */
-    double ms_total;           /* device time of the whole pipeline */
+    uint32_t levels;            /* octree depth (Region::withResolution) */
+    uint64_t cells_evaluated;   /* interval-evaluated cells, all levels */
+    uint64_t leaf_groups;       /* sibling groups evaluated at the finest level */
+    uint64_t leaves_ambiguous;  /* leaf records (ambiguous leaves + collapses) */
+    uint64_t clause_evals;      /* value-mode clause x point evaluations in
+                                   the leaf kernel (active lanes only) */
+    uint64_t clause_evals_grad; /* value+gradient clause x point evaluations */
+    uint64_t triangles;
+    uint64_t vertices;          /* excluding the placeholder vertex 0 */
+    uint64_t kernel_launches;   /* kernels of this library launched */
+    double ms_total;            /* host wall time of the whole call */
+    double ms_interval;         /* device time per stage (CUDA events) */
+    double ms_leaf;
+    double ms_collapse;
+    double ms_dual;
 } lfb_mesh_stats;
+
+/* Number of kernels this library has launched since it was loaded. */
+uint64_t lfb_kernel_launches(void);
 
 /* Mesh::render with DUAL_CONTOURING (mesh.cpp:35-125) on the GPU.  The
  * result is freed with libfive_mesh_delete; NULL on failure. */

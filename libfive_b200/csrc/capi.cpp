@@ -572,6 +572,8 @@ libfive_mesh* lfb_render_mesh(lfb_tape t, libfive_region3 R,
     return out;
 }
 
+uint64_t lfb_kernel_launches(void) { return launches(); }
+
 int lfb_tree_slot_tape(libfive_tree t, uint32_t counts[8], int32_t* clauses,
                        uint32_t* const_slots, float* const_values,
                        uint32_t* var_slots, const void** var_ids)

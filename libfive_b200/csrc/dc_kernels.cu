@@ -215,7 +215,8 @@ __device__ __forceinline__ float warp_fetch_v(uint8_t kind, uint16_t idx,
 /// saw equal arguments (ArrayEvaluator::getAmbiguous, eval_array.cpp:197-217).
 __device__ float warp_value(const DevTape& bt, const RegClause* cl,
                             uint32_t len, float* R, int lane, float x,
-                            float y, float z, bool* ambig, uint64_t* evals)
+                            float y, float z, bool* ambig, uint64_t* evals,
+                            bool active = true)
 {
     R[0 * 32 + lane] = x;
     R[1 * 32 + lane] = y;
@@ -231,7 +232,8 @@ __device__ float warp_value(const DevTape& bt, const RegClause* cl,
         R[(raw.x >> 16) * 32 + lane] = dv_value(o, a, b);
     }
     if (ambig) *ambig = amb;
-    if (evals && lane == 0) *evals += len;
+    const uint32_t act = __ballot_sync(0xffffffffu, active);
+    if (evals && lane == 0) *evals += static_cast<uint64_t>(__popc(act)) * len;
     return warp_fetch_v(bt.root_kind, bt.root, R, lane, bt.cpool);
 }
 
@@ -248,7 +250,7 @@ __device__ __forceinline__ D4 warp_fetch_d(uint8_t kind, uint16_t idx,
 
 __device__ D4 warp_deriv(const DevTape& bt, const RegClause* cl, uint32_t len,
                          float* R, int lane, float x, float y, float z,
-                         bool* ambig, uint64_t* evals)
+                         bool* ambig, uint64_t* evals, bool active = true)
 {
     const float in[3] = {x, y, z};
     for (int a = 0; a < 3; ++a) {
@@ -271,7 +273,8 @@ __device__ D4 warp_deriv(const DevTape& bt, const RegClause* cl, uint32_t len,
         out[0] = r.v; out[32] = r.dx; out[64] = r.dy; out[96] = r.dz;
     }
     if (ambig) *ambig = amb;
-    if (evals && lane == 0) *evals += len;
+    const uint32_t act = __ballot_sync(0xffffffffu, active);
+    if (evals && lane == 0) *evals += static_cast<uint64_t>(__popc(act)) * len;
     return warp_fetch_d(bt.root_kind, bt.root, R, lane, bt.cpool);
 }
 
@@ -332,7 +335,7 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
         base_coords = pc;
     }
     const RegClause* cl = A.arena + tr.off;
-    uint64_t my_evals = 0;
+    uint64_t my_evals = 0, my_devals = 0;
     const FeatCtx fc{R, &S->fs, A.status};
 
     // --- corners (dc_tree.inl:156-239) ---------------------------------
@@ -346,7 +349,8 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
         py = static_cast<float>(lat[1][ib]);
         pz = static_cast<float>(lat[2][ic]);
     }
-    cv = warp_value(A.bt, cl, tr.len, R, lane, px, py, pz, &camb, &my_evals);
+    cv = warp_value(A.bt, cl, tr.len, R, lane, px, py, pz, &camb, &my_evals,
+                    lane < npts);
     uint8_t cst = CELL_EMPTY;
     bool need_d = false, need_f = false;
     if (lane < npts) {
@@ -356,7 +360,8 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
         else need_f = true;
     }
     if (__any_sync(0xffffffffu, need_d)) {
-        const D4 d = warp_deriv(A.bt, cl, tr.len, R, lane, px, py, pz, nullptr, &my_evals);
+        const D4 d = warp_deriv(A.bt, cl, tr.len, R, lane, px, py, pz, nullptr,
+                                &my_devals, need_d);
         if (need_d) {
             cst = (d.dx != 0 || d.dy != 0 || d.dz != 0) ? CELL_FILLED : CELL_EMPTY;
         }
@@ -484,7 +489,7 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
                                        static_cast<float>(q[0]),
                                        static_cast<float>(q[1]),
                                        static_cast<float>(q[2]), nullptr,
-                                       &my_evals);
+                                       &my_evals, active);
             // A sample exactly on the surface is resolved with
             // FeatureEvaluator::isInside: for a point without tied min/max
             // that is "gradient is non-zero" (one feature), otherwise the
@@ -495,7 +500,7 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
                 bool amb = false;
                 const D4 dg = warp_deriv(A.bt, cl, tr.len, R, lane, static_cast<float>(q[0]),
                                          static_cast<float>(q[1]), static_cast<float>(q[2]),
-                                         &amb, &my_evals);
+                                         &amb, &my_devals, zero);
                 if (zero && !amb) {
                     const float g[3] = {dg.dx, dg.dy, dg.dz};
                     inside = sqrtf(fdot(g, g)) > 0;
@@ -554,7 +559,7 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
         bool amb = false;
         const D4 d = warp_deriv(A.bt, cl, tr.len, R, lane, static_cast<float>(q[0]),
                                 static_cast<float>(q[1]), static_cast<float>(q[2]),
-                                &amb, &my_evals);
+                                &amb, &my_devals, active);
         if (active) {
             EdgeSlot& es = S->e[p >> 1];
             float* g = (p & 1) ? es.g1 : es.g0;
@@ -669,7 +674,10 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
             }
         }
     }
-    if (lane == 0) atomicAdd(A.evals, static_cast<unsigned long long>(my_evals));
+    if (lane == 0) {
+        atomicAdd(A.evals, static_cast<unsigned long long>(my_evals));
+        atomicAdd(A.evals + 1, static_cast<unsigned long long>(my_devals));
+    }
     (void)base_coords;
 }
 
@@ -1309,6 +1317,14 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
         cudaMemsetAsync(o.lv[0].type, CELL_BRANCH, 1, s);
     }
 
+    // Stage timing with CUDA events on the pipeline's stream (only when the
+    // caller asks for statistics).
+    cudaEvent_t ev[5] = {};
+    if (stats) {
+        for (auto& e : ev) cudaEventCreate(&e);
+        cudaEventRecord(ev[0], s);
+    }
+    uint64_t n_launch = 1;   // k_init_root
     uint64_t cells_evaluated = 0;
     uint64_t dec_total = bt.n_choices;   // decision bytes needed by level 0
     for (int d = 0; d < L; ++d) {
@@ -1339,6 +1355,7 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
             cudaStreamSynchronize(s);
             k_interval_level<<<(lv.n_cells + block - 1) / block, block, smem, s>>>(
                 o, d, bt, arena, arena_top, static_cast<uint32_t>(arena_cap), dec, status);
+            ++n_launch;
             if (!cuda_ok(cudaGetLastError(), "interval kernel")) return LFB_E_CUDA;
             uint32_t st = 0;
             cudaMemcpyAsync(&st, status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
@@ -1382,6 +1399,7 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
         uint64_t* dec_sizes = ws.get<uint64_t>(K_DECSZ, n_groups + 1);
         if (!dec_sizes) return LFB_E_CUDA;
         k_build_groups<<<(lv.n_cells + 255) / 256, 256, 0, s>>>(o, d, scan, dec_sizes);
+        n_launch += 2;   // k_branch_flags + k_build_groups
         cudaMemsetAsync(dec_sizes + n_groups, 0, sizeof(uint64_t), s);
         if (!exclusive_scan(dec_sizes, o.lv[d + 1].group_dec, n_groups, s)) return LFB_E_CUDA;
         // total decision bytes of the next level
@@ -1402,6 +1420,7 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
         }
     }
 
+    if (stats) cudaEventRecord(ev[1], s);
     // Leaves.
     const uint32_t n_leaf_groups = (L == 0) ? 1 : o.lv[L].n_groups;
     const size_t rec_cap = static_cast<size_t>(n_leaf_groups) * 8 + cells_evaluated + 16;
@@ -1421,7 +1440,9 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
                              static_cast<int>(smem));
         k_leaf_groups<<<(n_leaf_groups + wpb - 1) / wpb, 32 * wpb, smem, s>>>(A, n_leaf_groups);
         if (!cuda_ok(cudaGetLastError(), "leaf kernel")) return LFB_E_CUDA;
+        ++n_launch;
     }
+    if (stats) cudaEventRecord(ev[2], s);
 
     // Bottom-up collapse.
     {
@@ -1438,10 +1459,12 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
             const uint32_t n = o.lv[d].n_cells;
             if (!n) continue;
             k_collapse_level<<<(n + block - 1) / block, block, smem, s>>>(C, d);
+            ++n_launch;
         }
         if (!cuda_ok(cudaGetLastError(), "collapse kernel")) return LFB_E_CUDA;
     }
 
+    if (stats) cudaEventRecord(ev[3], s);
     uint32_t st = 0, n_recs = 0;
     cudaMemcpyAsync(&st, status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(&n_recs, rec_top, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
@@ -1484,6 +1507,7 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
                 cudaMemsetAsync(n_out, 0, sizeof(uint32_t), s);
                 D.out = qb;
                 k_dual_round<<<(n_in + 127) / 128, 128, 0, s>>>(D, qa, n_in);
+                ++n_launch;
                 uint32_t st2 = 0;
                 cudaMemcpyAsync(&n_in, n_out, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
                 cudaMemcpyAsync(&st2, status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
@@ -1514,8 +1538,10 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
             if (!verts) return LFB_E_CUDA;
             cudaMemsetAsync(verts, 0, 3 * sizeof(float), s);
             k_vertex_ids<<<(n_keys + 255) / 256, 256, 0, s>>>(used, vscan, n_keys, recs, verts);
+            n_launch += 2;   // k_u8_to_u32 + k_vertex_ids
             if (n_tri) {
                 k_remap_tris<<<(3 * n_tri + 255) / 256, 256, 0, s>>>(tris, n_tri, vscan);
+                ++n_launch;
             }
             out.verts.resize(3 * (static_cast<size_t>(n_verts) + 1));
             out.tris.resize(3 * static_cast<size_t>(n_tri));
@@ -1530,14 +1556,28 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
         }
     }
 
+    note_launches(n_launch);
     if (stats) {
-        unsigned long long ev = 0;
-        cudaMemcpy(&ev, evals, sizeof(ev), cudaMemcpyDeviceToHost);
+        cudaEventRecord(ev[4], s);
+        cudaEventSynchronize(ev[4]);
+        unsigned long long ce[2] = {0, 0};
+        cudaMemcpy(ce, evals, sizeof(ce), cudaMemcpyDeviceToHost);
         stats->levels = static_cast<uint32_t>(L);
         stats->cells_evaluated = cells_evaluated;
         stats->leaf_groups = n_leaf_groups;
         stats->leaves_ambiguous = n_recs;
-        stats->clause_evals = ev * 32;
+        stats->clause_evals = ce[0];
+        stats->clause_evals_grad = ce[1];
+        stats->triangles = out.tris.size() / 3;
+        stats->vertices = out.verts.size() / 3 - 1;
+        stats->kernel_launches = n_launch;
+        float ms[4];
+        for (int k = 0; k < 4; ++k) cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]);
+        stats->ms_interval = ms[0];
+        stats->ms_leaf = ms[1];
+        stats->ms_collapse = ms[2];
+        stats->ms_dual = ms[3];
+        for (auto& e : ev) cudaEventDestroy(e);
         stats->ms_total = std::chrono::duration<double, std::milli>(
                               std::chrono::steady_clock::now() - t_start).count();
     }

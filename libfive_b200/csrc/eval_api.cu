@@ -20,6 +20,7 @@ int eval_values_device(GpuTape& g, uint64_t n, const float* x, const float* y,
                      "value kernel")) {
             return LFB_E_CUDA;
         }
+        note_launches(1);
     }
     return 0;
 }
@@ -75,6 +76,7 @@ int eval_derivs_device(GpuTape& g, uint64_t n, const float* x, const float* y,
                      "derivative kernel")) {
             return LFB_E_CUDA;
         }
+        note_launches(1);
     }
     return 0;
 }
@@ -125,6 +127,7 @@ int eval_intervals_device(GpuTape& g, uint64_t n, const float* xlo,
                      "interval kernel")) {
             return LFB_E_CUDA;
         }
+        note_launches(1);
     }
     return 0;
 }

@@ -1,5 +1,6 @@
 #include "runtime.hpp"
 
+#include <atomic>
 #include <cstdio>
 
 #include "libfive_b200.h"
@@ -55,6 +56,10 @@ bool require_device()
     }
     return true;
 }
+
+static std::atomic<uint64_t> g_launches{0};
+void note_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+uint64_t launches() { return g_launches.load(std::memory_order_relaxed); }
 
 std::mutex& global_mutex()
 {

@@ -57,6 +57,10 @@ struct DevBuf {
     template <class T> T* as() const { return static_cast<T*>(ptr); }
 };
 
+/// Counts kernel launches of this library (reported by lfb_kernel_launches).
+void note_launches(uint64_t n);
+uint64_t launches();
+
 /// Serialises use of the library's default stream and scratch buffers.
 std::mutex& global_mutex();
 

@@ -54,7 +54,15 @@ class MeshStats(ctypes.Structure):
                 ("leaf_groups", ctypes.c_uint64),
                 ("leaves_ambiguous", ctypes.c_uint64),
                 ("clause_evals", ctypes.c_uint64),
-                ("ms_total", ctypes.c_double)]
+                ("clause_evals_grad", ctypes.c_uint64),
+                ("triangles", ctypes.c_uint64),
+                ("vertices", ctypes.c_uint64),
+                ("kernel_launches", ctypes.c_uint64),
+                ("ms_total", ctypes.c_double),
+                ("ms_interval", ctypes.c_double),
+                ("ms_leaf", ctypes.c_double),
+                ("ms_collapse", ctypes.c_double),
+                ("ms_dual", ctypes.c_double)]
 
 
 tree_t = ctypes.c_void_p
@@ -125,6 +133,7 @@ SIGNATURES = [
     ("lfb_eval_jacobian", ctypes.c_int, [tape_t, ctypes.c_uint64, vp, vp, vp, vp, vp, ctypes.c_uint32]),
     ("lfb_eval_grad", ctypes.c_int, [tape_t, ctypes.c_uint64, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_uint32]),
     ("lfb_render_mesh", ctypes.POINTER(Mesh), [tape_t, Region3, MeshSettings, ctypes.POINTER(MeshStats)]),
+    ("lfb_kernel_launches", ctypes.c_uint64, []),
     ("lfb_tree_slot_tape", ctypes.c_int, [tree_t, u32p, i32p, u32p, fp, u32p, ctypes.POINTER(vp)]),
 ]
 

@@ -50,6 +50,18 @@ int lfb_tape_info(lfb_tape t, uint32_t counts[6]);
  * JacobianEvaluator::gradient, eval_jacobian.cpp:77-90). */
 int lfb_tape_var_ids(lfb_tape t, const void** var_ids, uint32_t len);
 
+/*  No counterpart in the reference.  Value and d/dx, d/dy, d/dz of at most
+ *  262144 host points per call (larger n is rejected with LFB_E_INVALID),
+ *  staged through a fixed 7 MiB device array that is part of the library,
+ *  so the call allocates no device memory: for callers that cannot call
+ *  cudaMalloc while they run.  All arguments are host pointers (dx, dy, dz
+ *  may be NULL).  The first call on each device looks the array up and
+ *  should come before any stream capture; calls must not overlap on the
+ *  GPU, since they share the array. */
+int lfb_eval_derivs_static(lfb_tape t, uint64_t n, const float* x,
+                           const float* y, const float* z, float* v,
+                           float* dx, float* dy, float* dz);
+
 /* ArrayEvaluator::values (eval_array.cpp:106-118) over n points. */
 int lfb_eval_values(lfb_tape t, uint64_t n, const float* x, const float* y,
                     const float* z, float* out, void* stream, uint32_t flags);

@@ -33,6 +33,12 @@ struct libfive_evaluator_ {
     std::shared_ptr<GpuTape> g;
 };
 
+namespace lfb {
+/// The device tape behind an lfb_tape handle (used by entry points that
+/// live in other translation units).
+GpuTape* tape_of(lfb_tape t) { return t ? t->g.get() : nullptr; }
+}  // namespace lfb
+
 extern "C" {
 
 ////////////////////////////////////////////////////////////////////////////////

@@ -34,6 +34,11 @@ SEED_BASE = 2
 N_PRIMS = 2000
 REGION = ((-1.5, -1.5, -1.5), (1.5, 1.5, 1.5))
 MIN_FEATURE = 3.0 / 1000.0      # Region::withResolution -> depth 10
+
+
+def min_feature_for(depth):
+    """min_feature giving `depth` levels over the 3-unit region."""
+    return 3.0 / (2 ** depth - 24) if depth >= 6 else 3.0 / (2 ** depth - 0.5)
 MAX_ERR = 1e-8
 SUBDIV = 8                       # CPU sample: sub-boxes of a 8x8x8 split
 
@@ -56,6 +61,11 @@ def parse():
     p.add_argument("--cpu-sample", type=int, default=24,
                    help="sub-boxes meshed per CPU baseline step")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true",
+                   help="skip the end-to-end pass (profiling runs)")
+    p.add_argument("--depth", type=int, default=10,
+                   help="octree depth; 10 is the benchmark workload, smaller "
+                        "depths are for profiling captures")
     return p.parse_args()
 
 
@@ -230,7 +240,8 @@ def run_ours(args, world, rank, local):
     wv, wg, n_clauses = tape_weights(shape)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
     region = ffi.Region3(*[ffi.Interval(a, b) for a, b in zip(*REGION)])
-    settings = ffi.MeshSettings(MIN_FEATURE, MAX_ERR)
+    settings = ffi.MeshSettings(MIN_FEATURE if args.depth == 10 else
+                                min_feature_for(args.depth), MAX_ERR)
 
     def mesh_once(t):
         st = ffi.MeshStats()
@@ -273,7 +284,7 @@ def run_ours(args, world, rank, local):
     # End to end through the public API: flatten + upload the tape, mesh,
     # download and copy into a libfive_mesh, every step.
     e2e_ms, h2d, d2h = 0.0, 0, 0
-    for _ in range(args.steps):
+    for _ in range(0 if args.no_e2e else args.steps):
         flush.fill_(1)
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
@@ -292,7 +303,7 @@ def run_ours(args, world, rank, local):
         pg.all_reduce(times, op=pg.ReduceOp.MAX)
     total_ms, e2e_ms = times.tolist()
     value = world * args.steps / (total_ms / 1000.0)
-    e2e_value = world * args.steps / (e2e_ms / 1000.0)
+    e2e_value = world * args.steps / (e2e_ms / 1000.0) if e2e_ms > 0 else None
 
     if rank == 0:
         sm_mhz = clk.get("sm_mhz") or 1965.0

@@ -25,6 +25,16 @@ enum : uint32_t {
     ST_QUEUE_OVERFLOW = 1u << 2,
     ST_FEATURE_OVERFLOW = 1u << 3,
     ST_REGS = 1u << 4,
+    ST_LIST_OVERFLOW = 1u << 5,
+};
+
+/// A level-ordered clause list (WideEntry) in a list arena, with the list
+/// slot of the tape's root (or its pool index when the root is a constant).
+struct ListRef {
+    uint32_t off;
+    uint32_t len;
+    uint32_t root;
+    uint32_t pad;
 };
 
 struct TapeRef {
@@ -59,7 +69,8 @@ struct LevelView {
     uint32_t n_groups;       // groups of 8 cells at this depth (depth > 0)
     uint32_t* group_parent;  // cell index at depth - 1
     TapeRef* group_tape;
-    uint64_t* group_dec;     // decision scratch offset per group
+    ListRef* cell_list;      // level-ordered form of cell_tape
+    ListRef* group_list;
 };
 
 struct Octree {

@@ -43,7 +43,7 @@ __device__ __forceinline__ float fdot(const float* a, const float* b)
 }
 
 /// Feature::check(e, dup) (feature.cpp:100-245).
-__device__ inline bool feat_check(const FeatCtx& C, const float* f, const float* e,
+static __device__ __noinline__ bool feat_check(const FeatCtx& C, const float* f, const float* e,
                                   bool* dup)
 {
     const int n = static_cast<int>(f[3]);
@@ -213,7 +213,7 @@ __device__ __forceinline__ void feat_copy(float* dst, const float* src)
 ////////////////////////////////////////////////////////////////////////////////
 // FeatureEvaluator::operator() (eval_feature.cpp:171-372) over a register tape
 
-__device__ inline void feat_eval(const FeatCtx& C, const DevTape& bt,
+static __device__ __noinline__ void feat_eval(const FeatCtx& C, const DevTape& bt,
                                  const RegClause* cl, uint32_t len, float x,
                                  float y, float z, float* root_val,
                                  const float** root_list, int* root_n)
@@ -415,7 +415,7 @@ __device__ inline void feat_eval(const FeatCtx& C, const DevTape& bt,
 
 /// FeatureEvaluator::isInside (eval_feature.cpp:56-116).  Warp-collective:
 /// every lane passes the same point.
-__device__ inline bool dev_is_inside(const FeatCtx& C, const DevTape& bt,
+static __device__ __noinline__ bool dev_is_inside(const FeatCtx& C, const DevTape& bt,
                                      const RegClause* cl, uint32_t len, float x,
                                      float y, float z, int lane)
 {
@@ -449,7 +449,7 @@ __device__ inline bool dev_is_inside(const FeatCtx& C, const DevTape& bt,
 
 /// One QEF sample per distinct feature gradient (dc_tree.inl:456-469 with
 /// FeatureEvaluator::features, eval_feature.cpp:151-169).  Warp-collective.
-__device__ inline void dev_push_features(const FeatCtx& C, const DevTape& bt,
+static __device__ __noinline__ void dev_push_features(const FeatCtx& C, const DevTape& bt,
                                          const RegClause* cl, uint32_t len,
                                          const double pos[3], double value,
                                          Qef* q, uint8_t* exists, int lane)

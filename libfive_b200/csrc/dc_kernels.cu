@@ -28,6 +28,7 @@
 
 #include "dc_device.cuh"
 #include "dc_features.cuh"
+#include "eval_kernels.cuh"
 
 namespace lfb {
 
@@ -36,154 +37,408 @@ __constant__ DcTables c_tab;
 ////////////////////////////////////////////////////////////////////////////////
 // 1. Interval classification and tape pruning
 
-__device__ __forceinline__ Iv iv_fetch(uint8_t kind, uint16_t idx,
-                                       const float* L, const float* H,
-                                       const uint8_t* N, int tid, int B,
-                                       const float* __restrict__ cp)
+// One warp per cell.  The tape a cell inherits is held twice: as a register
+// tape (for point evaluation) and as a list of its clauses sorted by
+// dependency level whose operands name list slots (WideEntry), so the lanes
+// of a warp evaluate the independent clauses of one level at once.  The
+// per-slot state of a list of up to kWideSmemSlots entries lives in shared
+// memory, that of longer lists in a per-warp global scratch slice.
+
+constexpr uint32_t kWideSmemSlots = 512;
+
+struct WideSmem {
+    float2 S[kWideSmemSlots + 3];      // slot intervals
+    uint32_t newpos[kWideSmemSlots];   // entry -> position in the child list
+    uint8_t SN[kWideSmemSlots + 3];    // slot maybe-NaN flags
+    uint8_t pst[kWideSmemSlots];       // entry state for the children
+    uint8_t live[kWideSmemSlots];      // entry still needed by the children
+};
+
+struct WideArgs {
+    Octree o;
+    DevTape bt;
+    uint32_t n;                    // clauses of the unpruned tape
+    const WideEntry* in_lists;     // lists of this depth's groups
+    ListRef root_list;             // the unpruned list (depth 0)
+    WideEntry* out_lists;          // lists handed to the next depth
+    unsigned long long* out_top;
+    uint64_t out_cap;
+    int write_lists;
+    RegClause* arena;              // register tapes
+    unsigned long long* arena_top;
+    uint64_t arena_cap;
+    // Per-warp global scratch: slot state of long lists, and the two-level
+    // bitmap of clause states that orders the register tape (zero between
+    // cells).
+    float2* S;                     // [warps][n + 3]
+    uint8_t* SN;                   // [warps][n + 3]
+    uint8_t* pst;                  // [warps][n]
+    uint8_t* live;                 // [warps][n]
+    uint32_t* newpos;              // [warps][n]
+    uint32_t* st2;                 // [warps][nw]   2-bit state per clause
+    uint32_t* l1;                  // [warps][nw1]  non-zero words of st2
+    uint32_t* wl;                  // [warps][nw]   word list
+    uint32_t* status;
+};
+
+__device__ __forceinline__ Iv wide_fetch(uint32_t kind, uint32_t idx,
+                                         const float2* S, const uint8_t* SN,
+                                         const float* __restrict__ cp)
 {
     if (kind == OPND_REG) {
-        return {L[idx * B + tid], H[idx * B + tid], N[idx * B + tid] != 0};
+        const float2 v = S[idx];
+        return {v.x, v.y, SN[idx] != 0};
     }
     const float v = __ldg(cp + idx);
     return iv_make(v, v);
 }
 
-__global__ void __launch_bounds__(128)
-k_interval_level(Octree o, int d, DevTape bt, RegClause* arena,
-                 uint32_t* arena_top, uint32_t arena_cap, uint8_t* dec,
-                 uint32_t* status)
+/// Interval of list entry k, stored in slot 3 + k, and the entry's state for
+/// the cell's children; returns whether a min/max got decided
+/// (IntervalEvaluator::eval + push, eval_interval.cpp:116-167).
+__device__ __forceinline__ bool wide_forward(const uint4& e, uint32_t k, const float* cp,
+                                             float2* S, uint8_t* SN, uint8_t* pst)
 {
-    extern __shared__ float smem[];
-    const int B = blockDim.x;
-    const int tid = threadIdx.x;
-    float* L = smem;
-    float* H = smem + bt.n_regs * B;
-    uint8_t* N = reinterpret_cast<uint8_t*>(smem + 2 * bt.n_regs * B);
-
-    const LevelView& lv = o.lv[d];
-    const uint32_t i = blockIdx.x * B + tid;
-    if (i >= lv.n_cells) return;
-
-    TapeRef tr;
-    uint64_t dec_base;
-    if (d == 0) {
-        tr = {0u, bt.n, bt.n_choices, 0u};
-        dec_base = 0;
+    const uint8_t o = e.x & 0xff;
+    const uint32_t kinds = (e.x >> 8) & 0xf;
+    const uint32_t st = (e.x >> 12) & 3;
+    Iv r;
+    uint8_t ps = static_cast<uint8_t>(st);
+    bool decided = false;
+    if (st == WIDE_A) {
+        r = wide_fetch(kinds & 3, e.y, S, SN, cp);
+    } else if (st == WIDE_B) {
+        r = wide_fetch((kinds >> 2) & 3, e.z, S, SN, cp);
     } else {
-        tr = lv.group_tape[i >> 3];
-        dec_base = lv.group_dec[i >> 3] + static_cast<uint64_t>(i & 7) * tr.nch;
-    }
-
-    double blo[3], bhi[3];
-    cell_bounds(o, d, lv.coords[i], blo, bhi);
-    for (int a = 0; a < 3; ++a) {
-        const Iv v = iv_make(static_cast<float>(blo[a]), static_cast<float>(bhi[a]));
-        L[a * B + tid] = v.lo;
-        H[a * B + tid] = v.hi;
-        N[a * B + tid] = v.nan;
-    }
-
-    // Forward interval pass, recording the push decision of every min/max
-    // (IntervalEvaluator::push, eval_interval.cpp:116-167).
-    const RegClause* cl = arena + tr.off;
-    bool changed = false;
-    uint32_t ch = 0;
-    for (uint32_t c = 0; c < tr.len; ++c) {
-        const uint2 raw = *reinterpret_cast<const uint2*>(cl + c);
-        const uint8_t op_ = raw.x & 0xff;
-        const uint8_t kinds = (raw.x >> 8) & 0xff;
-        const uint16_t ro = raw.x >> 16;
-        const Iv a = iv_fetch(kinds & 3, raw.y & 0xffff, L, H, N, tid, B, bt.cpool);
-        const Iv b = iv_fetch((kinds >> 2) & 3, raw.y >> 16, L, H, N, tid, B, bt.cpool);
-        const Iv r = iv_apply(op_, a, b);
-        if (op_ == op::MIN || op_ == op::MAX) {
+        const Iv a = wide_fetch(kinds & 3, e.y, S, SN, cp);
+        const Iv b = dev_is_binary(o) ? wide_fetch((kinds >> 2) & 3, e.z, S, SN, cp) : a;
+        r = iv_apply(o, a, b);
+        if (o == op::MIN || o == op::MAX) {
             uint8_t keep = 0;   // 0 both, 1 a, 2 b
-            if (a.lo > b.hi) keep = (op_ == op::MAX) ? 1 : 2;
-            else if (b.lo > a.hi) keep = (op_ == op::MAX) ? 2 : 1;
-            changed |= keep != 0;
-            dec[dec_base + ch++] = keep;
-        }
-        L[ro * B + tid] = r.lo;
-        H[ro * B + tid] = r.hi;
-        N[ro * B + tid] = r.nan;
-    }
-    const Iv root = iv_fetch(bt.root_kind, bt.root, L, H, N, tid, B, bt.cpool);
-    const uint8_t state = iv_state(root);
-    lv.type[i] = state == ST_EMPTY ? CELL_EMPTY
-               : state == ST_FILLED ? CELL_FILLED : CELL_BRANCH;
-    if (state != ST_AMBIGUOUS) {
-        return;
-    }
-    // NaN-unsafe results keep the unpruned tape (dc_tree.inl:107-111).
-    if (root.nan || !changed) {
-        lv.cell_tape[i] = tr;
-        return;
-    }
-
-    // Backward liveness pass over the register tape: N now marks registers
-    // whose value is still needed.  Count first, then allocate and write.
-    uint32_t kept = 0, kept_ch = 0;
-    for (int pass = 0; pass < 2; ++pass) {
-        for (uint32_t r = 0; r < bt.n_regs; ++r) N[r * B + tid] = 0;
-        if (bt.root_kind == OPND_REG) N[bt.root * B + tid] = 1;
-        uint32_t out_pos = kept;
-        uint32_t chi = ch;
-        uint32_t off = 0;
-        if (pass == 1) {
-            off = atomicAdd(arena_top, kept);
-            if (off + kept > arena_cap || off + kept < off) {
-                atomicOr(status, ST_ARENA_OVERFLOW);
-                lv.cell_tape[i] = tr;
-                return;
-            }
-        }
-        for (int64_t c = static_cast<int64_t>(tr.len) - 1; c >= 0; --c) {
-            const uint2 raw = *reinterpret_cast<const uint2*>(cl + c);
-            const uint8_t op_ = raw.x & 0xff;
-            const uint8_t kinds = (raw.x >> 8) & 0xff;
-            const uint16_t ro = raw.x >> 16;
-            const bool is_choice = (op_ == op::MIN || op_ == op::MAX);
-            uint8_t keep = 0;
-            if (is_choice) keep = dec[dec_base + (--chi)];
-            if (!N[ro * B + tid]) continue;
-            N[ro * B + tid] = 0;
-            RegClause outc;
-            bool emit = true;
+            if (a.lo > b.hi) keep = (o == op::MAX) ? 1 : 2;
+            else if (b.lo > a.hi) keep = (o == op::MAX) ? 2 : 1;
             if (keep) {
-                const uint8_t k = keep == 1 ? (kinds & 3) : ((kinds >> 2) & 3);
-                const uint16_t src = keep == 1 ? (raw.y & 0xffff) : (raw.y >> 16);
-                if (k == OPND_REG) {
-                    N[src * B + tid] = 1;
-                    emit = (src != ro);
-                }
-                outc.op = OP_COPY;
-                outc.kinds = k;
-                outc.out = ro;
-                outc.a = src;
-                outc.b = 0;
-            } else {
-                if ((kinds & 3) == OPND_REG) N[(raw.y & 0xffff) * B + tid] = 1;
-                if (dev_is_binary(op_) && ((kinds >> 2) & 3) == OPND_REG) {
-                    N[(raw.y >> 16) * B + tid] = 1;
-                }
-                *reinterpret_cast<uint2*>(&outc) = raw;
-            }
-            if (!emit) continue;
-            if (pass == 0) {
-                ++kept;
-                if (is_choice && !keep) ++kept_ch;
-            } else {
-                arena[off + (--out_pos)] = outc;
+                ps = keep == 1 ? WIDE_A : WIDE_B;
+                decided = true;
             }
         }
-        if (pass == 1) {
-            lv.cell_tape[i] = {off, kept, kept_ch, 0u};
+    }
+    S[3 + k] = make_float2(r.lo, r.hi);
+    SN[3 + k] = r.nan;
+    pst[k] = ps;
+    return decided;
+}
+
+/// Marks the operands a live entry still needs (Tape::push's remapping,
+/// tape.cpp:23-160, as liveness).
+__device__ __forceinline__ void wide_mark(const uint4& e, uint8_t ps, uint8_t* live)
+{
+    const uint8_t o = e.x & 0xff;
+    const uint32_t kinds = (e.x >> 8) & 0xf;
+    if (ps != WIDE_B && (kinds & 3) == OPND_REG && e.y >= 3) live[e.y - 3] = 1;
+    if (ps != WIDE_A && dev_is_binary(o) && ((kinds >> 2) & 3) == OPND_REG && e.z >= 3) {
+        live[e.z - 3] = 1;
+    }
+}
+
+/// Emitted register clauses for one 16-clause word of 2-bit states, and how
+/// many of them are undecided min/max clauses.
+__device__ __forceinline__ void wide_word_counts(uint32_t word, uint32_t w,
+                                                 const RegClause* root,
+                                                 uint32_t& emit, uint32_t& nch)
+{
+    emit = 0;
+    nch = 0;
+    while (word) {
+        const int j = (__ffs(word) - 1) >> 1;
+        const uint32_t ps = (word >> (2 * j)) & 3;
+        word &= ~(3u << (2 * j));
+        const uint2 raw = __ldg(reinterpret_cast<const uint2*>(root + w * 16 + j));
+        const uint8_t o = raw.x & 0xff;
+        if (ps == WIDE_BOTH) {
+            ++emit;
+            nch += (o == op::MIN || o == op::MAX);
+        } else {
+            const uint32_t kinds = (raw.x >> 8) & 0xff;
+            const uint32_t k = ps == WIDE_A ? (kinds & 3) : ((kinds >> 2) & 3);
+            const uint32_t src = ps == WIDE_A ? (raw.y & 0xffff) : (raw.y >> 16);
+            emit += !(k == OPND_REG && src == (raw.x >> 16));
         }
+    }
+}
+
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v, int lane)
+{
+    for (int sh = 1; sh < 32; sh <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, v, sh);
+        if (lane >= sh) v += t;
+    }
+    return v;
+}
+
+__global__ void __launch_bounds__(256)
+k_interval_wide(WideArgs A, int d)
+{
+    extern __shared__ __align__(16) unsigned char wsm[];
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + warp;
+    const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+    WideSmem* SM = reinterpret_cast<WideSmem*>(wsm) + warp;
+    const Octree& o = A.o;
+    const LevelView& lv = o.lv[d];
+    const DevTape& bt = A.bt;
+    const uint32_t n = A.n;
+    const uint32_t nw = (n + 15) / 16;
+    const uint32_t nw1 = (nw + 31) / 32;
+    float2* gS = A.S + static_cast<size_t>(gw) * (n + 3);
+    uint8_t* gSN = A.SN + static_cast<size_t>(gw) * (n + 3);
+    uint8_t* gP = A.pst + static_cast<size_t>(gw) * n;
+    uint8_t* gL = A.live + static_cast<size_t>(gw) * n;
+    uint32_t* gN = A.newpos + static_cast<size_t>(gw) * n;
+    uint32_t* st2 = A.st2 + static_cast<size_t>(gw) * nw;
+    uint32_t* l1 = A.l1 + static_cast<size_t>(gw) * nw1;
+    uint32_t* wl = A.wl + static_cast<size_t>(gw) * nw;
+    const unsigned full = 0xffffffffu;
+    const uint32_t lt_mask = (1u << lane) - 1;
+
+    for (uint32_t i = gw; i < lv.n_cells; i += nwarps) {
+        ListRef P;
+        TapeRef T;
+        if (d == 0) {
+            P = A.root_list;
+            T = {0u, bt.n, bt.n_choices, 0u};
+        } else {
+            P = lv.group_list[i >> 3];
+            T = lv.group_tape[i >> 3];
+        }
+        const uint4* PL = reinterpret_cast<const uint4*>(A.in_lists + P.off);
+        const bool small = P.len <= kWideSmemSlots;
+        float2* S = small ? SM->S : gS;
+        uint8_t* SN = small ? SM->SN : gSN;
+        uint8_t* pst = small ? SM->pst : gP;
+        uint8_t* live = small ? SM->live : gL;
+        uint32_t* newpos = small ? SM->newpos : gN;
+        if (lane < 3) {
+            double blo[3], bhi[3];
+            cell_bounds(o, d, lv.coords[i], blo, bhi);
+            const Iv v = iv_make(static_cast<float>(blo[lane]), static_cast<float>(bhi[lane]));
+            S[lane] = make_float2(v.lo, v.hi);
+            SN[lane] = v.nan;
+        }
+        for (uint32_t k = lane; k < P.len; k += 32) live[k] = 0;
+        __syncwarp();
+
+        // Forward pass, level by level (entries are sorted by level, so a
+        // chunk of 32 spans few levels; the warp steps through them).
+        const uint32_t nchunks = (P.len + 31) / 32;
+        bool changed = false;
+        for (uint32_t ch = 0; ch < nchunks; ++ch) {
+            const uint32_t k = ch * 32 + lane;
+            const bool valid = k < P.len;
+            const uint4 e = valid ? PL[k] : make_uint4(0, 0, 0, 0);
+            const uint32_t lev = valid ? (e.x >> kWideLevelShift) : 0xffffffffu;
+            const int last = static_cast<int>(min(31u, P.len - 1 - ch * 32));
+            uint32_t l = __shfl_sync(full, lev, 0);
+            const uint32_t lmax = __shfl_sync(full, lev, last);
+            while (true) {
+                if (lev == l) changed |= wide_forward(e, k, bt.cpool, S, SN, pst);
+                __syncwarp();
+                if (l == lmax) break;
+                const uint32_t m = __ballot_sync(full, valid && lev > l);
+                l = __shfl_sync(full, lev, __ffs(m) - 1);
+            }
+        }
+        changed = __any_sync(full, changed);
+        const Iv root = wide_fetch(bt.root_kind, P.root, S, SN, bt.cpool);
+        const uint8_t state = iv_state(root);
+        if (lane == 0) {
+            lv.type[i] = state == ST_EMPTY ? CELL_EMPTY
+                       : state == ST_FILLED ? CELL_FILLED : CELL_BRANCH;
+        }
+        if (state != ST_AMBIGUOUS) continue;
+
+        if (root.nan || !changed) {
+            // NaN-unsafe or nothing decided: the children keep this tape
+            // (dc_tree.inl:107-111).  Its list moves to the next arena.
+            uint32_t off = 0;
+            if (A.write_lists) {
+                unsigned long long o64 = 0;
+                if (lane == 0) o64 = atomicAdd(A.out_top, static_cast<unsigned long long>(P.len));
+                o64 = __shfl_sync(full, o64, 0);
+                if (o64 + P.len <= A.out_cap) {
+                    off = static_cast<uint32_t>(o64);
+                    uint4* out = reinterpret_cast<uint4*>(A.out_lists + off);
+                    for (uint32_t k = lane; k < P.len; k += 32) out[k] = PL[k];
+                } else if (lane == 0) {
+                    atomicOr(A.status, ST_LIST_OVERFLOW);
+                }
+            }
+            if (lane == 0) {
+                lv.cell_list[i] = {off, P.len, P.root, 0u};
+                lv.cell_tape[i] = T;
+            }
+            continue;
+        }
+
+        // Backward liveness pass, levels in decreasing order.
+        if (lane == 0 && bt.root_kind == OPND_REG && P.root >= 3) live[P.root - 3] = 1;
+        __syncwarp();
+        for (int ch = static_cast<int>(nchunks) - 1; ch >= 0; --ch) {
+            const uint32_t k = ch * 32 + lane;
+            const bool valid = k < P.len;
+            const uint4 e = valid ? PL[k] : make_uint4(0, 0, 0, 0);
+            const uint32_t lev = valid ? (e.x >> kWideLevelShift) : 0u;
+            const int last = static_cast<int>(min(31u, P.len - 1 - ch * 32));
+            const uint32_t lmin = __shfl_sync(full, lev, 0);
+            uint32_t l = __shfl_sync(full, lev, last);
+            while (true) {
+                if (valid && lev == l && live[k]) wide_mark(e, pst[k], live);
+                __syncwarp();
+                if (l == lmin) break;
+                const uint32_t m = __ballot_sync(full, valid && lev < l);
+                l = __shfl_sync(full, lev, 31 - __clz(m));
+            }
+        }
+
+        // Child positions of the live entries, and their 2-bit states by
+        // clause index (for the register tape, which is in clause order).
+        uint32_t cnt = 0;
+        for (uint32_t ch = 0; ch < nchunks; ++ch) {
+            const uint32_t k = ch * 32 + lane;
+            const bool lv_ = k < P.len && live[k];
+            const uint32_t m = __ballot_sync(full, lv_);
+            if (lv_) {
+                newpos[k] = cnt + __popc(m & lt_mask);
+                const uint32_t c = PL[k].w;
+                atomicOr(st2 + (c >> 4), static_cast<uint32_t>(pst[k]) << (2 * (c & 15)));
+                atomicOr(l1 + (c >> 9), 1u << ((c >> 4) & 31));
+            }
+            cnt += __popc(m);
+        }
+        __syncwarp();
+        const uint32_t new_root = (bt.root_kind == OPND_REG && P.root >= 3)
+                                      ? newpos[P.root - 3] + 3 : P.root;
+        uint32_t loff = 0;
+        if (A.write_lists) {
+            unsigned long long o64 = 0;
+            if (lane == 0) o64 = atomicAdd(A.out_top, static_cast<unsigned long long>(cnt));
+            o64 = __shfl_sync(full, o64, 0);
+            const bool ok = o64 + cnt <= A.out_cap;
+            if (!ok && lane == 0) atomicOr(A.status, ST_LIST_OVERFLOW);
+            if (ok) {
+                loff = static_cast<uint32_t>(o64);
+                uint4* out = reinterpret_cast<uint4*>(A.out_lists + loff);
+                for (uint32_t k = lane; k < P.len; k += 32) {
+                    if (!live[k]) continue;
+                    uint4 e = PL[k];
+                    const uint32_t ps = pst[k];
+                    const uint32_t kinds = (e.x >> 8) & 0xf;
+                    const bool binary = dev_is_binary(e.x & 0xff);
+                    if (ps == WIDE_B) e.y = 0;
+                    else if ((kinds & 3) == OPND_REG && e.y >= 3) e.y = newpos[e.y - 3] + 3;
+                    if (ps == WIDE_A) e.z = 0;
+                    else if (binary && ((kinds >> 2) & 3) == OPND_REG && e.z >= 3) {
+                        e.z = newpos[e.z - 3] + 3;
+                    }
+                    e.x = (e.x & ~(3u << 12)) | (ps << 12);
+                    out[newpos[k]] = e;
+                }
+            }
+        }
+
+        // Register tape for this cell: the live clauses in clause order, with
+        // decided min/max clauses as copies (dropped when the copy is onto
+        // the same register).  First the non-zero state words, in order.
+        uint32_t nwl = 0;
+        for (uint32_t j0 = 0; j0 < nw1; j0 += 32) {
+            const uint32_t j = j0 + lane;
+            uint32_t bits = 0;
+            if (j < nw1) {
+                bits = l1[j];
+                l1[j] = 0;
+            }
+            const uint32_t c_ = __popc(bits);
+            const uint32_t incl = warp_incl_scan(c_, lane);
+            uint32_t at = nwl + incl - c_;
+            while (bits) {
+                const int b = __ffs(bits) - 1;
+                bits &= bits - 1;
+                wl[at++] = j * 32 + b;
+            }
+            nwl += __shfl_sync(full, incl, 31);
+        }
+        __syncwarp();
+        uint32_t emit = 0, nch = 0;
+        for (uint32_t k0 = 0; k0 < nwl; k0 += 32) {
+            const uint32_t k = k0 + lane;
+            uint32_t e_ = 0, c_ = 0;
+            if (k < nwl) {
+                const uint32_t w = wl[k];
+                wide_word_counts(st2[w], w, bt.clauses, e_, c_);
+            }
+            emit += __reduce_add_sync(full, e_);
+            nch += __reduce_add_sync(full, c_);
+        }
+        unsigned long long a64 = 0;
+        if (lane == 0) a64 = atomicAdd(A.arena_top, static_cast<unsigned long long>(emit));
+        a64 = __shfl_sync(full, a64, 0);
+        const bool aok = a64 + emit <= A.arena_cap;
+        if (!aok && lane == 0) atomicOr(A.status, ST_ARENA_OVERFLOW);
+        uint32_t pos = static_cast<uint32_t>(a64);
+        for (uint32_t k0 = 0; k0 < nwl; k0 += 32) {
+            const uint32_t k = k0 + lane;
+            uint32_t word = 0, w = 0, e_ = 0, c_ = 0;
+            if (k < nwl) {
+                w = wl[k];
+                word = st2[w];
+                wide_word_counts(word, w, bt.clauses, e_, c_);
+                st2[w] = 0;
+            }
+            const uint32_t incl = warp_incl_scan(e_, lane);
+            uint32_t at = pos + incl - e_;
+            if (aok) {
+                while (word) {
+                    const int j = (__ffs(word) - 1) >> 1;
+                    const uint32_t ps = (word >> (2 * j)) & 3;
+                    word &= ~(3u << (2 * j));
+                    const uint2 raw = __ldg(reinterpret_cast<const uint2*>(bt.clauses + w * 16 + j));
+                    if (ps == WIDE_BOTH) {
+                        *reinterpret_cast<uint2*>(A.arena + at++) = raw;
+                        continue;
+                    }
+                    const uint32_t kinds = (raw.x >> 8) & 0xff;
+                    const uint32_t kk = ps == WIDE_A ? (kinds & 3) : ((kinds >> 2) & 3);
+                    const uint32_t src = ps == WIDE_A ? (raw.y & 0xffff) : (raw.y >> 16);
+                    const uint32_t ro = raw.x >> 16;
+                    if (kk == OPND_REG && src == ro) continue;
+                    RegClause cc;
+                    cc.op = OP_COPY;
+                    cc.kinds = static_cast<uint8_t>(kk);
+                    cc.out = static_cast<uint16_t>(ro);
+                    cc.a = static_cast<uint16_t>(src);
+                    cc.b = 0;
+                    A.arena[at++] = cc;
+                }
+            }
+            pos += __shfl_sync(full, incl, 31);
+        }
+        if (lane == 0) {
+            lv.cell_list[i] = {loff, cnt, new_root, 0u};
+            lv.cell_tape[i] = aok ? TapeRef{static_cast<uint32_t>(a64), emit, nch, 0u} : T;
+        }
+        __syncwarp();
     }
 }
 
 ////////////////////////////////////////////////////////////////////////////////
 // 2. Leaves: one warp per group of eight sibling cells
+
+static __device__ __noinline__ int qef_rank_nd(const Qef& q) { return qef_rank(q); }
+static __device__ __noinline__ double qef_vertex_nd(const Qef& q, double v[3], int* r)
+{
+    return qef_vertex(q, v, r);
+}
 
 struct EdgeSlot {
     double t0[3], t1[3];   // current search bracket: inside, outside
@@ -195,13 +450,19 @@ struct EdgeSlot {
     uint8_t amb[2];        // tied min/max at t0 / t1
 };
 
+/// Per-warp state kept in shared memory (small: occupancy is set by it).
 struct LeafWarpShared {
-    FeatureScratch fs;
-    EdgeSlot e[54];
     int8_t slot_of[54];    // lattice edge -> slot, -1 if not crossing
     uint8_t st[27];        // corner states (CELL_EMPTY / CELL_FILLED)
-    int32_t rec[8];
     uint8_t nslots;
+    int32_t rec[8];
+};
+
+/// Per-warp state kept in global memory (L1-cached): edge brackets / QEFs
+/// and the feature evaluator's scratch, one slice per resident warp.
+struct LeafWarpScratch {
+    FeatureScratch fs;
+    EdgeSlot e[54];
 };
 
 __device__ __forceinline__ float warp_fetch_v(uint8_t kind, uint16_t idx,
@@ -213,7 +474,7 @@ __device__ __forceinline__ float warp_fetch_v(uint8_t kind, uint16_t idx,
 
 /// Value of the tape at (x, y, z) for this lane, plus whether any min/max
 /// saw equal arguments (ArrayEvaluator::getAmbiguous, eval_array.cpp:197-217).
-__device__ float warp_value(const DevTape& bt, const RegClause* cl,
+static __device__ __noinline__ float warp_value(const DevTape& bt, const RegClause* cl,
                             uint32_t len, float* R, int lane, float x,
                             float y, float z, bool* ambig, uint64_t* evals,
                             bool active = true)
@@ -248,7 +509,7 @@ __device__ __forceinline__ D4 warp_fetch_d(uint8_t kind, uint16_t idx,
     return {__ldg(cp + idx), 0.0f, 0.0f, 0.0f};
 }
 
-__device__ D4 warp_deriv(const DevTape& bt, const RegClause* cl, uint32_t len,
+static __device__ __noinline__ D4 warp_deriv(const DevTape& bt, const RegClause* cl, uint32_t len,
                          float* R, int lane, float x, float y, float z,
                          bool* ambig, uint64_t* evals, bool active = true)
 {
@@ -278,6 +539,8 @@ __device__ D4 warp_deriv(const DevTape& bt, const RegClause* cl, uint32_t len,
     return warp_fetch_d(bt.root_kind, bt.root, R, lane, bt.cpool);
 }
 
+constexpr size_t kLeafSmallBytes = (sizeof(LeafWarpShared) + 15) / 16 * 16;
+
 struct LeafArgs {
     Octree o;
     DevTape bt;
@@ -287,9 +550,10 @@ struct LeafArgs {
     uint32_t rec_cap;
     uint32_t* status;
     unsigned long long* evals;
+    LeafWarpScratch* scratch;   // gridDim.x * warps-per-block slices
 };
 
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(256)
 k_leaf_groups(LeafArgs A, uint32_t n_groups)
 {
     extern __shared__ __align__(16) unsigned char lsmem[];
@@ -297,11 +561,13 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
     const int lane = threadIdx.x & 31;
     const int wpb = blockDim.x >> 5;
     LeafWarpShared* S = reinterpret_cast<LeafWarpShared*>(lsmem) + warp;
-    float* R = reinterpret_cast<float*>(reinterpret_cast<LeafWarpShared*>(lsmem) + wpb) +
+    float* R = reinterpret_cast<float*>(lsmem + kLeafSmallBytes * wpb) +
                static_cast<size_t>(warp) * A.bt.n_regs * 128;
-    const uint32_t g = blockIdx.x * wpb + warp;
-    if (g >= n_groups) return;
-
+    LeafWarpScratch* W = A.scratch + static_cast<size_t>(blockIdx.x) * wpb + warp;
+    uint64_t my_evals = 0, my_devals = 0;
+    // Persistent warps: each takes groups g, g + stride, ...
+    const uint32_t stride = gridDim.x * wpb;
+    for (uint32_t g = blockIdx.x * wpb + warp; g < n_groups; g += stride) {
     const Octree& o = A.o;
     const int Ld = o.levels;
     const bool single = (Ld == 0);       // the root itself is the only leaf
@@ -335,8 +601,7 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
         base_coords = pc;
     }
     const RegClause* cl = A.arena + tr.off;
-    uint64_t my_evals = 0, my_devals = 0;
-    const FeatCtx fc{R, &S->fs, A.status};
+    const FeatCtx fc{R, &W->fs, A.status};
 
     // --- corners (dc_tree.inl:156-239) ---------------------------------
     const int npts = n * n * n;
@@ -455,7 +720,7 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
             S->slot_of[e] = crossing ? static_cast<int8_t>(first_slot + before) : -1;
         }
         if (crossing) {
-            EdgeSlot& es = S->e[first_slot + before];
+            EdgeSlot& es = W->e[first_slot + before];
             const bool f0 = S->st[p0] == CELL_FILLED;
             double a[3], b[3];
             pt_pos(f0 ? p0 : p1, a);
@@ -480,7 +745,7 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
             double q[3] = {0, 0, 0};
             if (active) {
                 const double frac = j / (16 - 1.0);
-                const EdgeSlot& es = S->e[slot];
+                const EdgeSlot& es = W->e[slot];
                 for (int k = 0; k < 3; ++k) {
                     q[k] = es.t0[k] * (1 - frac) + es.t1[k] * frac;
                 }
@@ -538,7 +803,7 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
                         nt1[k] = __shfl_sync(0xffffffffu, q[k], hi_lane);
                     }
                     if (lane == 0) {
-                        EdgeSlot& es = S->e[s];
+                        EdgeSlot& es = W->e[s];
                         for (int k = 0; k < 3; ++k) { es.t0[k] = nt0[k]; es.t1[k] = nt1[k]; }
                     }
                 }
@@ -553,7 +818,7 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
         const bool active = p < 2 * E;
         double q[3] = {0, 0, 0};
         if (active) {
-            const EdgeSlot& es = S->e[p >> 1];
+            const EdgeSlot& es = W->e[p >> 1];
             for (int k = 0; k < 3; ++k) q[k] = (p & 1) ? es.t1[k] : es.t0[k];
         }
         bool amb = false;
@@ -561,7 +826,7 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
                                 static_cast<float>(q[1]), static_cast<float>(q[2]),
                                 &amb, &my_devals, active);
         if (active) {
-            EdgeSlot& es = S->e[p >> 1];
+            EdgeSlot& es = W->e[p >> 1];
             float* g = (p & 1) ? es.g1 : es.g0;
             g[0] = d.dx; g[1] = d.dy; g[2] = d.dz; g[3] = d.v;
             es.amb[p & 1] = amb;
@@ -573,12 +838,12 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
     // is tied use every feature gradient instead (eval_feature.cpp:125-169).
     const uint32_t any_amb = __ballot_sync(0xffffffffu, [&] {
         bool a = false;
-        for (int s = lane; s < E; s += 32) a |= S->e[s].amb[0] || S->e[s].amb[1];
+        for (int s = lane; s < E; s += 32) a |= W->e[s].amb[0] || W->e[s].amb[1];
         return a;
     }());
     if (!any_amb) {
         for (int s = lane; s < E; s += 32) {
-            EdgeSlot& es = S->e[s];
+            EdgeSlot& es = W->e[s];
             for (int side = 0; side < 2; ++side) {
                 const float* g = side ? es.g1 : es.g0;
                 const double* pos = side ? es.t1 : es.t0;
@@ -589,7 +854,7 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
         }
     } else {
         for (int s = 0; s < E; ++s) {
-            EdgeSlot& es = S->e[s];
+            EdgeSlot& es = W->e[s];
             for (int side = 0; side < 2; ++side) {
                 const float* g = side ? es.g1 : es.g0;
                 const double* pos = side ? es.t1 : es.t0;
@@ -608,7 +873,7 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
     }
     __syncwarp();
     for (int s = lane; s < E; s += 32) {
-        S->e[s].rank = qef_rank(S->e[s].q);
+        W->e[s].rank = qef_rank_nd(W->e[s].q);
     }
     __syncwarp();
 
@@ -639,16 +904,16 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
                 }
                 int max_rank = 0;
                 for (int k = 0; k < ne; ++k) {
-                    if (slots[k] >= 0 && S->e[slots[k]].exists &&
-                        S->e[slots[k]].rank > max_rank) {
-                        max_rank = S->e[slots[k]].rank;
+                    if (slots[k] >= 0 && W->e[slots[k]].exists &&
+                        W->e[slots[k]].rank > max_rank) {
+                        max_rank = W->e[slots[k]].rank;
                     }
                 }
                 Qef q;
                 qef_zero(q);
                 for (int k = 0; k < ne; ++k) {
-                    if (slots[k] < 0 || !S->e[slots[k]].exists) continue;
-                    const EdgeSlot& es = S->e[slots[k]];
+                    if (slots[k] < 0 || !W->e[slots[k]].exists) continue;
+                    const EdgeSlot& es = W->e[slots[k]];
                     if (es.rank == max_rank) {
                         q.mass[0] += es.q.mass[0] / es.q.mass[3];
                         q.mass[1] += es.q.mass[1] / es.q.mass[3];
@@ -657,12 +922,12 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
                     }
                 }
                 for (int k = 0; k < ne; ++k) {
-                    if (slots[k] < 0 || !S->e[slots[k]].exists) continue;
-                    qef_add(q, S->e[slots[k]].q);
+                    if (slots[k] < 0 || !W->e[slots[k]].exists) continue;
+                    qef_add(q, W->e[slots[k]].q);
                 }
                 double v[3];
                 int rank = 0;
-                qef_vertex(q, v, &rank);
+                qef_vertex_nd(q, v, &rank);
                 for (int k = 0; k < 3; ++k) L.vert[patch][k] = v[k];
                 if (patch == c_tab.npatch[mask] - 1) {
                     for (int k = 0; k < 4; ++k) L.mass[k] = q.mass[k];
@@ -674,11 +939,12 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
             }
         }
     }
+    (void)base_coords;
+    }   // groups
     if (lane == 0) {
         atomicAdd(A.evals, static_cast<unsigned long long>(my_evals));
         atomicAdd(A.evals + 1, static_cast<unsigned long long>(my_devals));
     }
-    (void)base_coords;
 }
 
 }  // namespace lfb
@@ -1122,9 +1388,8 @@ __global__ void k_branch_flags(const uint8_t* type, uint32_t n, uint32_t* flags)
 }
 
 /// For each branch cell at depth d: its group index at d + 1, and the
-/// group's parent, tape, decision scratch size and child coordinates.
-__global__ void k_build_groups(Octree o, int d, const uint32_t* scan,
-                               uint64_t* dec_sizes)
+/// group's parent, tapes and child coordinates.
+__global__ void k_build_groups(Octree o, int d, const uint32_t* scan)
 {
     const LevelView& lv = o.lv[d];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1137,9 +1402,8 @@ __global__ void k_build_groups(Octree o, int d, const uint32_t* scan,
     lv.child_group[i] = static_cast<int32_t>(g);
     LevelView& nv = o.lv[d + 1];
     nv.group_parent[g] = i;
-    const TapeRef tr = lv.cell_tape[i];
-    nv.group_tape[g] = tr;
-    dec_sizes[g] = 8ull * tr.nch;
+    nv.group_tape[g] = lv.cell_tape[i];
+    nv.group_list[g] = lv.cell_list[i];
     uint32_t x, y, z;
     unpack_coords(lv.coords[i], x, y, z);
     for (int k = 0; k < 8; ++k) {
@@ -1177,6 +1441,8 @@ __global__ void k_remap_tris(uint32_t* tris, uint32_t n, const uint32_t* scan)
 // Host driver
 
 #include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <map>
 #include <vector>
 
@@ -1205,9 +1471,11 @@ Workspace& workspace()
 }
 
 enum BufKey {
-    K_ARENA = 1, K_DEC, K_STATUS, K_COUNTERS, K_RECS, K_FLAGS, K_SCAN,
-    K_CUBTMP, K_DECSZ, K_DECOFF, K_TASK_A, K_TASK_B, K_TRIS, K_USED,
-    K_VSCAN, K_VERTS, K_FEAT, K_LEVEL = 100,
+    K_ARENA = 1, K_STATUS, K_COUNTERS, K_RECS, K_FLAGS, K_SCAN,
+    K_CUBTMP, K_TASK_A, K_TASK_B, K_TRIS, K_USED, K_VSCAN, K_VERTS, K_FEAT,
+    K_LIST_A, K_LIST_B, K_WIDE_S, K_WIDE_SN, K_WIDE_P, K_WIDE_LIVE, K_WIDE_NEW,
+    K_WIDE_ST2, K_WIDE_L1, K_WIDE_WL,
+    K_LEVEL = 100,
 };
 
 bool tables_ready = false;
@@ -1230,6 +1498,16 @@ int level_from_resolution(const double lo[3], const double hi[3], double min_fea
     const float l = std::ceil(std::fmax(0.0f, logf(static_cast<float>(md / min_feature))) /
                               logf(2.0f));
     return static_cast<int>(l);
+}
+
+bool debug_levels()
+{
+    static int on = -1;
+    if (on < 0) {
+        const char* e = std::getenv("LFB_DEBUG_LEVELS");
+        on = (e && e[0] == '1') ? 1 : 0;
+    }
+    return on == 1;
 }
 
 template <class T>
@@ -1274,22 +1552,30 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
     if (!status || !counters) return LFB_E_CUDA;
     cudaMemsetAsync(status, 0, sizeof(uint32_t), s);
     cudaMemsetAsync(counters, 0, 8 * sizeof(unsigned long long), s);
-    uint32_t* arena_top = reinterpret_cast<uint32_t*>(counters + 1);
+    unsigned long long* arena_top = counters + 1;
     uint32_t* rec_top = reinterpret_cast<uint32_t*>(counters + 2);
     unsigned long long* evals = counters + 3;
+    unsigned long long* list_top = counters + 5;
+    if (!g.ensure_wide()) return LFB_E_UNSUPPORTED;
 
-    // Tape arena: the unpruned tape first, pruned tapes appended.
-    size_t arena_cap = std::max<size_t>(bt.n * 64 + (1u << 20), 1u << 22);
-    RegClause* arena = ws.get<RegClause>(K_ARENA, arena_cap);
+    // Register-tape arena: the unpruned tape first, pruned tapes appended
+    // (every depth's tapes stay: the collapse pass evaluates points with
+    // them).  It keeps its size from call to call.
+    auto cap_of = [&](int key, size_t elem) {
+        return static_cast<uint64_t>(ws.bufs[key].bytes / elem);
+    };
+    RegClause* arena = ws.get<RegClause>(
+        K_ARENA, std::max<uint64_t>(cap_of(K_ARENA, sizeof(RegClause)),
+                                    std::max<size_t>(bt.n * 64 + (1u << 20), 1u << 22)));
     if (!arena) return LFB_E_CUDA;
+    uint64_t arena_cap = cap_of(K_ARENA, sizeof(RegClause));
     if (bt.n && !cuda_ok(cudaMemcpyAsync(arena, bt.clauses, bt.n * sizeof(RegClause),
                                          cudaMemcpyDeviceToDevice, s), "arena")) {
         return LFB_E_CUDA;
     }
-    uint32_t top_host = bt.n;
-    cudaMemcpyAsync(arena_top, &top_host, sizeof(uint32_t), cudaMemcpyHostToDevice, s);
+    unsigned long long top_host = bt.n;
+    cudaMemcpyAsync(arena_top, &top_host, sizeof(top_host), cudaMemcpyHostToDevice, s);
 
-    // Level 0: the root cell.
     auto alloc_level = [&](int d, uint32_t n_cells, uint32_t n_groups) -> bool {
         LevelView& lv = o.lv[d];
         lv.n_cells = n_cells;
@@ -1302,14 +1588,16 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
         lv.cell_tape = ws.get<TapeRef>(k + 4, n_cells);
         lv.group_parent = ws.get<uint32_t>(k + 5, n_groups);
         lv.group_tape = ws.get<TapeRef>(k + 6, n_groups);
-        lv.group_dec = ws.get<uint64_t>(k + 7, n_groups);
+        lv.cell_list = ws.get<ListRef>(k + 7, n_cells);
+        lv.group_list = ws.get<ListRef>(k + 8, n_groups);
         if (!lv.coords || !lv.type || !lv.rec || !lv.child_group || !lv.cell_tape ||
-            !lv.group_parent || !lv.group_tape || !lv.group_dec) {
+            !lv.group_parent || !lv.group_tape || !lv.cell_list || !lv.group_list) {
             return false;
         }
         cudaMemsetAsync(lv.rec, 0xff, n_cells * sizeof(int32_t), s);
         return true;
     };
+    // Level 0: the root cell.
     if (!alloc_level(0, 1, 0)) return LFB_E_CUDA;
     k_init_root<<<1, 1, 0, s>>>(o);
     if (L == 0) {
@@ -1326,62 +1614,122 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
     }
     uint64_t n_launch = 1;   // k_init_root
     uint64_t cells_evaluated = 0;
-    uint64_t dec_total = bt.n_choices;   // decision bytes needed by level 0
+
+    // Per-warp global scratch of the interval kernel (see WideArgs).
+    const uint64_t n = bt.n;
+    const uint64_t nw16 = (n + 15) / 16;
+    const uint64_t nw1 = (nw16 + 31) / 32;
+    const uint64_t per_warp = 9 * (n + 3) + 6 * n + 8 * nw16 + 4 * nw1;
+    const uint64_t max_warps = static_cast<uint64_t>(device_sm_count()) * 32;
+    const uint64_t budget_warps = std::max<uint64_t>(8, (768ull << 20) / std::max<uint64_t>(per_warp, 1));
+    const uint32_t scratch_warps =
+        static_cast<uint32_t>(std::min(max_warps, budget_warps) / 8 * 8);
+    float2* wS = ws.get<float2>(K_WIDE_S, scratch_warps * (n + 3));
+    uint8_t* wSN = ws.get<uint8_t>(K_WIDE_SN, scratch_warps * (n + 3));
+    uint8_t* wP = ws.get<uint8_t>(K_WIDE_P, scratch_warps * n);
+    uint8_t* wLive = ws.get<uint8_t>(K_WIDE_LIVE, scratch_warps * n);
+    uint32_t* wNew = ws.get<uint32_t>(K_WIDE_NEW, scratch_warps * n);
+    uint32_t* wSt2 = ws.get<uint32_t>(K_WIDE_ST2, scratch_warps * nw16);
+    uint32_t* wL1 = ws.get<uint32_t>(K_WIDE_L1, scratch_warps * nw1);
+    uint32_t* wWl = ws.get<uint32_t>(K_WIDE_WL, scratch_warps * nw16);
+    if (!wS || !wSN || !wP || !wLive || !wNew || !wSt2 || !wL1 || !wWl) return LFB_E_CUDA;
+    if (L > 0) {
+        cudaMemsetAsync(wSt2, 0, scratch_warps * nw16 * 4, s);
+        cudaMemsetAsync(wL1, 0, scratch_warps * nw1 * 4, s);
+    }
+    const size_t wide_smem = sizeof(WideSmem) * 8;
+    cudaFuncSetAttribute(k_interval_wide, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(wide_smem));
+    // Two list arenas, one per parity of depth: depth d reads the lists of
+    // its groups from one and writes its children's lists to the other.
+    const int list_key[2] = {K_LIST_A, K_LIST_B};
+    for (int k = 0; k < 2; ++k) {
+        if (!ws.get<WideEntry>(list_key[k], std::max<uint64_t>(cap_of(list_key[k], sizeof(WideEntry)),
+                                                                4 * n + 1024))) {
+            return LFB_E_CUDA;
+        }
+    }
+
     for (int d = 0; d < L; ++d) {
         LevelView& lv = o.lv[d];
         cells_evaluated += lv.n_cells;
-        uint8_t* dec = ws.get<uint8_t>(K_DEC, std::max<uint64_t>(dec_total, 1));
-        if (!dec) return LFB_E_CUDA;
-        // Arena: worst case every cell writes a tape as long as its input.
-        uint64_t need = 0;
-        {
-            // Upper bound: n_cells * (longest group tape) is cheap to get as
-            // dec_total/choices is not a length; use the running input size.
-            need = static_cast<uint64_t>(lv.n_cells) * std::max<uint32_t>(bt.n, 1);
-        }
-        (void)need;
-        int block = 128;
-        while (block > 32 && static_cast<size_t>(bt.n_regs) * block * 9 > 96 * 1024) block /= 2;
-        const size_t smem = static_cast<size_t>(bt.n_regs) * block * 9 + 16;
-        if (smem > 48 * 1024) {
-            cudaFuncSetAttribute(k_interval_level, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem));
-        }
-        for (int attempt = 0; attempt < 6; ++attempt) {
-            const uint32_t saved_top_dummy = 0;
-            (void)saved_top_dummy;
-            uint32_t top_before = 0;
-            cudaMemcpyAsync(&top_before, arena_top, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
-            cudaStreamSynchronize(s);
-            k_interval_level<<<(lv.n_cells + block - 1) / block, block, smem, s>>>(
-                o, d, bt, arena, arena_top, static_cast<uint32_t>(arena_cap), dec, status);
+        const bool write_lists = d + 1 < L;
+        const int out_key = list_key[(d + 1) & 1];
+        const auto t_level = std::chrono::steady_clock::now();
+        unsigned long long arena_before = 0;
+        cudaMemcpyAsync(&arena_before, arena_top, sizeof(arena_before), cudaMemcpyDeviceToHost, s);
+        if (!cuda_ok(cudaStreamSynchronize(s), "interval stage")) return LFB_E_CUDA;
+        for (int attempt = 0; attempt < 4; ++attempt) {
+            WideArgs W;
+            W.o = o;
+            W.bt = bt;
+            W.n = bt.n;
+            W.in_lists = d == 0 ? g.d_wide : ws.bufs[list_key[d & 1]].as<WideEntry>();
+            W.root_list = {0u, bt.n, g.wide_root, 0u};
+            W.out_lists = ws.bufs[out_key].as<WideEntry>();
+            W.out_top = list_top;
+            W.out_cap = cap_of(out_key, sizeof(WideEntry));
+            W.write_lists = write_lists ? 1 : 0;
+            W.arena = arena;
+            W.arena_top = arena_top;
+            W.arena_cap = arena_cap;
+            W.S = wS;
+            W.SN = wSN;
+            W.pst = wP;
+            W.live = wLive;
+            W.newpos = wNew;
+            W.st2 = wSt2;
+            W.l1 = wL1;
+            W.wl = wWl;
+            W.status = status;
+            cudaMemsetAsync(list_top, 0, sizeof(unsigned long long), s);
+            const uint32_t warps = std::min<uint32_t>(scratch_warps, (lv.n_cells + 7) / 8 * 8);
+            k_interval_wide<<<warps / 8, 256, wide_smem, s>>>(W, d);
             ++n_launch;
             if (!cuda_ok(cudaGetLastError(), "interval kernel")) return LFB_E_CUDA;
             uint32_t st = 0;
+            unsigned long long tops[2] = {0, 0};
             cudaMemcpyAsync(&st, status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+            cudaMemcpyAsync(&tops[0], arena_top, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
+            cudaMemcpyAsync(&tops[1], list_top, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
             if (!cuda_ok(cudaStreamSynchronize(s), "interval kernel")) return LFB_E_CUDA;
-            if (!(st & ST_ARENA_OVERFLOW)) break;
-            // Grow the arena (keeping its contents) and redo this level.
-            const size_t new_cap = arena_cap * 4;
-            RegClause* bigger = nullptr;
-            if (!cuda_ok(cudaMalloc(&bigger, new_cap * sizeof(RegClause)), "arena grow")) {
-                return LFB_E_CUDA;
+            if (!(st & (ST_ARENA_OVERFLOW | ST_LIST_OVERFLOW))) break;
+            if (attempt == 3) return set_error(LFB_E_CAPACITY, "tape arena overflow");
+            // The counters kept counting past the capacity: grow to what this
+            // depth needs and run it again.
+            if (st & ST_LIST_OVERFLOW) {
+                // The output arena holds nothing yet: no copy needed.
+                if (!ws.get<WideEntry>(out_key, tops[1] + tops[1] / 4 + 1024)) return LFB_E_CUDA;
             }
-            cudaMemcpyAsync(bigger, arena, static_cast<size_t>(top_before) * sizeof(RegClause),
-                            cudaMemcpyDeviceToDevice, s);
-            DevBuf& b = ws.bufs[K_ARENA];
-            cudaStreamSynchronize(s);
-            cudaFree(b.ptr);
-            b.ptr = bigger;
-            b.bytes = new_cap * sizeof(RegClause);
-            arena = bigger;
-            arena_cap = new_cap;
-            cudaMemcpyAsync(arena_top, &top_before, sizeof(uint32_t), cudaMemcpyHostToDevice, s);
-            const uint32_t zero = 0;
-            cudaMemcpyAsync(status, &zero, sizeof(uint32_t), cudaMemcpyHostToDevice, s);
-            if (attempt == 5) return set_error(LFB_E_CAPACITY, "tape arena overflow");
+            if (st & ST_ARENA_OVERFLOW) {
+                const uint64_t new_cap = tops[0] + tops[0] / 4 + (1u << 20);
+                RegClause* bigger = nullptr;
+                if (!cuda_ok(cudaMalloc(&bigger, new_cap * sizeof(RegClause)), "arena grow")) {
+                    return LFB_E_CUDA;
+                }
+                cudaMemcpyAsync(bigger, arena, arena_before * sizeof(RegClause),
+                                cudaMemcpyDeviceToDevice, s);
+                DevBuf& b = ws.bufs[K_ARENA];
+                cudaStreamSynchronize(s);
+                cudaFree(b.ptr);
+                b.ptr = bigger;
+                b.bytes = new_cap * sizeof(RegClause);
+                arena = bigger;
+                arena_cap = new_cap;
+            }
+            cudaMemcpyAsync(arena_top, &arena_before, sizeof(arena_before), cudaMemcpyHostToDevice, s);
+            cudaMemsetAsync(status, 0, sizeof(uint32_t), s);
         }
 
+        if (debug_levels()) {
+            unsigned long long top_now = 0, lt = 0;
+            cudaMemcpy(&top_now, arena_top, sizeof(top_now), cudaMemcpyDeviceToHost);
+            cudaMemcpy(&lt, list_top, sizeof(lt), cudaMemcpyDeviceToHost);
+            const double ms = std::chrono::duration<double, std::milli>(
+                std::chrono::steady_clock::now() - t_level).count();
+            std::fprintf(stderr, "[lfb] depth %d: %u cells, arena %llu clauses, lists %llu, %.3f ms\n",
+                         d, lv.n_cells, top_now, lt, ms);
+        }
         // Compact the branch cells into the groups of depth d + 1.
         uint32_t* flags = ws.get<uint32_t>(K_FLAGS, lv.n_cells + 1);
         uint32_t* scan = ws.get<uint32_t>(K_SCAN, lv.n_cells + 1);
@@ -1396,20 +1744,8 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
             return set_error(LFB_E_CAPACITY, "more than 2^27 cells on one octree level");
         }
         if (!alloc_level(d + 1, n_groups * 8, n_groups)) return LFB_E_CUDA;
-        uint64_t* dec_sizes = ws.get<uint64_t>(K_DECSZ, n_groups + 1);
-        if (!dec_sizes) return LFB_E_CUDA;
-        k_build_groups<<<(lv.n_cells + 255) / 256, 256, 0, s>>>(o, d, scan, dec_sizes);
+        k_build_groups<<<(lv.n_cells + 255) / 256, 256, 0, s>>>(o, d, scan);
         n_launch += 2;   // k_branch_flags + k_build_groups
-        cudaMemsetAsync(dec_sizes + n_groups, 0, sizeof(uint64_t), s);
-        if (!exclusive_scan(dec_sizes, o.lv[d + 1].group_dec, n_groups, s)) return LFB_E_CUDA;
-        // total decision bytes of the next level
-        uint64_t last_off = 0, last_sz = 0;
-        if (n_groups) {
-            cudaMemcpyAsync(&last_off, o.lv[d + 1].group_dec + n_groups - 1, 8, cudaMemcpyDeviceToHost, s);
-            cudaMemcpyAsync(&last_sz, dec_sizes + n_groups - 1, 8, cudaMemcpyDeviceToHost, s);
-        }
-        if (!cuda_ok(cudaStreamSynchronize(s), "groups")) return LFB_E_CUDA;
-        dec_total = last_off + last_sz;
         if (n_groups == 0) {
             // Nothing ambiguous below this depth: no leaves, no faces.
             o.levels = L;
@@ -1427,18 +1763,26 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
     LeafRec* recs = ws.get<LeafRec>(K_RECS, rec_cap);
     if (!recs) return LFB_E_CUDA;
     if (n_leaf_groups) {
-        LeafArgs A{o, bt, arena, recs, rec_top, static_cast<uint32_t>(rec_cap), status,
-                   evals};
-        int wpb = 4;
-        const size_t per_warp = sizeof(LeafWarpShared) + static_cast<size_t>(bt.n_regs) * 128 * 4;
-        while (wpb > 1 && per_warp * wpb > 200 * 1024) --wpb;
+        // Shared memory per warp: the register file (n_regs x 4 floats x 32
+        // lanes, reused by the feature evaluator) and the small lattice state.
+        const int wpb = 8;
+        const size_t per_warp = kLeafSmallBytes + static_cast<size_t>(bt.n_regs) * 128 * 4;
         const size_t smem = per_warp * wpb;
         if (smem > 220 * 1024) {
             return set_error(LFB_E_UNSUPPORTED, "tape register file too large for the leaf kernel");
         }
         cudaFuncSetAttribute(k_leaf_groups, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(smem));
-        k_leaf_groups<<<(n_leaf_groups + wpb - 1) / wpb, 32 * wpb, smem, s>>>(A, n_leaf_groups);
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_leaf_groups, 32 * wpb, smem);
+        per_sm = std::max(per_sm, 1);
+        const uint32_t want = (n_leaf_groups + wpb - 1) / wpb;
+        const uint32_t grid = std::min<uint32_t>(want, static_cast<uint32_t>(device_sm_count() * per_sm));
+        LeafWarpScratch* scratch = ws.get<LeafWarpScratch>(K_FEAT, static_cast<size_t>(grid) * wpb);
+        if (!scratch) return LFB_E_CUDA;
+        LeafArgs A{o, bt, arena, recs, rec_top, static_cast<uint32_t>(rec_cap), status,
+                   evals, scratch};
+        k_leaf_groups<<<grid, 32 * wpb, smem, s>>>(A, n_leaf_groups);
         if (!cuda_ok(cudaGetLastError(), "leaf kernel")) return LFB_E_CUDA;
         ++n_launch;
     }

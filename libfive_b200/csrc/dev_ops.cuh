@@ -27,15 +27,11 @@ namespace lfb {
 ////////////////////////////////////////////////////////////////////////////////
 // Value mode
 
-__device__ __forceinline__ float dv_value(uint8_t o, float a, float b)
+/// Opcodes that call a math-library function or have long bodies; kept out
+/// of line so that the interpreters' hot switch stays small.
+static __device__ __noinline__ float dv_value_rare(uint8_t o, float a, float b)
 {
     switch (o) {
-        case op::ADD: return __fadd_rn(a, b);
-        case op::MUL: return __fmul_rn(a, b);
-        case op::MIN: return sc_min(a, b);
-        case op::MAX: return sc_max(a, b);
-        case op::SUB: return __fsub_rn(a, b);
-        case op::DIV: return __fdiv_rn(a, b);
         case op::ATAN2: return atan2f(a, b);
         case op::POW: return powf(a, b);
         case op::NTH_ROOT: return sc_nth_root(a, b);
@@ -49,22 +45,35 @@ __device__ __forceinline__ float dv_value(uint8_t o, float a, float b)
         }
         case op::NANFILL: return (a != a) ? b : a;
         case op::COMPARE: return sc_compare(a, b);
-        case op::SQUARE: return __fmul_rn(a, a);
-        case op::SQRT: return __fsqrt_rn(a);
-        case op::NEG: return -a;
         case op::SIN: return sinf(a);
         case op::COS: return cosf(a);
         case op::TAN: return tanf(a);
         case op::ASIN: return asinf(a);
         case op::ACOS: return acosf(a);
         case op::ATAN: return atanf(a);
+        default: return __int_as_float(0x7fc00000);
+    }
+}
+
+__device__ __forceinline__ float dv_value(uint8_t o, float a, float b)
+{
+    switch (o) {
+        case op::ADD: return __fadd_rn(a, b);
+        case op::MUL: return __fmul_rn(a, b);
+        case op::MIN: return sc_min(a, b);
+        case op::MAX: return sc_max(a, b);
+        case op::SUB: return __fsub_rn(a, b);
+        case op::DIV: return __fdiv_rn(a, b);
+        case op::SQUARE: return __fmul_rn(a, a);
+        case op::SQRT: return __fsqrt_rn(a);
+        case op::NEG: return -a;
         case op::LOG: return logf(a);
         case op::EXP: return expf(a);
         case op::ABS: return fabsf(a);
         case op::RECIP: return __fdiv_rn(1.0f, a);
         case op::CONST_VAR: return a;
         case OP_COPY: return a;
-        default: return __int_as_float(0x7fc00000);
+        default: return dv_value_rare(o, a, b);
     }
 }
 
@@ -82,8 +91,8 @@ __device__ __forceinline__ D4 d4_scale(float v, const D4& a, float f)
     return {v, __fmul_rn(a.dx, f), __fmul_rn(a.dy, f), __fmul_rn(a.dz, f)};
 }
 
-__device__ __forceinline__ D4 dv_deriv(uint8_t o, const D4& a, const D4& b,
-                                       bool clear_vars)
+static __device__ __noinline__ D4 dv_deriv_all(uint8_t o, const D4& a, const D4& b,
+                                               bool clear_vars)
 {
     const float av = a.v, bv = b.v;
     const float ov = dv_value(o, av, bv);
@@ -196,6 +205,45 @@ __device__ __forceinline__ D4 dv_deriv(uint8_t o, const D4& a, const D4& b,
             return a;
         default:
             return {__int_as_float(0x7fc00000), 0.0f, 0.0f, 0.0f};
+    }
+}
+
+/// Hot-path derivative rules inline; everything else out of line.
+__device__ __forceinline__ D4 dv_deriv(uint8_t o, const D4& a, const D4& b,
+                                       bool clear_vars)
+{
+    const float av = a.v, bv = b.v;
+    switch (o) {
+        case op::ADD:
+            return {__fadd_rn(av, bv), __fadd_rn(a.dx, b.dx), __fadd_rn(a.dy, b.dy),
+                    __fadd_rn(a.dz, b.dz)};
+        case op::SUB:
+            return {__fsub_rn(av, bv), __fsub_rn(a.dx, b.dx), __fsub_rn(a.dy, b.dy),
+                    __fsub_rn(a.dz, b.dz)};
+        case op::MUL:
+            return {__fmul_rn(av, bv),
+                    __fadd_rn(__fmul_rn(b.dx, av), __fmul_rn(a.dx, bv)),
+                    __fadd_rn(__fmul_rn(b.dy, av), __fmul_rn(a.dy, bv)),
+                    __fadd_rn(__fmul_rn(b.dz, av), __fmul_rn(a.dz, bv))};
+        case op::MIN:
+            return (av < bv) ? D4{sc_min(av, bv), a.dx, a.dy, a.dz}
+                             : D4{sc_min(av, bv), b.dx, b.dy, b.dz};
+        case op::MAX:
+            return (av < bv) ? D4{sc_max(av, bv), b.dx, b.dy, b.dz}
+                             : D4{sc_max(av, bv), a.dx, a.dy, a.dz};
+        case op::SQUARE:
+            return {__fmul_rn(av, av), __fmul_rn(__fmul_rn(a.dx, av), 2.0f),
+                    __fmul_rn(__fmul_rn(a.dy, av), 2.0f),
+                    __fmul_rn(__fmul_rn(a.dz, av), 2.0f)};
+        case op::NEG:
+            return {-av, -a.dx, -a.dy, -a.dz};
+        case op::ABS:
+            return (av > 0) ? D4{fabsf(av), a.dx, a.dy, a.dz}
+                            : D4{fabsf(av), -a.dx, -a.dy, -a.dz};
+        case OP_COPY:
+            return a;
+        default:
+            return dv_deriv_all(o, a, b, clear_vars);
     }
 }
 

@@ -71,6 +71,28 @@ GpuTape::~GpuTape()
 {
     if (d_clauses) cudaFree(d_clauses);
     if (d_cpool) cudaFree(d_cpool);
+    if (d_wide) cudaFree(d_wide);
+}
+
+bool GpuTape::ensure_wide()
+{
+    std::lock_guard<std::mutex> lock(mu);
+    if (wide_ready) return true;
+    std::vector<WideEntry> w;
+    std::string err;
+    if (!build_wide_list(reg, w, wide_root, &err)) {
+        set_error(LFB_E_UNSUPPORTED, err);
+        return false;
+    }
+    const size_t bytes = std::max<size_t>(w.size(), 1) * sizeof(WideEntry);
+    if (!cuda_ok(cudaMalloc(&d_wide, bytes), "level-ordered tape alloc")) return false;
+    if (!w.empty() &&
+        !cuda_ok(cudaMemcpy(d_wide, w.data(), w.size() * sizeof(WideEntry),
+                            cudaMemcpyHostToDevice), "level-ordered tape upload")) {
+        return false;
+    }
+    wide_ready = true;
+    return true;
 }
 
 DevTape GpuTape::dev() const

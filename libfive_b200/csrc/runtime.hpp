@@ -33,7 +33,14 @@ struct GpuTape {
     RegTape reg;
     RegClause* d_clauses = nullptr;
     float* d_cpool = nullptr;
-    std::mutex mu;   // guards cpool updates
+    std::mutex mu;   // guards cpool updates and the level-ordered copy
+
+    // Level-ordered copy of the tape for the mesher's interval stage, built
+    // on first use (build_wide_list).
+    WideEntry* d_wide = nullptr;
+    uint32_t wide_root = 0;
+    bool wide_ready = false;
+    bool ensure_wide();
 
     ~GpuTape();
     DevTape dev() const;

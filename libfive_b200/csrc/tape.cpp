@@ -179,4 +179,59 @@ bool build_reg_tape(const SlotTape& st, RegTape& out, std::string* err)
     return true;
 }
 
+bool build_wide_list(const RegTape& t, std::vector<WideEntry>& out,
+                     uint32_t& root_slot, std::string* err)
+{
+    const size_t n = t.clauses.size();
+    // Register -> slot of the value it holds, walking the tape in order.
+    std::vector<uint32_t> slot_of(std::max<uint32_t>(t.n_regs, 3), 0);
+    for (uint32_t r = 0; r < 3; ++r) slot_of[r] = r;
+    std::vector<uint32_t> level(n + 3, 0);
+    std::vector<WideEntry> tmp(n);
+    uint32_t max_level = 0;
+    for (size_t c = 0; c < n; ++c) {
+        const RegClause& rc = t.clauses[c];
+        const uint8_t ka = rc.kinds & 3, kb = (rc.kinds >> 2) & 3;
+        const bool binary = op::arity(rc.op) == 2;
+        WideEntry e{};
+        e.a = ka == OPND_REG ? slot_of[rc.a] : rc.a;
+        e.b = (binary && kb == OPND_REG) ? slot_of[rc.b] : (binary ? rc.b : 0u);
+        uint32_t lv = 0;
+        if (ka == OPND_REG) lv = std::max(lv, level[e.a]);
+        if (binary && kb == OPND_REG) lv = std::max(lv, level[e.b]);
+        ++lv;
+        if (lv > kWideMaxLevel) {
+            if (err) *err = "tape dependency chain longer than 262143 clauses";
+            return false;
+        }
+        max_level = std::max(max_level, lv);
+        const uint32_t kinds = binary ? (rc.kinds & 0xf) : (rc.kinds & 3);
+        e.head = rc.op | (kinds << 8) | (WIDE_BOTH << 12) | (lv << kWideLevelShift);
+        e.c = static_cast<uint32_t>(c);
+        level[3 + c] = lv;
+        tmp[c] = e;
+        slot_of[rc.out] = static_cast<uint32_t>(3 + c);
+    }
+    // Counting sort by level, stable in clause order; then operands and the
+    // root are renamed from clause slots to list slots.
+    std::vector<uint32_t> start(max_level + 2, 0);
+    for (size_t c = 0; c < n; ++c) ++start[level[3 + c] + 1];
+    for (uint32_t l = 1; l < start.size(); ++l) start[l] += start[l - 1];
+    std::vector<uint32_t> pos(n);
+    out.assign(n, WideEntry{});
+    for (size_t c = 0; c < n; ++c) {
+        pos[c] = start[level[3 + c]]++;
+        out[pos[c]] = tmp[c];
+    }
+    for (WideEntry& e : out) {
+        const uint32_t kinds = (e.head >> 8) & 0xf;
+        const bool binary = op::arity(e.head & 0xff) == 2;
+        if ((kinds & 3) == OPND_REG && e.a >= 3) e.a = 3 + pos[e.a - 3];
+        if (binary && ((kinds >> 2) & 3) == OPND_REG && e.b >= 3) e.b = 3 + pos[e.b - 3];
+    }
+    root_slot = t.root_kind == OPND_REG ? slot_of[t.root] : t.root;
+    if (t.root_kind == OPND_REG && root_slot >= 3) root_slot = 3 + pos[root_slot - 3];
+    return true;
+}
+
 }  // namespace lfb

@@ -80,4 +80,30 @@ bool build_slot_tape(const Tree& root, SlotTape& out, std::string* err);
 /// Derives the register-allocated device tape from a slot tape.
 bool build_reg_tape(const SlotTape& st, RegTape& out, std::string* err);
 
+/// One clause of a register tape in dependency-level form, as an entry of a
+/// list sorted by level.  Operands name value slots instead of registers:
+/// slots 0-2 hold X, Y, Z and slot 3 + k the result of the list's entry k,
+/// so the entries of one level are independent.  Constant / variable
+/// operands keep their pool index.  `head` packs op (bits 0-7), operand
+/// kinds (8-11), pruning state (12-13: WIDE_BOTH, WIDE_A = copy of operand
+/// a, WIDE_B = copy of operand b) and the level (14-31, clauses start at
+/// level 1); `c` is the clause's index in the register tape.
+struct WideEntry {
+    uint32_t head;
+    uint32_t a;
+    uint32_t b;
+    uint32_t c;
+};
+static_assert(sizeof(WideEntry) == 16, "WideEntry must pack into 16 bytes");
+
+enum : uint32_t { WIDE_BOTH = 1, WIDE_A = 2, WIDE_B = 3 };
+constexpr uint32_t kWideLevelShift = 14;
+constexpr uint32_t kWideMaxLevel = (1u << (32 - kWideLevelShift)) - 1;
+
+/// The register tape's clauses sorted by level (stable within a level), all
+/// in state WIDE_BOTH, plus the list slot (or pool index) of the root.  Fails for
+/// tapes whose dependency chain is longer than kWideMaxLevel.
+bool build_wide_list(const RegTape& t, std::vector<WideEntry>& out,
+                     uint32_t& root_slot, std::string* err);
+
 }  // namespace lfb

@@ -38,11 +38,27 @@ struct ListRef {
 };
 
 struct TapeRef {
-    uint32_t off;   // first clause in the arena
-    uint32_t len;   // clauses
-    uint32_t nch;   // min/max clauses
-    uint32_t pad;
+    uint32_t off;     // first clause in the arena
+    uint32_t len;     // clauses
+    uint32_t nregs;   // registers the tape uses (X, Y, Z included)
+    uint32_t root;    // root operand: index | kind << 16
 };
+
+__host__ __device__ inline TapeRef root_tape_ref(const DevTape& bt)
+{
+    return {0u, bt.n, bt.n_regs, static_cast<uint32_t>(bt.root) |
+                                     (static_cast<uint32_t>(bt.root_kind) << 16)};
+}
+
+/// The device tape with the register count and root of a pruned tape.
+__host__ __device__ inline DevTape with_tape(const DevTape& bt, const TapeRef& tr)
+{
+    DevTape t = bt;
+    t.n_regs = tr.nregs;
+    t.root = static_cast<uint16_t>(tr.root & 0xffff);
+    t.root_kind = static_cast<uint8_t>(tr.root >> 16);
+    return t;
+}
 
 /// Per-leaf data: DCLeaf (libfive/include/libfive/render/brep/dc/dc_tree.hpp:34-89).
 struct LeafRec {

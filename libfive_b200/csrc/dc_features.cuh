@@ -20,12 +20,23 @@ constexpr int kRegBlock = 128;       // floats per register in the workspace
 constexpr int kValOff = kMaxFeat * kFeatFloats;          // 112
 constexpr int kCountOff = kValOff + 1;                   // 113
 constexpr int kTmpFeat = 64;         // candidate features of one clause
-constexpr int kTmpCorners = 192;     // polytope corners in Feature::check
+constexpr int kTmpCorners = 168;     // plane triples in Feature::check: C(11, 3) = 165
 
-struct FeatureScratch {
+/// A Feature::check request from the evaluating lane to the whole warp.
+struct FeatCheckReq {
+    float f[kFeatFloats];
+    float e[3];
+    int op;                          // FEAT_REQ_CHECK or FEAT_REQ_DONE
+    int found1;                      // some vertex is inside
+    int found2;                      // some midpoint is inside
+};
+enum : int { FEAT_REQ_CHECK = 1, FEAT_REQ_DONE = 2 };
+
+struct __align__(16) FeatureScratch {
     float feats[kTmpFeat][kFeatFloats];
-    float corners[kTmpCorners][3];
+    float corners[kTmpCorners][3];   // one slot per plane triple
     float one[2][kFeatFloats];       // constant operands
+    FeatCheckReq req;
 };
 
 struct FeatCtx {
@@ -42,112 +53,174 @@ __device__ __forceinline__ float fdot(const float* a, const float* b)
     return (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2];
 }
 
-/// Feature::check(e, dup) (feature.cpp:100-245).
-static __device__ __noinline__ bool feat_check(const FeatCtx& C, const float* f, const float* e,
-                                  bool* dup)
+/// Feature::check(e, dup) (feature.cpp:100-245), evaluated by all 32 lanes
+/// of a warp together; every lane reads the same request and gets the same
+/// answer.  The polytope vertices (one per triple of planes, in the
+/// reference's loop order) are spread over the lanes, then the vertex and
+/// midpoint tests.  The reference skips exact-duplicate vertices; the
+/// answer ("some vertex, or some midpoint of two vertices, lies strictly
+/// inside every plane") is the same with or without them, so none are
+/// removed here.  Triples with a repeated plane have two equal columns and
+/// an exactly zero determinant, so they are not enumerated.
+///
+/// Every call passes exactly four __syncwarp barriers on every lane, early
+/// answers included, so the evaluating lane and the helpers stay paired.
+static __device__ __noinline__ bool feat_check_warp(const FeatCtx& C, bool* dup, int lane)
 {
+    FeatCheckReq* R = &C.tmp->req;
+    float f[kFeatFloats], e[3];
+    for (int i = 0; i < kFeatFloats; ++i) f[i] = R->f[i];
+    for (int i = 0; i < 3; ++i) e[i] = R->e[i];
+    __syncwarp();                                   // 1: request read
+
     const int n = static_cast<int>(f[3]);
     const float* eps = f + 4;
-    for (int i = 0; i < n; ++i) {
+    bool early = false, early_val = false;
+    for (int i = 0; i < n && !early; ++i) {
         if (static_cast<double>(fdot(e, eps + 3 * i)) > 1 - 1e-8) {
             if (dup) *dup = true;
-            return true;
+            early = true;
+            early_val = true;
         }
     }
-    if (n == 0) return true;
-    if (n == 1) return fdot(e, eps) != -1;
+    if (!early && n == 0) {
+        early = true;
+        early_val = true;
+    }
+    if (!early && n == 1) {
+        early = true;
+        early_val = fdot(e, eps) != -1;
+    }
 
     // Planes: the epsilons (d = 0) and the six faces of a unit cube (d = 1).
     float pn[kMaxEps + 1 + 6][3];
     float pd[kMaxEps + 1 + 6];
-    int np = 0;
-    for (int i = 0; i < n; ++i) {
-        pn[np][0] = eps[3 * i]; pn[np][1] = eps[3 * i + 1]; pn[np][2] = eps[3 * i + 2];
-        pd[np++] = 0.0f;
-    }
-    pn[np][0] = e[0]; pn[np][1] = e[1]; pn[np][2] = e[2];
-    pd[np++] = 0.0f;
-    const int ne = np;   // es = epsilons + e
-    const float axes[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0},
-                              {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
-    for (int k = 0; k < 6; ++k) {
-        pn[np][0] = axes[k][0]; pn[np][1] = axes[k][1]; pn[np][2] = axes[k][2];
-        pd[np++] = 1.0f;
-    }
+    int np = 0, ne = 0, nc = 0;
     float (*corners)[3] = C.tmp->corners;
-    int nc = 0;
-    for (int i = 0; i < np; ++i) {
-        for (int j = i; j < np; ++j) {
-            for (int k = j; k < np; ++k) {
-                if (pd[i] == 0.0f && pd[j] == 0.0f && pd[k] == 0.0f) continue;
-                // M = [a b c] as columns (Eigen's comma initializer)
-                float m[3][3];
-                for (int r = 0; r < 3; ++r) {
-                    m[r][0] = pn[i][r];
-                    m[r][1] = pn[j][r];
-                    m[r][2] = pn[k][r];
-                }
-                auto det3h = [&](int a, int b, int c) {
-                    const float p = m[1][b] * m[2][c];
-                    const float q = m[1][c] * m[2][b];
-                    return m[0][a] * (p - q);
-                };
-                const float det = (det3h(0, 1, 2) - det3h(1, 0, 2)) + det3h(2, 0, 1);
-                if (static_cast<double>(fabsf(det)) < 1e-6) continue;
-                auto cof = [&](int i_, int j_) {
-                    const int i1 = (i_ + 1) % 3, i2 = (i_ + 2) % 3;
-                    const int j1 = (j_ + 1) % 3, j2 = (j_ + 2) % 3;
-                    const float p = m[i1][j1] * m[i2][j2];
-                    const float q = m[i1][j2] * m[i2][j1];
-                    return p - q;
-                };
-                const float c00 = cof(0, 0), c10 = cof(1, 0), c20 = cof(2, 0);
-                const float dd = (c00 * m[0][0] + c10 * m[1][0]) + c20 * m[2][0];
-                const float inv = 1.0f / dd;
-                float mi[3][3];
-                for (int jj = 0; jj < 3; ++jj) {
-                    for (int ii = 0; ii < 3; ++ii) mi[ii][jj] = cof(jj, ii) * inv;
-                }
-                const float dv[3] = {pd[i], pd[j], pd[k]};
-                float v[3];
-                for (int r = 0; r < 3; ++r) {
-                    const float p0 = mi[r][0] * dv[0], p1 = mi[r][1] * dv[1],
-                                p2 = mi[r][2] * dv[2];
-                    v[r] = (p0 + p1) + p2;
-                }
-                bool duplicate = false;
-                for (int q = 0; q < nc; ++q) {
-                    if (corners[q][0] == v[0] && corners[q][1] == v[1] && corners[q][2] == v[2]) {
-                        duplicate = true;
-                        break;
+    auto inside_all = [&](const float* v) {
+        for (int s = 0; s < ne; ++s) {
+            if (fdot(v, pn[s]) <= 0) return false;
+        }
+        return true;
+    };
+    if (!early) {
+        for (int i = 0; i < n; ++i) {
+            pn[np][0] = eps[3 * i]; pn[np][1] = eps[3 * i + 1]; pn[np][2] = eps[3 * i + 2];
+            pd[np++] = 0.0f;
+        }
+        pn[np][0] = e[0]; pn[np][1] = e[1]; pn[np][2] = e[2];
+        pd[np++] = 0.0f;
+        ne = np;   // es = epsilons + e
+        const float axes[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0},
+                                  {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+        for (int k = 0; k < 6; ++k) {
+            pn[np][0] = axes[k][0]; pn[np][1] = axes[k][1]; pn[np][2] = axes[k][2];
+            pd[np++] = 1.0f;
+        }
+        bool found = false;
+        for (int i = 0; i < np; ++i) {
+            for (int j = i + 1; j < np; ++j) {
+                for (int k = j + 1; k < np; ++k) {
+                    if (pd[i] == 0.0f && pd[j] == 0.0f && pd[k] == 0.0f) continue;
+                    const int slot = nc++;
+                    if ((slot & 31) != lane) continue;
+                    // M = [a b c] as columns (Eigen's comma initializer)
+                    float m[3][3];
+                    for (int r = 0; r < 3; ++r) {
+                        m[r][0] = pn[i][r];
+                        m[r][1] = pn[j][r];
+                        m[r][2] = pn[k][r];
                     }
-                }
-                if (!duplicate) {
-                    if (nc >= kTmpCorners) {
-                        atomicOr(C.status, ST_FEATURE_OVERFLOW);
-                        return false;
+                    auto det3h = [&](int a, int b, int c) {
+                        const float p = m[1][b] * m[2][c];
+                        const float q = m[1][c] * m[2][b];
+                        return m[0][a] * (p - q);
+                    };
+                    const float det = (det3h(0, 1, 2) - det3h(1, 0, 2)) + det3h(2, 0, 1);
+                    if (static_cast<double>(fabsf(det)) < 1e-6) {
+                        corners[slot][0] = LF_QNAN;   // no vertex
+                        continue;
                     }
-                    corners[nc][0] = v[0]; corners[nc][1] = v[1]; corners[nc][2] = v[2];
-                    ++nc;
+                    auto cof = [&](int i_, int j_) {
+                        const int i1 = (i_ + 1) % 3, i2 = (i_ + 2) % 3;
+                        const int j1 = (j_ + 1) % 3, j2 = (j_ + 2) % 3;
+                        const float p = m[i1][j1] * m[i2][j2];
+                        const float q = m[i1][j2] * m[i2][j1];
+                        return p - q;
+                    };
+                    const float c00 = cof(0, 0), c10 = cof(1, 0), c20 = cof(2, 0);
+                    const float dd = (c00 * m[0][0] + c10 * m[1][0]) + c20 * m[2][0];
+                    const float inv = 1.0f / dd;
+                    float mi[3][3];
+                    for (int jj = 0; jj < 3; ++jj) {
+                        for (int ii = 0; ii < 3; ++ii) mi[ii][jj] = cof(jj, ii) * inv;
+                    }
+                    const float dv[3] = {pd[i], pd[j], pd[k]};
+                    float v[3];
+                    for (int r = 0; r < 3; ++r) {
+                        const float p0 = mi[r][0] * dv[0], p1 = mi[r][1] * dv[1],
+                                    p2 = mi[r][2] * dv[2];
+                        v[r] = (p0 + p1) + p2;
+                    }
+                    corners[slot][0] = v[0]; corners[slot][1] = v[1]; corners[slot][2] = v[2];
+                    found |= inside_all(v);
                 }
             }
         }
+        if (found) R->found1 = 1;
     }
-    for (int q = 0; q < nc; ++q) {
-        bool okay = true;
-        for (int s = 0; s < ne && okay; ++s) okay = fdot(corners[q], pn[s]) > 0;
-        if (okay) return true;
-    }
-    for (int q = 0; q < nc; ++q) {
-        for (int w = 0; w < nc; ++w) {
+    __syncwarp();                                   // 2: vertices written
+    const bool any1 = !early && R->found1 != 0;
+    if (!early && !any1) {
+        bool found = false;
+        for (int pq = lane; pq < nc * nc && !found; pq += 32) {
+            const int q = pq / nc, w = pq - q * nc;
+            const float* cq = corners[q];
+            const float* cw = corners[w];
+            if (cq[0] != cq[0] || cw[0] != cw[0]) continue;
             float p[3];
-            for (int r = 0; r < 3; ++r) p[r] = (corners[q][r] + corners[w][r]) / 2.0f;
-            bool okay = true;
-            for (int s = 0; s < ne && okay; ++s) okay = fdot(p, pn[s]) > 0;
-            if (okay) return true;
+            for (int r = 0; r < 3; ++r) p[r] = (cq[r] + cw[r]) / 2.0f;
+            found = inside_all(p);
         }
+        if (found) R->found2 = 1;
     }
-    return false;
+    __syncwarp();                                   // 3: midpoints tested
+    const bool any2 = R->found2 != 0;
+    __syncwarp();                                   // 4: flags read
+    return early ? early_val : (any1 || any2);
+}
+
+/// Feature::check from the evaluating lane (lane 0): posts the request and
+/// joins the other lanes, which wait in feat_serve.
+__device__ inline bool feat_check(const FeatCtx& C, const float* f, const float* e,
+                                  bool* dup)
+{
+    FeatCheckReq* R = &C.tmp->req;
+    for (int i = 0; i < kFeatFloats; ++i) R->f[i] = f[i];
+    R->e[0] = e[0]; R->e[1] = e[1]; R->e[2] = e[2];
+    R->found1 = 0;
+    R->found2 = 0;
+    R->op = FEAT_REQ_CHECK;
+    __syncwarp();
+    return feat_check_warp(C, dup, 0);
+}
+
+/// The other lanes' side of feat_check, until lane 0 posts FEAT_REQ_DONE.
+__device__ inline void feat_serve(const FeatCtx& C, int lane)
+{
+    FeatCheckReq* R = &C.tmp->req;
+    while (true) {
+        __syncwarp();
+        if (*reinterpret_cast<volatile int*>(&R->op) == FEAT_REQ_DONE) break;
+        feat_check_warp(C, nullptr, lane);
+    }
+}
+
+/// Ends lane 0's side of a warp-collective feature evaluation.
+__device__ inline void feat_done(const FeatCtx& C)
+{
+    C.tmp->req.op = FEAT_REQ_DONE;
+    __syncwarp();
 }
 
 /// Feature::push(e) (feature.cpp:50-72).
@@ -205,9 +278,39 @@ __device__ __forceinline__ bool feat_same_eps(const float* a, const float* b)
     return true;
 }
 
+/// Copies one feature (both pointers 16-byte aligned).
 __device__ __forceinline__ void feat_copy(float* dst, const float* src)
 {
-    for (int i = 0; i < kFeatFloats; ++i) dst[i] = src[i];
+    const float4* s = reinterpret_cast<const float4*>(src);
+    float4* d = reinterpret_cast<float4*>(dst);
+    const float4 a = s[0], b = s[1], c = s[2], e = s[3];
+    d[0] = a; d[1] = b; d[2] = c; d[3] = e;
+}
+
+/// One feature held in registers (all indices static after unrolling).
+struct FeatReg {
+    float v[kFeatFloats];
+};
+
+__device__ __forceinline__ FeatReg feat_get(const float* src)
+{
+    FeatReg r;
+    const float4* s = reinterpret_cast<const float4*>(src);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const float4 q = s[i];
+        r.v[4 * i] = q.x; r.v[4 * i + 1] = q.y; r.v[4 * i + 2] = q.z; r.v[4 * i + 3] = q.w;
+    }
+    return r;
+}
+
+__device__ __forceinline__ void feat_put(float* dst, const FeatReg& r)
+{
+    float4* d = reinterpret_cast<float4*>(dst);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        d[i] = make_float4(r.v[4 * i], r.v[4 * i + 1], r.v[4 * i + 2], r.v[4 * i + 3]);
+    }
 }
 
 ////////////////////////////////////////////////////////////////////////////////
@@ -261,6 +364,78 @@ static __device__ __noinline__ void feat_eval(const FeatCtx& C, const DevTape& b
             }
         }
         const float ov = dv_value(o, av, bv);
+        float* out = W + ro * kRegBlock;
+
+        // Fast paths (the result needs no sorting or merging): a min/max
+        // whose arguments differ or a copy passes one operand's list on; a
+        // clause over single features gives a single feature.  The general
+        // path below produces the same lists for these cases.
+        {
+            const float* src = nullptr;
+            int ns = 0;
+            if ((o == op::MIN || o == op::MAX) && av != bv) {
+                const bool take_a = (o == op::MIN) == (av < bv);
+                src = take_a ? fa : fb;
+                ns = take_a ? na : nb;
+            } else if (o == OP_COPY) {
+                src = fa;
+                ns = na;
+            }
+            if (src) {
+                if (src != out) {
+                    for (int i = 0; i < ns; ++i) {
+                        feat_copy(out + i * kFeatFloats, src + i * kFeatFloats);
+                    }
+                }
+                out[kValOff] = ov;
+                out[kCountOff] = static_cast<float>(ns);
+                continue;
+            }
+            if (na == 1 && (!binary || (nb == 1 && o != op::MIN && o != op::MAX))) {
+                FeatReg d = feat_get(fa);
+                const D4 r = binary ? dv_deriv(o, D4{av, d.v[0], d.v[1], d.v[2]},
+                                               D4{bv, fb[0], fb[1], fb[2]}, false)
+                                    : dv_deriv(o, D4{av, d.v[0], d.v[1], d.v[2]},
+                                               D4{0, 0, 0, 0}, false);
+                d.v[0] = r.dx; d.v[1] = r.dy; d.v[2] = r.dz;
+                if (binary && fb[3] != 0.0f) {
+                    // Merge B's epsilons, skipping exact duplicates.
+                    const FeatReg B = feat_get(fb);
+                    const int nbe = static_cast<int>(B.v[3]);
+                    int n = static_cast<int>(d.v[3]);
+#pragma unroll
+                    for (int q = 0; q < kMaxEps; ++q) {
+                        if (q >= nbe) break;
+                        const float e0 = B.v[4 + 3 * q], e1 = B.v[5 + 3 * q], e2 = B.v[6 + 3 * q];
+                        bool found = false;
+#pragma unroll
+                        for (int w = 0; w < kMaxEps; ++w) {
+                            // vcmp3(e, eps_w) == 0: no component orders either way
+                            found |= w < n && !(e0 < d.v[4 + 3 * w]) && !(e0 > d.v[4 + 3 * w]) &&
+                                     !(e1 < d.v[5 + 3 * w]) && !(e1 > d.v[5 + 3 * w]) &&
+                                     !(e2 < d.v[6 + 3 * w]) && !(e2 > d.v[6 + 3 * w]);
+                        }
+                        if (found) continue;
+                        if (n >= kMaxEps) {
+                            atomicOr(C.status, ST_FEATURE_OVERFLOW);
+                            break;
+                        }
+#pragma unroll
+                        for (int w = 0; w < kMaxEps; ++w) {
+                            if (w == n) {
+                                d.v[4 + 3 * w] = e0; d.v[5 + 3 * w] = e1; d.v[6 + 3 * w] = e2;
+                            }
+                        }
+                        ++n;
+                        d.v[3] = static_cast<float>(n);
+                    }
+                }
+                feat_put(out, d);
+                out[kValOff] = ov;
+                out[kCountOff] = 1.0f;
+                continue;
+            }
+        }
 
         int nt = 0;
         bool overflow = false;
@@ -298,17 +473,17 @@ static __device__ __noinline__ void feat_eval(const FeatCtx& C, const DevTape& b
                             if (A[3] == 0 && B[3] == 0) emit(A);
                         } else {
                             // combined = A with B's epsilons pushed
-                            float comb[kFeatFloats];
+                            __align__(16) float comb[kFeatFloats];
                             feat_copy(comb, A);
                             bool ok = true;
                             const int nbe = static_cast<int>(B[3]);
                             for (int q = 0; q < nbe && ok; ++q) ok = feat_push(C, comb, B + 4 + 3 * q);
                             if (ok) {
-                                float fa2[kFeatFloats];
+                                __align__(16) float fa2[kFeatFloats];
                                 feat_copy(fa2, comb);
                                 fa2[0] = A[0]; fa2[1] = A[1]; fa2[2] = A[2];
                                 if (feat_push(C, fa2, eps)) emit(fa2);
-                                float fb2[kFeatFloats];
+                                __align__(16) float fb2[kFeatFloats];
                                 feat_copy(fb2, comb);
                                 fb2[0] = B[0]; fb2[1] = B[1]; fb2[2] = B[2];
                                 const float neg[3] = {-eps[0], -eps[1], -eps[2]};
@@ -359,7 +534,7 @@ static __device__ __noinline__ void feat_eval(const FeatCtx& C, const DevTape& b
         // collapse to one plain feature if all gradients agree.
         if (nt > 1) {
             for (int i = 1; i < nt; ++i) {
-                float cur[kFeatFloats];
+                __align__(16) float cur[kFeatFloats];
                 feat_copy(cur, T->feats[i]);
                 int j = i - 1;
                 while (j >= 0 && feat_less(cur, T->feats[j])) {
@@ -396,7 +571,6 @@ static __device__ __noinline__ void feat_eval(const FeatCtx& C, const DevTape& b
             atomicOr(C.status, ST_FEATURE_OVERFLOW);
             if (nt > kMaxFeat) nt = kMaxFeat;
         }
-        float* out = W + ro * kRegBlock;
         for (int i = 0; i < nt; ++i) feat_copy(out + i * kFeatFloats, T->feats[i]);
         out[kValOff] = ov;
         out[kCountOff] = static_cast<float>(nt);
@@ -442,6 +616,9 @@ static __device__ __noinline__ bool dev_is_inside(const FeatCtx& C, const DevTap
             }
             inside = !(pos && !neg);
         }
+        feat_done(C);
+    } else {
+        feat_serve(C, lane);
     }
     __syncwarp();
     return __shfl_sync(0xffffffffu, inside, 0) != 0;
@@ -470,6 +647,9 @@ static __device__ __noinline__ void dev_push_features(const FeatCtx& C, const De
             qef_push(*q, pos, g, value);
             *exists = 1;
         }
+        feat_done(C);
+    } else {
+        feat_serve(C, lane);
     }
     __syncwarp();
 }

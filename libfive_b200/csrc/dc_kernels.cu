@@ -45,10 +45,14 @@ __constant__ DcTables c_tab;
 // memory, that of longer lists in a per-warp global scratch slice.
 
 constexpr uint32_t kWideSmemSlots = 512;
+constexpr uint32_t kMaxTapeRegs = 400;
+constexpr uint32_t kRenumberMax = kWideSmemSlots;   // tapes up to this length get compact registers
 
 struct WideSmem {
     float2 S[kWideSmemSlots + 3];      // slot intervals
     uint32_t newpos[kWideSmemSlots];   // entry -> position in the child list
+    uint32_t mask[(kMaxTapeRegs + 31) / 32];   // register bitmask (renumbering)
+    uint16_t regmap[kMaxTapeRegs];     // old -> new register (renumbering)
     uint8_t SN[kWideSmemSlots + 3];    // slot maybe-NaN flags
     uint8_t pst[kWideSmemSlots];       // entry state for the children
     uint8_t live[kWideSmemSlots];      // entry still needed by the children
@@ -79,6 +83,7 @@ struct WideArgs {
     uint32_t* l1;                  // [warps][nw1]  non-zero words of st2
     uint32_t* wl;                  // [warps][nw]   word list
     uint32_t* status;
+    uint32_t* next_cell;           // work counter (zero at launch)
 };
 
 __device__ __forceinline__ Iv wide_fetch(uint32_t kind, uint32_t idx,
@@ -141,30 +146,26 @@ __device__ __forceinline__ void wide_mark(const uint4& e, uint8_t ps, uint8_t* l
     }
 }
 
-/// Emitted register clauses for one 16-clause word of 2-bit states, and how
-/// many of them are undecided min/max clauses.
-__device__ __forceinline__ void wide_word_counts(uint32_t word, uint32_t w,
-                                                 const RegClause* root,
-                                                 uint32_t& emit, uint32_t& nch)
+/// Register clauses emitted for one 16-clause word of 2-bit states.
+__device__ __forceinline__ uint32_t wide_word_emits(uint32_t word, uint32_t w,
+                                                    const RegClause* root)
 {
-    emit = 0;
-    nch = 0;
+    uint32_t emit = 0;
     while (word) {
         const int j = (__ffs(word) - 1) >> 1;
         const uint32_t ps = (word >> (2 * j)) & 3;
         word &= ~(3u << (2 * j));
-        const uint2 raw = __ldg(reinterpret_cast<const uint2*>(root + w * 16 + j));
-        const uint8_t o = raw.x & 0xff;
         if (ps == WIDE_BOTH) {
             ++emit;
-            nch += (o == op::MIN || o == op::MAX);
-        } else {
-            const uint32_t kinds = (raw.x >> 8) & 0xff;
-            const uint32_t k = ps == WIDE_A ? (kinds & 3) : ((kinds >> 2) & 3);
-            const uint32_t src = ps == WIDE_A ? (raw.y & 0xffff) : (raw.y >> 16);
-            emit += !(k == OPND_REG && src == (raw.x >> 16));
+            continue;
         }
+        const uint2 raw = __ldg(reinterpret_cast<const uint2*>(root + w * 16 + j));
+        const uint32_t kinds = (raw.x >> 8) & 0xff;
+        const uint32_t k = ps == WIDE_A ? (kinds & 3) : ((kinds >> 2) & 3);
+        const uint32_t src = ps == WIDE_A ? (raw.y & 0xffff) : (raw.y >> 16);
+        emit += !(k == OPND_REG && src == (raw.x >> 16));
     }
+    return emit;
 }
 
 __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v, int lane)
@@ -176,6 +177,74 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v, int lane)
     return v;
 }
 
+/// Linear-scan register allocation of a pruned tape, in place (one thread):
+/// a backward pass marks each operand's last use, a forward pass gives every
+/// result the lowest free register.  On straight-line code this uses as many
+/// registers as values are live at once, which is at most the unpruned
+/// tape's count; the leaf kernel then fits the register file of most leaf
+/// tapes in shared memory.  Values are unchanged: only storage moves.
+static __device__ __noinline__ TapeRef renumber_tape(uint2* raw_t, TapeRef tr,
+                                                     uint8_t* lastuse,
+                                                     uint16_t* regmap,
+                                                     uint32_t* mask,
+                                                     uint32_t* status)
+{
+    const uint32_t nm = (tr.nregs + 31) / 32;
+    const uint32_t rk = tr.root >> 16, rr = tr.root & 0xffff;
+    for (uint32_t w = 0; w < nm; ++w) mask[w] = 0;   // live-after bits
+    if (rk == OPND_REG) mask[rr >> 5] |= 1u << (rr & 31);
+    for (int64_t c = static_cast<int64_t>(tr.len) - 1; c >= 0; --c) {
+        const uint2 raw = raw_t[c];
+        const uint32_t o = raw.x >> 16, kinds = (raw.x >> 8) & 0xff;
+        const uint32_t a = raw.y & 0xffff, b = raw.y >> 16;
+        mask[o >> 5] &= ~(1u << (o & 31));
+        uint8_t f = 0;
+        if ((kinds & 3) == OPND_REG) {
+            if (!(mask[a >> 5] & (1u << (a & 31)))) f |= 1;
+            mask[a >> 5] |= 1u << (a & 31);
+        }
+        if (dev_is_binary(raw.x & 0xff) && ((kinds >> 2) & 3) == OPND_REG) {
+            if (!(mask[b >> 5] & (1u << (b & 31)))) f |= 2;
+            mask[b >> 5] |= 1u << (b & 31);
+        }
+        lastuse[c] = f;
+    }
+    for (uint32_t w = 0; w < nm; ++w) mask[w] = ~0u;   // free bits
+    mask[0] &= ~7u;
+    for (uint32_t r = 0; r < 3; ++r) regmap[r] = static_cast<uint16_t>(r);
+    uint32_t hi = 3;
+    for (uint32_t c = 0; c < tr.len; ++c) {
+        uint2 raw = raw_t[c];
+        const uint32_t o = raw.x >> 16, kinds = (raw.x >> 8) & 0xff;
+        const bool binary = dev_is_binary(raw.x & 0xff);
+        uint32_t a = raw.y & 0xffff, b = raw.y >> 16;
+        const uint8_t f = lastuse[c];
+        if ((kinds & 3) == OPND_REG) a = regmap[a];
+        if (binary && ((kinds >> 2) & 3) == OPND_REG) b = regmap[b];
+        if (f & 1) mask[a >> 5] |= 1u << (a & 31);
+        if (f & 2) mask[b >> 5] |= 1u << (b & 31);
+        uint32_t r = 0xffffffffu;
+        for (uint32_t w = 0; w < nm; ++w) {
+            if (mask[w]) {
+                r = w * 32 + __ffs(mask[w]) - 1;
+                break;
+            }
+        }
+        if (r >= tr.nregs) {   // cannot happen for a tape from this pipeline
+            atomicOr(status, ST_REGS);
+            return tr;
+        }
+        mask[r >> 5] &= ~(1u << (r & 31));
+        regmap[o] = static_cast<uint16_t>(r);
+        hi = max(hi, r + 1);
+        raw.x = (raw.x & 0xffffu) | (r << 16);
+        raw.y = a | (b << 16);
+        raw_t[c] = raw;
+    }
+    const uint32_t root = rk == OPND_REG ? regmap[rr] : rr;
+    return {tr.off, tr.len, hi, root | (rk << 16)};
+}
+
 __global__ void __launch_bounds__(256)
 k_interval_wide(WideArgs A, int d)
 {
@@ -183,7 +252,6 @@ k_interval_wide(WideArgs A, int d)
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + warp;
-    const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
     WideSmem* SM = reinterpret_cast<WideSmem*>(wsm) + warp;
     const Octree& o = A.o;
     const LevelView& lv = o.lv[d];
@@ -202,12 +270,16 @@ k_interval_wide(WideArgs A, int d)
     const unsigned full = 0xffffffffu;
     const uint32_t lt_mask = (1u << lane) - 1;
 
-    for (uint32_t i = gw; i < lv.n_cells; i += nwarps) {
+    while (true) {
+        uint32_t i = 0;
+        if (lane == 0) i = atomicAdd(A.next_cell, 1u);
+        i = __shfl_sync(full, i, 0);
+        if (i >= lv.n_cells) break;
         ListRef P;
         TapeRef T;
         if (d == 0) {
             P = A.root_list;
-            T = {0u, bt.n, bt.n_choices, 0u};
+            T = root_tape_ref(bt);
         } else {
             P = lv.group_list[i >> 3];
             T = lv.group_tape[i >> 3];
@@ -369,16 +441,15 @@ k_interval_wide(WideArgs A, int d)
             nwl += __shfl_sync(full, incl, 31);
         }
         __syncwarp();
-        uint32_t emit = 0, nch = 0;
+        uint32_t emit = 0;
         for (uint32_t k0 = 0; k0 < nwl; k0 += 32) {
             const uint32_t k = k0 + lane;
-            uint32_t e_ = 0, c_ = 0;
+            uint32_t e_ = 0;
             if (k < nwl) {
                 const uint32_t w = wl[k];
-                wide_word_counts(st2[w], w, bt.clauses, e_, c_);
+                e_ = wide_word_emits(st2[w], w, bt.clauses);
             }
             emit += __reduce_add_sync(full, e_);
-            nch += __reduce_add_sync(full, c_);
         }
         unsigned long long a64 = 0;
         if (lane == 0) a64 = atomicAdd(A.arena_top, static_cast<unsigned long long>(emit));
@@ -388,11 +459,11 @@ k_interval_wide(WideArgs A, int d)
         uint32_t pos = static_cast<uint32_t>(a64);
         for (uint32_t k0 = 0; k0 < nwl; k0 += 32) {
             const uint32_t k = k0 + lane;
-            uint32_t word = 0, w = 0, e_ = 0, c_ = 0;
+            uint32_t word = 0, w = 0, e_ = 0;
             if (k < nwl) {
                 w = wl[k];
                 word = st2[w];
-                wide_word_counts(word, w, bt.clauses, e_, c_);
+                e_ = wide_word_emits(word, w, bt.clauses);
                 st2[w] = 0;
             }
             const uint32_t incl = warp_incl_scan(e_, lane);
@@ -423,9 +494,30 @@ k_interval_wide(WideArgs A, int d)
             }
             pos += __shfl_sync(full, incl, 31);
         }
+        __syncwarp();
+        TapeRef out_t = T;
+        if (aok) {
+            out_t = {static_cast<uint32_t>(a64), emit, bt.n_regs,
+                     static_cast<uint32_t>(bt.root) | (static_cast<uint32_t>(bt.root_kind) << 16)};
+            if (emit <= kRenumberMax) {
+                // Short tapes get compact registers: staged through the
+                // warp's shared slot area (free again at this point).
+                uint2* buf = reinterpret_cast<uint2*>(SM->S);
+                uint2* dst = reinterpret_cast<uint2*>(A.arena + a64);
+                for (uint32_t k = lane; k < emit; k += 32) buf[k] = dst[k];
+                __syncwarp();
+                if (lane == 0) {
+                    out_t = renumber_tape(buf, out_t, SM->live, SM->regmap, SM->mask, A.status);
+                }
+                __syncwarp();
+                for (uint32_t k = lane; k < emit; k += 32) dst[k] = buf[k];
+                out_t.nregs = __shfl_sync(full, out_t.nregs, 0);
+                out_t.root = __shfl_sync(full, out_t.root, 0);
+            }
+        }
         if (lane == 0) {
             lv.cell_list[i] = {loff, cnt, new_root, 0u};
-            lv.cell_tape[i] = aok ? TapeRef{static_cast<uint32_t>(a64), emit, nch, 0u} : T;
+            lv.cell_tape[i] = out_t;
         }
         __syncwarp();
     }
@@ -498,6 +590,62 @@ static __device__ __noinline__ float warp_value(const DevTape& bt, const RegClau
     return warp_fetch_v(bt.root_kind, bt.root, R, lane, bt.cpool);
 }
 
+/// Values of the tape at four points per lane (the edge search): register
+/// r of point k lives at R[(4 r + k) * 32 + lane].
+static __device__ __noinline__ float4 warp_value4(const DevTape& bt, const RegClause* cl,
+                                                  uint32_t len, float* R, int lane,
+                                                  float4 x, float4 y, float4 z)
+{
+    const float xs[4] = {x.x, x.y, x.z, x.w};
+    const float ys[4] = {y.x, y.y, y.z, y.w};
+    const float zs[4] = {z.x, z.y, z.z, z.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        R[(0 + k) * 32 + lane] = xs[k];
+        R[(4 + k) * 32 + lane] = ys[k];
+        R[(8 + k) * 32 + lane] = zs[k];
+    }
+    float* Rl = R + lane;
+    for (uint32_t c = 0; c < len; ++c) {
+        const uint2 raw = __ldg(reinterpret_cast<const uint2*>(cl + c));
+        const uint8_t o = raw.x & 0xff;
+        const uint32_t kinds = (raw.x >> 8) & 0xff;
+        float a[4], b[4], r[4];
+        if ((kinds & 3) == OPND_REG) {
+            const float* p = Rl + (raw.y & 0xffff) * 128;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) a[k] = p[32 * k];
+        } else {
+            const float v = __ldg(bt.cpool + (raw.y & 0xffff));
+#pragma unroll
+            for (int k = 0; k < 4; ++k) a[k] = v;
+        }
+        if (((kinds >> 2) & 3) == OPND_REG) {
+            const float* p = Rl + (raw.y >> 16) * 128;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) b[k] = p[32 * k];
+        } else {
+            const float v = __ldg(bt.cpool + (raw.y >> 16));
+#pragma unroll
+            for (int k = 0; k < 4; ++k) b[k] = v;
+        }
+        dv_value4(o, a, b, r);
+        float* q = Rl + (raw.x >> 16) * 128;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) q[32 * k] = r[k];
+    }
+    float out[4];
+    if (bt.root_kind == OPND_REG) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) out[k] = Rl[bt.root * 128 + 32 * k];
+    } else {
+        const float v = __ldg(bt.cpool + bt.root);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) out[k] = v;
+    }
+    return make_float4(out[0], out[1], out[2], out[3]);
+}
+
 __device__ __forceinline__ D4 warp_fetch_d(uint8_t kind, uint16_t idx,
                                            const float* R, int lane,
                                            const float* __restrict__ cp)
@@ -540,6 +688,7 @@ static __device__ __noinline__ D4 warp_deriv(const DevTape& bt, const RegClause*
 }
 
 constexpr size_t kLeafSmallBytes = (sizeof(LeafWarpShared) + 15) / 16 * 16;
+constexpr uint32_t kLeafSmemRegs = 16;   // shared-memory register file per warp
 
 struct LeafArgs {
     Octree o;
@@ -551,9 +700,14 @@ struct LeafArgs {
     uint32_t* status;
     unsigned long long* evals;
     LeafWarpScratch* scratch;   // gridDim.x * warps-per-block slices
+    float* rd;                  // per warp: n_regs x 4 x 32 floats (long tapes)
+    uint32_t smem_regs;         // registers of the shared-memory register file
+    uint32_t* next_group;       // work counter (zero at launch)
+    const uint32_t* order;      // processing order of the groups (or null)
+    unsigned long long* prof;   // debug: per group {cycles, feature cycles, feature calls, E}
 };
 
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
 k_leaf_groups(LeafArgs A, uint32_t n_groups)
 {
     extern __shared__ __align__(16) unsigned char lsmem[];
@@ -561,13 +715,23 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
     const int lane = threadIdx.x & 31;
     const int wpb = blockDim.x >> 5;
     LeafWarpShared* S = reinterpret_cast<LeafWarpShared*>(lsmem) + warp;
-    float* R = reinterpret_cast<float*>(lsmem + kLeafSmallBytes * wpb) +
-               static_cast<size_t>(warp) * A.bt.n_regs * 128;
+    // Register file of the tape interpreters and the feature evaluator
+    // (n_regs x 4 x 32 floats): in shared memory when the group's tape uses
+    // at most A.smem_regs registers (leaf tapes are renumbered compactly, so
+    // nearly all do), else in a per-warp slice of global memory.
+    float* Rs = reinterpret_cast<float*>(lsmem + kLeafSmallBytes * wpb) +
+                static_cast<size_t>(warp) * A.smem_regs * 128;
+    float* Rgl = A.rd + (static_cast<size_t>(blockIdx.x) * wpb + warp) * A.bt.n_regs * 128;
     LeafWarpScratch* W = A.scratch + static_cast<size_t>(blockIdx.x) * wpb + warp;
     uint64_t my_evals = 0, my_devals = 0;
-    // Persistent warps: each takes groups g, g + stride, ...
-    const uint32_t stride = gridDim.x * wpb;
-    for (uint32_t g = blockIdx.x * wpb + warp; g < n_groups; g += stride) {
+    // Persistent warps take the next group from a shared counter (group
+    // costs vary by orders of magnitude with the tape length).
+    while (true) {
+    uint32_t g = 0;
+    if (lane == 0) g = atomicAdd(A.next_group, 1u);
+    g = __shfl_sync(0xffffffffu, g, 0);
+    if (g >= n_groups) break;
+    if (A.order) g = A.order[g];
     const Octree& o = A.o;
     const int Ld = o.levels;
     const bool single = (Ld == 0);       // the root itself is the only leaf
@@ -584,7 +748,7 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
             lat[a][0] = o.lo[a];
             lat[a][1] = o.hi[a];
         }
-        tr = {0u, A.bt.n, A.bt.n_choices, 0u};
+        tr = root_tape_ref(A.bt);
         base_coords = 0;
     } else {
         const LevelView& lv = o.lv[Ld];
@@ -601,6 +765,10 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
         base_coords = pc;
     }
     const RegClause* cl = A.arena + tr.off;
+    const long long t_group = clock64();
+    unsigned long long feat_cycles = 0, feat_calls = 0;
+    const DevTape tb = with_tape(A.bt, tr);
+    float* R = tb.n_regs <= A.smem_regs ? Rs : Rgl;
     const FeatCtx fc{R, &W->fs, A.status};
 
     // --- corners (dc_tree.inl:156-239) ---------------------------------
@@ -614,7 +782,7 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
         py = static_cast<float>(lat[1][ib]);
         pz = static_cast<float>(lat[2][ic]);
     }
-    cv = warp_value(A.bt, cl, tr.len, R, lane, px, py, pz, &camb, &my_evals,
+    cv = warp_value(tb, cl, tr.len, R, lane, px, py, pz, &camb, &my_evals,
                     lane < npts);
     uint8_t cst = CELL_EMPTY;
     bool need_d = false, need_f = false;
@@ -625,7 +793,7 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
         else need_f = true;
     }
     if (__any_sync(0xffffffffu, need_d)) {
-        const D4 d = warp_deriv(A.bt, cl, tr.len, R, lane, px, py, pz, nullptr,
+        const D4 d = warp_deriv(tb, cl, tr.len, R, lane, px, py, pz, nullptr,
                                 &my_devals, need_d);
         if (need_d) {
             cst = (d.dx != 0 || d.dy != 0 || d.dz != 0) ? CELL_FILLED : CELL_EMPTY;
@@ -639,7 +807,10 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
             const float qx = __shfl_sync(0xffffffffu, px, src);
             const float qy = __shfl_sync(0xffffffffu, py, src);
             const float qz = __shfl_sync(0xffffffffu, pz, src);
-            const bool inside = dev_is_inside(fc, A.bt, cl, tr.len, qx, qy, qz, lane);
+            const long long t0 = clock64();
+            const bool inside = dev_is_inside(fc, tb, cl, tr.len, qx, qy, qz, lane);
+            feat_cycles += clock64() - t0;
+            ++feat_calls;
             if (lane == src) cst = inside ? CELL_FILLED : CELL_EMPTY;
         }
     }
@@ -737,77 +908,102 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
     const int E = S->nslots;
 
     // --- edge search: 4 rounds of 16 points (dc_tree.inl:326-410) -------
+    // One pass evaluates up to eight edges: sub-batch k of a lane holds
+    // sample j = lane & 15 of edge base + 2k + (lane >> 4).
+    auto sample = [&](int slot, int j, double q[3]) {
+        const double frac = j / (16 - 1.0);
+        const EdgeSlot& es = W->e[slot];
+        for (int k = 0; k < 3; ++k) q[k] = es.t0[k] * (1 - frac) + es.t1[k] * frac;
+    };
     for (int round = 0; round < 4; ++round) {
-        for (int base = 0; base < E; base += 2) {
-            const int slot = base + (lane >> 4);
+        for (int base = 0; base < E; base += 8) {
             const int j = lane & 15;
-            const bool active = slot < E;
-            double q[3] = {0, 0, 0};
-            if (active) {
-                const double frac = j / (16 - 1.0);
-                const EdgeSlot& es = W->e[slot];
-                for (int k = 0; k < 3; ++k) {
-                    q[k] = es.t0[k] * (1 - frac) + es.t1[k] * frac;
+            float qx[4] = {0, 0, 0, 0}, qy[4] = {0, 0, 0, 0}, qz[4] = {0, 0, 0, 0};
+            int n_act = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int slot = base + 2 * k + (lane >> 4);
+                if (slot < E) {
+                    double q[3];
+                    sample(slot, j, q);
+                    qx[k] = static_cast<float>(q[0]);
+                    qy[k] = static_cast<float>(q[1]);
+                    qz[k] = static_cast<float>(q[2]);
+                    ++n_act;
                 }
             }
-            const float v = warp_value(A.bt, cl, tr.len, R, lane,
-                                       static_cast<float>(q[0]),
-                                       static_cast<float>(q[1]),
-                                       static_cast<float>(q[2]), nullptr,
-                                       &my_evals, active);
-            // A sample exactly on the surface is resolved with
-            // FeatureEvaluator::isInside: for a point without tied min/max
-            // that is "gradient is non-zero" (one feature), otherwise the
-            // full feature search.
-            const bool zero = active && j >= 1 && v == 0;
-            bool inside = true;
-            if (__any_sync(0xffffffffu, zero)) {
-                bool amb = false;
-                const D4 dg = warp_deriv(A.bt, cl, tr.len, R, lane, static_cast<float>(q[0]),
-                                         static_cast<float>(q[1]), static_cast<float>(q[2]),
-                                         &amb, &my_devals, zero);
-                if (zero && !amb) {
-                    const float g[3] = {dg.dx, dg.dy, dg.dz};
-                    inside = sqrtf(fdot(g, g)) > 0;
-                }
-                uint32_t full = __ballot_sync(0xffffffffu, zero && amb);
-                while (full) {
-                    const int src = __ffs(full) - 1;
-                    full &= full - 1;
-                    const float zx = __shfl_sync(0xffffffffu, static_cast<float>(q[0]), src);
-                    const float zy = __shfl_sync(0xffffffffu, static_cast<float>(q[1]), src);
-                    const float zz = __shfl_sync(0xffffffffu, static_cast<float>(q[2]), src);
-                    const bool in = dev_is_inside(fc, A.bt, cl, tr.len, zx, zy, zz, lane);
-                    if (lane == src) inside = in;
-                }
-            }
-            // dc_tree.inl:372-407: the bracket ends at the first sample that
-            // is outside (value > 0, or an exact zero that is not inside);
-            // failing that, at the last sample unless it is an inside zero.
-            const uint32_t term = __ballot_sync(0xffffffffu,
-                active && j >= 1 && (v > 0 || (v == 0 && !inside)));
-            const uint32_t last_ok = __ballot_sync(0xffffffffu,
-                active && j == 15 && !(v > 0) && !(v == 0));
-            for (int h = 0; h < 2; ++h) {
-                const int s = base + h;
-                if (s >= E) break;
-                const uint32_t ht = (term >> (16 * h)) & 0xffff;
-                int pick = -1;
-                if (ht) pick = __ffs(ht) - 1;
-                else if ((last_ok >> (16 * h + 15)) & 1) pick = 15;
-                if (pick > 0) {
-                    const int lo_lane = 16 * h + pick - 1, hi_lane = 16 * h + pick;
-                    double nt0[3], nt1[3];
-                    for (int k = 0; k < 3; ++k) {
-                        nt0[k] = __shfl_sync(0xffffffffu, q[k], lo_lane);
-                        nt1[k] = __shfl_sync(0xffffffffu, q[k], hi_lane);
+            const float4 v4 = warp_value4(tb, cl, tr.len, R, lane,
+                                          make_float4(qx[0], qx[1], qx[2], qx[3]),
+                                          make_float4(qy[0], qy[1], qy[2], qy[3]),
+                                          make_float4(qz[0], qz[1], qz[2], qz[3]));
+            my_evals += static_cast<uint64_t>(__reduce_add_sync(0xffffffffu, n_act)) * tr.len;
+            const float vs[4] = {v4.x, v4.y, v4.z, v4.w};
+            for (int k = 0; k < 4; ++k) {
+                const int kbase = base + 2 * k;
+                if (kbase >= E) break;
+                const int slot = kbase + (lane >> 4);
+                const bool active = slot < E;
+                const float v = vs[k];
+                // A sample exactly on the surface is resolved with
+                // FeatureEvaluator::isInside: for a point without tied
+                // min/max that is "gradient is non-zero" (one feature),
+                // otherwise the full feature search.
+                const bool zero = active && j >= 1 && v == 0;
+                bool inside = true;
+                if (__any_sync(0xffffffffu, zero)) {
+                    bool amb = false;
+                    const D4 dg = warp_deriv(tb, cl, tr.len, R, lane, qx[k], qy[k], qz[k],
+                                             &amb, &my_devals, zero);
+                    if (zero && !amb) {
+                        const float g[3] = {dg.dx, dg.dy, dg.dz};
+                        inside = sqrtf(fdot(g, g)) > 0;
                     }
-                    if (lane == 0) {
-                        EdgeSlot& es = W->e[s];
-                        for (int k = 0; k < 3; ++k) { es.t0[k] = nt0[k]; es.t1[k] = nt1[k]; }
+                    uint32_t full = __ballot_sync(0xffffffffu, zero && amb);
+                    while (full) {
+                        const int src = __ffs(full) - 1;
+                        full &= full - 1;
+                        const float zx = __shfl_sync(0xffffffffu, qx[k], src);
+                        const float zy = __shfl_sync(0xffffffffu, qy[k], src);
+                        const float zz = __shfl_sync(0xffffffffu, qz[k], src);
+                        const long long t0 = clock64();
+                        const bool in = dev_is_inside(fc, tb, cl, tr.len, zx, zy, zz, lane);
+                        feat_cycles += clock64() - t0;
+                        ++feat_calls;
+                        if (lane == src) inside = in;
                     }
                 }
+                // dc_tree.inl:372-407: the bracket ends at the first sample
+                // that is outside (value > 0, or an exact zero that is not
+                // inside); failing that, at the last sample unless it is an
+                // inside zero.
+                const uint32_t term = __ballot_sync(0xffffffffu,
+                    active && j >= 1 && (v > 0 || (v == 0 && !inside)));
+                const uint32_t last_ok = __ballot_sync(0xffffffffu,
+                    active && j == 15 && !(v > 0) && !(v == 0));
+                double q[3] = {0, 0, 0};
+                if (active) sample(slot, j, q);
                 __syncwarp();
+                for (int h = 0; h < 2; ++h) {
+                    const int s = kbase + h;
+                    if (s >= E) break;
+                    const uint32_t ht = (term >> (16 * h)) & 0xffff;
+                    int pick = -1;
+                    if (ht) pick = __ffs(ht) - 1;
+                    else if ((last_ok >> (16 * h + 15)) & 1) pick = 15;
+                    if (pick > 0) {
+                        const int lo_lane = 16 * h + pick - 1, hi_lane = 16 * h + pick;
+                        double nt0[3], nt1[3];
+                        for (int c = 0; c < 3; ++c) {
+                            nt0[c] = __shfl_sync(0xffffffffu, q[c], lo_lane);
+                            nt1[c] = __shfl_sync(0xffffffffu, q[c], hi_lane);
+                        }
+                        if (lane == 0) {
+                            EdgeSlot& es = W->e[s];
+                            for (int c = 0; c < 3; ++c) { es.t0[c] = nt0[c]; es.t1[c] = nt1[c]; }
+                        }
+                    }
+                    __syncwarp();
+                }
             }
         }
     }
@@ -822,7 +1018,7 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
             for (int k = 0; k < 3; ++k) q[k] = (p & 1) ? es.t1[k] : es.t0[k];
         }
         bool amb = false;
-        const D4 d = warp_deriv(A.bt, cl, tr.len, R, lane, static_cast<float>(q[0]),
+        const D4 d = warp_deriv(tb, cl, tr.len, R, lane, static_cast<float>(q[0]),
                                 static_cast<float>(q[1]), static_cast<float>(q[2]),
                                 &amb, &my_devals, active);
         if (active) {
@@ -859,9 +1055,12 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
                 const float* g = side ? es.g1 : es.g0;
                 const double* pos = side ? es.t1 : es.t0;
                 if (es.amb[side]) {
-                    dev_push_features(fc, A.bt, cl, tr.len, pos,
+                    const long long t0 = clock64();
+                    dev_push_features(fc, tb, cl, tr.len, pos,
                                       static_cast<double>(g[3]), &es.q,
                                       &es.exists, lane);
+                    feat_cycles += clock64() - t0;
+                    ++feat_calls;
                 } else if (lane == 0) {
                     const double gd[3] = {g[0], g[1], g[2]};
                     qef_push(es.q, pos, gd, static_cast<double>(g[3]));
@@ -940,6 +1139,12 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
         }
     }
     (void)base_coords;
+    if (A.prof && lane == 0) {
+        A.prof[4 * g + 0] = clock64() - t_group;
+        A.prof[4 * g + 1] = feat_cycles;
+        A.prof[4 * g + 2] = feat_calls;
+        A.prof[4 * g + 3] = E;
+    }
     }   // groups
     if (lane == 0) {
         atomicAdd(A.evals, static_cast<unsigned long long>(my_evals));
@@ -1093,7 +1298,7 @@ k_collapse_level(CollapseArgs A, int d)
     // (Tape::getBase, tape.cpp:188-209); the unpruned tape otherwise.
     const float vf[3] = {static_cast<float>(v[0]), static_cast<float>(v[1]),
                          static_cast<float>(v[2])};
-    TapeRef tr = {0u, A.bt.n, A.bt.n_choices, 0u};
+    TapeRef tr = root_tape_ref(A.bt);
     {
         int dd = d;
         uint32_t ii = i;
@@ -1114,7 +1319,7 @@ k_collapse_level(CollapseArgs A, int d)
             --dd;
         }
     }
-    const float value = thread_value(A.bt, A.arena + tr.off, tr.len, csmem, tid, B,
+    const float value = thread_value(with_tape(A.bt, tr), A.arena + tr.off, tr.len, csmem, tid, B,
                                      vf[0], vf[1], vf[2]);
     if (!(fabsf(value) < A.max_err)) return;
 
@@ -1376,6 +1581,17 @@ k_dual_round(DualArgs A, const DualTask* in, uint32_t n_in)
 ////////////////////////////////////////////////////////////////////////////////
 // Small helpers for the host driver
 
+/// Sort keys for the leaf groups: tape length (longest first), so that the
+/// persistent leaf kernel starts the expensive groups early.
+__global__ void k_leaf_order_keys(const TapeRef* group_tape, uint32_t n,
+                                  uint32_t* keys, uint32_t* vals)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    keys[i] = group_tape[i].len;
+    vals[i] = i;
+}
+
 __global__ void k_init_root(Octree o)
 {
     o.lv[0].coords[0] = 0;
@@ -1443,6 +1659,7 @@ __global__ void k_remap_tris(uint32_t* tris, uint32_t n, const uint32_t* scan)
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <map>
 #include <vector>
 
@@ -1474,7 +1691,8 @@ enum BufKey {
     K_ARENA = 1, K_STATUS, K_COUNTERS, K_RECS, K_FLAGS, K_SCAN,
     K_CUBTMP, K_TASK_A, K_TASK_B, K_TRIS, K_USED, K_VSCAN, K_VERTS, K_FEAT,
     K_LIST_A, K_LIST_B, K_WIDE_S, K_WIDE_SN, K_WIDE_P, K_WIDE_LIVE, K_WIDE_NEW,
-    K_WIDE_ST2, K_WIDE_L1, K_WIDE_WL,
+    K_WIDE_ST2, K_WIDE_L1, K_WIDE_WL, K_LEAF_RD, K_ORDER_K0, K_ORDER_K1,
+    K_ORDER_V0, K_ORDER_V1, K_SORTTMP, K_PROF,
     K_LEVEL = 100,
 };
 
@@ -1682,6 +1900,8 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
             W.l1 = wL1;
             W.wl = wWl;
             W.status = status;
+            W.next_cell = reinterpret_cast<uint32_t*>(counters + 6);
+            cudaMemsetAsync(W.next_cell, 0, sizeof(uint32_t), s);
             cudaMemsetAsync(list_top, 0, sizeof(unsigned long long), s);
             const uint32_t warps = std::min<uint32_t>(scratch_warps, (lv.n_cells + 7) / 8 * 8);
             k_interval_wide<<<warps / 8, 256, wide_smem, s>>>(W, d);
@@ -1763,10 +1983,37 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
     LeafRec* recs = ws.get<LeafRec>(K_RECS, rec_cap);
     if (!recs) return LFB_E_CUDA;
     if (n_leaf_groups) {
-        // Shared memory per warp: the register file (n_regs x 4 floats x 32
-        // lanes, reused by the feature evaluator) and the small lattice state.
+        // Shared memory per warp: the small lattice state and a register
+        // file of smem_regs x 4 x 32 floats; groups whose tape needs more
+        // registers use global memory instead.
         const int wpb = 8;
-        const size_t per_warp = kLeafSmallBytes + static_cast<size_t>(bt.n_regs) * 128 * 4;
+        const uint32_t smem_regs = std::min<uint32_t>(bt.n_regs, kLeafSmemRegs);
+        if (debug_levels() && L > 0) {
+            std::vector<TapeRef> gt(n_leaf_groups);
+            cudaMemcpy(gt.data(), o.lv[L].group_tape, n_leaf_groups * sizeof(TapeRef),
+                       cudaMemcpyDeviceToHost);
+            std::map<uint32_t, uint64_t> hist, lhist;
+            uint64_t len_sum = 0;
+            for (const TapeRef& t : gt) {
+                ++hist[t.nregs];
+                len_sum += t.len;
+                uint32_t b = 0;
+                while ((1u << (b + 1)) <= t.len) ++b;
+                lhist[b] += t.len;
+            }
+            std::fprintf(stderr, "[lfb] leaf tape clauses by log2(length):");
+            for (const auto& h : lhist) {
+                std::fprintf(stderr, " %u:%llu", h.first, static_cast<unsigned long long>(h.second));
+            }
+            std::fprintf(stderr, "\n");
+            std::fprintf(stderr, "[lfb] leaf groups %u, mean tape %.1f, registers:",
+                         n_leaf_groups, static_cast<double>(len_sum) / std::max<uint32_t>(n_leaf_groups, 1));
+            for (const auto& h : hist) {
+                std::fprintf(stderr, " %u:%llu", h.first, static_cast<unsigned long long>(h.second));
+            }
+            std::fprintf(stderr, "\n");
+        }
+        const size_t per_warp = kLeafSmallBytes + static_cast<size_t>(smem_regs) * 128 * 4;
         const size_t smem = per_warp * wpb;
         if (smem > 220 * 1024) {
             return set_error(LFB_E_UNSUPPORTED, "tape register file too large for the leaf kernel");
@@ -1780,10 +2027,59 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
         const uint32_t grid = std::min<uint32_t>(want, static_cast<uint32_t>(device_sm_count() * per_sm));
         LeafWarpScratch* scratch = ws.get<LeafWarpScratch>(K_FEAT, static_cast<size_t>(grid) * wpb);
         if (!scratch) return LFB_E_CUDA;
+        float* rd = ws.get<float>(K_LEAF_RD, static_cast<size_t>(grid) * wpb * bt.n_regs * 128);
+        if (!rd) return LFB_E_CUDA;
+        uint32_t* next_group = reinterpret_cast<uint32_t*>(counters + 7);
+        cudaMemsetAsync(next_group, 0, sizeof(uint32_t), s);
+        // Longest tapes first.
+        const uint32_t* order = nullptr;
+        if (L > 0 && n_leaf_groups > 1) {
+            uint32_t* k0 = ws.get<uint32_t>(K_ORDER_K0, n_leaf_groups);
+            uint32_t* k1 = ws.get<uint32_t>(K_ORDER_K1, n_leaf_groups);
+            uint32_t* v0 = ws.get<uint32_t>(K_ORDER_V0, n_leaf_groups);
+            uint32_t* v1 = ws.get<uint32_t>(K_ORDER_V1, n_leaf_groups);
+            if (!k0 || !k1 || !v0 || !v1) return LFB_E_CUDA;
+            k_leaf_order_keys<<<(n_leaf_groups + 255) / 256, 256, 0, s>>>(
+                o.lv[L].group_tape, n_leaf_groups, k0, v0);
+            ++n_launch;
+            size_t tmp = 0;
+            cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp, k0, k1, v0, v1,
+                                                      static_cast<int>(n_leaf_groups), 0, 32, s);
+            void* t = ws.get<unsigned char>(K_SORTTMP, tmp);
+            if (!t || !cuda_ok(cub::DeviceRadixSort::SortPairsDescending(
+                                   t, tmp, k0, k1, v0, v1, static_cast<int>(n_leaf_groups), 0,
+                                   32, s), "leaf order")) {
+                return LFB_E_CUDA;
+            }
+            order = v1;
+        }
+        unsigned long long* prof = nullptr;
+        if (debug_levels()) prof = ws.get<unsigned long long>(K_PROF, 4ull * n_leaf_groups);
         LeafArgs A{o, bt, arena, recs, rec_top, static_cast<uint32_t>(rec_cap), status,
-                   evals, scratch};
+                   evals, scratch, rd, smem_regs, next_group, order, prof};
         k_leaf_groups<<<grid, 32 * wpb, smem, s>>>(A, n_leaf_groups);
         if (!cuda_ok(cudaGetLastError(), "leaf kernel")) return LFB_E_CUDA;
+        if (prof) {
+            std::vector<unsigned long long> pf(4ull * n_leaf_groups);
+            std::vector<TapeRef> gt(n_leaf_groups);
+            cudaMemcpy(pf.data(), prof, pf.size() * 8, cudaMemcpyDeviceToHost);
+            if (L > 0) {
+                cudaMemcpy(gt.data(), o.lv[L].group_tape, n_leaf_groups * sizeof(TapeRef),
+                           cudaMemcpyDeviceToHost);
+            }
+            std::vector<uint32_t> idx(n_leaf_groups);
+            for (uint32_t k = 0; k < n_leaf_groups; ++k) idx[k] = k;
+            std::sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) { return pf[4 * a] > pf[4 * b]; });
+            unsigned long long tot = 0, ftot = 0;
+            for (uint32_t k = 0; k < n_leaf_groups; ++k) { tot += pf[4 * k]; ftot += pf[4 * k + 1]; }
+            std::fprintf(stderr, "[lfb] leaf cycles total %llu, in features %llu\n", tot, ftot);
+            for (uint32_t k = 0; k < std::min<uint32_t>(12, n_leaf_groups); ++k) {
+                const uint32_t gg = idx[k];
+                std::fprintf(stderr, "[lfb]   group %u: %llu cycles, features %llu cycles / %llu calls, E %llu, tape %u regs %u\n",
+                             gg, pf[4 * gg], pf[4 * gg + 1], pf[4 * gg + 2], pf[4 * gg + 3],
+                             L > 0 ? gt[gg].len : bt.n, L > 0 ? gt[gg].nregs : bt.n_regs);
+            }
+        }
         ++n_launch;
     }
     if (stats) cudaEventRecord(ev[2], s);

@@ -77,6 +77,33 @@ __device__ __forceinline__ float dv_value(uint8_t o, float a, float b)
     }
 }
 
+/// dv_value on four independent points (one clause, four lanes' worth of
+/// work per thread): the clause is decoded once for all four.
+__device__ __forceinline__ void dv_value4(uint8_t o, const float (&a)[4],
+                                          const float (&b)[4], float (&r)[4])
+{
+#define LFB_EACH(expr) _Pragma("unroll") for (int k = 0; k < 4; ++k) r[k] = (expr); break
+    switch (o) {
+        case op::ADD: LFB_EACH(__fadd_rn(a[k], b[k]));
+        case op::MUL: LFB_EACH(__fmul_rn(a[k], b[k]));
+        case op::MIN: LFB_EACH(sc_min(a[k], b[k]));
+        case op::MAX: LFB_EACH(sc_max(a[k], b[k]));
+        case op::SUB: LFB_EACH(__fsub_rn(a[k], b[k]));
+        case op::DIV: LFB_EACH(__fdiv_rn(a[k], b[k]));
+        case op::SQUARE: LFB_EACH(__fmul_rn(a[k], a[k]));
+        case op::SQRT: LFB_EACH(__fsqrt_rn(a[k]));
+        case op::NEG: LFB_EACH(-a[k]);
+        case op::LOG: LFB_EACH(logf(a[k]));
+        case op::EXP: LFB_EACH(expf(a[k]));
+        case op::ABS: LFB_EACH(fabsf(a[k]));
+        case op::RECIP: LFB_EACH(__fdiv_rn(1.0f, a[k]));
+        case op::CONST_VAR:
+        case OP_COPY: LFB_EACH(a[k]);
+        default: LFB_EACH(dv_value_rare(o, a[k], b[k]));
+    }
+#undef LFB_EACH
+}
+
 ////////////////////////////////////////////////////////////////////////////////
 // Derivative mode: value in .x, partials in .y/.z/.w (d/dx, d/dy, d/dz)
 

@@ -335,12 +335,49 @@ static __device__ __noinline__ void feat_eval(const FeatCtx& C, const DevTape& b
         T->one[0][i] = 0.0f;
         T->one[1][i] = 0.0f;
     }
+    uint2 next = len ? __ldg(reinterpret_cast<const uint2*>(cl)) : make_uint2(0, 0);
     for (uint32_t c = 0; c < len; ++c) {
-        const uint2 raw = __ldg(reinterpret_cast<const uint2*>(cl + c));
+        const uint2 raw = next;
+        if (c + 1 < len) next = __ldg(reinterpret_cast<const uint2*>(cl + c + 1));
         const uint8_t o = raw.x & 0xff;
         const uint8_t kinds = (raw.x >> 8) & 0xff;
         const uint16_t ro = raw.x >> 16;
         const bool binary = dev_is_binary(o);
+
+        // Plain fast path: operands with one feature and no epsilons (a
+        // plain value and gradient) and no tied min/max give a plain
+        // result, the clause's ordinary derivative; this is what the
+        // general path below computes for them.
+        {
+            float4 ga = make_float4(0.0f, 0.0f, 0.0f, 0.0f), gb = ga;
+            float2 va, vb = make_float2(0.0f, 1.0f);
+            const uint16_t ia = raw.y & 0xffff, ib = raw.y >> 16;
+            if ((kinds & 3) == OPND_REG) {
+                ga = *reinterpret_cast<const float4*>(W + ia * kRegBlock);
+                va = *reinterpret_cast<const float2*>(W + ia * kRegBlock + kValOff);
+            } else {
+                va = make_float2(__ldg(bt.cpool + ia), 1.0f);
+            }
+            if (binary) {
+                if (((kinds >> 2) & 3) == OPND_REG) {
+                    gb = *reinterpret_cast<const float4*>(W + ib * kRegBlock);
+                    vb = *reinterpret_cast<const float2*>(W + ib * kRegBlock + kValOff);
+                } else {
+                    vb = make_float2(__ldg(bt.cpool + ib), 1.0f);
+                }
+            }
+            const bool plain = va.y == 1.0f && ga.w == 0.0f &&
+                               (!binary || (vb.y == 1.0f && gb.w == 0.0f));
+            const bool tie = (o == op::MIN || o == op::MAX) && va.x == vb.x;
+            if (plain && !tie) {
+                const D4 r = dv_deriv(o, D4{va.x, ga.x, ga.y, ga.z}, D4{vb.x, gb.x, gb.y, gb.z},
+                                      false);
+                float* out = W + ro * kRegBlock;
+                *reinterpret_cast<float4*>(out) = make_float4(r.dx, r.dy, r.dz, 0.0f);
+                *reinterpret_cast<float2*>(out + kValOff) = make_float2(r.v, 1.0f);
+                continue;
+            }
+        }
         float av, bv = 0.0f;
         const float* fa;
         const float* fb = T->one[1];

@@ -687,6 +687,92 @@ static __device__ __noinline__ D4 warp_deriv(const DevTape& bt, const RegClause*
     return warp_fetch_d(bt.root_kind, bt.root, R, lane, bt.cpool);
 }
 
+/// warp_deriv that also works out, for most points, FeatureEvaluator's
+/// feature list (eval_feature.cpp:171-372) without building it.  Every
+/// register is either plain (one feature: its gradient, no epsilons) or
+/// tainted (anything else).  A tied min/max of two plain features is
+/// settled as the general feature path settles it (Feature::push and
+/// operator<, feature.cpp:50-72, 247-284): a gradient difference of zero
+/// length keeps the first argument; otherwise the two candidates (each
+/// gradient with the normalised difference, or its negation, as epsilon)
+/// are sorted and, when their gradients agree to within 1e-10 (squared),
+/// collapse to the first, epsilons dropped.  Any other tie taints the result;
+/// a min/max without a tie passes on the chosen side, taint included; all
+/// other clauses are tainted when an operand is.  Values are always exact.
+/// *plain says the root is untainted: its single feature is then the
+/// returned gradient.  *ambig reports any tie (ArrayEvaluator::getAmbiguous).
+/// Tapes with more than 64 registers report every tie as not plain.
+static __device__ __noinline__ D4 warp_deriv_lite(const DevTape& bt, const RegClause* cl,
+                                                  uint32_t len, float* R, int lane, float x,
+                                                  float y, float z, bool* ambig, bool* plain,
+                                                  uint64_t* evals, bool active)
+{
+    const float in[3] = {x, y, z};
+    for (int a = 0; a < 3; ++a) {
+        float* r = R + a * 128 + lane;
+        r[0] = in[a];
+        r[32] = a == 0 ? 1.0f : 0.0f;
+        r[64] = a == 1 ? 1.0f : 0.0f;
+        r[96] = a == 2 ? 1.0f : 0.0f;
+    }
+    const bool trackable = bt.n_regs <= 64;
+    uint64_t taint = 0;
+    bool amb = false, lost = false;
+    for (uint32_t c = 0; c < len; ++c) {
+        const uint2 raw = __ldg(reinterpret_cast<const uint2*>(cl + c));
+        const uint8_t o = raw.x & 0xff;
+        const uint8_t kinds = (raw.x >> 8) & 0xff;
+        const uint32_t ra = raw.y & 0xffff, rb = raw.y >> 16, ro = raw.x >> 16;
+        const D4 a = warp_fetch_d(kinds & 3, ra, R, lane, bt.cpool);
+        const D4 b = warp_fetch_d((kinds >> 2) & 3, rb, R, lane, bt.cpool);
+        const bool ta = (kinds & 3) == OPND_REG && ((taint >> (ra & 63)) & 1);
+        const bool tbb = dev_is_binary(o) && ((kinds >> 2) & 3) == OPND_REG &&
+                         ((taint >> (rb & 63)) & 1);
+        D4 r;
+        bool t_out;
+        if ((o == op::MIN || o == op::MAX) && a.v == b.v) {
+            amb = true;
+            lost |= !trackable;
+            const bool is_min = o == op::MIN;
+            const float e[3] = {is_min ? b.dx - a.dx : a.dx - b.dx,
+                                is_min ? b.dy - a.dy : a.dy - b.dy,
+                                is_min ? b.dz - a.dz : a.dz - b.dz};
+            const float nrm = sqrtf(fdot(e, e));
+            bool take_b = false;
+            t_out = ta || tbb;
+            if (!t_out && nrm != 0) {
+                const float dd[3] = {b.dx - a.dx, b.dy - a.dy, b.dz - a.dz};
+                if (!(static_cast<double>(fdot(dd, dd)) < 1e-10)) {
+                    t_out = true;
+                } else {
+                    const float en[3] = {e[0] / nrm, e[1] / nrm, e[2] / nrm};
+                    const float ep[3] = {-en[0], -en[1], -en[2]};
+                    const float ad[3] = {a.dx, a.dy, a.dz}, bd[3] = {b.dx, b.dy, b.dz};
+                    // Candidate order: b's feature carries -e, a's carries e.
+                    const int cmp = vcmp3(ep, en);
+                    take_b = cmp != 0 ? cmp < 0 : vcmp3(bd, ad) < 0;
+                }
+            }
+            r = take_b ? D4{dv_value(o, a.v, b.v), b.dx, b.dy, b.dz}
+                       : D4{dv_value(o, a.v, b.v), a.dx, a.dy, a.dz};
+        } else {
+            r = dv_deriv(o, a, b, false);
+            if (o == op::MIN) t_out = (a.v < b.v) ? ta : tbb;
+            else if (o == op::MAX) t_out = (a.v < b.v) ? tbb : ta;
+            else t_out = ta || tbb;
+        }
+        if (t_out) taint |= 1ull << (ro & 63);
+        else taint &= ~(1ull << (ro & 63));
+        float* out = R + ro * 128 + lane;
+        out[0] = r.v; out[32] = r.dx; out[64] = r.dy; out[96] = r.dz;
+    }
+    *ambig = amb;
+    *plain = !lost && !(bt.root_kind == OPND_REG && ((taint >> (bt.root & 63)) & 1));
+    const uint32_t act = __ballot_sync(0xffffffffu, active);
+    if (evals && lane == 0) *evals += static_cast<uint64_t>(__popc(act)) * len;
+    return warp_fetch_d(bt.root_kind, bt.root, R, lane, bt.cpool);
+}
+
 constexpr size_t kLeafSmallBytes = (sizeof(LeafWarpShared) + 15) / 16 * 16;
 constexpr uint32_t kLeafSmemRegs = 16;   // shared-memory register file per warp
 
@@ -792,11 +878,18 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
         else if (!camb) need_d = true;
         else need_f = true;
     }
-    if (__any_sync(0xffffffffu, need_d)) {
-        const D4 d = warp_deriv(tb, cl, tr.len, R, lane, px, py, pz, nullptr,
-                                &my_devals, need_d);
+    if (__any_sync(0xffffffffu, need_d || need_f)) {
+        bool amb = false, plain = false;
+        const D4 d = warp_deriv_lite(tb, cl, tr.len, R, lane, px, py, pz, &amb, &plain,
+                                     &my_devals, need_d || need_f);
         if (need_d) {
             cst = (d.dx != 0 || d.dy != 0 || d.dz != 0) ? CELL_FILLED : CELL_EMPTY;
+        }
+        if (need_f && plain) {
+            // FeatureEvaluator::isInside with one feature at a zero value.
+            const float g[3] = {d.dx, d.dy, d.dz};
+            cst = sqrtf(fdot(g, g)) > 0 ? CELL_FILLED : CELL_EMPTY;
+            need_f = false;
         }
     }
     {
@@ -951,9 +1044,10 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
                 const bool zero = active && j >= 1 && v == 0;
                 bool inside = true;
                 if (__any_sync(0xffffffffu, zero)) {
-                    bool amb = false;
-                    const D4 dg = warp_deriv(tb, cl, tr.len, R, lane, qx[k], qy[k], qz[k],
-                                             &amb, &my_devals, zero);
+                    bool amb = false, plain = false;
+                    const D4 dg = warp_deriv_lite(tb, cl, tr.len, R, lane, qx[k], qy[k], qz[k],
+                                                  &amb, &plain, &my_devals, zero);
+                    amb = amb && !plain;   // a settled tie leaves one plain feature
                     if (zero && !amb) {
                         const float g[3] = {dg.dx, dg.dy, dg.dz};
                         inside = sqrtf(fdot(g, g)) > 0;
@@ -1017,10 +1111,11 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
             const EdgeSlot& es = W->e[p >> 1];
             for (int k = 0; k < 3; ++k) q[k] = (p & 1) ? es.t1[k] : es.t0[k];
         }
-        bool amb = false;
-        const D4 d = warp_deriv(tb, cl, tr.len, R, lane, static_cast<float>(q[0]),
-                                static_cast<float>(q[1]), static_cast<float>(q[2]),
-                                &amb, &my_devals, active);
+        bool amb = false, plain = false;
+        const D4 d = warp_deriv_lite(tb, cl, tr.len, R, lane, static_cast<float>(q[0]),
+                                     static_cast<float>(q[1]), static_cast<float>(q[2]),
+                                     &amb, &plain, &my_devals, active);
+        amb = amb && !plain;   // a settled tie leaves one plain feature
         if (active) {
             EdgeSlot& es = W->e[p >> 1];
             float* g = (p & 1) ? es.g1 : es.g0;

@@ -311,10 +311,14 @@ def run_ours(args, world, rank, local):
         peak = sms * 128 * sm_mhz * 1e6 / 1e9          # G lane-ops/s
         ops = (evals_v * wv + evals_g * wg) / args.steps
         achieved = ops / (leaf_ms / args.steps / 1000.0) / 1e9
+        # DRAM bytes of one leaf launch, from the committed ncu summary of
+        # this workload (dram__bytes_read.sum + dram__bytes_write.sum).
         traffic = None
-        tpath = os.path.join(ROOT, "profiles", "leaf_kernel_traffic.json")
-        if os.path.exists(tpath):
-            traffic = json.load(open(tpath)).get("dram_bytes_per_launch")
+        tpath = os.path.join(ROOT, "profiles", "k_leaf_groups_csg2000_depth10_dram.md")
+        if args.depth == 10 and os.path.exists(tpath):
+            for ln in open(tpath):
+                if ln.startswith("dram_bytes_per_launch:"):
+                    traffic = int(ln.split(":", 1)[1].strip())
         line = {
             "metric": "DC meshes/s", "value": value, "unit": "meshes/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,

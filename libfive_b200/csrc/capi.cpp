@@ -63,15 +63,15 @@ void libfive_contours3_delete(libfive_contours3* cs)
 void libfive_mesh_delete(libfive_mesh* m)
 {
     if (!m) return;
-    delete[] m->verts;
-    delete[] m->tris;
+    host_free(m->verts);
+    host_free(m->tris);
     delete m;
 }
 
 void libfive_mesh_coords_delete(libfive_mesh_coords* m)
 {
     if (!m) return;
-    delete[] m->verts;
+    host_free(m->verts);
     delete[] m->coord_indices;
     delete m;
 }
@@ -305,14 +305,7 @@ static libfive_mesh* render_with(const std::shared_ptr<GpuTape>& g,
         std::fprintf(stderr, "%s: %s\n", who, msg.c_str());
         return nullptr;
     }
-    auto out = new libfive_mesh;
-    out->vert_count = static_cast<uint32_t>(mesh.verts.size() / 3);
-    out->tri_count = static_cast<uint32_t>(mesh.tris.size() / 3);
-    out->verts = new libfive_vec3[out->vert_count];
-    out->tris = new libfive_tri[out->tri_count];
-    std::memcpy(out->verts, mesh.verts.data(), mesh.verts.size() * sizeof(float));
-    std::memcpy(out->tris, mesh.tris.data(), mesh.tris.size() * sizeof(uint32_t));
-    return out;
+    return mesh.release();
 }
 
 libfive_mesh* libfive_tree_render_mesh(libfive_tree tree, libfive_region3 R,
@@ -348,7 +341,7 @@ libfive_mesh_coords* libfive_tree_render_mesh_coords(libfive_tree tree,
         out->coord_indices[4 * i + 2] = static_cast<int32_t>(m->tris[i].c);
         out->coord_indices[4 * i + 3] = -1;
     }
-    delete[] m->tris;
+    host_free(m->tris);
     delete m;
     return out;
 }
@@ -568,14 +561,7 @@ libfive_mesh* lfb_render_mesh(lfb_tape t, libfive_region3 R,
     if (render_dc_mesh(*t->g, R, s.min_feature, s.max_err, mesh, stats) != 0) {
         return nullptr;
     }
-    auto out = new libfive_mesh;
-    out->vert_count = static_cast<uint32_t>(mesh.verts.size() / 3);
-    out->tri_count = static_cast<uint32_t>(mesh.tris.size() / 3);
-    out->verts = new libfive_vec3[out->vert_count];
-    out->tris = new libfive_tri[out->tri_count];
-    std::memcpy(out->verts, mesh.verts.data(), mesh.verts.size() * sizeof(float));
-    std::memcpy(out->tris, mesh.tris.data(), mesh.tris.size() * sizeof(uint32_t));
-    return out;
+    return mesh.release();
 }
 
 uint64_t lfb_kernel_launches(void) { return launches(); }

@@ -25,6 +25,9 @@
 // Every numeric decision uses the same float32 / float64 operations as the
 // reference's scalar code, so the octree and the mesh are reproducible.
 #include <cub/cub.cuh>
+#include <sys/mman.h>
+#include <cstdlib>
+#include <cstring>
 
 #include "dc_device.cuh"
 #include "dc_features.cuh"
@@ -774,7 +777,7 @@ static __device__ __noinline__ D4 warp_deriv_lite(const DevTape& bt, const RegCl
 }
 
 constexpr size_t kLeafSmallBytes = (sizeof(LeafWarpShared) + 15) / 16 * 16;
-constexpr uint32_t kLeafSmemRegs = 16;   // shared-memory register file per warp
+constexpr uint32_t kLeafSmemRegs = 12;   // shared-memory register file per warp
 
 struct LeafArgs {
     Octree o;
@@ -790,10 +793,10 @@ struct LeafArgs {
     uint32_t smem_regs;         // registers of the shared-memory register file
     uint32_t* next_group;       // work counter (zero at launch)
     const uint32_t* order;      // processing order of the groups (or null)
-    unsigned long long* prof;   // debug: per group {cycles, feature cycles, feature calls, E}
+    unsigned long long* prof;   // debug: 8 per group (cycles by section, feature calls, E)
 };
 
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(256, 4)
 k_leaf_groups(LeafArgs A, uint32_t n_groups)
 {
     extern __shared__ __align__(16) unsigned char lsmem[];
@@ -944,6 +947,7 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
         S->rec[lane] = rec;
     }
 
+    const long long t_crossing = clock64();
     // --- crossing lattice edges -----------------------------------------
     const int seg = n - 1;
     const int n_lat_edges = 3 * seg * n * n;
@@ -1102,6 +1106,7 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
         }
     }
 
+    const long long t_gradients = clock64();
     // --- gradients at the bracket ends and QEFs (dc_tree.inl:412-471) ---
     for (int base = 0; base < 2 * E; base += 32) {
         const int p = base + lane;
@@ -1171,6 +1176,7 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
     }
     __syncwarp();
 
+    const long long t_vertices = clock64();
     // --- vertices: one lane per (cell, patch) (dc_tree.inl:474-549) -----
     {
         const int cell = lane >> 2, patch = lane & 3;
@@ -1235,10 +1241,16 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
     }
     (void)base_coords;
     if (A.prof && lane == 0) {
-        A.prof[4 * g + 0] = clock64() - t_group;
-        A.prof[4 * g + 1] = feat_cycles;
-        A.prof[4 * g + 2] = feat_calls;
-        A.prof[4 * g + 3] = E;
+        const long long t_end = clock64();
+        unsigned long long* P = A.prof + 8ull * g;
+        P[0] = t_end - t_group;
+        P[1] = feat_cycles;
+        P[2] = feat_calls;
+        P[3] = E;
+        P[4] = t_crossing - t_group;      // corners, classification
+        P[5] = t_gradients - t_crossing;  // crossing edges, edge search
+        P[6] = t_vertices - t_gradients;  // gradients, QEF pushes, ranks
+        P[7] = t_end - t_vertices;        // vertices
     }
     }   // groups
     if (lane == 0) {
@@ -1836,6 +1848,78 @@ bool exclusive_scan(const T* in, T* out, uint32_t n, cudaStream_t s)
 
 }  // namespace
 
+void* host_alloc(size_t bytes)
+{
+    constexpr size_t kHuge = size_t(2) << 20;
+    const size_t n = std::max<size_t>((bytes + kHuge - 1) / kHuge * kHuge, kHuge);
+    void* p = std::aligned_alloc(kHuge, n);
+    if (p) madvise(p, n, MADV_HUGEPAGE);   // advice only: failure is harmless
+    return p;
+}
+
+void host_free(void* p) { std::free(p); }
+
+MeshOut::~MeshOut()
+{
+    host_free(verts);
+    host_free(tris);
+}
+
+libfive_mesh* MeshOut::release()
+{
+    auto m = new libfive_mesh;
+    m->verts = verts;
+    m->tris = tris;
+    m->vert_count = vert_count;
+    m->tri_count = tri_count;
+    verts = nullptr;
+    tris = nullptr;
+    return m;
+}
+
+namespace {
+
+/// Device -> pageable host copy through two pinned staging buffers, so that
+/// the PCIe transfer of one chunk overlaps the host copy of the previous.
+bool download(void* dst, const void* src, size_t bytes, cudaStream_t s)
+{
+    constexpr size_t kChunk = size_t(8) << 20;
+    static void* pinned[2] = {nullptr, nullptr};
+    static cudaEvent_t done[2];
+    if (!pinned[0]) {
+        for (int b = 0; b < 2; ++b) {
+            if (!cuda_ok(cudaMallocHost(&pinned[b], kChunk), "pinned staging") ||
+                !cuda_ok(cudaEventCreateWithFlags(&done[b], cudaEventDisableTiming),
+                         "staging event")) {
+                return false;
+            }
+        }
+    }
+    const size_t n = (bytes + kChunk - 1) / kChunk;
+    auto len = [&](size_t i) { return std::min(kChunk, bytes - i * kChunk); };
+    auto drain = [&](size_t i) {
+        const int b = static_cast<int>(i & 1);
+        if (!cuda_ok(cudaEventSynchronize(done[b]), "download")) return false;
+        std::memcpy(static_cast<char*>(dst) + i * kChunk, pinned[b], len(i));
+        return true;
+    };
+    for (size_t i = 0; i < n; ++i) {
+        const int b = static_cast<int>(i & 1);
+        if (i >= 2 && !drain(i - 2)) return false;
+        if (!cuda_ok(cudaMemcpyAsync(pinned[b], static_cast<const char*>(src) + i * kChunk,
+                                     len(i), cudaMemcpyDeviceToHost, s), "download") ||
+            !cuda_ok(cudaEventRecord(done[b], s), "download")) {
+            return false;
+        }
+    }
+    for (size_t i = n >= 2 ? n - 2 : 0; i < n; ++i) {
+        if (!drain(i)) return false;
+    }
+    return true;
+}
+
+}  // namespace
+
 int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
                    double max_err, MeshOut& out, lfb_mesh_stats* stats)
 {
@@ -2149,13 +2233,13 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
             order = v1;
         }
         unsigned long long* prof = nullptr;
-        if (debug_levels()) prof = ws.get<unsigned long long>(K_PROF, 4ull * n_leaf_groups);
+        if (debug_levels()) prof = ws.get<unsigned long long>(K_PROF, 8ull * n_leaf_groups);
         LeafArgs A{o, bt, arena, recs, rec_top, static_cast<uint32_t>(rec_cap), status,
                    evals, scratch, rd, smem_regs, next_group, order, prof};
         k_leaf_groups<<<grid, 32 * wpb, smem, s>>>(A, n_leaf_groups);
         if (!cuda_ok(cudaGetLastError(), "leaf kernel")) return LFB_E_CUDA;
         if (prof) {
-            std::vector<unsigned long long> pf(4ull * n_leaf_groups);
+            std::vector<unsigned long long> pf(8ull * n_leaf_groups);
             std::vector<TapeRef> gt(n_leaf_groups);
             cudaMemcpy(pf.data(), prof, pf.size() * 8, cudaMemcpyDeviceToHost);
             if (L > 0) {
@@ -2164,14 +2248,18 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
             }
             std::vector<uint32_t> idx(n_leaf_groups);
             for (uint32_t k = 0; k < n_leaf_groups; ++k) idx[k] = k;
-            std::sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) { return pf[4 * a] > pf[4 * b]; });
-            unsigned long long tot = 0, ftot = 0;
-            for (uint32_t k = 0; k < n_leaf_groups; ++k) { tot += pf[4 * k]; ftot += pf[4 * k + 1]; }
-            std::fprintf(stderr, "[lfb] leaf cycles total %llu, in features %llu\n", tot, ftot);
+            std::sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) { return pf[8 * a] > pf[8 * b]; });
+            unsigned long long sec[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            for (uint32_t k = 0; k < n_leaf_groups; ++k) {
+                for (int q = 0; q < 8; ++q) sec[q] += pf[8 * k + q];
+            }
+            std::fprintf(stderr, "[lfb] leaf cycles total %llu: corners %llu, edge search %llu, "
+                         "gradients+QEF %llu, vertices %llu; features %llu in %llu calls\n",
+                         sec[0], sec[4], sec[5], sec[6], sec[7], sec[1], sec[2]);
             for (uint32_t k = 0; k < std::min<uint32_t>(12, n_leaf_groups); ++k) {
                 const uint32_t gg = idx[k];
                 std::fprintf(stderr, "[lfb]   group %u: %llu cycles, features %llu cycles / %llu calls, E %llu, tape %u regs %u\n",
-                             gg, pf[4 * gg], pf[4 * gg + 1], pf[4 * gg + 2], pf[4 * gg + 3],
+                             gg, pf[8 * gg], pf[8 * gg + 1], pf[8 * gg + 2], pf[8 * gg + 3],
                              L > 0 ? gt[gg].len : bt.n, L > 0 ? gt[gg].nregs : bt.n_regs);
             }
         }
@@ -2211,8 +2299,14 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
     }
 
     // Dual walk.
-    out.verts.assign(3, 0.0f);
-    out.tris.clear();
+    host_free(out.verts);
+    host_free(out.tris);
+    out.verts = static_cast<libfive_vec3*>(host_alloc(sizeof(libfive_vec3)));
+    out.tris = nullptr;
+    out.vert_count = 1;
+    out.tri_count = 0;
+    if (!out.verts) return set_error(LFB_E_CAPACITY, "host allocation failed");
+    out.verts[0] = {0.0f, 0.0f, 0.0f};
     uint8_t root_type = 0;
     cudaMemcpyAsync(&root_type, o.lv[0].type, 1, cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
@@ -2278,15 +2372,18 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
                 k_remap_tris<<<(3 * n_tri + 255) / 256, 256, 0, s>>>(tris, n_tri, vscan);
                 ++n_launch;
             }
-            out.verts.resize(3 * (static_cast<size_t>(n_verts) + 1));
-            out.tris.resize(3 * static_cast<size_t>(n_tri));
-            cudaMemcpyAsync(out.verts.data(), verts, out.verts.size() * sizeof(float),
-                            cudaMemcpyDeviceToHost, s);
-            if (n_tri) {
-                cudaMemcpyAsync(out.tris.data(), tris, out.tris.size() * sizeof(uint32_t),
-                                cudaMemcpyDeviceToHost, s);
+            host_free(out.verts);
+            out.verts = static_cast<libfive_vec3*>(
+                host_alloc((static_cast<size_t>(n_verts) + 1) * sizeof(libfive_vec3)));
+            out.tris = static_cast<libfive_tri*>(
+                host_alloc(static_cast<size_t>(n_tri) * sizeof(libfive_tri)));
+            if (!out.verts || !out.tris) return set_error(LFB_E_CAPACITY, "host allocation failed");
+            out.vert_count = n_verts + 1;
+            out.tri_count = n_tri;
+            if (!download(out.verts, verts, out.vert_count * sizeof(libfive_vec3), s) ||
+                !download(out.tris, tris, static_cast<size_t>(n_tri) * sizeof(libfive_tri), s)) {
+                return LFB_E_CUDA;
             }
-            if (!cuda_ok(cudaStreamSynchronize(s), "mesh download")) return LFB_E_CUDA;
             break;
         }
     }
@@ -2303,8 +2400,8 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
         stats->leaves_ambiguous = n_recs;
         stats->clause_evals = ce[0];
         stats->clause_evals_grad = ce[1];
-        stats->triangles = out.tris.size() / 3;
-        stats->vertices = out.verts.size() / 3 - 1;
+        stats->triangles = out.tri_count;
+        stats->vertices = out.vert_count - 1;
         stats->kernel_launches = n_launch;
         float ms[4];
         for (int k = 0; k < 4; ++k) cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]);

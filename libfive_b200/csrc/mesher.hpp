@@ -10,10 +10,25 @@
 
 namespace lfb {
 
+/// Mesh arrays in host memory from host_alloc (freed with host_free); the
+/// C API hands them to the caller's libfive_mesh without a copy.
 struct MeshOut {
-    std::vector<float> verts;      // xyz triples; verts[0..2] is the dummy
-    std::vector<uint32_t> tris;    // index triples (indices start at 1)
+    libfive_vec3* verts = nullptr;   // verts[0] is the dummy vertex
+    libfive_tri* tris = nullptr;     // indices start at 1
+    uint32_t vert_count = 0;
+    uint32_t tri_count = 0;
+    MeshOut() = default;
+    MeshOut(const MeshOut&) = delete;
+    MeshOut& operator=(const MeshOut&) = delete;
+    ~MeshOut();
+    /// Moves the arrays into a new libfive_mesh (freed by libfive_mesh_delete).
+    libfive_mesh* release();
 };
+
+/// Large host arrays: 2 MiB aligned and advised for transparent huge pages,
+/// so that writing a fresh multi-megabyte mesh costs few page faults.
+void* host_alloc(size_t bytes);
+void host_free(void* p);
 
 /// Mesh::render with DUAL_CONTOURING (libfive/src/render/brep/mesh.cpp:48-72)
 /// for one tree; returns 0 or a negative LFB_E* code.

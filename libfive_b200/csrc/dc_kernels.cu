@@ -50,6 +50,7 @@ __constant__ DcTables c_tab;
 constexpr uint32_t kWideSmemSlots = 512;
 constexpr uint32_t kMaxTapeRegs = 400;
 constexpr uint32_t kRenumberMax = kWideSmemSlots;   // tapes up to this length get compact registers
+constexpr uint32_t kGroupModeCells = 8192;          // cells per level from which k_interval_group runs
 
 struct WideSmem {
     float2 S[kWideSmemSlots + 3];      // slot intervals
@@ -182,10 +183,11 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v, int lane)
 
 /// Linear-scan register allocation of a pruned tape, in place (one thread):
 /// a backward pass marks each operand's last use, a forward pass gives every
-/// result the lowest free register.  On straight-line code this uses as many
-/// registers as values are live at once, which is at most the unpruned
-/// tape's count; the leaf kernel then fits the register file of most leaf
-/// tapes in shared memory.  Values are unchanged: only storage moves.
+/// result the lowest free register (X, Y and Z keep registers 0-2 while they
+/// are still to be read).  On straight-line code this uses as many registers
+/// as values are live at once, which is at most the unpruned tape's count;
+/// the leaf kernel then fits the register file of most leaf tapes in shared
+/// memory.  Values are unchanged: only storage moves.
 static __device__ __noinline__ TapeRef renumber_tape(uint2* raw_t, TapeRef tr,
                                                      uint8_t* lastuse,
                                                      uint16_t* regmap,
@@ -212,8 +214,12 @@ static __device__ __noinline__ TapeRef renumber_tape(uint2* raw_t, TapeRef tr,
         }
         lastuse[c] = f;
     }
-    for (uint32_t w = 0; w < nm; ++w) mask[w] = ~0u;   // free bits
-    mask[0] &= ~7u;
+    // X, Y, Z start in registers 0-2; those not read by the tape are free.
+    const uint32_t xyz_live = mask[0] & 7u;
+    constexpr uint32_t kWords = (kMaxTapeRegs + 31) / 32;
+    for (uint32_t w = 0; w < kWords; ++w) mask[w] = ~0u;   // free bits
+    if (kMaxTapeRegs % 32) mask[kWords - 1] = (1u << (kMaxTapeRegs % 32)) - 1;
+    mask[0] &= ~xyz_live;
     for (uint32_t r = 0; r < 3; ++r) regmap[r] = static_cast<uint16_t>(r);
     uint32_t hi = 3;
     for (uint32_t c = 0; c < tr.len; ++c) {
@@ -227,13 +233,13 @@ static __device__ __noinline__ TapeRef renumber_tape(uint2* raw_t, TapeRef tr,
         if (f & 1) mask[a >> 5] |= 1u << (a & 31);
         if (f & 2) mask[b >> 5] |= 1u << (b & 31);
         uint32_t r = 0xffffffffu;
-        for (uint32_t w = 0; w < nm; ++w) {
+        for (uint32_t w = 0; w < kWords; ++w) {
             if (mask[w]) {
                 r = w * 32 + __ffs(mask[w]) - 1;
                 break;
             }
         }
-        if (r >= tr.nregs) {   // cannot happen for a tape from this pipeline
+        if (r >= kMaxTapeRegs) {   // more live values than registers: cannot happen
             atomicOr(status, ST_REGS);
             return tr;
         }
@@ -523,6 +529,184 @@ k_interval_wide(WideArgs A, int d)
             lv.cell_tape[i] = out_t;
         }
         __syncwarp();
+    }
+}
+
+// Deep levels: one warp per sibling group, one lane per cell.  The eight
+// cells share their parent's register tape, so lanes 0-7 walk the same
+// clause stream (no divergence) with the interval register file in shared
+// memory, as IntervalEvaluator does, and prune with a backward liveness pass
+// over registers (Tape::push, tape.cpp:23-160).  Used once cells are many
+// and tapes short, where the per-cell overheads of the level-ordered form
+// dominate; it writes register tapes only.
+
+struct GroupArgs {
+    Octree o;
+    DevTape bt;
+    RegClause* arena;
+    unsigned long long* arena_top;
+    uint64_t arena_cap;
+    uint8_t* dec;                  // [warps][8][dec_cap] min/max decisions
+    uint32_t dec_cap;
+    uint8_t* lastuse;              // [warps][8][kRenumberMax] renumbering flags
+    uint32_t nregs_max;            // register file size (the unpruned tape's)
+    uint32_t* status;
+    uint32_t* next_group;          // work counter (zero at launch)
+};
+
+__host__ __device__ inline size_t group_smem_per_warp(uint32_t nregs_max)
+{
+    // L, H (float), regmap (u16) per register and lane; masks; N (u8).
+    const size_t b = static_cast<size_t>(nregs_max) * 8 * (4 + 4 + 2) + 8 * 13 * 4 +
+                     static_cast<size_t>(nregs_max) * 8;
+    return (b + 15) / 16 * 16;
+}
+
+__global__ void __launch_bounds__(128)
+k_interval_group(GroupArgs A, int d)
+{
+    extern __shared__ __align__(16) unsigned char gsm[];
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    const uint32_t nr = A.nregs_max;
+    unsigned char* base = gsm + group_smem_per_warp(nr) * warp;
+    float* Lo = reinterpret_cast<float*>(base);
+    float* Hi = Lo + nr * 8;
+    uint16_t* RM = reinterpret_cast<uint16_t*>(Hi + nr * 8) + lane * nr;
+    uint32_t* MK = reinterpret_cast<uint32_t*>(reinterpret_cast<uint16_t*>(Hi + nr * 8) + nr * 8) +
+                   lane * 13;
+    uint8_t* Nn = reinterpret_cast<uint8_t*>(reinterpret_cast<uint32_t*>(
+                      reinterpret_cast<uint16_t*>(Hi + nr * 8) + nr * 8) + 8 * 13);
+    const uint32_t gw = blockIdx.x * wpb + warp;
+    uint8_t* dec = A.dec + (static_cast<size_t>(gw) * 8 + (lane & 7)) * A.dec_cap;
+    uint8_t* lastuse = A.lastuse + (static_cast<size_t>(gw) * 8 + (lane & 7)) * kRenumberMax;
+    const Octree& o = A.o;
+    const LevelView& lv = o.lv[d];
+    const DevTape& bt = A.bt;
+    auto fetch = [&](uint32_t kind, uint32_t idx) -> Iv {
+        if (kind == OPND_REG) return {Lo[idx * 8 + lane], Hi[idx * 8 + lane], Nn[idx * 8 + lane] != 0};
+        const float v = __ldg(bt.cpool + idx);
+        return iv_make(v, v);
+    };
+
+    while (true) {
+        uint32_t g = 0;
+        if (lane == 0) g = atomicAdd(A.next_group, 1u);
+        g = __shfl_sync(0xffffffffu, g, 0);
+        if (g >= lv.n_groups) break;
+        if (lane >= 8) continue;
+        const uint32_t i = 8 * g + lane;
+        const TapeRef T = lv.group_tape[g];
+        const RegClause* cl = A.arena + T.off;
+        const uint32_t rk = T.root >> 16, rr = T.root & 0xffff;
+
+        double blo[3], bhi[3];
+        cell_bounds(o, d, lv.coords[i], blo, bhi);
+        for (int a = 0; a < 3; ++a) {
+            const Iv v = iv_make(static_cast<float>(blo[a]), static_cast<float>(bhi[a]));
+            Lo[a * 8 + lane] = v.lo;
+            Hi[a * 8 + lane] = v.hi;
+            Nn[a * 8 + lane] = v.nan;
+        }
+        // Forward pass, recording the push decision of every min/max
+        // (IntervalEvaluator::push, eval_interval.cpp:116-167).
+        bool changed = false;
+        uint32_t ch = 0;
+        for (uint32_t c = 0; c < T.len; ++c) {
+            const uint2 raw = __ldg(reinterpret_cast<const uint2*>(cl + c));
+            const uint8_t o_ = raw.x & 0xff;
+            const uint32_t kinds = (raw.x >> 8) & 0xff;
+            const uint32_t ro = raw.x >> 16;
+            const Iv a = fetch(kinds & 3, raw.y & 0xffff);
+            const Iv b = fetch((kinds >> 2) & 3, raw.y >> 16);
+            const Iv r = iv_apply(o_, a, b);
+            if (o_ == op::MIN || o_ == op::MAX) {
+                uint8_t keep = 0;   // 0 both, 1 a, 2 b
+                if (a.lo > b.hi) keep = (o_ == op::MAX) ? 1 : 2;
+                else if (b.lo > a.hi) keep = (o_ == op::MAX) ? 2 : 1;
+                changed |= keep != 0;
+                if (ch < A.dec_cap) dec[ch] = keep;
+                ++ch;
+            }
+            Lo[ro * 8 + lane] = r.lo;
+            Hi[ro * 8 + lane] = r.hi;
+            Nn[ro * 8 + lane] = r.nan;
+        }
+        const Iv root = fetch(rk, rr);
+        const uint8_t state = iv_state(root);
+        lv.type[i] = state == ST_EMPTY ? CELL_EMPTY
+                   : state == ST_FILLED ? CELL_FILLED : CELL_BRANCH;
+        if (state != ST_AMBIGUOUS) continue;
+        if (ch > A.dec_cap) {   // cannot happen: dec_cap is the unpruned tape's count
+            atomicOr(A.status, ST_REGS);
+            lv.cell_tape[i] = T;
+            continue;
+        }
+        // NaN-unsafe results keep the unpruned tape (dc_tree.inl:107-111).
+        if (root.nan || !changed) {
+            lv.cell_tape[i] = T;
+            continue;
+        }
+        // Backward liveness pass over registers: count, then allocate and
+        // write the kept clauses from the back.
+        uint32_t kept = 0;
+        TapeRef out = T;
+        for (int pass = 0; pass < 2; ++pass) {
+            for (uint32_t r = 0; r < T.nregs; ++r) Nn[r * 8 + lane] = 0;
+            if (rk == OPND_REG) Nn[rr * 8 + lane] = 1;
+            uint32_t pos = kept;
+            uint32_t chi = ch;
+            unsigned long long off = 0;
+            if (pass == 1) {
+                off = atomicAdd(A.arena_top, static_cast<unsigned long long>(kept));
+                if (off + kept > A.arena_cap) {
+                    atomicOr(A.status, ST_ARENA_OVERFLOW);
+                    break;
+                }
+            }
+            for (int64_t c = static_cast<int64_t>(T.len) - 1; c >= 0; --c) {
+                const uint2 raw = __ldg(reinterpret_cast<const uint2*>(cl + c));
+                const uint8_t o_ = raw.x & 0xff;
+                const uint32_t kinds = (raw.x >> 8) & 0xff;
+                const uint32_t ro = raw.x >> 16;
+                uint8_t keep = 0;
+                if (o_ == op::MIN || o_ == op::MAX) keep = dec[--chi];
+                if (!Nn[ro * 8 + lane]) continue;
+                Nn[ro * 8 + lane] = 0;
+                uint2 outc = raw;
+                bool emit = true;
+                if (keep) {
+                    const uint32_t k = keep == 1 ? (kinds & 3) : ((kinds >> 2) & 3);
+                    const uint32_t src = keep == 1 ? (raw.y & 0xffff) : (raw.y >> 16);
+                    if (k == OPND_REG) {
+                        Nn[src * 8 + lane] = 1;
+                        emit = src != ro;
+                    }
+                    outc.x = OP_COPY | (k << 8) | (ro << 16);
+                    outc.y = src;
+                } else {
+                    if ((kinds & 3) == OPND_REG) Nn[(raw.y & 0xffff) * 8 + lane] = 1;
+                    if (dev_is_binary(o_) && ((kinds >> 2) & 3) == OPND_REG) {
+                        Nn[(raw.y >> 16) * 8 + lane] = 1;
+                    }
+                }
+                if (!emit) continue;
+                if (pass == 0) {
+                    ++kept;
+                } else {
+                    *reinterpret_cast<uint2*>(A.arena + off + (--pos)) = outc;
+                }
+            }
+            if (pass == 1) {
+                out = {static_cast<uint32_t>(off), kept, T.nregs, T.root};
+                if (kept <= kRenumberMax) {
+                    out = renumber_tape(reinterpret_cast<uint2*>(A.arena + off), out, lastuse,
+                                        RM, MK, A.status);
+                }
+            }
+        }
+        lv.cell_tape[i] = out;
     }
 }
 
@@ -1799,7 +1983,7 @@ enum BufKey {
     K_CUBTMP, K_TASK_A, K_TASK_B, K_TRIS, K_USED, K_VSCAN, K_VERTS, K_FEAT,
     K_LIST_A, K_LIST_B, K_WIDE_S, K_WIDE_SN, K_WIDE_P, K_WIDE_LIVE, K_WIDE_NEW,
     K_WIDE_ST2, K_WIDE_L1, K_WIDE_WL, K_LEAF_RD, K_ORDER_K0, K_ORDER_K1,
-    K_ORDER_V0, K_ORDER_V1, K_SORTTMP, K_PROF,
+    K_ORDER_V0, K_ORDER_V1, K_SORTTMP, K_PROF, K_GDEC, K_GLAST,
     K_LEVEL = 100,
 };
 
@@ -1823,6 +2007,19 @@ int level_from_resolution(const double lo[3], const double hi[3], double min_fea
     const float l = std::ceil(std::fmax(0.0f, logf(static_cast<float>(md / min_feature))) /
                               logf(2.0f));
     return static_cast<int>(l);
+}
+
+/// Cells per level from which the interval stage switches to group mode
+/// (kGroupModeCells; the LFB_GROUP_MODE_CELLS environment variable overrides
+/// it, which the parity tests use to run both modes on small shapes).
+uint32_t group_mode_cells()
+{
+    static uint32_t v = 0;
+    if (v == 0) {
+        const char* e = std::getenv("LFB_GROUP_MODE_CELLS");
+        v = e ? static_cast<uint32_t>(std::max(1L, std::atol(e))) : kGroupModeCells;
+    }
+    return v;
 }
 
 bool debug_levels()
@@ -2047,10 +2244,26 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
         }
     }
 
+    // Deep levels (many cells, short tapes) switch to one warp per sibling
+    // group over register tapes; every level below stays in that mode.
+    const uint32_t group_warps = static_cast<uint32_t>(device_sm_count()) * 16;
+    const uint32_t gdec_cap = std::max<uint32_t>(bt.n_choices, 1);
+    const size_t group_smem = group_smem_per_warp(bt.n_regs) * 4;
+    uint8_t* gdec = ws.get<uint8_t>(K_GDEC, static_cast<size_t>(group_warps) * 8 * gdec_cap);
+    uint8_t* glast = ws.get<uint8_t>(K_GLAST, static_cast<size_t>(group_warps) * 8 * kRenumberMax);
+    if (!gdec || !glast) return LFB_E_CUDA;
+    if (group_smem > 48 * 1024) {
+        cudaFuncSetAttribute(k_interval_group, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(group_smem));
+    }
+    bool group_mode = false;
+
     for (int d = 0; d < L; ++d) {
         LevelView& lv = o.lv[d];
         cells_evaluated += lv.n_cells;
-        const bool write_lists = d + 1 < L;
+        group_mode = group_mode || (d > 0 && lv.n_cells >= group_mode_cells() &&
+                                    group_smem <= 200 * 1024);
+        const bool write_lists = d + 1 < L && !group_mode;
         const int out_key = list_key[(d + 1) & 1];
         const auto t_level = std::chrono::steady_clock::now();
         unsigned long long arena_before = 0;
@@ -2082,8 +2295,15 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
             W.next_cell = reinterpret_cast<uint32_t*>(counters + 6);
             cudaMemsetAsync(W.next_cell, 0, sizeof(uint32_t), s);
             cudaMemsetAsync(list_top, 0, sizeof(unsigned long long), s);
-            const uint32_t warps = std::min<uint32_t>(scratch_warps, (lv.n_cells + 7) / 8 * 8);
-            k_interval_wide<<<warps / 8, 256, wide_smem, s>>>(W, d);
+            if (group_mode) {
+                GroupArgs G{o, bt, arena, arena_top, arena_cap, gdec, gdec_cap, glast,
+                            bt.n_regs, status, W.next_cell};
+                const uint32_t blocks = std::min<uint32_t>(group_warps / 4, (lv.n_groups + 3) / 4);
+                k_interval_group<<<std::max<uint32_t>(blocks, 1), 128, group_smem, s>>>(G, d);
+            } else {
+                const uint32_t warps = std::min<uint32_t>(scratch_warps, (lv.n_cells + 7) / 8 * 8);
+                k_interval_wide<<<warps / 8, 256, wide_smem, s>>>(W, d);
+            }
             ++n_launch;
             if (!cuda_ok(cudaGetLastError(), "interval kernel")) return LFB_E_CUDA;
             uint32_t st = 0;
@@ -2092,6 +2312,9 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
             cudaMemcpyAsync(&tops[0], arena_top, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
             cudaMemcpyAsync(&tops[1], list_top, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
             if (!cuda_ok(cudaStreamSynchronize(s), "interval kernel")) return LFB_E_CUDA;
+            if (st & ST_REGS) {
+                return set_error(LFB_E_UNSUPPORTED, "tape register renumbering failed");
+            }
             if (!(st & (ST_ARENA_OVERFLOW | ST_LIST_OVERFLOW))) break;
             if (attempt == 3) return set_error(LFB_E_CAPACITY, "tape arena overflow");
             // The counters kept counting past the capacity: grow to what this

@@ -51,6 +51,7 @@ constexpr uint32_t kWideSmemSlots = 512;
 constexpr uint32_t kMaxTapeRegs = 400;
 constexpr uint32_t kRenumberMax = kWideSmemSlots;   // tapes up to this length get compact registers
 constexpr uint32_t kGroupModeCells = 8192;          // cells per level from which k_interval_group runs
+constexpr uint32_t kBlockModeCells = 2048;          // cells per level up to which k_interval_block runs
 
 struct WideSmem {
     float2 S[kWideSmemSlots + 3];      // slot intervals
@@ -529,6 +530,253 @@ k_interval_wide(WideArgs A, int d)
             lv.cell_tape[i] = out_t;
         }
         __syncwarp();
+    }
+}
+
+// Top levels: one block per cell.  The first levels have few cells with
+// long lists (the unpruned tape at depth 0), so all warps of a block work on
+// one cell: a wave of kBlockThreads consecutive entries at a time, stepping
+// through the levels the wave spans with a block barrier per level.  Same
+// results as k_interval_wide (lists, register tapes); tapes are not
+// renumbered (they are long at these depths).
+
+constexpr int kBlockThreads = 512;
+constexpr int kBlockWarps = kBlockThreads / 32;
+
+/// Exclusive prefix over the block of one count per thread, and the total.
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* warp_tot,
+                                                    uint32_t& total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t incl = warp_incl_scan(v, lane);
+    if (lane == 31) warp_tot[warp] = incl;
+    __syncthreads();
+    uint32_t before = 0;
+    total = 0;
+    for (int w = 0; w < kBlockWarps; ++w) {
+        const uint32_t t = warp_tot[w];
+        if (w < warp) before += t;
+        total += t;
+    }
+    __syncthreads();
+    return before + incl - v;
+}
+
+__global__ void __launch_bounds__(kBlockThreads)
+k_interval_block(WideArgs A, int d)
+{
+    __shared__ uint32_t warp_tot[kBlockWarps];
+    __shared__ unsigned long long bcast;
+    __shared__ uint32_t cell;
+    const int tid = threadIdx.x;
+    const Octree& o = A.o;
+    const LevelView& lv = o.lv[d];
+    const DevTape& bt = A.bt;
+    const uint32_t n = A.n;
+    const uint32_t nw = (n + 15) / 16;
+    const size_t slot = blockIdx.x;
+    float2* S = A.S + slot * (n + 3);
+    uint8_t* SN = A.SN + slot * (n + 3);
+    uint8_t* pst = A.pst + slot * n;
+    uint8_t* live = A.live + slot * n;
+    uint32_t* newpos = A.newpos + slot * n;
+    uint32_t* st2 = A.st2 + slot * nw;
+
+    while (true) {
+        if (tid == 0) cell = atomicAdd(A.next_cell, 1u);
+        __syncthreads();
+        const uint32_t i = cell;
+        __syncthreads();
+        if (i >= lv.n_cells) break;
+        ListRef P;
+        TapeRef T;
+        if (d == 0) {
+            P = A.root_list;
+            T = root_tape_ref(bt);
+        } else {
+            P = lv.group_list[i >> 3];
+            T = lv.group_tape[i >> 3];
+        }
+        const uint4* PL = reinterpret_cast<const uint4*>(A.in_lists + P.off);
+        if (tid < 3) {
+            double blo[3], bhi[3];
+            cell_bounds(o, d, lv.coords[i], blo, bhi);
+            const Iv v = iv_make(static_cast<float>(blo[tid]), static_cast<float>(bhi[tid]));
+            S[tid] = make_float2(v.lo, v.hi);
+            SN[tid] = v.nan;
+        }
+        for (uint32_t k = tid; k < P.len; k += kBlockThreads) live[k] = 0;
+        __syncthreads();
+
+        // Forward pass: waves of consecutive entries, levels in order.
+        const uint32_t nwaves = (P.len + kBlockThreads - 1) / kBlockThreads;
+        bool changed = false;
+        for (uint32_t w = 0; w < nwaves; ++w) {
+            const uint32_t b0 = w * kBlockThreads;
+            const uint32_t k = b0 + tid;
+            const bool valid = k < P.len;
+            const uint4 e = valid ? PL[k] : make_uint4(0, 0, 0, 0);
+            const uint32_t lev = valid ? (e.x >> kWideLevelShift) : 0xffffffffu;
+            const uint32_t lf = PL[b0].x >> kWideLevelShift;
+            const uint32_t ll = PL[min(b0 + kBlockThreads, P.len) - 1].x >> kWideLevelShift;
+            for (uint32_t l = lf; l <= ll; ++l) {
+                if (lev == l) changed |= wide_forward(e, k, bt.cpool, S, SN, pst);
+                __syncthreads();
+            }
+        }
+        changed = __syncthreads_or(changed) != 0;
+        const Iv root = wide_fetch(bt.root_kind, P.root, S, SN, bt.cpool);
+        const uint8_t state = iv_state(root);
+        if (tid == 0) {
+            lv.type[i] = state == ST_EMPTY ? CELL_EMPTY
+                       : state == ST_FILLED ? CELL_FILLED : CELL_BRANCH;
+        }
+        if (state != ST_AMBIGUOUS) continue;
+
+        if (root.nan || !changed) {
+            // The children keep this tape; its list moves to the next arena.
+            uint32_t off = 0;
+            if (A.write_lists) {
+                if (tid == 0) bcast = atomicAdd(A.out_top, static_cast<unsigned long long>(P.len));
+                __syncthreads();
+                const unsigned long long o64 = bcast;
+                __syncthreads();
+                if (o64 + P.len <= A.out_cap) {
+                    off = static_cast<uint32_t>(o64);
+                    uint4* out = reinterpret_cast<uint4*>(A.out_lists + off);
+                    for (uint32_t k = tid; k < P.len; k += kBlockThreads) out[k] = PL[k];
+                } else if (tid == 0) {
+                    atomicOr(A.status, ST_LIST_OVERFLOW);
+                }
+            }
+            if (tid == 0) {
+                lv.cell_list[i] = {off, P.len, P.root, 0u};
+                lv.cell_tape[i] = T;
+            }
+            continue;
+        }
+
+        // Backward liveness pass: waves in reverse, levels decreasing.
+        if (tid == 0 && bt.root_kind == OPND_REG && P.root >= 3) live[P.root - 3] = 1;
+        __syncthreads();
+        for (int w = static_cast<int>(nwaves) - 1; w >= 0; --w) {
+            const uint32_t b0 = w * kBlockThreads;
+            const uint32_t k = b0 + tid;
+            const bool valid = k < P.len;
+            const uint4 e = valid ? PL[k] : make_uint4(0, 0, 0, 0);
+            const uint32_t lev = valid ? (e.x >> kWideLevelShift) : 0xffffffffu;
+            const uint32_t lf = PL[b0].x >> kWideLevelShift;
+            const uint32_t ll = PL[min(b0 + kBlockThreads, P.len) - 1].x >> kWideLevelShift;
+            for (uint32_t l = ll + 1; l-- > lf;) {
+                if (lev == l && live[k]) wide_mark(e, pst[k], live);
+                __syncthreads();
+            }
+        }
+
+        // Child positions of the live entries and their 2-bit states.
+        uint32_t cnt = 0;
+        for (uint32_t w = 0; w < nwaves; ++w) {
+            const uint32_t k = w * kBlockThreads + tid;
+            const bool lv_ = k < P.len && live[k];
+            uint32_t tot = 0;
+            const uint32_t before = block_excl_scan(lv_ ? 1u : 0u, warp_tot, tot);
+            if (lv_) {
+                newpos[k] = cnt + before;
+                const uint32_t c = PL[k].w;
+                atomicOr(st2 + (c >> 4), static_cast<uint32_t>(pst[k]) << (2 * (c & 15)));
+            }
+            cnt += tot;
+        }
+        __syncthreads();
+        const uint32_t new_root = (bt.root_kind == OPND_REG && P.root >= 3)
+                                      ? newpos[P.root - 3] + 3 : P.root;
+        uint32_t loff = 0;
+        if (A.write_lists) {
+            if (tid == 0) bcast = atomicAdd(A.out_top, static_cast<unsigned long long>(cnt));
+            __syncthreads();
+            const unsigned long long o64 = bcast;
+            __syncthreads();
+            const bool ok = o64 + cnt <= A.out_cap;
+            if (!ok && tid == 0) atomicOr(A.status, ST_LIST_OVERFLOW);
+            if (ok) {
+                loff = static_cast<uint32_t>(o64);
+                uint4* out = reinterpret_cast<uint4*>(A.out_lists + loff);
+                for (uint32_t k = tid; k < P.len; k += kBlockThreads) {
+                    if (!live[k]) continue;
+                    uint4 e = PL[k];
+                    const uint32_t ps = pst[k];
+                    const uint32_t kinds = (e.x >> 8) & 0xf;
+                    const bool binary = dev_is_binary(e.x & 0xff);
+                    if (ps == WIDE_B) e.y = 0;
+                    else if ((kinds & 3) == OPND_REG && e.y >= 3) e.y = newpos[e.y - 3] + 3;
+                    if (ps == WIDE_A) e.z = 0;
+                    else if (binary && ((kinds >> 2) & 3) == OPND_REG && e.z >= 3) {
+                        e.z = newpos[e.z - 3] + 3;
+                    }
+                    e.x = (e.x & ~(3u << 12)) | (ps << 12);
+                    out[newpos[k]] = e;
+                }
+            }
+        }
+
+        // Register tape: live clauses in clause order (dense over the state
+        // words, which hold the whole tape at these depths).
+        uint32_t emit = 0;
+        for (uint32_t w = tid; w < nw; w += kBlockThreads) emit += wide_word_emits(st2[w], w, bt.clauses);
+        uint32_t etot = 0;
+        block_excl_scan(emit, warp_tot, etot);
+        if (tid == 0) bcast = atomicAdd(A.arena_top, static_cast<unsigned long long>(etot));
+        __syncthreads();
+        const unsigned long long a64 = bcast;
+        __syncthreads();
+        const bool aok = a64 + etot <= A.arena_cap;
+        if (!aok && tid == 0) atomicOr(A.status, ST_ARENA_OVERFLOW);
+        uint32_t pos = static_cast<uint32_t>(a64);
+        const uint32_t nwwaves = (nw + kBlockThreads - 1) / kBlockThreads;
+        for (uint32_t ww = 0; ww < nwwaves; ++ww) {
+            const uint32_t w = ww * kBlockThreads + tid;
+            uint32_t word = 0, e_ = 0;
+            if (w < nw) {
+                word = st2[w];
+                e_ = wide_word_emits(word, w, bt.clauses);
+                st2[w] = 0;
+            }
+            uint32_t tot = 0;
+            uint32_t at = pos + block_excl_scan(e_, warp_tot, tot);
+            if (aok) {
+                while (word) {
+                    const int j = (__ffs(word) - 1) >> 1;
+                    const uint32_t ps = (word >> (2 * j)) & 3;
+                    word &= ~(3u << (2 * j));
+                    const uint2 raw = __ldg(reinterpret_cast<const uint2*>(bt.clauses + w * 16 + j));
+                    if (ps == WIDE_BOTH) {
+                        *reinterpret_cast<uint2*>(A.arena + at++) = raw;
+                        continue;
+                    }
+                    const uint32_t kinds = (raw.x >> 8) & 0xff;
+                    const uint32_t kk = ps == WIDE_A ? (kinds & 3) : ((kinds >> 2) & 3);
+                    const uint32_t src = ps == WIDE_A ? (raw.y & 0xffff) : (raw.y >> 16);
+                    const uint32_t ro = raw.x >> 16;
+                    if (kk == OPND_REG && src == ro) continue;
+                    RegClause cc;
+                    cc.op = OP_COPY;
+                    cc.kinds = static_cast<uint8_t>(kk);
+                    cc.out = static_cast<uint16_t>(ro);
+                    cc.a = static_cast<uint16_t>(src);
+                    cc.b = 0;
+                    A.arena[at++] = cc;
+                }
+            }
+            pos += tot;
+        }
+        if (tid == 0) {
+            lv.cell_list[i] = {loff, cnt, new_root, 0u};
+            lv.cell_tape[i] = aok ? TapeRef{static_cast<uint32_t>(a64), etot, bt.n_regs,
+                                             static_cast<uint32_t>(bt.root) |
+                                                 (static_cast<uint32_t>(bt.root_kind) << 16)}
+                                  : T;
+        }
+        __syncthreads();
     }
 }
 
@@ -2009,6 +2257,18 @@ int level_from_resolution(const double lo[3], const double hi[3], double min_fea
     return static_cast<int>(l);
 }
 
+/// Cells per level up to which a whole block works on each cell
+/// (kBlockModeCells; LFB_BLOCK_MODE_CELLS overrides it, for the parity tests).
+uint32_t block_mode_cells()
+{
+    static long v = -1;
+    if (v < 0) {
+        const char* e = std::getenv("LFB_BLOCK_MODE_CELLS");
+        v = e ? std::max(0L, std::atol(e)) : static_cast<long>(kBlockModeCells);
+    }
+    return static_cast<uint32_t>(v);
+}
+
 /// Cells per level from which the interval stage switches to group mode
 /// (kGroupModeCells; the LFB_GROUP_MODE_CELLS environment variable overrides
 /// it, which the parity tests use to run both modes on small shapes).
@@ -2300,6 +2560,10 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
                             bt.n_regs, status, W.next_cell};
                 const uint32_t blocks = std::min<uint32_t>(group_warps / 4, (lv.n_groups + 3) / 4);
                 k_interval_group<<<std::max<uint32_t>(blocks, 1), 128, group_smem, s>>>(G, d);
+            } else if (lv.n_cells <= block_mode_cells()) {
+                const uint32_t blocks = std::min<uint32_t>(
+                    std::min<uint32_t>(scratch_warps, device_sm_count() * 2), lv.n_cells);
+                k_interval_block<<<std::max<uint32_t>(blocks, 1), kBlockThreads, 0, s>>>(W, d);
             } else {
                 const uint32_t warps = std::min<uint32_t>(scratch_warps, (lv.n_cells + 7) / 8 * 8);
                 k_interval_wide<<<warps / 8, 256, wide_smem, s>>>(W, d);

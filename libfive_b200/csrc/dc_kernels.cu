@@ -1437,24 +1437,35 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
     const int E = S->nslots;
 
     // --- edge search: 4 rounds of 16 points (dc_tree.inl:326-410) -------
-    // One pass evaluates up to eight edges: sub-batch k of a lane holds
-    // sample j = lane & 15 of edge base + 2k + (lane >> 4).
+    // Each round samples an edge's bracket [t0, t1] at 16 evenly spaced
+    // points j = 0..15 and keeps [s(j-1), s(j)] around the first sample j >= 1
+    // that is outside; failing that, the last one, unless it is an inside
+    // zero.  s(0) = t0 is never tested, and s(15) = t1 is the previous
+    // round's outside end (round 1: the corner known to be outside), which is
+    // never an inside zero, so the outcome is "first outside j in 1..14,
+    // else 15": only 14 samples per edge are evaluated.  One pass holds nine
+    // edges (126 of the 4 x 32 sample slots): slot p = 32k + lane of
+    // sub-batch k is sample 1 + p % 14 of edge base + p / 14.  Most groups
+    // have nine crossing edges, one pass per round.
     auto sample = [&](int slot, int j, double q[3]) {
         const double frac = j / (16 - 1.0);
         const EdgeSlot& es = W->e[slot];
         for (int k = 0; k < 3; ++k) q[k] = es.t0[k] * (1 - frac) + es.t1[k] * frac;
     };
+    constexpr int kEdgesPerPass = 9, kSamples = 14;
     for (int round = 0; round < 4; ++round) {
-        for (int base = 0; base < E; base += 8) {
-            const int j = lane & 15;
+        for (int base = 0; base < E; base += kEdgesPerPass) {
             float qx[4] = {0, 0, 0, 0}, qy[4] = {0, 0, 0, 0}, qz[4] = {0, 0, 0, 0};
+            bool act[4];
             int n_act = 0;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                const int slot = base + 2 * k + (lane >> 4);
-                if (slot < E) {
+                const int p = 32 * k + lane;
+                const int slot = base + p / kSamples;
+                act[k] = p < kEdgesPerPass * kSamples && slot < E;
+                if (act[k]) {
                     double q[3];
-                    sample(slot, j, q);
+                    sample(slot, 1 + p % kSamples, q);
                     qx[k] = static_cast<float>(q[0]);
                     qy[k] = static_cast<float>(q[1]);
                     qz[k] = static_cast<float>(q[2]);
@@ -1467,17 +1478,15 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
                                           make_float4(qz[0], qz[1], qz[2], qz[3]));
             my_evals += static_cast<uint64_t>(__reduce_add_sync(0xffffffffu, n_act)) * tr.len;
             const float vs[4] = {v4.x, v4.y, v4.z, v4.w};
+            uint32_t term[4];
+#pragma unroll
             for (int k = 0; k < 4; ++k) {
-                const int kbase = base + 2 * k;
-                if (kbase >= E) break;
-                const int slot = kbase + (lane >> 4);
-                const bool active = slot < E;
                 const float v = vs[k];
                 // A sample exactly on the surface is resolved with
                 // FeatureEvaluator::isInside: for a point without tied
                 // min/max that is "gradient is non-zero" (one feature),
                 // otherwise the full feature search.
-                const bool zero = active && j >= 1 && v == 0;
+                const bool zero = act[k] && v == 0;
                 bool inside = true;
                 if (__any_sync(0xffffffffu, zero)) {
                     bool amb = false, plain = false;
@@ -1502,39 +1511,29 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
                         if (lane == src) inside = in;
                     }
                 }
-                // dc_tree.inl:372-407: the bracket ends at the first sample
-                // that is outside (value > 0, or an exact zero that is not
-                // inside); failing that, at the last sample unless it is an
-                // inside zero.
-                const uint32_t term = __ballot_sync(0xffffffffu,
-                    active && j >= 1 && (v > 0 || (v == 0 && !inside)));
-                const uint32_t last_ok = __ballot_sync(0xffffffffu,
-                    active && j == 15 && !(v > 0) && !(v == 0));
-                double q[3] = {0, 0, 0};
-                if (active) sample(slot, j, q);
-                __syncwarp();
-                for (int h = 0; h < 2; ++h) {
-                    const int s = kbase + h;
-                    if (s >= E) break;
-                    const uint32_t ht = (term >> (16 * h)) & 0xffff;
-                    int pick = -1;
-                    if (ht) pick = __ffs(ht) - 1;
-                    else if ((last_ok >> (16 * h + 15)) & 1) pick = 15;
-                    if (pick > 0) {
-                        const int lo_lane = 16 * h + pick - 1, hi_lane = 16 * h + pick;
-                        double nt0[3], nt1[3];
-                        for (int c = 0; c < 3; ++c) {
-                            nt0[c] = __shfl_sync(0xffffffffu, q[c], lo_lane);
-                            nt1[c] = __shfl_sync(0xffffffffu, q[c], hi_lane);
-                        }
-                        if (lane == 0) {
-                            EdgeSlot& es = W->e[s];
-                            for (int c = 0; c < 3; ++c) { es.t0[c] = nt0[c]; es.t1[c] = nt1[c]; }
-                        }
-                    }
-                    __syncwarp();
-                }
+                term[k] = __ballot_sync(0xffffffffu, act[k] && (v > 0 || (v == 0 && !inside)));
             }
+            // New brackets, one lane per edge, from the old ones.
+            if (lane < kEdgesPerPass && base + lane < E) {
+                const int p0 = kSamples * lane;
+                const int w0 = p0 >> 5, sh = p0 & 31;
+                uint32_t lo_w = 0, hi_w = 0;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    if (k == w0) lo_w = term[k];
+                    if (k == w0 + 1) hi_w = term[k];
+                }
+                const uint64_t bits = ((static_cast<uint64_t>(hi_w) << 32) | lo_w) >> sh;
+                const uint32_t t = static_cast<uint32_t>(bits) & ((1u << kSamples) - 1);
+                const int pick = t ? __ffs(t) : 15;   // sample index of the outside end
+                const int s_ = base + lane;
+                double nt0[3], nt1[3];
+                sample(s_, pick - 1, nt0);
+                sample(s_, pick, nt1);
+                EdgeSlot& es = W->e[s_];
+                for (int c = 0; c < 3; ++c) { es.t0[c] = nt0[c]; es.t1[c] = nt1[c]; }
+            }
+            __syncwarp();
         }
     }
 
@@ -2739,6 +2738,15 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
             unsigned long long sec[8] = {0, 0, 0, 0, 0, 0, 0, 0};
             for (uint32_t k = 0; k < n_leaf_groups; ++k) {
                 for (int q = 0; q < 8; ++q) sec[q] += pf[8 * k + q];
+            }
+            {
+                std::map<uint32_t, uint64_t> eh;
+                for (uint32_t k = 0; k < n_leaf_groups; ++k) ++eh[static_cast<uint32_t>(pf[8 * k + 3])];
+                std::fprintf(stderr, "[lfb] crossing edges per group:");
+                for (const auto& h : eh) {
+                    std::fprintf(stderr, " %u:%llu", h.first, static_cast<unsigned long long>(h.second));
+                }
+                std::fprintf(stderr, "\n");
             }
             std::fprintf(stderr, "[lfb] leaf cycles total %llu: corners %llu, edge search %llu, "
                          "gradients+QEF %llu, vertices %llu; features %llu in %llu calls\n",

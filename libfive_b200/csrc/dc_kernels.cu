@@ -26,6 +26,7 @@
 // reference's scalar code, so the octree and the mesh are reproducible.
 #include <cub/cub.cuh>
 #include <sys/mman.h>
+#include <thread>
 #include <cstdlib>
 #include <cstring>
 
@@ -2335,42 +2336,41 @@ libfive_mesh* MeshOut::release()
 
 namespace {
 
-/// Device -> pageable host copy through two pinned staging buffers, so that
-/// the PCIe transfer of one chunk overlaps the host copy of the previous.
+/// Device -> pageable host copy: one transfer into a pinned staging buffer
+/// (grow-only, kept between calls), then a host copy split over a few
+/// threads (a single thread's memcpy is the slow part of a mesh download).
 bool download(void* dst, const void* src, size_t bytes, cudaStream_t s)
 {
-    constexpr size_t kChunk = size_t(8) << 20;
-    static void* pinned[2] = {nullptr, nullptr};
-    static cudaEvent_t done[2];
-    if (!pinned[0]) {
-        for (int b = 0; b < 2; ++b) {
-            if (!cuda_ok(cudaMallocHost(&pinned[b], kChunk), "pinned staging") ||
-                !cuda_ok(cudaEventCreateWithFlags(&done[b], cudaEventDisableTiming),
-                         "staging event")) {
-                return false;
-            }
-        }
+    static void* pinned = nullptr;
+    static size_t pinned_bytes = 0;
+    if (bytes == 0) return true;
+    if (bytes > pinned_bytes) {
+        if (pinned) cudaFreeHost(pinned);
+        pinned = nullptr;
+        pinned_bytes = 0;
+        const size_t want = std::max<size_t>(bytes + bytes / 4, size_t(8) << 20);
+        if (!cuda_ok(cudaMallocHost(&pinned, want), "pinned staging")) return false;
+        pinned_bytes = want;
     }
-    const size_t n = (bytes + kChunk - 1) / kChunk;
-    auto len = [&](size_t i) { return std::min(kChunk, bytes - i * kChunk); };
-    auto drain = [&](size_t i) {
-        const int b = static_cast<int>(i & 1);
-        if (!cuda_ok(cudaEventSynchronize(done[b]), "download")) return false;
-        std::memcpy(static_cast<char*>(dst) + i * kChunk, pinned[b], len(i));
-        return true;
+    if (!cuda_ok(cudaMemcpyAsync(pinned, src, bytes, cudaMemcpyDeviceToHost, s), "download") ||
+        !cuda_ok(cudaStreamSynchronize(s), "download")) {
+        return false;
+    }
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t n_threads = std::min<size_t>(std::min<unsigned>(hw, 8u),
+                                              std::max<size_t>(1, bytes >> 22));
+    const size_t part = (bytes + n_threads - 1) / n_threads;
+    auto copy = [&](size_t t) {
+        const size_t lo = t * part, hi = std::min(bytes, lo + part);
+        if (lo < hi) {
+            std::memcpy(static_cast<char*>(dst) + lo, static_cast<const char*>(pinned) + lo,
+                        hi - lo);
+        }
     };
-    for (size_t i = 0; i < n; ++i) {
-        const int b = static_cast<int>(i & 1);
-        if (i >= 2 && !drain(i - 2)) return false;
-        if (!cuda_ok(cudaMemcpyAsync(pinned[b], static_cast<const char*>(src) + i * kChunk,
-                                     len(i), cudaMemcpyDeviceToHost, s), "download") ||
-            !cuda_ok(cudaEventRecord(done[b], s), "download")) {
-            return false;
-        }
-    }
-    for (size_t i = n >= 2 ? n - 2 : 0; i < n; ++i) {
-        if (!drain(i)) return false;
-    }
+    std::vector<std::thread> pool;
+    for (size_t t = 1; t < n_threads; ++t) pool.emplace_back(copy, t);
+    copy(0);
+    for (auto& th : pool) th.join();
     return true;
 }
 

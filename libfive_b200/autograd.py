@@ -1,0 +1,51 @@
+"""torch.autograd binding of the batched GPU tapes.
+
+`shape_value(tape, x, y, z, vars=None)` returns f at the points (CUDA float32
+tensors of one shape) and is differentiable with respect to the point
+coordinates and, when given, to the free variables (`vars`: a 1-D CUDA
+float32 tensor of the tape's variables in `tape.var_ids()` order).  The
+forward pass is lfb_eval_values, the backward pass the reverse-mode
+lfb_eval_grad: one launch pair per call, no CPU work on the data.
+"""
+import torch
+
+from .shape import Tape
+
+
+def _stream():
+    return torch.cuda.current_stream().cuda_stream
+
+
+class _ShapeValue(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, tape, x, y, z, vars_):
+        if vars_ is not None:
+            tape.set_vars(dict(zip(tape.var_ids(), vars_.detach().cpu().tolist())))
+        x, y, z = (t.detach().contiguous() for t in (x, y, z))
+        f = torch.empty_like(x)
+        tape.values(x, y, z, out=f, stream=_stream())
+        ctx.tape = tape
+        ctx.has_vars = vars_ is not None
+        ctx.save_for_backward(x, y, z)
+        return f
+
+    @staticmethod
+    def backward(ctx, grad_f):
+        x, y, z = ctx.saved_tensors
+        tape = ctx.tape
+        seed = grad_f.detach().contiguous()
+        need = ctx.needs_input_grad
+        gx = torch.empty_like(x) if need[1] else None
+        gy = torch.empty_like(x) if need[2] else None
+        gz = torch.empty_like(x) if need[3] else None
+        gv = None
+        if ctx.has_vars and need[4]:
+            gv = torch.zeros(tape.n_vars, dtype=torch.float32, device=x.device)
+        if gx is not None or gy is not None or gz is not None or gv is not None:
+            tape.grad(x, y, z, seed=seed, gx=gx, gy=gy, gz=gz, gvars=gv, stream=_stream())
+        return None, gx, gy, gz, gv
+
+
+def shape_value(tape: Tape, x, y, z, vars=None):
+    """f(x, y, z) of a Tape as a differentiable torch operation."""
+    return _ShapeValue.apply(tape, x, y, z, vars)

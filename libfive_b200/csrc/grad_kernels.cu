@@ -1,0 +1,379 @@
+// Gradients with respect to free variables and point coordinates.
+//
+//  * k_jacobian: JacobianEvaluator::gradient (eval_jacobian.cpp:49-115) in
+//    its own forward mode.  One thread per (point, three variables): X, Y, Z
+//    carry zero tangents, variable k0 + c carries a unit tangent in slot c,
+//    and CONST_VAR clears tangents (clear_vars).  Each output is the same
+//    sequence of float operations as the reference's per-variable column.
+//  * k_grad_forward / k_grad_backward: reverse mode (the reference has none).
+//    The forward pass stores every clause's local partials (the forward
+//    derivative rules of DerivArrayEvaluator, eval_deriv_array.cpp:119-256,
+//    applied to unit tangents, so min / max / abs pick the same branch); the
+//    backward pass walks the register tape from the end, one adjoint per
+//    register, and sends variable adjoints to a warp-reduced atomic sum.
+#include <cfloat>
+
+#include "eval_api.hpp"
+#include "eval_kernels.cuh"
+#include "libfive_b200.h"
+
+namespace lfb {
+
+namespace {
+
+__device__ __forceinline__ D4 jac_fetch(uint8_t kind, uint16_t idx, const float* R,
+                                        int tid, int B, const float* __restrict__ cp,
+                                        uint32_t n_const, uint32_t k0)
+{
+    if (kind == OPND_REG) {
+        const float* r = R + idx * 4 * B + tid;
+        return {r[0], r[B], r[2 * B], r[3 * B]};
+    }
+    const float v = __ldg(cp + idx);
+    if (kind == OPND_VAR) {
+        const uint32_t k = idx - n_const;
+        return {v, k == k0 ? 1.0f : 0.0f, k == k0 + 1 ? 1.0f : 0.0f, k == k0 + 2 ? 1.0f : 0.0f};
+    }
+    return {v, 0.0f, 0.0f, 0.0f};
+}
+
+__global__ void __launch_bounds__(128)
+k_jacobian(DevTape t, uint32_t n, uint32_t n_vars, const float* __restrict__ X,
+           const float* __restrict__ Y, const float* __restrict__ Z, float* __restrict__ out)
+{
+    extern __shared__ float smem[];
+    const int B = blockDim.x;
+    const int tid = threadIdx.x;
+    const uint32_t ntrip = (n_vars + 2) / 3;
+    const uint64_t items = static_cast<uint64_t>(n) * ntrip;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * B;
+    float* R = smem;
+    for (uint64_t it = static_cast<uint64_t>(blockIdx.x) * B + tid; it - tid < items;
+         it += stride) {
+        const bool ok = it < items;
+        const uint32_t i = ok ? static_cast<uint32_t>(it / ntrip) : 0u;
+        const uint32_t k0 = ok ? static_cast<uint32_t>(it % ntrip) * 3 : 0u;
+        const float p[3] = {ok ? X[i] : 0.0f, ok ? Y[i] : 0.0f, ok ? Z[i] : 0.0f};
+        for (int a = 0; a < 3; ++a) {
+            float* r = R + a * 4 * B + tid;
+            r[0] = p[a];
+            r[B] = 0.0f;
+            r[2 * B] = 0.0f;
+            r[3 * B] = 0.0f;
+        }
+        for (uint32_t c = 0; c < t.n; ++c) {
+            const uint2 raw = __ldg(reinterpret_cast<const uint2*>(t.clauses + c));
+            const uint8_t o = raw.x & 0xff;
+            const uint8_t kinds = (raw.x >> 8) & 0xff;
+            const D4 a = jac_fetch(kinds & 3, raw.y & 0xffff, R, tid, B, t.cpool, t.n_const, k0);
+            const D4 b = jac_fetch((kinds >> 2) & 3, raw.y >> 16, R, tid, B, t.cpool, t.n_const, k0);
+            const D4 d = dv_deriv(o, a, b, true);
+            float* r = R + (raw.x >> 16) * 4 * B + tid;
+            r[0] = d.v; r[B] = d.dx; r[2 * B] = d.dy; r[3 * B] = d.dz;
+        }
+        if (ok) {
+            const D4 d = jac_fetch(t.root_kind, t.root, R, tid, B, t.cpool, t.n_const, k0);
+            float* row = out + static_cast<size_t>(i) * n_vars;
+            row[k0] = d.dx;
+            if (k0 + 1 < n_vars) row[k0 + 1] = d.dy;
+            if (k0 + 2 < n_vars) row[k0 + 2] = d.dz;
+        }
+    }
+}
+
+__device__ __forceinline__ float gv_fetch(uint8_t kind, uint16_t idx, const float* R, int tid,
+                                          int B, const float* __restrict__ cp)
+{
+    return kind == OPND_REG ? R[idx * B + tid] : __ldg(cp + idx);
+}
+
+/// Forward pass of the reverse mode: value of every clause, and its local
+/// partials d out / d a, d out / d b stored at P[c * m + i] (one float2).
+__global__ void __launch_bounds__(128)
+k_grad_forward(DevTape t, uint32_t m, const float* __restrict__ X,
+               const float* __restrict__ Y, const float* __restrict__ Z,
+               float2* __restrict__ P, float* __restrict__ f)
+{
+    extern __shared__ float smem[];
+    const int B = blockDim.x;
+    const int tid = threadIdx.x;
+    const uint32_t i = blockIdx.x * B + tid;
+    float* R = smem;
+    const bool ok = i < m;
+    R[0 * B + tid] = ok ? X[i] : 0.0f;
+    R[1 * B + tid] = ok ? Y[i] : 0.0f;
+    R[2 * B + tid] = ok ? Z[i] : 0.0f;
+    for (uint32_t c = 0; c < t.n; ++c) {
+        const uint2 raw = __ldg(reinterpret_cast<const uint2*>(t.clauses + c));
+        const uint8_t o = raw.x & 0xff;
+        const uint8_t kinds = (raw.x >> 8) & 0xff;
+        const float av = gv_fetch(kinds & 3, raw.y & 0xffff, R, tid, B, t.cpool);
+        const float bv = gv_fetch((kinds >> 2) & 3, raw.y >> 16, R, tid, B, t.cpool);
+        // Unit tangents: dx slot = d/da, dy slot = d/db (CONST_VAR passes
+        // its argument's tangent here; the backward pass blocks it for
+        // variables).
+        const D4 d = dv_deriv(o, D4{av, 1.0f, 0.0f, 0.0f}, D4{bv, 0.0f, 1.0f, 0.0f}, false);
+        R[(raw.x >> 16) * B + tid] = d.v;
+        if (ok) P[static_cast<size_t>(c) * m + i] = make_float2(d.dx, d.dy);
+    }
+    if (ok && f) f[i] = gv_fetch(t.root_kind, t.root, R, tid, B, t.cpool);
+}
+
+__device__ __forceinline__ float warp_sum(float v)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+/// Backward pass: adjoints per register from the root (seeded with s_i) to
+/// the start; X, Y, Z adjoints are registers 0-2 at the end.  With
+/// block_const_var, CONST_VAR stops the adjoint (variable gradients, as
+/// clear_vars does in the forward Jacobian); otherwise it passes through
+/// (point gradients, as in DerivArrayEvaluator).
+__global__ void __launch_bounds__(128)
+k_grad_backward(DevTape t, uint32_t m, const float2* __restrict__ P,
+                const float* __restrict__ seed, float* __restrict__ gx,
+                float* __restrict__ gy, float* __restrict__ gz, float* __restrict__ gvars,
+                int block_const_var)
+{
+    extern __shared__ float smem[];
+    const int B = blockDim.x;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const uint32_t i = blockIdx.x * B + tid;
+    const bool ok = i < m;
+    float* A = smem;
+    for (uint32_t r = 0; r < t.n_regs; ++r) A[r * B + tid] = 0.0f;
+    const float s0 = ok ? (seed ? seed[i] : 1.0f) : 0.0f;
+    if (t.root_kind == OPND_REG) {
+        A[t.root * B + tid] = s0;
+    } else if (t.root_kind == OPND_VAR && gvars) {
+        const float w = warp_sum(s0);
+        if (lane == 0 && w != 0.0f) atomicAdd(gvars + (t.root - t.n_const), w);
+    }
+    for (int64_t c = static_cast<int64_t>(t.n) - 1; c >= 0; --c) {
+        const uint2 raw = __ldg(reinterpret_cast<const uint2*>(t.clauses + c));
+        const uint8_t o = raw.x & 0xff;
+        const uint8_t kinds = (raw.x >> 8) & 0xff;
+        const uint32_t ro = raw.x >> 16, ra = raw.y & 0xffff, rb = raw.y >> 16;
+        const float adj = A[ro * B + tid];
+        A[ro * B + tid] = 0.0f;
+        float2 pd = ok ? P[static_cast<size_t>(c) * m + i] : make_float2(0.0f, 0.0f);
+        if (block_const_var && o == op::CONST_VAR) pd = make_float2(0.0f, 0.0f);
+        const float ga = adj * pd.x;
+        const uint8_t ka = kinds & 3, kb = (kinds >> 2) & 3;
+        if (ka == OPND_REG) {
+            A[ra * B + tid] += ga;
+        } else if (ka == OPND_VAR && gvars) {
+            const float w = warp_sum(ga);
+            if (lane == 0 && w != 0.0f) atomicAdd(gvars + (ra - t.n_const), w);
+        }
+        if (dev_is_binary(o)) {
+            const float gb = adj * pd.y;
+            if (kb == OPND_REG) {
+                A[rb * B + tid] += gb;
+            } else if (kb == OPND_VAR && gvars) {
+                const float w = warp_sum(gb);
+                if (lane == 0 && w != 0.0f) atomicAdd(gvars + (rb - t.n_const), w);
+            }
+        }
+    }
+    if (ok) {
+        if (gx) gx[i] = A[0 * B + tid];
+        if (gy) gy[i] = A[1 * B + tid];
+        if (gz) gz[i] = A[2 * B + tid];
+    }
+}
+
+bool tape_has_const_var(const GpuTape& g)
+{
+    for (const RegClause& c : g.reg.clauses) {
+        if (c.op == op::CONST_VAR) return true;
+    }
+    return false;
+}
+
+/// Device buffers of a call on host data (grow-only, reused).
+struct GradStaging {
+    DevBuf in, out, partials;
+};
+
+GradStaging& grad_staging()
+{
+    static GradStaging s;
+    return s;
+}
+
+constexpr int kBlock = 128;
+
+bool set_smem(const void* fn, size_t bytes)
+{
+    if (bytes <= 48 * 1024) return true;
+    return cuda_ok(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(bytes)),
+                   "shared memory size");
+}
+
+int jacobian_device(GpuTape& g, uint64_t n, const float* x, const float* y, const float* z,
+                    float* out, cudaStream_t s)
+{
+    const DevTape t = g.dev();
+    const uint32_t nv = g.reg.n_vars;
+    if (nv == 0 || n == 0) return 0;
+    const size_t smem = static_cast<size_t>(t.n_regs) * kBlock * 4 * sizeof(float);
+    if (smem > 200 * 1024) return set_error(LFB_E_UNSUPPORTED, "tape needs too many registers");
+    if (!set_smem(reinterpret_cast<const void*>(k_jacobian), smem)) return LFB_E_CUDA;
+    const uint64_t kChunk = uint64_t(1) << 22;   // points per launch
+    for (uint64_t off = 0; off < n; off += kChunk) {
+        const uint32_t m = static_cast<uint32_t>(std::min(kChunk, n - off));
+        const uint64_t items = static_cast<uint64_t>(m) * ((nv + 2) / 3);
+        const uint64_t blocks = std::min<uint64_t>((items + kBlock - 1) / kBlock,
+                                                   static_cast<uint64_t>(device_sm_count()) * 64);
+        k_jacobian<<<static_cast<unsigned>(blocks), kBlock, smem, s>>>(
+            t, m, nv, x + off, y + off, z + off, out + off * nv);
+        if (!cuda_ok(cudaGetLastError(), "jacobian kernel")) return LFB_E_CUDA;
+        note_launches(1);
+    }
+    return 0;
+}
+
+int grad_device(GpuTape& g, uint64_t n, const float* x, const float* y, const float* z,
+                const float* seed, float* f, float* gx, float* gy, float* gz, float* gvars,
+                cudaStream_t s)
+{
+    const DevTape t = g.dev();
+    if (n == 0) return 0;
+    const size_t smem = static_cast<size_t>(t.n_regs) * kBlock * sizeof(float);
+    if (smem > 200 * 1024) return set_error(LFB_E_UNSUPPORTED, "tape needs too many registers");
+    if (!set_smem(reinterpret_cast<const void*>(k_grad_forward), smem) ||
+        !set_smem(reinterpret_cast<const void*>(k_grad_backward), smem)) {
+        return LFB_E_CUDA;
+    }
+    // Partials take 8 bytes per clause and point: points per launch so that
+    // they stay within 1 GiB.
+    const uint64_t per_point = std::max<uint64_t>(8ull * t.n, 8);
+    const uint64_t chunk = std::max<uint64_t>(kBlock, std::min<uint64_t>(
+        (1ull << 30) / per_point / kBlock * kBlock, uint64_t(1) << 22));
+    auto& st = grad_staging();
+    if (!st.partials.reserve(std::min(chunk, n) * per_point)) return LFB_E_CUDA;
+    float2* P = st.partials.as<float2>();
+    const bool has_cv = tape_has_const_var(g);
+    const bool want_xyz = gx || gy || gz;
+    for (uint64_t off = 0; off < n; off += chunk) {
+        const uint32_t m = static_cast<uint32_t>(std::min(chunk, n - off));
+        const unsigned blocks = (m + kBlock - 1) / kBlock;
+        k_grad_forward<<<blocks, kBlock, smem, s>>>(t, m, x + off, y + off, z + off, P,
+                                                    f ? f + off : nullptr);
+        note_launches(1);
+        const float* sd = seed ? seed + off : nullptr;
+        if (!has_cv) {
+            if (want_xyz || gvars) {
+                k_grad_backward<<<blocks, kBlock, smem, s>>>(
+                    t, m, P, sd, gx ? gx + off : nullptr, gy ? gy + off : nullptr,
+                    gz ? gz + off : nullptr, gvars, 0);
+                note_launches(1);
+            }
+        } else {
+            // CONST_VAR passes point gradients but blocks variable ones.
+            if (want_xyz) {
+                k_grad_backward<<<blocks, kBlock, smem, s>>>(
+                    t, m, P, sd, gx ? gx + off : nullptr, gy ? gy + off : nullptr,
+                    gz ? gz + off : nullptr, nullptr, 0);
+                note_launches(1);
+            }
+            if (gvars) {
+                k_grad_backward<<<blocks, kBlock, smem, s>>>(
+                    t, m, P, sd, nullptr, nullptr, nullptr, gvars, 1);
+                note_launches(1);
+            }
+        }
+        if (!cuda_ok(cudaGetLastError(), "gradient kernels")) return LFB_E_CUDA;
+    }
+    return 0;
+}
+
+}  // namespace
+
+int eval_jacobian(GpuTape& g, uint64_t n, const float* x, const float* y, const float* z,
+                  float* out, cudaStream_t s, bool device)
+{
+    if (!require_device()) return LFB_E_CUDA;
+    if (!x || !y || !z || (!out && g.reg.n_vars)) {
+        return set_error(LFB_E_INVALID, "lfb_eval_jacobian: null argument");
+    }
+    std::lock_guard<std::mutex> lock(global_mutex());
+    if (device) return jacobian_device(g, n, x, y, z, out, s);
+    if (n == 0 || g.reg.n_vars == 0) return 0;
+    auto& st = grad_staging();
+    const size_t nv = g.reg.n_vars;
+    if (!st.in.reserve(n * 3 * sizeof(float)) || !st.out.reserve(n * nv * sizeof(float))) {
+        return LFB_E_CUDA;
+    }
+    float* d = st.in.as<float>();
+    const size_t b = n * sizeof(float);
+    cudaStream_t s0 = 0;
+    if (!cuda_ok(cudaMemcpyAsync(d, x, b, cudaMemcpyHostToDevice, s0), "copy") ||
+        !cuda_ok(cudaMemcpyAsync(d + n, y, b, cudaMemcpyHostToDevice, s0), "copy") ||
+        !cuda_ok(cudaMemcpyAsync(d + 2 * n, z, b, cudaMemcpyHostToDevice, s0), "copy")) {
+        return LFB_E_CUDA;
+    }
+    const int rc = jacobian_device(g, n, d, d + n, d + 2 * n, st.out.as<float>(), s0);
+    if (rc) return rc;
+    if (!cuda_ok(cudaMemcpyAsync(out, st.out.ptr, n * nv * sizeof(float),
+                                 cudaMemcpyDeviceToHost, s0), "copy")) {
+        return LFB_E_CUDA;
+    }
+    return cuda_ok(cudaStreamSynchronize(s0), "sync") ? 0 : LFB_E_CUDA;
+}
+
+int eval_grad(GpuTape& g, uint64_t n, const float* x, const float* y, const float* z,
+              const float* seed, float* f, float* gx, float* gy, float* gz, float* gvars,
+              cudaStream_t s, bool device)
+{
+    if (!require_device()) return LFB_E_CUDA;
+    if (!x || !y || !z) return set_error(LFB_E_INVALID, "lfb_eval_grad: null argument");
+    std::lock_guard<std::mutex> lock(global_mutex());
+    if (device) return grad_device(g, n, x, y, z, seed, f, gx, gy, gz, gvars, s);
+    if (n == 0) return 0;
+    // Host arrays: inputs x, y, z, seed; outputs f, gx, gy, gz; gvars.
+    auto& st = grad_staging();
+    const size_t nv = g.reg.n_vars;
+    if (!st.in.reserve(n * 4 * sizeof(float)) ||
+        !st.out.reserve((n * 4 + std::max<size_t>(nv, 1)) * sizeof(float))) {
+        return LFB_E_CUDA;
+    }
+    float* d = st.in.as<float>();
+    float* o = st.out.as<float>();
+    const size_t b = n * sizeof(float);
+    cudaStream_t s0 = 0;
+    const float* ins[4] = {x, y, z, seed};
+    for (int k = 0; k < 4; ++k) {
+        if (ins[k] && !cuda_ok(cudaMemcpyAsync(d + k * n, ins[k], b, cudaMemcpyHostToDevice, s0),
+                               "copy")) {
+            return LFB_E_CUDA;
+        }
+    }
+    float* gv = gvars ? o + 4 * n : nullptr;
+    if (gv && !cuda_ok(cudaMemcpyAsync(gv, gvars, nv * sizeof(float), cudaMemcpyHostToDevice, s0),
+                       "copy")) {
+        return LFB_E_CUDA;
+    }
+    float* outs[4] = {f, gx, gy, gz};
+    const int rc = grad_device(g, n, d, d + n, d + 2 * n, seed ? d + 3 * n : nullptr,
+                               f ? o : nullptr, gx ? o + n : nullptr, gy ? o + 2 * n : nullptr,
+                               gz ? o + 3 * n : nullptr, gv, s0);
+    if (rc) return rc;
+    for (int k = 0; k < 4; ++k) {
+        if (outs[k] && !cuda_ok(cudaMemcpyAsync(outs[k], o + k * n, b, cudaMemcpyDeviceToHost, s0),
+                                "copy")) {
+            return LFB_E_CUDA;
+        }
+    }
+    if (gv && !cuda_ok(cudaMemcpyAsync(gvars, gv, nv * sizeof(float), cudaMemcpyDeviceToHost, s0),
+                       "copy")) {
+        return LFB_E_CUDA;
+    }
+    return cuda_ok(cudaStreamSynchronize(s0), "sync") ? 0 : LFB_E_CUDA;
+}
+
+}  // namespace lfb

@@ -1042,33 +1042,55 @@ static __device__ __noinline__ float4 warp_value4(const DevTape& bt, const RegCl
         R[(8 + k) * 32 + lane] = zs[k];
     }
     float* Rl = R + lane;
+    // The previous clause's result stays in registers: most clauses read it,
+    // which takes a shared-memory round trip off the dependency chain.  The
+    // next clause is fetched one iteration ahead.
+    uint32_t last = 0xffffffffu;
+    float lv[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    uint2 next = len ? __ldg(reinterpret_cast<const uint2*>(cl)) : make_uint2(0, 0);
     for (uint32_t c = 0; c < len; ++c) {
-        const uint2 raw = __ldg(reinterpret_cast<const uint2*>(cl + c));
+        const uint2 raw = next;
+        if (c + 1 < len) next = __ldg(reinterpret_cast<const uint2*>(cl + c + 1));
         const uint8_t o = raw.x & 0xff;
         const uint32_t kinds = (raw.x >> 8) & 0xff;
+        const uint32_t ra = raw.y & 0xffff, rb = raw.y >> 16, ro = raw.x >> 16;
         float a[4], b[4], r[4];
         if ((kinds & 3) == OPND_REG) {
-            const float* p = Rl + (raw.y & 0xffff) * 128;
+            if (ra == last) {
 #pragma unroll
-            for (int k = 0; k < 4; ++k) a[k] = p[32 * k];
+                for (int k = 0; k < 4; ++k) a[k] = lv[k];
+            } else {
+                const float* p = Rl + ra * 128;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) a[k] = p[32 * k];
+            }
         } else {
-            const float v = __ldg(bt.cpool + (raw.y & 0xffff));
+            const float v = __ldg(bt.cpool + ra);
 #pragma unroll
             for (int k = 0; k < 4; ++k) a[k] = v;
         }
         if (((kinds >> 2) & 3) == OPND_REG) {
-            const float* p = Rl + (raw.y >> 16) * 128;
+            if (rb == last) {
 #pragma unroll
-            for (int k = 0; k < 4; ++k) b[k] = p[32 * k];
+                for (int k = 0; k < 4; ++k) b[k] = lv[k];
+            } else {
+                const float* p = Rl + rb * 128;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) b[k] = p[32 * k];
+            }
         } else {
-            const float v = __ldg(bt.cpool + (raw.y >> 16));
+            const float v = __ldg(bt.cpool + rb);
 #pragma unroll
             for (int k = 0; k < 4; ++k) b[k] = v;
         }
         dv_value4(o, a, b, r);
-        float* q = Rl + (raw.x >> 16) * 128;
+        float* q = Rl + ro * 128;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) q[32 * k] = r[k];
+        for (int k = 0; k < 4; ++k) {
+            q[32 * k] = r[k];
+            lv[k] = r[k];
+        }
+        last = ro;
     }
     float out[4];
     if (bt.root_kind == OPND_REG) {

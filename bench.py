@@ -76,6 +76,25 @@ def dist_setup(args):
     return world, rank, local
 
 
+def rank_seed(rank):
+    """Weak scaling: every rank meshes its own seeded shape."""
+    return SEED_BASE + rank
+
+
+def combine_ranks(total_ms, e2e_ms, world, steps, pg, device):
+    """Max over ranks of the device-timed totals (one all-reduce; the only
+    collective of the run) and the whole-job meshes/s: every rank meshes
+    `steps` shapes in the slowest rank's time."""
+    import torch
+    times = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=device)
+    if pg:
+        pg.all_reduce(times, op=pg.ReduceOp.MAX)
+    total_ms, e2e_ms = times.tolist()
+    value = world * steps / (total_ms / 1000.0)
+    e2e_value = world * steps / (e2e_ms / 1000.0) if e2e_ms > 0 else None
+    return total_ms, e2e_ms, value, e2e_value
+
+
 def build_shape(seed):
     from libfive_b200 import workloads
     return workloads.random_csg(N_PRIMS, seed=seed)
@@ -235,7 +254,7 @@ def run_ours(args, world, rank, local):
     from libfive_b200 import ffi
     from libfive_b200.shape import Tape
     lib = ffi.load()
-    shape = build_shape(SEED_BASE + rank)
+    shape = build_shape(rank_seed(rank))
     tape = Tape(shape)
     wv, wg, n_clauses = tape_weights(shape)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
@@ -298,12 +317,8 @@ def run_ours(args, world, rank, local):
         d2h = (st.vertices + 1) * 12 + st.triangles * 12
         del t
 
-    times = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device="cuda")
-    if pg:
-        pg.all_reduce(times, op=pg.ReduceOp.MAX)
-    total_ms, e2e_ms = times.tolist()
-    value = world * args.steps / (total_ms / 1000.0)
-    e2e_value = world * args.steps / (e2e_ms / 1000.0) if e2e_ms > 0 else None
+    total_ms, e2e_ms, value, e2e_value = combine_ranks(total_ms, e2e_ms, world, args.steps,
+                                                       pg, "cuda")
 
     if rank == 0:
         sm_mhz = clk.get("sm_mhz") or 1965.0

@@ -1856,28 +1856,51 @@ k_collapse_level(CollapseArgs A, int d)
 
     // Value at the vertex with a tape that is valid there: walk up from this
     // cell to the first ancestor whose (float) box contains the point
-    // (Tape::getBase, tape.cpp:188-209); the unpruned tape otherwise.
+    // (Tape::getBase, tape.cpp:188-209); the unpruned tape otherwise.  Any
+    // tape valid at the point gives the same value, so when this cell
+    // contains the vertex, the shortest one is taken instead: that of the
+    // deepest cell below it that contains the vertex and was ambiguous when
+    // its interval was evaluated (so has a pruned tape).
     const float vf[3] = {static_cast<float>(v[0]), static_cast<float>(v[1]),
                          static_cast<float>(v[2])};
+    auto contains = [&](int dd, uint32_t ii) {
+        double blo[3], bhi[3];
+        cell_bounds(o, dd, o.lv[dd].coords[ii], blo, bhi);
+        bool in = true;
+        for (int a = 0; a < 3; ++a) {
+            in &= vf[a] >= static_cast<float>(blo[a]) && vf[a] <= static_cast<float>(bhi[a]);
+        }
+        return in;
+    };
     TapeRef tr = root_tape_ref(A.bt);
-    {
+    if (contains(d, i)) {
         int dd = d;
         uint32_t ii = i;
-        while (dd >= 0) {
-            double blo[3], bhi[3];
-            cell_bounds(o, dd, o.lv[dd].coords[ii], blo, bhi);
-            bool in = true;
-            for (int a = 0; a < 3; ++a) {
-                in &= vf[a] >= static_cast<float>(blo[a]) &&
-                      vf[a] <= static_cast<float>(bhi[a]);
+        while (dd + 1 < o.levels) {
+            const int32_t k = o.lv[dd].child_group[ii];
+            if (k < 0) break;
+            bool found = false;
+            for (uint32_t j = 0; j < 8 && !found; ++j) {
+                const uint32_t c = 8 * static_cast<uint32_t>(k) + j;
+                if (o.lv[dd + 1].child_group[c] >= 0 && contains(dd + 1, c)) {
+                    ii = c;
+                    found = true;
+                }
             }
-            if (in) {
+            if (!found) break;
+            ++dd;
+        }
+        tr = o.lv[dd].cell_tape[ii];
+    } else {
+        int dd = d;
+        uint32_t ii = i;
+        while (dd > 0) {
+            ii = o.lv[dd].group_parent[ii >> 3];
+            --dd;
+            if (contains(dd, ii)) {
                 tr = o.lv[dd].cell_tape[ii];
                 break;
             }
-            if (dd == 0) break;
-            ii = o.lv[dd].group_parent[ii >> 3];
-            --dd;
         }
     }
     const float value = thread_value(with_tape(A.bt, tr), A.arena + tr.off, tr.len, csmem, tid, B,
@@ -2527,7 +2550,7 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
 
     // Deep levels (many cells, short tapes) switch to one warp per sibling
     // group over register tapes; every level below stays in that mode.
-    const uint32_t group_warps = static_cast<uint32_t>(device_sm_count()) * 16;
+    const uint32_t group_warps = static_cast<uint32_t>(device_sm_count()) * 32;
     const uint32_t gdec_cap = std::max<uint32_t>(bt.n_choices, 1);
     const size_t group_smem = group_smem_per_warp(bt.n_regs) * 4;
     uint8_t* gdec = ws.get<uint8_t>(K_GDEC, static_cast<size_t>(group_warps) * 8 * gdec_cap);
@@ -2798,8 +2821,15 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
         for (int d = L - 1; d >= 0; --d) {
             const uint32_t n = o.lv[d].n_cells;
             if (!n) continue;
+            const auto t_c = std::chrono::steady_clock::now();
             k_collapse_level<<<(n + block - 1) / block, block, smem, s>>>(C, d);
             ++n_launch;
+            if (debug_levels()) {
+                cudaStreamSynchronize(s);
+                std::fprintf(stderr, "[lfb] collapse depth %d: %u cells, %.3f ms\n", d, n,
+                             std::chrono::duration<double, std::milli>(
+                                 std::chrono::steady_clock::now() - t_c).count());
+            }
         }
         if (!cuda_ok(cudaGetLastError(), "collapse kernel")) return LFB_E_CUDA;
     }

@@ -1000,13 +1000,30 @@ __device__ __forceinline__ float warp_fetch_v(uint8_t kind, uint16_t idx,
     return kind == OPND_REG ? R[idx * 32 + lane] : __ldg(cp + idx);
 }
 
+/// The interpreters' register file: in the block's dynamic shared memory at
+/// byte offset `soff` (S = true: the compiler then emits shared-memory loads
+/// and stores, and knows they cannot alias anything else), or in global
+/// memory at `g` (tapes with too many registers).
+template <bool S>
+__device__ __forceinline__ float* regfile(uint32_t soff, float* g)
+{
+    if (S) {
+        extern __shared__ __align__(16) unsigned char rf_smem[];
+        return reinterpret_cast<float*>(rf_smem + soff);
+    }
+    return g;
+}
+
 /// Value of the tape at (x, y, z) for this lane, plus whether any min/max
 /// saw equal arguments (ArrayEvaluator::getAmbiguous, eval_array.cpp:197-217).
-static __device__ __noinline__ float warp_value(const DevTape& bt, const RegClause* cl,
-                            uint32_t len, float* R, int lane, float x,
-                            float y, float z, bool* ambig, uint64_t* evals,
-                            bool active = true)
+template <bool S>
+static __device__ __noinline__ float warp_value(const float* __restrict__ cpool, uint32_t root_kind,
+                                                uint32_t root, const RegClause* __restrict__ cl,
+                                                uint32_t len, uint32_t soff, float* Rg, int lane,
+                                                float x, float y, float z, bool* ambig,
+                                                uint64_t* evals, bool active)
 {
+    float* R = regfile<S>(soff, Rg);
     R[0 * 32 + lane] = x;
     R[1 * 32 + lane] = y;
     R[2 * 32 + lane] = z;
@@ -1015,23 +1032,27 @@ static __device__ __noinline__ float warp_value(const DevTape& bt, const RegClau
         const uint2 raw = __ldg(reinterpret_cast<const uint2*>(cl + c));
         const uint8_t o = raw.x & 0xff;
         const uint8_t kinds = (raw.x >> 8) & 0xff;
-        const float a = warp_fetch_v(kinds & 3, raw.y & 0xffff, R, lane, bt.cpool);
-        const float b = warp_fetch_v((kinds >> 2) & 3, raw.y >> 16, R, lane, bt.cpool);
+        const float a = warp_fetch_v(kinds & 3, raw.y & 0xffff, R, lane, cpool);
+        const float b = warp_fetch_v((kinds >> 2) & 3, raw.y >> 16, R, lane, cpool);
         if (o == op::MIN || o == op::MAX) amb |= (a == b);
         R[(raw.x >> 16) * 32 + lane] = dv_value(o, a, b);
     }
     if (ambig) *ambig = amb;
     const uint32_t act = __ballot_sync(0xffffffffu, active);
     if (evals && lane == 0) *evals += static_cast<uint64_t>(__popc(act)) * len;
-    return warp_fetch_v(bt.root_kind, bt.root, R, lane, bt.cpool);
+    return warp_fetch_v(root_kind, root, R, lane, cpool);
 }
 
 /// Values of the tape at four points per lane (the edge search): register
 /// r of point k lives at R[(4 r + k) * 32 + lane].
-static __device__ __noinline__ float4 warp_value4(const DevTape& bt, const RegClause* cl,
-                                                  uint32_t len, float* R, int lane,
+template <bool S>
+static __device__ __noinline__ float4 warp_value4(const float* __restrict__ cpool,
+                                                  uint32_t root_kind, uint32_t root,
+                                                  const RegClause* __restrict__ cl, uint32_t len,
+                                                  uint32_t soff, float* Rg, int lane,
                                                   float4 x, float4 y, float4 z)
 {
+    float* R = regfile<S>(soff, Rg);
     const float xs[4] = {x.x, x.y, x.z, x.w};
     const float ys[4] = {y.x, y.y, y.z, y.w};
     const float zs[4] = {z.x, z.y, z.z, z.w};
@@ -1065,7 +1086,7 @@ static __device__ __noinline__ float4 warp_value4(const DevTape& bt, const RegCl
                 for (int k = 0; k < 4; ++k) a[k] = p[32 * k];
             }
         } else {
-            const float v = __ldg(bt.cpool + ra);
+            const float v = __ldg(cpool + ra);
 #pragma unroll
             for (int k = 0; k < 4; ++k) a[k] = v;
         }
@@ -1079,7 +1100,7 @@ static __device__ __noinline__ float4 warp_value4(const DevTape& bt, const RegCl
                 for (int k = 0; k < 4; ++k) b[k] = p[32 * k];
             }
         } else {
-            const float v = __ldg(bt.cpool + rb);
+            const float v = __ldg(cpool + rb);
 #pragma unroll
             for (int k = 0; k < 4; ++k) b[k] = v;
         }
@@ -1093,11 +1114,11 @@ static __device__ __noinline__ float4 warp_value4(const DevTape& bt, const RegCl
         last = ro;
     }
     float out[4];
-    if (bt.root_kind == OPND_REG) {
+    if (root_kind == OPND_REG) {
 #pragma unroll
-        for (int k = 0; k < 4; ++k) out[k] = Rl[bt.root * 128 + 32 * k];
+        for (int k = 0; k < 4; ++k) out[k] = Rl[root * 128 + 32 * k];
     } else {
-        const float v = __ldg(bt.cpool + bt.root);
+        const float v = __ldg(cpool + root);
 #pragma unroll
         for (int k = 0; k < 4; ++k) out[k] = v;
     }
@@ -1115,35 +1136,6 @@ __device__ __forceinline__ D4 warp_fetch_d(uint8_t kind, uint16_t idx,
     return {__ldg(cp + idx), 0.0f, 0.0f, 0.0f};
 }
 
-static __device__ __noinline__ D4 warp_deriv(const DevTape& bt, const RegClause* cl, uint32_t len,
-                         float* R, int lane, float x, float y, float z,
-                         bool* ambig, uint64_t* evals, bool active = true)
-{
-    const float in[3] = {x, y, z};
-    for (int a = 0; a < 3; ++a) {
-        float* r = R + a * 128 + lane;
-        r[0] = in[a];
-        r[32] = a == 0 ? 1.0f : 0.0f;
-        r[64] = a == 1 ? 1.0f : 0.0f;
-        r[96] = a == 2 ? 1.0f : 0.0f;
-    }
-    bool amb = false;
-    for (uint32_t c = 0; c < len; ++c) {
-        const uint2 raw = __ldg(reinterpret_cast<const uint2*>(cl + c));
-        const uint8_t o = raw.x & 0xff;
-        const uint8_t kinds = (raw.x >> 8) & 0xff;
-        const D4 a = warp_fetch_d(kinds & 3, raw.y & 0xffff, R, lane, bt.cpool);
-        const D4 b = warp_fetch_d((kinds >> 2) & 3, raw.y >> 16, R, lane, bt.cpool);
-        if (o == op::MIN || o == op::MAX) amb |= (a.v == b.v);
-        const D4 r = dv_deriv(o, a, b, false);
-        float* out = R + (raw.x >> 16) * 128 + lane;
-        out[0] = r.v; out[32] = r.dx; out[64] = r.dy; out[96] = r.dz;
-    }
-    if (ambig) *ambig = amb;
-    const uint32_t act = __ballot_sync(0xffffffffu, active);
-    if (evals && lane == 0) *evals += static_cast<uint64_t>(__popc(act)) * len;
-    return warp_fetch_d(bt.root_kind, bt.root, R, lane, bt.cpool);
-}
 
 /// warp_deriv that also works out, for most points, FeatureEvaluator's
 /// feature list (eval_feature.cpp:171-372) without building it.  Every
@@ -1160,11 +1152,16 @@ static __device__ __noinline__ D4 warp_deriv(const DevTape& bt, const RegClause*
 /// *plain says the root is untainted: its single feature is then the
 /// returned gradient.  *ambig reports any tie (ArrayEvaluator::getAmbiguous).
 /// Tapes with more than 64 registers report every tie as not plain.
-static __device__ __noinline__ D4 warp_deriv_lite(const DevTape& bt, const RegClause* cl,
-                                                  uint32_t len, float* R, int lane, float x,
+template <bool S>
+static __device__ __noinline__ D4 warp_deriv_lite(const float* __restrict__ cpool,
+                                                  uint32_t root_kind, uint32_t root,
+                                                  uint32_t n_regs,
+                                                  const RegClause* __restrict__ cl, uint32_t len,
+                                                  uint32_t soff, float* Rg, int lane, float x,
                                                   float y, float z, bool* ambig, bool* plain,
                                                   uint64_t* evals, bool active)
 {
+    float* R = regfile<S>(soff, Rg);
     const float in[3] = {x, y, z};
     for (int a = 0; a < 3; ++a) {
         float* r = R + a * 128 + lane;
@@ -1173,7 +1170,7 @@ static __device__ __noinline__ D4 warp_deriv_lite(const DevTape& bt, const RegCl
         r[64] = a == 1 ? 1.0f : 0.0f;
         r[96] = a == 2 ? 1.0f : 0.0f;
     }
-    const bool trackable = bt.n_regs <= 64;
+    const bool trackable = n_regs <= 64;
     uint64_t taint = 0;
     bool amb = false, lost = false;
     for (uint32_t c = 0; c < len; ++c) {
@@ -1181,8 +1178,8 @@ static __device__ __noinline__ D4 warp_deriv_lite(const DevTape& bt, const RegCl
         const uint8_t o = raw.x & 0xff;
         const uint8_t kinds = (raw.x >> 8) & 0xff;
         const uint32_t ra = raw.y & 0xffff, rb = raw.y >> 16, ro = raw.x >> 16;
-        const D4 a = warp_fetch_d(kinds & 3, ra, R, lane, bt.cpool);
-        const D4 b = warp_fetch_d((kinds >> 2) & 3, rb, R, lane, bt.cpool);
+        const D4 a = warp_fetch_d(kinds & 3, ra, R, lane, cpool);
+        const D4 b = warp_fetch_d((kinds >> 2) & 3, rb, R, lane, cpool);
         const bool ta = (kinds & 3) == OPND_REG && ((taint >> (ra & 63)) & 1);
         const bool tbb = dev_is_binary(o) && ((kinds >> 2) & 3) == OPND_REG &&
                          ((taint >> (rb & 63)) & 1);
@@ -1225,14 +1222,14 @@ static __device__ __noinline__ D4 warp_deriv_lite(const DevTape& bt, const RegCl
         out[0] = r.v; out[32] = r.dx; out[64] = r.dy; out[96] = r.dz;
     }
     *ambig = amb;
-    *plain = !lost && !(bt.root_kind == OPND_REG && ((taint >> (bt.root & 63)) & 1));
+    *plain = !lost && !(root_kind == OPND_REG && ((taint >> (root & 63)) & 1));
     const uint32_t act = __ballot_sync(0xffffffffu, active);
     if (evals && lane == 0) *evals += static_cast<uint64_t>(__popc(act)) * len;
-    return warp_fetch_d(bt.root_kind, bt.root, R, lane, bt.cpool);
+    return warp_fetch_d(root_kind, root, R, lane, cpool);
 }
 
 constexpr size_t kLeafSmallBytes = (sizeof(LeafWarpShared) + 15) / 16 * 16;
-constexpr uint32_t kLeafSmemRegs = 12;   // shared-memory register file per warp
+constexpr uint32_t kLeafSmemRegs = 16;   // shared-memory register file per warp
 
 struct LeafArgs {
     Octree o;
@@ -1251,7 +1248,7 @@ struct LeafArgs {
     unsigned long long* prof;   // debug: 8 per group (cycles by section, feature calls, E)
 };
 
-__global__ void __launch_bounds__(256, 4)
+__global__ void __launch_bounds__(256, 3)
 k_leaf_groups(LeafArgs A, uint32_t n_groups)
 {
     extern __shared__ __align__(16) unsigned char lsmem[];
@@ -1312,7 +1309,10 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
     const long long t_group = clock64();
     unsigned long long feat_cycles = 0, feat_calls = 0;
     const DevTape tb = with_tape(A.bt, tr);
-    float* R = tb.n_regs <= A.smem_regs ? Rs : Rgl;
+    const bool rs = tb.n_regs <= A.smem_regs;
+    float* R = rs ? Rs : Rgl;
+    const uint32_t rsoff = static_cast<uint32_t>(reinterpret_cast<unsigned char*>(Rs) - lsmem);
+#define RF_CALL(fn, ...) (rs ? fn<true>(__VA_ARGS__) : fn<false>(__VA_ARGS__))
     const FeatCtx fc{R, &W->fs, A.status};
 
     // --- corners (dc_tree.inl:156-239) ---------------------------------
@@ -1326,7 +1326,8 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
         py = static_cast<float>(lat[1][ib]);
         pz = static_cast<float>(lat[2][ic]);
     }
-    cv = warp_value(tb, cl, tr.len, R, lane, px, py, pz, &camb, &my_evals,
+    cv = RF_CALL(warp_value, tb.cpool, tb.root_kind, tb.root, cl, tr.len, rsoff, R, lane,
+                 px, py, pz, &camb, &my_evals,
                     lane < npts);
     uint8_t cst = CELL_EMPTY;
     bool need_d = false, need_f = false;
@@ -1338,7 +1339,8 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
     }
     if (__any_sync(0xffffffffu, need_d || need_f)) {
         bool amb = false, plain = false;
-        const D4 d = warp_deriv_lite(tb, cl, tr.len, R, lane, px, py, pz, &amb, &plain,
+        const D4 d = RF_CALL(warp_deriv_lite, tb.cpool, tb.root_kind, tb.root, tb.n_regs, cl,
+                             tr.len, rsoff, R, lane, px, py, pz, &amb, &plain,
                                      &my_devals, need_d || need_f);
         if (need_d) {
             cst = (d.dx != 0 || d.dy != 0 || d.dz != 0) ? CELL_FILLED : CELL_EMPTY;
@@ -1495,7 +1497,8 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
                     ++n_act;
                 }
             }
-            const float4 v4 = warp_value4(tb, cl, tr.len, R, lane,
+            const float4 v4 = RF_CALL(warp_value4, tb.cpool, tb.root_kind, tb.root, cl, tr.len,
+                                      rsoff, R, lane,
                                           make_float4(qx[0], qx[1], qx[2], qx[3]),
                                           make_float4(qy[0], qy[1], qy[2], qy[3]),
                                           make_float4(qz[0], qz[1], qz[2], qz[3]));
@@ -1513,7 +1516,9 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
                 bool inside = true;
                 if (__any_sync(0xffffffffu, zero)) {
                     bool amb = false, plain = false;
-                    const D4 dg = warp_deriv_lite(tb, cl, tr.len, R, lane, qx[k], qy[k], qz[k],
+                    const D4 dg = RF_CALL(warp_deriv_lite, tb.cpool, tb.root_kind, tb.root,
+                                          tb.n_regs, cl, tr.len, rsoff, R, lane,
+                                          qx[k], qy[k], qz[k],
                                                   &amb, &plain, &my_devals, zero);
                     amb = amb && !plain;   // a settled tie leaves one plain feature
                     if (zero && !amb) {
@@ -1571,7 +1576,8 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
             for (int k = 0; k < 3; ++k) q[k] = (p & 1) ? es.t1[k] : es.t0[k];
         }
         bool amb = false, plain = false;
-        const D4 d = warp_deriv_lite(tb, cl, tr.len, R, lane, static_cast<float>(q[0]),
+        const D4 d = RF_CALL(warp_deriv_lite, tb.cpool, tb.root_kind, tb.root, tb.n_regs, cl,
+                             tr.len, rsoff, R, lane, static_cast<float>(q[0]),
                                      static_cast<float>(q[1]), static_cast<float>(q[2]),
                                      &amb, &plain, &my_devals, active);
         amb = amb && !plain;   // a settled tie leaves one plain feature
@@ -1707,6 +1713,7 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
         P[7] = t_end - t_vertices;        // vertices
     }
     }   // groups
+#undef RF_CALL
     if (lane == 0) {
         atomicAdd(A.evals, static_cast<unsigned long long>(my_evals));
         atomicAdd(A.evals + 1, static_cast<unsigned long long>(my_devals));

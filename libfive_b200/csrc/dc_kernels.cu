@@ -2357,16 +2357,74 @@ bool exclusive_scan(const T* in, T* out, uint32_t n, cudaStream_t s)
 
 }  // namespace
 
-void* host_alloc(size_t bytes)
+namespace {
+
+/// Page-locked host blocks for mesh arrays, recycled: a mesh freed by
+/// libfive_mesh_delete gives its blocks back for the next one, so a render
+/// loop pins memory once and every download is a single direct copy.
+struct PinnedPool {
+    std::mutex mu;
+    std::multimap<size_t, void*> free_blocks;   // capacity -> block
+    std::map<void*, size_t> owned;              // every pool block
+    size_t free_bytes = 0;
+    static constexpr size_t kKeepBytes = size_t(1) << 30;   // cached when free
+};
+
+PinnedPool& pinned_pool()
 {
-    constexpr size_t kHuge = size_t(2) << 20;
-    const size_t n = std::max<size_t>((bytes + kHuge - 1) / kHuge * kHuge, kHuge);
-    void* p = std::aligned_alloc(kHuge, n);
-    if (p) madvise(p, n, MADV_HUGEPAGE);   // advice only: failure is harmless
-    return p;
+    static PinnedPool* p = new PinnedPool;   // never destroyed: meshes may outlive statics
+    return *p;
 }
 
-void host_free(void* p) { std::free(p); }
+}  // namespace
+
+void* host_alloc(size_t bytes)
+{
+    constexpr size_t kGrain = size_t(2) << 20;
+    const size_t n = std::max<size_t>((bytes + kGrain - 1) / kGrain * kGrain, kGrain);
+    auto& P = pinned_pool();
+    {
+        std::lock_guard<std::mutex> lock(P.mu);
+        auto it = P.free_blocks.lower_bound(n);
+        if (it != P.free_blocks.end() && it->first <= 2 * n) {
+            void* blk = it->second;
+            P.free_bytes -= it->first;
+            P.free_blocks.erase(it);
+            return blk;
+        }
+    }
+    void* blk = nullptr;
+    if (cudaMallocHost(&blk, n) != cudaSuccess || !blk) {
+        cudaGetLastError();
+        blk = std::aligned_alloc(kGrain, n);   // pageable fallback; same interface
+        return blk;
+    }
+    std::lock_guard<std::mutex> lock(P.mu);
+    P.owned[blk] = n;
+    return blk;
+}
+
+void host_free(void* p)
+{
+    if (!p) return;
+    auto& P = pinned_pool();
+    std::lock_guard<std::mutex> lock(P.mu);
+    auto it = P.owned.find(p);
+    if (it == P.owned.end()) {
+        std::free(p);
+        return;
+    }
+    P.free_blocks.emplace(it->second, p);
+    P.free_bytes += it->second;
+    // Keep at most kKeepBytes of idle blocks, largest first out.
+    while (P.free_bytes > PinnedPool::kKeepBytes && !P.free_blocks.empty()) {
+        auto last = std::prev(P.free_blocks.end());
+        P.free_bytes -= last->first;
+        P.owned.erase(last->second);
+        cudaFreeHost(last->second);
+        P.free_blocks.erase(last);
+    }
+}
 
 MeshOut::~MeshOut()
 {
@@ -2393,6 +2451,18 @@ namespace {
 /// threads (a single thread's memcpy is the slow part of a mesh download).
 bool download(void* dst, const void* src, size_t bytes, cudaStream_t s)
 {
+    if (bytes == 0) return true;
+    bool page_locked = false;
+    {
+        auto& P = pinned_pool();
+        std::lock_guard<std::mutex> lock(P.mu);
+        page_locked = P.owned.count(dst) != 0;
+    }
+    if (page_locked) {
+        // Page-locked destination: one direct transfer.
+        return cuda_ok(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s), "download") &&
+               cuda_ok(cudaStreamSynchronize(s), "download");
+    }
     static void* pinned = nullptr;
     static size_t pinned_bytes = 0;
     if (bytes == 0) return true;

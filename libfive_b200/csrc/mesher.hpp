@@ -25,8 +25,10 @@ struct MeshOut {
     libfive_mesh* release();
 };
 
-/// Large host arrays: 2 MiB aligned and advised for transparent huge pages,
-/// so that writing a fresh multi-megabyte mesh costs few page faults.
+/// Mesh arrays in page-locked host memory, recycled between meshes (a freed
+/// block serves the next allocation of up to twice its size; at most 1 GiB
+/// of idle blocks is kept), so that a mesh downloads in one direct copy.
+/// Falls back to pageable memory when page-locked memory is unavailable.
 void* host_alloc(size_t bytes);
 void host_free(void* p);
 

@@ -4,6 +4,8 @@
 #include <queue>
 #include <unordered_map>
 
+#include "flat_map.hpp"
+
 namespace lfb {
 
 bool build_slot_tape(const Tree& root_, SlotTape& out, std::string* err)
@@ -13,8 +15,11 @@ bool build_slot_tape(const Tree& root_, SlotTape& out, std::string* err)
 
     // Slot ids count down from flat.size() so that the root lands on 1
     // (deck.cpp:24-58); slot 0 is the reference's placeholder.
-    std::unordered_map<const Node*, uint32_t> slot;
+    FlatMap<const Node*, uint32_t, PtrHash> slot(flat.size() + 4);
     slot[nullptr] = 0;
+    // walk() lists every child before its parents, so operands always
+    // have a slot by the time they are read.
+    auto slot_of = [&slot](const Node* n) { return *slot.find(n); };
     uint32_t id = static_cast<uint32_t>(flat.size());
     std::vector<SlotClause> rev;
     rev.reserve(flat.size());
@@ -33,11 +38,11 @@ bool build_slot_tape(const Tree& root_, SlotTape& out, std::string* err)
                 }
                 break;
             case Kind::Unary:
-                rev.push_back({m->op, id, slot.at(m->kid[0]), 0});
+                rev.push_back({m->op, id, slot_of(m->kid[0]), 0});
                 break;
             case Kind::Binary:
-                rev.push_back({m->op, id, slot.at(m->kid[0]),
-                               slot.at(m->kid[1])});
+                rev.push_back({m->op, id, slot_of(m->kid[0]),
+                               slot_of(m->kid[1])});
                 break;
             default:
                 if (err) *err = "tree contains an unsupported node";
@@ -49,18 +54,18 @@ bool build_slot_tape(const Tree& root_, SlotTape& out, std::string* err)
 
     const Node* axes[3] = {Tree::X().get(), Tree::Y().get(), Tree::Z().get()};
     for (auto a : axes) {
-        if (slot.find(a) == slot.end()) {
+        if (!slot.find(a)) {
             const uint32_t next = static_cast<uint32_t>(slot.size());
             slot[a] = next;
         }
     }
     out.num_clauses = static_cast<uint32_t>(slot.size() - 1);
-    out.X = slot.at(axes[0]);
-    out.Y = slot.at(axes[1]);
-    out.Z = slot.at(axes[2]);
+    out.X = slot_of(axes[0]);
+    out.Y = slot_of(axes[1]);
+    out.Z = slot_of(axes[2]);
     std::sort(out.vars.begin(), out.vars.end(),
               [](const auto& a, const auto& b) { return a.first < b.first; });
-    out.root = slot.at(root.get());
+    out.root = slot_of(root.get());
     return true;
 }
 

@@ -11,6 +11,7 @@
 #include <unordered_set>
 #include <variant>
 
+#include "flat_map.hpp"
 #include "scalar_ops.h"
 
 namespace lfb {
@@ -29,20 +30,28 @@ Tree::~Tree()
         return;
     }
     // Iterative teardown so that deep chains do not overflow the stack
-    // (same reason as libfive/src/tree/tree.cpp:27-69).
-    std::vector<const Node*> todo{p};
-    bool first = true;
-    while (!todo.empty()) {
-        const Node* n = todo.back();
-        todo.pop_back();
-        if (!first) {
-            if (n->refs.fetch_sub(1, std::memory_order_acq_rel) != 1) {
-                continue;
-            }
+    // (same reason as libfive/src/tree/tree.cpp:27-69).  The pending list
+    // lives on the stack until it outgrows 64 entries.
+    const Node* local[64];
+    size_t n_local = 0;
+    std::vector<const Node*> spill;
+    local[n_local++] = p;
+    while (n_local || !spill.empty()) {
+        const Node* n;
+        if (!spill.empty()) {
+            n = spill.back();
+            spill.pop_back();
+        } else {
+            n = local[--n_local];
         }
-        first = false;
         for (auto k : n->kid) {
-            if (k) todo.push_back(k);
+            if (k && k->refs.fetch_sub(1, std::memory_order_acq_rel) == 1) {
+                if (n_local < 64) {
+                    local[n_local++] = k;
+                } else {
+                    spill.push_back(k);
+                }
+            }
         }
         delete n;
     }
@@ -216,6 +225,11 @@ float fold_constant(int o, float a, float b)
 // Local simplifications follow tree.cpp:95-123.
 Tree Tree::unary(int o, const Tree& a)
 {
+    return unary_n(o, a.p);
+}
+
+Tree Tree::unary_n(int o, const Node* a)
+{
     if (op::arity(o) != 1) {
         return invalid();
     }
@@ -225,14 +239,26 @@ Tree Tree::unary(int o, const Tree& a)
     if (o == op::ABS) {
         if (a->kind == Kind::Unary &&
             (a->op == op::ABS || a->op == op::SQUARE)) {
-            return a;
+            return Tree(a);
         }
     } else if (o == op::NEG) {
         if (a->kind == Kind::Unary && a->op == op::NEG) {
             return Tree(a->kid[0]);
         }
     }
-    return make(Kind::Unary, o, 0, a.p, nullptr);
+    return make(Kind::Unary, o, 0, a, nullptr);
+}
+
+/// Tree::op() of a bare node.
+static int op_of(const Node* n)
+{
+    switch (n->kind) {
+        case Kind::Constant: return op::CONSTANT;
+        case Kind::Nullary:
+        case Kind::Unary:
+        case Kind::Binary: return n->op;
+        default: return op::INVALID;
+    }
 }
 
 // Local simplifications follow tree.cpp:141-230, including the exact
@@ -240,61 +266,66 @@ Tree Tree::unary(int o, const Tree& a)
 // when it is non-zero).
 Tree Tree::binary(int o, const Tree& a, const Tree& b)
 {
+    return binary_n(o, a.p, b.p);
+}
+
+Tree Tree::binary_n(int o, const Node* a, const Node* b)
+{
     if (op::arity(o) != 2) {
         return invalid();
     }
     const bool ac = a->kind == Kind::Constant;
     const bool bc = b->kind == Kind::Constant;
-    if (a.op() == op::CONSTANT && b.op() == op::CONSTANT) {
+    if (op_of(a) == op::CONSTANT && op_of(b) == op::CONSTANT) {
         return constant(fold_constant(o, a->value, b->value));
     }
-    auto is_neg = [](const Tree& t) {
+    auto is_neg = [](const Node* t) {
         return t->kind == Kind::Unary && t->op == op::NEG;
     };
     if (o == op::DIV) {
         if (bc && b->value == 1.0f) {
-            return a;
+            return Tree(a);
         }
     } else if (o == op::ADD) {
         if (ac) {
-            if (a->value == 0.0f) return b;
+            if (a->value == 0.0f) return Tree(b);
         } else if (bc) {
-            if (b->value == 0.0f) return a;
+            if (b->value == 0.0f) return Tree(a);
         } else if (a->kind == Kind::Unary) {
-            if (a->op == op::NEG) return b - Tree(a->kid[0]);
+            if (a->op == op::NEG) return binary_n(op::SUB, b, a->kid[0]);
         } else if (b->kind == Kind::Unary) {
-            if (b->op == op::NEG) return a - Tree(b->kid[0]);
+            if (b->op == op::NEG) return binary_n(op::SUB, a, b->kid[0]);
         }
     } else if (o == op::SUB) {
         if (ac) {
-            if (a->value == 0.0f) return -b;
+            if (a->value == 0.0f) return unary_n(op::NEG, b);
         } else if (bc) {
-            if (b->value == 0.0f) return a;
+            if (b->value == 0.0f) return Tree(a);
         } else if (is_neg(b)) {
-            return a + Tree(b->kid[0]);
+            return binary_n(op::ADD, a, b->kid[0]);
         }
     } else if (o == op::MUL) {
         if (ac) {
-            if (a->value == 0) return a;
-            if (a->value == 1) return b;
-            if (a->value == -1) return -b;
+            if (a->value == 0) return Tree(a);
+            if (a->value == 1) return Tree(b);
+            if (a->value == -1) return unary_n(op::NEG, b);
         } else if (bc) {
-            if (b->value == 0) return b;
-            if (b->value == 1) return a;
-            if (b->value == -1) return -a;
-        } else if (a.p == b.p) {
-            return unary(op::SQUARE, a);
+            if (b->value == 0) return Tree(b);
+            if (b->value == 1) return Tree(a);
+            if (b->value == -1) return unary_n(op::NEG, a);
+        } else if (a == b) {
+            return unary_n(op::SQUARE, a);
         }
     } else if (o == op::NTH_ROOT || o == op::POW) {
         if (bc && b->value == 1.0f) {
-            return a;
+            return Tree(a);
         }
     } else if (o == op::MIN || o == op::MAX) {
-        if (a.p == b.p) {
-            return a;
+        if (a == b) {
+            return Tree(a);
         }
     }
-    return make(Kind::Binary, o, 0, a.p, b.p);
+    return make(Kind::Binary, o, 0, a, b);
 }
 
 Tree operator+(const Tree& a, const Tree& b) { return Tree::binary(op::ADD, a, b); }
@@ -431,7 +462,7 @@ std::vector<const Node*> Tree::walk() const
     if (p->flags & Node::HAS_REMAP) {
         return flatten().walk();
     }
-    std::unordered_map<const Node*, unsigned> count;
+    FlatMap<const Node*, unsigned, PtrHash> count(1024);
     std::vector<const Node*> todo{p};
     auto nkids = [](const Node* n) {
         return n->kind == Kind::Unary ? 1 : n->kind == Kind::Binary ? 2 : 0;
@@ -446,13 +477,14 @@ std::vector<const Node*> Tree::walk() const
         }
     }
     std::vector<const Node*> flat;
+    flat.reserve(count.size() + 1);
     todo.push_back(p);
     while (!todo.empty()) {
         const Node* n = todo.back();
         todo.pop_back();
         flat.push_back(n);
         for (int i = 0; i < nkids(n); ++i) {
-            if (--count.at(n->kid[i]) == 0) {
+            if (--*count.find(n->kid[i]) == 0) {
                 todo.push_back(n->kid[i]);
             }
         }
@@ -605,40 +637,87 @@ Tree Tree::optimized() const
         return flatten().optimized();
     }
 
-    std::unordered_map<Key, Tree, KeyHash> canonical;
-    auto uniq = [&canonical](const Tree& t) -> Tree {
+    // `canonical` owns one reference to every tree this pass hands around;
+    // everything below it (the output stack, affine terms, commutative
+    // lists) holds plain pointers, which stay valid because each of them
+    // is either a node of the input tree or a canonical entry.
+    FlatMap<Key, Tree, KeyHash> canonical(1024);
+    auto uniq_new = [&canonical](Tree&& t) -> const Node* {
         const Key k = key_of(t.p);
-        auto it = canonical.find(k);
-        if (it != canonical.end()) {
-            return it->second;
+        return canonical.emplace(k, std::move(t)).first->p;
+    };
+    auto uniq_old = [&canonical](const Node* n) -> const Node* {
+        const Key k = key_of(n);
+        if (Tree* found = canonical.find(k)) {
+            return found->p;
         }
-        canonical.emplace(k, t);
-        return t;
+        canonical.emplace(k, Tree(n));
+        return n;
+    };
+    // The constant 1 is created on first use, like the reference's static
+    // (tree.cpp:251-254); its creation serial orders it among affine terms,
+    // so it must not be touched any earlier than the reference would.
+    const Node* one_p = nullptr;
+    auto ONE = [&one_p]() {
+        if (!one_p) one_p = one().p;
+        return one_p;
     };
 
-    // Affine accumulators map a tree to its scale factor.  The iteration
-    // order of this map does not matter: terms are sorted before use.
-    struct AffineMap {
-        std::unordered_map<const Node*, std::pair<Tree, float>> terms;
-        void add(const Tree& t, float s)
+    // One frame per DOWN task: the affine accumulator (tree -> scale factor)
+    // and the commutative list that the reference keeps on two parallel
+    // stacks of optionals.  Frames are pooled, so their buffers are reused.
+    struct Frame {
+        bool has_affine = false;
+        bool has_comm = false;
+        int comm_op = 0;
+        std::vector<std::pair<const Node*, float>> terms;
+        FlatMap<const Node*, uint32_t, PtrHash> index{16};
+        std::vector<const Node*> list;
+
+        void reset()
         {
-            auto it = terms.find(t.get());
-            if (it == terms.end()) {
-                terms.emplace(t.get(), std::make_pair(t, s));
+            has_affine = has_comm = false;
+            terms.clear();
+            index.clear();
+            list.clear();
+        }
+        // Adds s to the scale of t.  Terms are looked up by a linear scan
+        // while there are few of them, then through `index`.
+        void add(const Node* t, float s)
+        {
+            if (terms.size() < 16) {
+                for (auto& e : terms) {
+                    if (e.first == t) {
+                        e.second += s;
+                        return;
+                    }
+                }
+                terms.push_back({t, s});
+                if (terms.size() == 16) {
+                    for (uint32_t i = 0; i < 16; ++i) {
+                        index.emplace(terms[i].first, i);
+                    }
+                }
+                return;
+            }
+            auto r = index.emplace(t, static_cast<uint32_t>(terms.size()));
+            if (r.second) {
+                terms.push_back({t, s});
             } else {
-                it->second.second += s;
+                terms[*r.first].second += s;
             }
         }
     };
-    struct CommList {
-        int op;
-        std::vector<Tree> list;
+    std::vector<Frame> frames(1);
+    size_t depth = 1;
+    auto push_frame = [&]() {
+        if (depth == frames.size()) {
+            frames.emplace_back();
+        } else {
+            frames[depth].reset();
+        }
+        ++depth;
     };
-
-    std::vector<std::optional<AffineMap>> affine;
-    affine.emplace_back(std::nullopt);
-    std::vector<std::optional<CommList>> comm;
-    comm.emplace_back(std::nullopt);
 
     struct Task {
         enum { DOWN, UP, UP_AFFINE, UP_COMM } type;
@@ -646,17 +725,19 @@ Tree Tree::optimized() const
         float scale;
     };
     std::vector<Task> todo{{Task::DOWN, p, 1.0f}};
-    std::vector<Tree> out;
+    std::vector<const Node*> out;
+    std::vector<std::pair<const Node*, float>> pos, neg;
 
-    auto deliver = [&](const Tree& self, float scale) {
-        if (affine.back().has_value()) {
+    auto deliver = [&](const Node* self, float scale) {
+        Frame& f = frames[depth - 1];
+        if (f.has_affine) {
             if (self->kind == Kind::Constant) {
-                affine.back()->add(one(), scale * self->value);
+                f.add(ONE(), scale * self->value);
             } else {
-                affine.back()->add(self, scale);
+                f.add(self, scale);
             }
-        } else if (comm.back().has_value()) {
-            comm.back()->list.push_back(self);
+        } else if (f.has_comm) {
+            f.list.push_back(self);
         } else {
             out.push_back(self);
         }
@@ -669,29 +750,32 @@ Tree Tree::optimized() const
         if (task.type == Task::DOWN) {
             const Node* d = task.t;
             todo.push_back({Task::UP, d, task.scale});
-            comm.emplace_back(std::nullopt);
-            affine.emplace_back(std::nullopt);
+            push_frame();
 
+            // Either turns this frame into an affine / commutative
+            // accumulator, or (when the parent frame already accumulates
+            // the same thing) drops it so that the children feed the
+            // parent's accumulator directly.
             bool marked_affine = false;
             auto mark_affine = [&]() {
                 todo.pop_back();
-                affine.pop_back();
-                if (!affine.back().has_value()) {
-                    affine.emplace_back(AffineMap());
+                if (!frames[depth - 2].has_affine) {
+                    frames[depth - 1].has_affine = true;
                     todo.push_back({Task::UP_AFFINE, nullptr, 0.0f});
                 } else {
-                    comm.pop_back();
+                    --depth;
                 }
                 marked_affine = true;
             };
             auto mark_comm = [&](int o) {
                 todo.pop_back();
-                comm.pop_back();
-                if (!comm.back().has_value() || comm.back()->op != o) {
-                    comm.emplace_back(CommList{o, {}});
+                const Frame& parent = frames[depth - 2];
+                if (!parent.has_comm || parent.comm_op != o) {
+                    frames[depth - 1].has_comm = true;
+                    frames[depth - 1].comm_op = o;
                     todo.push_back({Task::UP_COMM, nullptr, task.scale});
                 } else {
-                    affine.pop_back();
+                    --depth;
                 }
             };
 
@@ -740,104 +824,112 @@ Tree Tree::optimized() const
                 }
             }
         } else if (task.type == Task::UP) {
-            affine.pop_back();
-            comm.pop_back();
+            --depth;
             const Node* d = task.t;
-            Tree self = uniq(Tree(d));
+            const Node* self = uniq_old(d);
             if (d->kind == Kind::Unary) {
-                Tree a = std::move(out.back());
+                const Node* a = out.back();
                 out.pop_back();
-                if (a.p != d->kid[0]) {
-                    self = uniq(unary(d->op, a));
+                if (a != d->kid[0]) {
+                    self = uniq_new(unary_n(d->op, a));
                 }
             } else if (d->kind == Kind::Binary) {
-                Tree a = std::move(out.back());
+                const Node* a = out.back();
                 out.pop_back();
-                Tree b = std::move(out.back());
+                const Node* b = out.back();
                 out.pop_back();
-                if (a.p != d->kid[0] || b.p != d->kid[1]) {
-                    self = uniq(binary(d->op, a, b));
+                if (a != d->kid[0] || b != d->kid[1]) {
+                    self = uniq_new(binary_n(d->op, a, b));
                 }
             }
             deliver(self, task.scale);
         } else if (task.type == Task::UP_AFFINE) {
-            AffineMap map = std::move(*affine.back());
-            affine.pop_back();
-            comm.pop_back();
+            // Nothing below pushes a frame, so the popped frame's buffers
+            // stay valid while they are read.
+            const Frame& f = frames[depth - 1];
+            --depth;
 
             // Split into positive and negative terms; NaN scales go with the
             // positive terms and zero scales are dropped (tree.cpp:832-848).
-            std::vector<std::pair<Tree, float>> pos, neg;
-            for (auto& kv : map.terms) {
-                const float s = kv.second.second;
+            pos.clear();
+            neg.clear();
+            for (const auto& kv : f.terms) {
+                const float s = kv.second;
                 if (s > 0.0f) {
-                    pos.push_back({kv.second.first, s});
+                    pos.push_back({kv.first, s});
                 } else if (s < 0.0f) {
-                    neg.push_back({kv.second.first, -s});
+                    neg.push_back({kv.first, -s});
                 } else if (s != 0.0f) {
-                    pos.push_back({kv.second.first, s});
+                    pos.push_back({kv.first, s});
                 }
             }
-            auto order = [](const std::pair<Tree, float>& a,
-                            const std::pair<Tree, float>& b) {
-                if (a.second != b.second) {
+            // Ascending scale, then creation order.  NaN scales sort last:
+            // the reference compares them with `<` alone, which is not a
+            // strict weak order, so its placement of NaN terms depends on
+            // hash-table iteration order and is not reproducible anyway.
+            auto order = [](const std::pair<const Node*, float>& a,
+                            const std::pair<const Node*, float>& b) {
+                const bool an = std::isnan(a.second);
+                const bool bn = std::isnan(b.second);
+                if (an != bn) {
+                    return bn;
+                }
+                if (!an && a.second != b.second) {
                     return a.second < b.second;
                 }
-                return serial_less(a.first.get(), b.first.get());
+                return serial_less(a.first, b.first);
             };
             std::sort(pos.begin(), pos.end(), order);
             std::sort(neg.begin(), neg.end(), order);
 
-            auto collapse = [&](const std::vector<std::pair<Tree, float>>& v) {
-                Tree acc = invalid();
+            auto collapse = [&](const std::vector<std::pair<const Node*, float>>& v) {
+                const Node* acc = nullptr;
                 size_t i = 0;
                 while (i < v.size()) {
                     const float mult = v[i].second;
-                    Tree t = v[i].first;
+                    const Node* t = v[i].first;
                     ++i;
                     while (i < v.size() && v[i].second == mult) {
-                        t = uniq(t + v[i].first);
+                        t = uniq_new(binary_n(op::ADD, t, v[i].first));
                         ++i;
                     }
                     if (mult != 1) {
-                        if (t == one()) {
-                            t = uniq(constant(mult));
+                        if (t == ONE()) {
+                            t = uniq_new(constant(mult));
                         } else {
-                            t = uniq(t * uniq(constant(mult)));
+                            t = uniq_new(binary_n(op::MUL, t,
+                                                  uniq_new(constant(mult))));
                         }
                     }
-                    acc = acc.is_valid() ? uniq(acc + t) : t;
+                    acc = acc ? uniq_new(binary_n(op::ADD, acc, t)) : t;
                 }
-                return acc.is_valid() ? acc : uniq(constant(0.0f));
+                return acc ? acc : uniq_new(constant(0.0f));
             };
-            const Tree P = collapse(pos);
-            const Tree N = collapse(neg);
-            Tree self = uniq(P - N);
-            if (comm.back().has_value()) {
-                comm.back()->list.push_back(self);
+            const Node* P = collapse(pos);
+            const Node* N = collapse(neg);
+            const Node* self = uniq_new(binary_n(op::SUB, P, N));
+            Frame& parent = frames[depth - 1];
+            if (parent.has_comm) {
+                parent.list.push_back(self);
             } else {
                 out.push_back(self);
             }
         } else {  // UP_COMM
-            CommList c = std::move(*comm.back());
-            comm.pop_back();
-            affine.pop_back();
-            std::sort(c.list.begin(), c.list.end(),
-                      [](const Tree& a, const Tree& b) {
-                          return serial_less(a.get(), b.get());
-                      });
-            auto end = c.list.end();
-            if (op::is_idempotent(c.op)) {
-                end = std::unique(c.list.begin(), c.list.end());
+            Frame& f = frames[depth - 1];
+            --depth;
+            std::sort(f.list.begin(), f.list.end(), serial_less);
+            auto end = f.list.end();
+            if (op::is_idempotent(f.comm_op)) {
+                end = std::unique(f.list.begin(), f.list.end());
             }
-            Tree self = c.list.front();
-            for (auto it = c.list.begin() + 1; it != end; ++it) {
-                self = uniq(binary(c.op, self, *it));
+            const Node* self = f.list.front();
+            for (auto it = f.list.begin() + 1; it != end; ++it) {
+                self = uniq_new(binary_n(f.comm_op, self, *it));
             }
             deliver(self, task.scale);
         }
     }
-    return out.back().as_optimized();
+    return Tree(out.back(), true, true);
 }
 
 ////////////////////////////////////////////////////////////////////////////////

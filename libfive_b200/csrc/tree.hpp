@@ -101,6 +101,10 @@ private:
     static Tree make(Kind k, int op, float value, const Node* a,
                      const Node* b, const Node* c = nullptr,
                      const Node* d = nullptr);
+    // unary() / binary() on borrowed node pointers, so that passes which
+    // keep their operands alive elsewhere need no reference counting.
+    static Tree unary_n(int op, const Node* a);
+    static Tree binary_n(int op, const Node* a, const Node* b);
     static Tree one();
     Tree as_optimized() const { return Tree(p, true, true); }
     void inc() const

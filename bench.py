@@ -66,6 +66,12 @@ def parse():
     p.add_argument("--depth", type=int, default=10,
                    help="octree depth; 10 is the benchmark workload, smaller "
                         "depths are for profiling captures")
+    p.add_argument("--workload", default="csg2000", choices=["csg2000", "batch"],
+                   help="batch: many trees of mixed size and depth, meshed "
+                        "one after another and through lfb_render_meshes")
+    p.add_argument("--trees", type=int, default=512, help="batch workload: tree count")
+    p.add_argument("--workers", type=int, default=4,
+                   help="batch workload: meshes in flight at once")
     return p.parse_args()
 
 
@@ -379,10 +385,65 @@ def run_ours(args, world, rank, local):
         pg.destroy_process_group()
 
 
+def run_batch(args, world, rank, local):
+    """Many-tree meshing: `--trees` random CSG trees (primitive counts
+    log-uniform in [8, 4000], octree depth 8-11 over [-1.5,1.5]^3), each step
+    meshing all of them, timed once as a loop of lfb_render_mesh calls and
+    once as one lfb_render_meshes call.  Tapes are built before timing; every
+    mesh is downloaded to the host.  Rank r meshes its own trees (seed 11 + r)."""
+    import torch
+    from libfive_b200 import ffi, workloads
+    from libfive_b200.shape import Tape, render_meshes
+    torch.cuda.set_device(local)
+    lib = ffi.load()
+    specs = workloads.batch_specs(args.trees, seed=11 + rank)
+    tapes = [Tape(workloads.random_csg(n, seed=sd)) for n, sd, _ in specs]
+    jobs = [(t, REGION[0], REGION[1], float(1.0 / res), MAX_ERR)
+            for t, (_, _, res) in zip(tapes, specs)]
+    region = ffi.Region3(*[ffi.Interval(a, b) for a, b in zip(*REGION)])
+
+    def loop():
+        tris = 0
+        for t, _, _, mf, me in jobs:
+            st = ffi.MeshStats()
+            m = lib.lfb_render_mesh(t.ptr, region, ffi.MeshSettings(mf, me), ctypes.byref(st))
+            if not m:
+                raise RuntimeError("lfb_render_mesh failed: " + ffi.last_error()[1])
+            lib.libfive_mesh_delete(m)
+            tris += st.triangles
+        return tris
+
+    def batch():
+        return sum(len(t) for _, t in render_meshes(jobs, workers=args.workers))
+
+    timings = {}
+    for name, fn in (("loop", loop), ("batch", batch)):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        tris = [fn() for _ in range(args.steps)]
+        torch.cuda.synchronize()
+        timings[name] = (time.perf_counter() - t0) / args.steps
+        assert len(set(tris)) == 1
+    if rank == 0:
+        n = len(jobs)
+        print(json.dumps({
+            "metric": "meshes/s (many trees)", "value": n / timings["batch"], "unit": "meshes/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": timings["batch"] * 1e3, "higher_is_better": True,
+            "loop_value": n / timings["loop"], "batch_over_loop": timings["loop"] / timings["batch"],
+            "triangles_per_step": tris[0], "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "batch of %d random CSG trees, 8-4000 primitives, "
+                                   "depth 8-11" % n, "workers": args.workers}}))
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
-    if args.impl == "reference":
+    if args.workload == "batch":
+        run_batch(args, world, rank, local)
+    elif args.impl == "reference":
         run_reference(args, world, rank)
     else:
         run_ours(args, world, rank, local)

@@ -134,6 +134,20 @@ libfive_mesh* lfb_render_mesh(lfb_tape t, libfive_region3 R,
                               lfb_mesh_settings settings,
                               lfb_mesh_stats* stats);
 
+/* n meshes in one call, each tape over its own region with its own
+ * settings.  The reference has no such call (libfive_tree_save_meshes,
+ * libfive.cpp:419-440, renders its trees one after another through
+ * Mesh::render, mesh.cpp:35-125); here up to `workers` meshes are in flight
+ * at once, each on its own CUDA stream with its own scratch buffers, longest
+ * first (0 workers: 4).  meshes[i] receives tape i's mesh (free it with
+ * libfive_mesh_delete), or NULL if that mesh failed; stats is NULL or an
+ * array of n.  Returns 0 when every mesh succeeded, else the first failure's
+ * LFB_E* code (message from lfb_last_error). */
+int lfb_render_meshes(const lfb_tape* tapes, uint32_t n,
+                      const libfive_region3* regions,
+                      const lfb_mesh_settings* settings, uint32_t workers,
+                      libfive_mesh** meshes, lfb_mesh_stats* stats);
+
 /* The reference-layout tape of a tree (Deck, deck.cpp:19-94), for
  * checking slot numbering and for CPU cross-checks.  counts[0..7] =
  * num_clauses, tape length, constants, variables, X, Y, Z, root slot.

@@ -288,6 +288,13 @@ libfive_pixels* libfive_tree_render_pixels(libfive_tree, libfive_region2,
 ////////////////////////////////////////////////////////////////////////////////
 // Meshing (libfive.cpp:306-440)
 
+/// BRepSettings::min_feature as the reference's C API sets it: `1/res`
+/// divides in float (libfive.cpp:301), and that float is what is widened.
+static double min_feature_of(float res)
+{
+    return static_cast<double>(1 / res);
+}
+
 static libfive_mesh* render_with(const std::shared_ptr<GpuTape>& g,
                                  libfive_region3 R, double min_feature,
                                  double max_err, const char* who)
@@ -312,7 +319,7 @@ libfive_mesh* libfive_tree_render_mesh(libfive_tree tree, libfive_region3 R,
                                        float res)
 {
     if (!tree) return nullptr;
-    return render_with(cached_tape(N(tree)), R, 1.0 / res, 1e-8,
+    return render_with(cached_tape(N(tree)), R, min_feature_of(res), 1e-8,
                        "libfive_tree_render_mesh");
 }
 
@@ -320,7 +327,7 @@ libfive_mesh* libfive_tree_render_mesh_st(libfive_tree tree,
                                           libfive_region3 R, float res)
 {
     if (!tree) return nullptr;
-    return render_with(cached_tape(N(tree)), R, 1.0 / res, 1e-8,
+    return render_with(cached_tape(N(tree)), R, min_feature_of(res), 1e-8,
                        "libfive_tree_render_mesh_st");
 }
 
@@ -359,19 +366,35 @@ bool libfive_tree_save_mesh(libfive_tree tree, libfive_region3 R, float res,
 bool libfive_tree_save_meshes(libfive_tree trees[], libfive_region3 R,
                               float res, float quality, const char* f)
 {
-    std::vector<libfive_mesh*> ms;
-    bool ok = true;
-    const double max_err = std::pow(10.0, -quality);
+    // The reference renders the trees one after another (libfive.cpp:419-440);
+    // here they render concurrently, each on its own stream.
+    std::vector<std::shared_ptr<GpuTape>> tapes;
     for (unsigned i = 0; trees && trees[i] != nullptr; ++i) {
-        auto m = render_with(cached_tape(N(trees[i])), R, 1.0 / res, max_err,
-                             "libfive_tree_save_meshes");
-        if (!m) {
-            ok = false;
-            break;
+        auto g = cached_tape(N(trees[i]));
+        if (!g) {
+            std::string msg;
+            last_error(&msg);
+            std::fprintf(stderr, "libfive_tree_save_meshes: %s\n", msg.c_str());
+            return false;
         }
-        ms.push_back(m);
+        tapes.push_back(std::move(g));
     }
-    if (ok) ok = save_stl(f, ms);
+    std::vector<MeshJob> jobs(tapes.size());
+    for (size_t i = 0; i < tapes.size(); ++i) {
+        jobs[i].g = tapes[i].get();
+        jobs[i].R = R;
+        jobs[i].min_feature = min_feature_of(res);
+        jobs[i].max_err = std::pow(10.0, -quality);
+    }
+    if (render_dc_meshes(jobs.data(), jobs.size(), 4) != 0) {
+        std::string msg;
+        last_error(&msg);
+        std::fprintf(stderr, "libfive_tree_save_meshes: %s\n", msg.c_str());
+        return false;
+    }
+    std::vector<libfive_mesh*> ms;
+    for (auto& j : jobs) ms.push_back(j.out.release());
+    const bool ok = save_stl(f, ms);
     for (auto m : ms) libfive_mesh_delete(m);
     return ok;
 }
@@ -562,6 +585,34 @@ libfive_mesh* lfb_render_mesh(lfb_tape t, libfive_region3 R,
         return nullptr;
     }
     return mesh.release();
+}
+
+int lfb_render_meshes(const lfb_tape* tapes, uint32_t n, const libfive_region3* regions,
+                      const lfb_mesh_settings* settings, uint32_t workers,
+                      libfive_mesh** meshes, lfb_mesh_stats* stats)
+{
+    clear_error();
+    if (n && (!tapes || !regions || !settings || !meshes)) {
+        return set_error(LFB_E_INVALID, "null argument");
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        meshes[i] = nullptr;
+        if (!tapes[i]) return set_error(LFB_E_INVALID, "null tape");
+    }
+    std::vector<MeshJob> jobs(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        jobs[i].g = tapes[i]->g.get();
+        jobs[i].R = regions[i];
+        jobs[i].min_feature = settings[i].min_feature;
+        jobs[i].max_err = settings[i].max_err;
+        jobs[i].want_stats = stats != nullptr;
+    }
+    const int rc = render_dc_meshes(jobs.data(), n, workers ? workers : 4);
+    for (uint32_t i = 0; i < n; ++i) {
+        if (jobs[i].rc == 0) meshes[i] = jobs[i].out.release();
+        if (stats) stats[i] = jobs[i].stats;
+    }
+    return rc;
 }
 
 uint64_t lfb_kernel_launches(void) { return launches(); }

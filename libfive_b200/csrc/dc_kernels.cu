@@ -2247,10 +2247,12 @@ __global__ void k_remap_tris(uint32_t* tris, uint32_t n, const uint32_t* scan)
 ////////////////////////////////////////////////////////////////////////////////
 // Host driver
 
+#include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
-#include <algorithm>
 #include <map>
 #include <vector>
 
@@ -2260,9 +2262,17 @@ namespace lfb {
 
 namespace {
 
-/// Grow-only device buffers keyed by purpose, reused across calls.
+/// What one mesh in flight owns on the host side: grow-only device buffers
+/// keyed by purpose, the stream its work runs on and download()'s
+/// page-locked staging buffer.  A context serves one mesh at a time (its
+/// mutex) and keeps its buffers from call to call.
 struct Workspace {
+    std::mutex mu;
+    cudaStream_t s = 0;
     std::map<int, DevBuf> bufs;
+    void* pinned = nullptr;
+    size_t pinned_bytes = 0;
+
     template <class T>
     T* get(int key, size_t count)
     {
@@ -2272,10 +2282,31 @@ struct Workspace {
     }
 };
 
-Workspace& workspace()
+/// The context of single-mesh calls: work on the legacy default stream, as
+/// callers that time those calls with events on that stream expect.
+Workspace& default_workspace()
 {
-    static Workspace w;
-    return w;
+    static Workspace* w = new Workspace;   // never destroyed: see pinned_pool()
+    return *w;
+}
+
+/// Context k of the concurrent batch path, created on first use with its
+/// own non-blocking stream (so that batched meshes overlap each other and
+/// never wait on unrelated default-stream work).
+Workspace* stream_workspace(unsigned k)
+{
+    static std::mutex mu;
+    static std::vector<Workspace*> pool;
+    std::lock_guard<std::mutex> lock(mu);
+    while (pool.size() <= k) {
+        auto* w = new Workspace;
+        if (!cuda_ok(cudaStreamCreateWithFlags(&w->s, cudaStreamNonBlocking), "stream")) {
+            delete w;
+            return nullptr;
+        }
+        pool.push_back(w);
+    }
+    return pool[k];
 }
 
 enum BufKey {
@@ -2287,15 +2318,16 @@ enum BufKey {
     K_LEVEL = 100,
 };
 
-bool tables_ready = false;
-
 bool upload_tables()
 {
-    if (tables_ready) return true;
+    static std::mutex mu;
+    static bool ready = false;
+    std::lock_guard<std::mutex> lock(mu);
+    if (ready) return true;
     static DcTables t;
     build_dc_tables(t);
     if (!cuda_ok(cudaMemcpyToSymbol(c_tab, &t, sizeof(t)), "dc tables")) return false;
-    tables_ready = true;
+    ready = true;
     return true;
 }
 
@@ -2313,11 +2345,10 @@ int level_from_resolution(const double lo[3], const double hi[3], double min_fea
 /// (kBlockModeCells; LFB_BLOCK_MODE_CELLS overrides it, for the parity tests).
 uint32_t block_mode_cells()
 {
-    static long v = -1;
-    if (v < 0) {
+    static const long v = [] {
         const char* e = std::getenv("LFB_BLOCK_MODE_CELLS");
-        v = e ? std::max(0L, std::atol(e)) : static_cast<long>(kBlockModeCells);
-    }
+        return e ? std::max(0L, std::atol(e)) : static_cast<long>(kBlockModeCells);
+    }();
     return static_cast<uint32_t>(v);
 }
 
@@ -2326,28 +2357,25 @@ uint32_t block_mode_cells()
 /// it, which the parity tests use to run both modes on small shapes).
 uint32_t group_mode_cells()
 {
-    static uint32_t v = 0;
-    if (v == 0) {
+    static const uint32_t v = [] {
         const char* e = std::getenv("LFB_GROUP_MODE_CELLS");
-        v = e ? static_cast<uint32_t>(std::max(1L, std::atol(e))) : kGroupModeCells;
-    }
+        return e ? static_cast<uint32_t>(std::max(1L, std::atol(e))) : kGroupModeCells;
+    }();
     return v;
 }
 
 bool debug_levels()
 {
-    static int on = -1;
-    if (on < 0) {
+    static const bool on = [] {
         const char* e = std::getenv("LFB_DEBUG_LEVELS");
-        on = (e && e[0] == '1') ? 1 : 0;
-    }
-    return on == 1;
+        return e && e[0] == '1';
+    }();
+    return on;
 }
 
 template <class T>
-bool exclusive_scan(const T* in, T* out, uint32_t n, cudaStream_t s)
+bool exclusive_scan(Workspace& ws, const T* in, T* out, uint32_t n, cudaStream_t s)
 {
-    auto& ws = workspace();
     size_t tmp = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, tmp, in, out, n, s);
     void* t = ws.get<unsigned char>(K_CUBTMP, tmp);
@@ -2449,7 +2477,7 @@ namespace {
 /// Device -> pageable host copy: one transfer into a pinned staging buffer
 /// (grow-only, kept between calls), then a host copy split over a few
 /// threads (a single thread's memcpy is the slow part of a mesh download).
-bool download(void* dst, const void* src, size_t bytes, cudaStream_t s)
+bool download(Workspace& ws, void* dst, const void* src, size_t bytes, cudaStream_t s)
 {
     if (bytes == 0) return true;
     bool page_locked = false;
@@ -2463,16 +2491,14 @@ bool download(void* dst, const void* src, size_t bytes, cudaStream_t s)
         return cuda_ok(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s), "download") &&
                cuda_ok(cudaStreamSynchronize(s), "download");
     }
-    static void* pinned = nullptr;
-    static size_t pinned_bytes = 0;
-    if (bytes == 0) return true;
-    if (bytes > pinned_bytes) {
+    void*& pinned = ws.pinned;
+    if (bytes > ws.pinned_bytes) {
         if (pinned) cudaFreeHost(pinned);
         pinned = nullptr;
-        pinned_bytes = 0;
+        ws.pinned_bytes = 0;
         const size_t want = std::max<size_t>(bytes + bytes / 4, size_t(8) << 20);
         if (!cuda_ok(cudaMallocHost(&pinned, want), "pinned staging")) return false;
-        pinned_bytes = want;
+        ws.pinned_bytes = want;
     }
     if (!cuda_ok(cudaMemcpyAsync(pinned, src, bytes, cudaMemcpyDeviceToHost, s), "download") ||
         !cuda_ok(cudaStreamSynchronize(s), "download")) {
@@ -2498,14 +2524,31 @@ bool download(void* dst, const void* src, size_t bytes, cudaStream_t s)
 
 }  // namespace
 
-int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
-                   double max_err, MeshOut& out, lfb_mesh_stats* stats)
+namespace {
+
+/// Stage-timing events, destroyed on every way out of a render.
+struct StageEvents {
+    cudaEvent_t ev[5] = {};
+    bool on = false;
+    void create()
+    {
+        for (auto& e : ev) cudaEventCreate(&e);
+        on = true;
+    }
+    ~StageEvents()
+    {
+        if (on) {
+            for (auto& e : ev) cudaEventDestroy(e);
+        }
+    }
+};
+
+/// One mesh in the context `ws` (held by the caller), on its stream.
+int render_in(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_feature,
+              double max_err, MeshOut& out, lfb_mesh_stats* stats)
 {
-    if (!require_device()) return LFB_E_CUDA;
-    std::lock_guard<std::mutex> lock(global_mutex());
     if (!upload_tables()) return LFB_E_CUDA;
-    auto& ws = workspace();
-    cudaStream_t s = 0;
+    cudaStream_t s = ws.s;
     const auto t_start = std::chrono::steady_clock::now();
 
     Octree o{};
@@ -2582,9 +2625,10 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
 
     // Stage timing with CUDA events on the pipeline's stream (only when the
     // caller asks for statistics).
-    cudaEvent_t ev[5] = {};
+    StageEvents events;
+    cudaEvent_t* ev = events.ev;
     if (stats) {
-        for (auto& e : ev) cudaEventCreate(&e);
+        events.create();
         cudaEventRecord(ev[0], s);
     }
     uint64_t n_launch = 1;   // k_init_root
@@ -2730,8 +2774,9 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
 
         if (debug_levels()) {
             unsigned long long top_now = 0, lt = 0;
-            cudaMemcpy(&top_now, arena_top, sizeof(top_now), cudaMemcpyDeviceToHost);
-            cudaMemcpy(&lt, list_top, sizeof(lt), cudaMemcpyDeviceToHost);
+            cudaMemcpyAsync(&top_now, arena_top, sizeof(top_now), cudaMemcpyDeviceToHost, s);
+            cudaMemcpyAsync(&lt, list_top, sizeof(lt), cudaMemcpyDeviceToHost, s);
+            cudaStreamSynchronize(s);
             const double ms = std::chrono::duration<double, std::milli>(
                 std::chrono::steady_clock::now() - t_level).count();
             std::fprintf(stderr, "[lfb] depth %d: %u cells, arena %llu clauses, lists %llu, %.3f ms\n",
@@ -2743,7 +2788,7 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
         if (!flags || !scan) return LFB_E_CUDA;
         k_branch_flags<<<(lv.n_cells + 255) / 256, 256, 0, s>>>(lv.type, lv.n_cells, flags);
         cudaMemsetAsync(flags + lv.n_cells, 0, sizeof(uint32_t), s);
-        if (!exclusive_scan(flags, scan, lv.n_cells + 1, s)) return LFB_E_CUDA;
+        if (!exclusive_scan(ws, flags, scan, lv.n_cells + 1, s)) return LFB_E_CUDA;
         uint32_t n_groups = 0;
         cudaMemcpyAsync(&n_groups, scan + lv.n_cells, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
         if (!cuda_ok(cudaStreamSynchronize(s), "scan")) return LFB_E_CUDA;
@@ -2777,8 +2822,9 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
         const uint32_t smem_regs = std::min<uint32_t>(bt.n_regs, kLeafSmemRegs);
         if (debug_levels() && L > 0) {
             std::vector<TapeRef> gt(n_leaf_groups);
-            cudaMemcpy(gt.data(), o.lv[L].group_tape, n_leaf_groups * sizeof(TapeRef),
-                       cudaMemcpyDeviceToHost);
+            cudaMemcpyAsync(gt.data(), o.lv[L].group_tape, n_leaf_groups * sizeof(TapeRef),
+                            cudaMemcpyDeviceToHost, s);
+            cudaStreamSynchronize(s);
             std::map<uint32_t, uint64_t> hist, lhist;
             uint64_t len_sum = 0;
             for (const TapeRef& t : gt) {
@@ -2849,11 +2895,12 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
         if (prof) {
             std::vector<unsigned long long> pf(8ull * n_leaf_groups);
             std::vector<TapeRef> gt(n_leaf_groups);
-            cudaMemcpy(pf.data(), prof, pf.size() * 8, cudaMemcpyDeviceToHost);
+            cudaMemcpyAsync(pf.data(), prof, pf.size() * 8, cudaMemcpyDeviceToHost, s);
             if (L > 0) {
-                cudaMemcpy(gt.data(), o.lv[L].group_tape, n_leaf_groups * sizeof(TapeRef),
-                           cudaMemcpyDeviceToHost);
+                cudaMemcpyAsync(gt.data(), o.lv[L].group_tape, n_leaf_groups * sizeof(TapeRef),
+                                cudaMemcpyDeviceToHost, s);
             }
+            cudaStreamSynchronize(s);
             std::vector<uint32_t> idx(n_leaf_groups);
             for (uint32_t k = 0; k < n_leaf_groups; ++k) idx[k] = k;
             std::sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) { return pf[8 * a] > pf[8 * b]; });
@@ -2983,7 +3030,7 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
             uint32_t* vscan = ws.get<uint32_t>(K_VSCAN, n_keys + 1);
             if (!flags || !vscan) return LFB_E_CUDA;
             k_u8_to_u32<<<(n_keys + 1 + 255) / 256, 256, 0, s>>>(used, flags, n_keys + 1);
-            if (!exclusive_scan(flags, vscan, n_keys + 1, s)) return LFB_E_CUDA;
+            if (!exclusive_scan(ws, flags, vscan, n_keys + 1, s)) return LFB_E_CUDA;
             uint32_t n_verts = 0;
             cudaMemcpyAsync(&n_verts, vscan + n_keys, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
             if (!cuda_ok(cudaStreamSynchronize(s), "vertex scan")) return LFB_E_CUDA;
@@ -3004,8 +3051,8 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
             if (!out.verts || !out.tris) return set_error(LFB_E_CAPACITY, "host allocation failed");
             out.vert_count = n_verts + 1;
             out.tri_count = n_tri;
-            if (!download(out.verts, verts, out.vert_count * sizeof(libfive_vec3), s) ||
-                !download(out.tris, tris, static_cast<size_t>(n_tri) * sizeof(libfive_tri), s)) {
+            if (!download(ws, out.verts, verts, out.vert_count * sizeof(libfive_vec3), s) ||
+                !download(ws, out.tris, tris, static_cast<size_t>(n_tri) * sizeof(libfive_tri), s)) {
                 return LFB_E_CUDA;
             }
             break;
@@ -3017,7 +3064,8 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
         cudaEventRecord(ev[4], s);
         cudaEventSynchronize(ev[4]);
         unsigned long long ce[2] = {0, 0};
-        cudaMemcpy(ce, evals, sizeof(ce), cudaMemcpyDeviceToHost);
+        cudaMemcpyAsync(ce, evals, sizeof(ce), cudaMemcpyDeviceToHost, s);
+        cudaStreamSynchronize(s);
         stats->levels = static_cast<uint32_t>(L);
         stats->cells_evaluated = cells_evaluated;
         stats->leaf_groups = n_leaf_groups;
@@ -3033,9 +3081,75 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
         stats->ms_leaf = ms[1];
         stats->ms_collapse = ms[2];
         stats->ms_dual = ms[3];
-        for (auto& e : ev) cudaEventDestroy(e);
         stats->ms_total = std::chrono::duration<double, std::milli>(
                               std::chrono::steady_clock::now() - t_start).count();
+    }
+    return 0;
+}
+
+}  // namespace
+
+int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
+                   double max_err, MeshOut& out, lfb_mesh_stats* stats)
+{
+    if (!require_device()) return LFB_E_CUDA;
+    Workspace& ws = default_workspace();
+    std::lock_guard<std::mutex> lock(ws.mu);
+    return render_in(ws, g, R, min_feature, max_err, out, stats);
+}
+
+int render_dc_meshes(MeshJob* jobs, size_t n, unsigned workers)
+{
+    if (!require_device()) return LFB_E_CUDA;
+    if (n == 0) return 0;
+    for (size_t i = 0; i < n; ++i) {
+        if (!jobs[i].g) return set_error(LFB_E_INVALID, "null tape in a mesh batch");
+    }
+    int dev = 0;
+    if (!cuda_ok(cudaGetDevice(&dev), "device")) return LFB_E_CUDA;
+
+    // Longest first, so that the last meshes to start are short ones.
+    std::vector<double> cost(n);
+    for (size_t i = 0; i < n; ++i) {
+        const MeshJob& j = jobs[i];
+        const double lo[3] = {j.R.X.lower, j.R.Y.lower, j.R.Z.lower};
+        const double hi[3] = {j.R.X.upper, j.R.Y.upper, j.R.Z.upper};
+        const int L = std::min(level_from_resolution(lo, hi, j.min_feature), 30);
+        cost[i] = static_cast<double>(j.g->reg.clauses.size() + 1) * std::ldexp(1.0, 2 * L);
+    }
+    std::vector<size_t> order(n);
+    for (size_t i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](size_t a, size_t b) { return cost[a] > cost[b]; });
+
+    workers = std::max(1u, std::min<unsigned>(workers, static_cast<unsigned>(
+                                                           std::min<size_t>(n, 16))));
+    std::atomic<size_t> next{0};
+    auto work = [&](unsigned k) {
+        cudaSetDevice(dev);
+        Workspace* ws = stream_workspace(k);
+        if (!ws) return;
+        std::lock_guard<std::mutex> lock(ws->mu);
+        for (;;) {
+            const size_t i = next.fetch_add(1);
+            if (i >= n) break;
+            MeshJob& j = jobs[order[i]];
+            clear_error();
+            j.rc = render_in(*ws, *j.g, j.R, j.min_feature, j.max_err, j.out,
+                             j.want_stats ? &j.stats : nullptr);
+            if (j.rc != 0) last_error(&j.err);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (unsigned k = 1; k < workers; ++k) pool.emplace_back(work, k);
+    work(0);
+    for (auto& t : pool) t.join();
+
+    clear_error();
+    for (size_t i = 0; i < n; ++i) {
+        const MeshJob& j = jobs[i];
+        if (j.rc == 1) return set_error(LFB_E_CUDA, "no stream context for a mesh batch");
+        if (j.rc != 0) return set_error(j.rc, j.err);
     }
     return 0;
 }

@@ -204,13 +204,12 @@ static int grid_for(uint64_t n, int block, int sm_count, int per_sm)
 
 int device_sm_count()
 {
-    static int sms = -1;
-    if (sms < 0) {
-        int dev = 0;
+    static const int sms = [] {
+        int dev = 0, n = 0;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 1;
-    }
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        return n > 0 ? n : 1;
+    }();
     return sms;
 }
 

@@ -37,6 +37,25 @@ void host_free(void* p);
 int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
                    double max_err, MeshOut& out, lfb_mesh_stats* stats);
 
+/// One mesh of a batch (render_dc_meshes).
+struct MeshJob {
+    GpuTape* g = nullptr;
+    libfive_region3 R{};
+    double min_feature = 0.0;
+    double max_err = 0.0;
+    bool want_stats = false;
+    MeshOut out;
+    lfb_mesh_stats stats{};
+    int rc = 1;            // 1 until rendered, then 0 or a negative LFB_E* code
+    std::string err;       // the failure's message
+};
+
+/// Renders n meshes with up to `workers` of them in flight at once, each on
+/// its own CUDA stream and scratch context, longest (tape length x 4^depth)
+/// first.  Returns 0 when every job succeeded, else the first failing job's
+/// code (with its message set as this thread's error).
+int render_dc_meshes(MeshJob* jobs, size_t n, unsigned workers);
+
 /// Binary STL in the reference's layout (mesh.cpp:139-194): 80-byte header,
 /// uint32 triangle count, then per triangle a zero normal, three vertices
 /// and a zero attribute word.

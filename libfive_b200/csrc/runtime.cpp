@@ -40,15 +40,15 @@ bool cuda_ok(cudaError_t e, const char* what)
 
 bool require_device()
 {
-    static int state = -1;   // -1 unknown, 0 none, 1 ok
-    if (state < 0) {
+    static const int state = [] {   // 0 none, 1 ok
         int n = 0;
         const cudaError_t e = cudaGetDeviceCount(&n);
-        state = (e == cudaSuccess && n > 0) ? 1 : 0;
-        if (!state) {
+        if (e != cudaSuccess || n <= 0) {
             cudaGetLastError();
+            return 0;
         }
-    }
+        return 1;
+    }();
     if (!state) {
         set_error(LFB_E_CUDA,
                   "no CUDA device: libfive_b200 evaluates on the GPU only");

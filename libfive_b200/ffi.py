@@ -134,6 +134,10 @@ SIGNATURES = [
     ("lfb_eval_jacobian", ctypes.c_int, [tape_t, ctypes.c_uint64, vp, vp, vp, vp, vp, ctypes.c_uint32]),
     ("lfb_eval_grad", ctypes.c_int, [tape_t, ctypes.c_uint64, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_uint32]),
     ("lfb_render_mesh", ctypes.POINTER(Mesh), [tape_t, Region3, MeshSettings, ctypes.POINTER(MeshStats)]),
+    ("lfb_render_meshes", ctypes.c_int, [ctypes.POINTER(tape_t), ctypes.c_uint32,
+                                         ctypes.POINTER(Region3), ctypes.POINTER(MeshSettings),
+                                         ctypes.c_uint32, ctypes.POINTER(ctypes.POINTER(Mesh)),
+                                         ctypes.POINTER(MeshStats)]),
     ("lfb_kernel_launches", ctypes.c_uint64, []),
     ("lfb_tree_slot_tape", ctypes.c_int, [tree_t, u32p, i32p, u32p, fp, u32p, ctypes.POINTER(vp)]),
 ]

@@ -288,6 +288,38 @@ class Tape:
         return (v, t, st) if stats else (v, t)
 
 
+def render_meshes(jobs, workers=0, stats=False):
+    """Meshes of several tapes in one lfb_render_meshes call.
+
+    jobs: sequence of (tape, lower, upper, min_feature[, max_err]); the meshes
+    render concurrently, each on its own CUDA stream.  Returns a list of
+    (verts, tris) pairs (with an MeshStats third item when stats is true), in
+    the order of jobs; raises RuntimeError if any mesh failed.
+    """
+    n = len(jobs)
+    tapes = (ffi.tape_t * n)()
+    regions = (ffi.Region3 * n)()
+    settings = (ffi.MeshSettings * n)()
+    for i, job in enumerate(jobs):
+        tape, lower, upper, min_feature = job[:4]
+        max_err = job[4] if len(job) > 4 else 1e-8
+        tapes[i] = tape.ptr
+        regions[i] = ffi.Region3(*[ffi.Interval(a, b) for a, b in zip(lower, upper)])
+        settings[i] = ffi.MeshSettings(min_feature, max_err)
+    meshes = (ctypes.POINTER(ffi.Mesh) * n)()
+    st = (ffi.MeshStats * n)()
+    rc = _lib().lfb_render_meshes(tapes, n, regions, settings, workers, meshes,
+                                  st if stats else None)
+    out = []
+    for i in range(n):
+        if meshes[i]:
+            v, t = mesh_arrays(meshes[i])
+            out.append((v, t, st[i]) if stats else (v, t))
+    if rc != 0:
+        raise RuntimeError("lfb_render_meshes failed: %s" % ffi.last_error()[1])
+    return out
+
+
 def _vars_struct(var_values):
     if not var_values:
         return ffi.Vars(None, None, 0)

@@ -7,6 +7,8 @@ difference 51-65 (min / max / max(a, -b)), blend_expt_unit 79-85 (the Python
 `blend`), with a box as the max of three slab distances and a z-cylinder as
 max(radial distance, |z - cz| - h).
 """
+import math
+
 import numpy as np
 
 from .shape import Shape, X, Y, Z
@@ -121,6 +123,21 @@ def random_csg(n_prims=2000, seed=2, size=(0.02, 0.2)):
             nxt.append(level[-1])
         level = nxt
     return level[0]
+
+
+def batch_specs(n_trees=512, seed=11, prims=(8, 4000), resolutions=(64, 128, 256, 512)):
+    """Per-tree (primitive count, tree seed, resolution per unit) of the
+    many-tree meshing workload: primitive counts log-uniform over `prims`,
+    resolutions drawn uniformly from `resolutions` (over a 3-unit region:
+    octree depths 8, 9, 10 and 11)."""
+    rng = SplitMix64(seed)
+    lo, hi = math.log(prims[0]), math.log(prims[1])
+    out = []
+    for i in range(n_trees):
+        n = int(round(math.exp(rng.uniform(lo, hi))))
+        res = resolutions[min(int(rng.uniform() * len(resolutions)), len(resolutions) - 1)]
+        out.append((n, seed * 100003 + i, res))
+    return out
 
 
 def blended_spheres_vars(n=256, seed=4, m=0.05):

@@ -134,6 +134,18 @@ libfive_mesh* lfb_render_mesh(lfb_tape t, libfive_region3 R,
                               lfb_mesh_settings settings,
                               lfb_mesh_stats* stats);
 
+/* Heightmap::render (heightmap.cpp:247-296) on the GPU over the Voxels
+ * region (voxels.cpp:16-44) of lower / upper / res (per-axis voxels per
+ * unit; 0 gives one sample).  dims receives {cols, rows, z samples}; when
+ * depth is not NULL it receives rows x cols floats (row-major, row = y):
+ * the highest z sample at which the shape is filled, -inf where none is;
+ * norm (NULL to skip) receives the packed normals (0xAABBGGRR of the
+ * normalised gradient mapped to 0..255, 0xffff7f7f at the top sample, 0
+ * where empty).  Call with depth NULL to size the arrays. */
+int lfb_render_heightmap(lfb_tape t, const float lower[3], const float upper[3],
+                         const float res[3], uint32_t dims[3], float* depth,
+                         uint32_t* norm);
+
 /* n meshes in one call, each tape over its own region with its own
  * settings.  The reference has no such call (libfive_tree_save_meshes,
  * libfive.cpp:419-440, renders its trees one after another through

@@ -12,6 +12,7 @@
 
 #include "libfive.h"
 #include "libfive_b200.h"
+#include "heightmap.hpp"
 #include "mesher.hpp"
 #include "eval_api.hpp"
 #include "runtime.hpp"
@@ -277,12 +278,32 @@ void libfive_tree_save_slice(libfive_tree, libfive_region2, float, float,
                          "provided by libfive_b200\n");
 }
 
-libfive_pixels* libfive_tree_render_pixels(libfive_tree, libfive_region2,
-                                           float, float)
+libfive_pixels* libfive_tree_render_pixels(libfive_tree tree, libfive_region2 R,
+                                           float z, float res)
 {
-    std::fprintf(stderr, "libfive_tree_render_pixels: pixel rendering is "
-                         "not provided by libfive_b200\n");
-    return nullptr;
+    // libfive.cpp:442-465: a one-sample-deep Voxels region at height z, the
+    // height map rendered, and a pixel set wherever the depth is finite.
+    clear_error();
+    if (!tree) return nullptr;
+    const float lo[3] = {R.X.lower, R.Y.lower, z};
+    const float hi[3] = {R.X.upper, R.Y.upper, z};
+    const float r3[3] = {res, res, res};
+    const VoxelGrid V = make_voxel_grid(lo, hi, r3);
+    auto g = cached_tape(N(tree));
+    const size_t w = V.pts[0].size(), h = V.pts[1].size();
+    std::vector<float> depth(w * h);
+    if (!g || render_heightmap(*g, V, depth.data(), nullptr) != 0) {
+        std::string msg;
+        last_error(&msg);
+        std::fprintf(stderr, "libfive_tree_render_pixels: %s\n", msg.c_str());
+        return nullptr;
+    }
+    auto out = new libfive_pixels;
+    out->width = static_cast<uint32_t>(w);
+    out->height = static_cast<uint32_t>(h);
+    out->pixels = new bool[w * h];
+    for (size_t i = 0; i < w * h; ++i) out->pixels[i] = !std::isinf(depth[i]);
+    return out;
 }
 
 ////////////////////////////////////////////////////////////////////////////////
@@ -585,6 +606,19 @@ libfive_mesh* lfb_render_mesh(lfb_tape t, libfive_region3 R,
         return nullptr;
     }
     return mesh.release();
+}
+
+int lfb_render_heightmap(lfb_tape t, const float lower[3], const float upper[3],
+                         const float res[3], uint32_t dims[3], float* depth, uint32_t* norm)
+{
+    clear_error();
+    if (!t || !lower || !upper || !res || !dims) {
+        return set_error(LFB_E_INVALID, "null argument");
+    }
+    const VoxelGrid V = make_voxel_grid(lower, upper, res);
+    for (int a = 0; a < 3; ++a) dims[a] = static_cast<uint32_t>(V.pts[a].size());
+    if (!depth) return 0;
+    return render_heightmap(*t->g, V, depth, norm);
 }
 
 int lfb_render_meshes(const lfb_tape* tapes, uint32_t n, const libfive_region3* regions,

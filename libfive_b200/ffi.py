@@ -19,6 +19,15 @@ class Interval(ctypes.Structure):
     _fields_ = [("lower", ctypes.c_float), ("upper", ctypes.c_float)]
 
 
+class Region2(ctypes.Structure):
+    _fields_ = [("X", Interval), ("Y", Interval)]
+
+
+class Pixels(ctypes.Structure):
+    _fields_ = [("pixels", ctypes.POINTER(ctypes.c_bool)), ("width", ctypes.c_uint32),
+                ("height", ctypes.c_uint32)]
+
+
 class Region3(ctypes.Structure):
     _fields_ = [("X", Interval), ("Y", Interval), ("Z", Interval)]
 
@@ -79,7 +88,7 @@ SIGNATURES = [
     ("libfive_contours3_delete", None, [vp]),
     ("libfive_mesh_delete", None, [ctypes.POINTER(Mesh)]),
     ("libfive_mesh_coords_delete", None, [vp]),
-    ("libfive_pixels_delete", None, [vp]),
+    ("libfive_pixels_delete", None, [ctypes.POINTER(Pixels)]),
     ("libfive_opcode_enum", ctypes.c_int, [ctypes.c_char_p]),
     ("libfive_opcode_args", ctypes.c_int, [ctypes.c_int]),
     ("libfive_vars_delete", None, [vp]),
@@ -104,16 +113,16 @@ SIGNATURES = [
     ("libfive_tree_optimized", tree_t, [tree_t]),
     ("libfive_tree_print", ctypes.c_void_p, [tree_t]),
     ("libfive_free_str", None, [ctypes.c_void_p]),
-    ("libfive_tree_render_slice", vp, [tree_t, vp, ctypes.c_float, ctypes.c_float]),
-    ("libfive_tree_render_slice3", vp, [tree_t, vp, ctypes.c_float, ctypes.c_float]),
-    ("libfive_tree_save_slice", None, [tree_t, vp, ctypes.c_float, ctypes.c_float, ctypes.c_char_p]),
+    ("libfive_tree_render_slice", vp, [tree_t, Region2, ctypes.c_float, ctypes.c_float]),
+    ("libfive_tree_render_slice3", vp, [tree_t, Region2, ctypes.c_float, ctypes.c_float]),
+    ("libfive_tree_save_slice", None, [tree_t, Region2, ctypes.c_float, ctypes.c_float, ctypes.c_char_p]),
     ("libfive_tree_render_mesh", ctypes.POINTER(Mesh), [tree_t, Region3, ctypes.c_float]),
     ("libfive_tree_render_mesh_st", ctypes.POINTER(Mesh), [tree_t, Region3, ctypes.c_float]),
     ("libfive_tree_render_mesh_coords", vp, [tree_t, Region3, ctypes.c_float]),
     ("libfive_tree_save_mesh", ctypes.c_bool, [tree_t, Region3, ctypes.c_float, ctypes.c_char_p]),
     ("libfive_evaluator_save_mesh", ctypes.c_bool, [vp, Region3, ctypes.c_char_p]),
     ("libfive_tree_save_meshes", ctypes.c_bool, [ctypes.POINTER(tree_t), Region3, ctypes.c_float, ctypes.c_float, ctypes.c_char_p]),
-    ("libfive_tree_render_pixels", vp, [tree_t, vp, ctypes.c_float, ctypes.c_float]),
+    ("libfive_tree_render_pixels", ctypes.POINTER(Pixels), [tree_t, Region2, ctypes.c_float, ctypes.c_float]),
     ("libfive_tree_evaluator", vp, [tree_t, Vars]),
     ("libfive_evaluator_update_vars", ctypes.c_bool, [vp, Vars]),
     ("libfive_evaluator_delete", None, [vp]),
@@ -134,6 +143,7 @@ SIGNATURES = [
     ("lfb_eval_jacobian", ctypes.c_int, [tape_t, ctypes.c_uint64, vp, vp, vp, vp, vp, ctypes.c_uint32]),
     ("lfb_eval_grad", ctypes.c_int, [tape_t, ctypes.c_uint64, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_uint32]),
     ("lfb_render_mesh", ctypes.POINTER(Mesh), [tape_t, Region3, MeshSettings, ctypes.POINTER(MeshStats)]),
+    ("lfb_render_heightmap", ctypes.c_int, [tape_t, fp, fp, fp, u32p, fp, u32p]),
     ("lfb_render_meshes", ctypes.c_int, [ctypes.POINTER(tape_t), ctypes.c_uint32,
                                          ctypes.POINTER(Region3), ctypes.POINTER(MeshSettings),
                                          ctypes.c_uint32, ctypes.POINTER(ctypes.POINTER(Mesh)),

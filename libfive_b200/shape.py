@@ -288,6 +288,28 @@ class Tape:
         return (v, t, st) if stats else (v, t)
 
 
+def render_heightmap(tape, lower, upper, res, normals=True):
+    """Heightmap::render of a Tape over the Voxels region lower / upper at
+    `res` voxels per unit (a number or one per axis): (depth, norm) as
+    rows x cols arrays (norm is None when normals is false)."""
+    res = res if np.ndim(res) else (res, res, res)
+    lo, hi, r = (np.ascontiguousarray(np.asarray(v, np.float32).reshape(3))
+                 for v in (lower, upper, res))
+    fp = ctypes.POINTER(ctypes.c_float)
+    dims = np.zeros(3, np.uint32)
+    lib = _lib()
+    args = (lo.ctypes.data_as(fp), hi.ctypes.data_as(fp), r.ctypes.data_as(fp),
+            dims.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)))
+    ffi.check(lib.lfb_render_heightmap(tape.ptr, *args, None, None))
+    cols, rows = int(dims[0]), int(dims[1])
+    depth = np.empty((rows, cols), np.float32)
+    norm = np.empty((rows, cols), np.uint32) if normals else None
+    ffi.check(lib.lfb_render_heightmap(
+        tape.ptr, *args, depth.ctypes.data_as(fp),
+        norm.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)) if normals else None))
+    return depth, norm
+
+
 def render_meshes(jobs, workers=0, stats=False):
     """Meshes of several tapes in one lfb_render_meshes call.
 

@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "oracle_eval.hpp"
+#include "oracle_heightmap.hpp"
 
 using namespace ora;
 
@@ -176,6 +177,24 @@ int ora_features(void* h_, float x, float y, float z, float* out, int max)
         ++i;
     }
     return static_cast<int>(fs.size());
+}
+
+void ora_voxel_dims(const float lower[3], const float upper[3], const float res[3],
+                    uint32_t dims[3])
+{
+    voxel_dims(lower, upper, res, dims);
+}
+
+void ora_voxel_pts(const float lower[3], const float upper[3], const float res[3], int axis,
+                   float* out)
+{
+    voxel_pts(lower, upper, res, axis, out);
+}
+
+void ora_render_heightmap(void* h_, const float lower[3], const float upper[3],
+                          const float res[3], int workers, float* depth, uint32_t* norm)
+{
+    render_heightmap(static_cast<Handle*>(h_)->tape, lower, upper, res, workers, depth, norm);
 }
 
 }  // extern "C"

@@ -31,6 +31,9 @@ def load():
         _lib.ora_is_inside.argtypes = [vp, ctypes.c_float, ctypes.c_float, ctypes.c_float]
         _lib.ora_features.restype = ctypes.c_int
         _lib.ora_features.argtypes = [vp, ctypes.c_float, ctypes.c_float, ctypes.c_float, vp, ctypes.c_int]
+        _lib.ora_voxel_dims.argtypes = [vp, vp, vp, vp]
+        _lib.ora_voxel_pts.argtypes = [vp, vp, vp, ctypes.c_int, vp]
+        _lib.ora_render_heightmap.argtypes = [vp, vp, vp, vp, ctypes.c_int, vp, vp]
         if hasattr(_lib, "ora_render_mesh"):
             _lib.ora_render_mesh.restype = ctypes.c_int
             _lib.ora_render_mesh.argtypes = [vp] + [ctypes.c_float] * 6 + [
@@ -113,3 +116,37 @@ class OracleTape:
         out = np.zeros((max_n, 3), np.float32)
         n = load().ora_features(self.h, *p, _p(out), max_n)
         return out[:min(n, max_n)]
+
+
+def _f3(v):
+    return np.ascontiguousarray(np.asarray(v, np.float32).reshape(3))
+
+
+def _region(lower, upper, res):
+    res = res if np.ndim(res) else (res, res, res)
+    return _f3(lower), _f3(upper), _f3(res)
+
+
+def voxel_dims(lower, upper, res):
+    """(cols, rows, depth samples) of a Voxels region (voxels.cpp:23-44)."""
+    lo, hi, r = _region(lower, upper, res)
+    dims = np.zeros(3, np.uint32)
+    load().ora_voxel_dims(_p(lo), _p(hi), _p(r), _p(dims))
+    return tuple(int(d) for d in dims)
+
+
+def voxel_pts(lower, upper, res, axis):
+    lo, hi, r = _region(lower, upper, res)
+    out = np.zeros(voxel_dims(lower, upper, res)[axis], np.float32)
+    load().ora_voxel_pts(_p(lo), _p(hi), _p(r), axis, _p(out))
+    return out
+
+
+def render_heightmap(tape, lower, upper, res, workers=8):
+    """Heightmap::render restated: (depth, norm), rows x cols."""
+    lo, hi, r = _region(lower, upper, res)
+    w, h, _ = voxel_dims(lower, upper, res)
+    depth = np.zeros((h, w), np.float32)
+    norm = np.zeros((h, w), np.uint32)
+    load().ora_render_heightmap(tape.h, _p(lo), _p(hi), _p(r), workers, _p(depth), _p(norm))
+    return depth, norm

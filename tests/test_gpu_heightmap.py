@@ -62,7 +62,7 @@ def test_thin_and_anisotropic(gpu):
 def test_render_pixels_c_api(gpu):
     # libfive.cpp:442-465: pixels = finite depth of a one-sample-deep region
     lib = ffi.load()
-    shape = workloads.random_csg(60, seed=6)
+    shape = workloads.spheres_union(24, seed=3)
     R2 = ffi.Region2(ffi.Interval(-1.5, 1.5), ffi.Interval(-1.2, 1.4))
     for z, res in ((0.1, 40.0), (-0.35, 17.5)):
         p = lib.libfive_tree_render_pixels(shape.ptr, R2, z, res)

@@ -66,7 +66,8 @@ def parse():
     p.add_argument("--depth", type=int, default=10,
                    help="octree depth; 10 is the benchmark workload, smaller "
                         "depths are for profiling captures")
-    p.add_argument("--workload", default="csg2000", choices=["csg2000", "batch"],
+    p.add_argument("--workload", default="csg2000",
+                   choices=["csg2000", "batch", "eval", "adjoint"],
                    help="batch: many trees of mixed size and depth, meshed "
                         "one after another and through lfb_render_meshes")
     p.add_argument("--trees", type=int, default=512, help="batch workload: tree count")
@@ -438,11 +439,119 @@ def run_batch(args, world, rank, local):
                                    "depth 8-11" % n, "workers": args.workers}}))
 
 
+def _timed(fn, steps, warmup, flush):
+    """Device time of `steps` calls of fn (CUDA events on the current stream;
+    L2 flushed before each call, outside the events)."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    total = 0.0
+    for _ in range(steps):
+        flush.fill_(1)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        b.synchronize()
+        total += a.elapsed_time(b)
+    return total / steps
+
+
+def run_eval(args, world, rank, local):
+    """Point evaluation throughput: the union of 64 spheres (centres
+    U[-1,1]^3, radii U[0.1,0.35], seed 1 + rank) on the 128^3 inclusive
+    lattice over [-1.5,1.5]^3 (2,097,152 points), values and values +
+    derivatives, points resident on the device; e2e passes host arrays."""
+    import numpy as np
+    import torch
+    from libfive_b200 import workloads
+    from libfive_b200.shape import Tape
+    torch.cuda.set_device(local)
+    tape = Tape(workloads.spheres_union(64, seed=1 + rank))
+    pts = workloads.lattice(128)
+    n = len(pts[0])
+    x, y, z = (torch.from_numpy(a).cuda() for a in pts)
+    f, dx, dy, dz = (torch.empty(n, device="cuda") for _ in range(4))
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    st = lambda: torch.cuda.current_stream().cuda_stream  # noqa: E731
+    t_val = _timed(lambda: tape.values(x, y, z, out=f, stream=st()), args.steps, args.warmup, flush)
+    t_der = _timed(lambda: tape.derivs(x, y, z, v=f, dx=dx, dy=dy, dz=dz, stream=st()),
+                   args.steps, args.warmup, flush)
+    hx, hy, hz = (np.ascontiguousarray(a) for a in pts)
+    hf = np.empty(n, np.float32)
+    t_e2e = _timed(lambda: tape.values(hx, hy, hz, out=hf), args.steps, args.warmup, flush)
+    ce = n * tape.n_clauses
+    if rank == 0:
+        print(json.dumps({
+            "metric": "clause-evals/s", "value": ce / (t_val / 1e3), "unit": "clause-evals/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_val,
+            "higher_is_better": True, "deriv_value": ce / (t_der / 1e3), "ms_deriv": t_der,
+            "e2e": {"value": ce / (t_e2e / 1e3), "unit": "clause-evals/s",
+                    "h2d_bytes_per_step": 12 * n, "d2h_bytes_per_step": 4 * n},
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "64-sphere union, 128^3 lattice", "points": n,
+                       "clauses": tape.n_clauses, "l2": "flushed before each step"}}))
+
+
+def run_adjoint(args, world, rank, local):
+    """Gradients of loss = mean f(p)^2 with respect to 1024 free variables
+    (256 blended spheres' centres and radii) and the 2^22 points, the points
+    sampled area-uniformly from the mesh (64 voxels per unit) of a second
+    seed's spheres.
+    One step = the forward values, the seed 2 f / N, and the reverse sweep."""
+    import numpy as np
+    import torch
+    from libfive_b200 import workloads
+    from libfive_b200.shape import Tape
+    torch.cuda.set_device(local)
+    shape, vals = workloads.blended_spheres_vars(256, seed=4 + rank)
+    tape = Tape(shape, vals)
+    target, tvals = workloads.blended_spheres_vars(256, seed=1004 + rank)
+    v, t = Tape(target, tvals).render_mesh((-1.5,) * 3, (1.5,) * 3, 1.0 / 64)
+    tri = v[t.astype(np.int64)].astype(np.float64)
+    area = 0.5 * np.linalg.norm(np.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0]), axis=1)
+    rng = np.random.Generator(np.random.PCG64(7 + rank))
+    n = 1 << 22
+    k = rng.choice(len(tri), size=n, p=area / area.sum())
+    u, w = rng.random(n), rng.random(n)
+    flip = u + w > 1
+    u[flip], w[flip] = 1 - u[flip], 1 - w[flip]
+    p = tri[k, 0] + u[:, None] * (tri[k, 1] - tri[k, 0]) + w[:, None] * (tri[k, 2] - tri[k, 0])
+    x, y, z = (torch.from_numpy(np.ascontiguousarray(p[:, a], np.float32)).cuda() for a in range(3))
+    f, seed, gx, gy, gz = (torch.empty(n, device="cuda") for _ in range(5))
+    gv = torch.zeros(tape.n_vars, device="cuda")
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+
+    def step():
+        s = torch.cuda.current_stream().cuda_stream
+        tape.values(x, y, z, out=f, stream=s)
+        torch.mul(f, 2.0 / n, out=seed)
+        gv.zero_()
+        tape.grad(x, y, z, seed=seed, f=f, gx=gx, gy=gy, gz=gz, gvars=gv, stream=s)
+
+    ms = _timed(step, args.steps, args.warmup, flush)
+    comps = n * (3 + tape.n_vars)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "grads/s", "value": comps / (ms / 1e3), "unit": "gradient components/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "loss_grads_per_s": 1e3 / ms, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "256 blended spheres, 1024 free variables, 2^22 surface points",
+                       "points": n, "vars": tape.n_vars, "clauses": tape.n_clauses}}))
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
     if args.workload == "batch":
         run_batch(args, world, rank, local)
+    elif args.workload == "eval":
+        run_eval(args, world, rank, local)
+    elif args.workload == "adjoint":
+        run_adjoint(args, world, rank, local)
     elif args.impl == "reference":
         run_reference(args, world, rank)
     else:

@@ -67,7 +67,7 @@ def parse():
                    help="octree depth; 10 is the benchmark workload, smaller "
                         "depths are for profiling captures")
     p.add_argument("--workload", default="csg2000",
-                   choices=["csg2000", "batch", "eval", "adjoint"],
+                   choices=["csg2000", "batch", "eval", "adjoint", "heightmap"],
                    help="batch: many trees of mixed size and depth, meshed "
                         "one after another and through lfb_render_meshes")
     p.add_argument("--trees", type=int, default=512, help="batch workload: tree count")
@@ -543,6 +543,46 @@ def run_adjoint(args, world, rank, local):
                        "points": n, "vars": tape.n_vars, "clauses": tape.n_clauses}}))
 
 
+def run_heightmap(args, world, rank, local):
+    """Height maps: the 64-sphere union (seed 1 + rank) over [-1.5,1.5]^3 at
+    512 / 3 voxels per unit (512^3 voxels: a 512 x 512 image with 512 z
+    samples), depth and normals, downloaded to the host every step.  The
+    CPU line is the oracle's restatement of Heightmap::render on one core,
+    on a 128^3 grid of the same region, scaled by the voxel count."""
+    import numpy as np
+    import torch
+    from libfive_b200 import workloads
+    from libfive_b200.shape import Tape, render_heightmap
+    torch.cuda.set_device(local)
+    shape = workloads.spheres_union(64, seed=1 + rank)
+    tape = Tape(shape)
+    lo, hi, res = (-1.5,) * 3, (1.5,) * 3, 512 / 3.0
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    out = {}
+    ms = _timed(lambda: out.update(r=render_heightmap(tape, lo, hi, res)), args.steps,
+                args.warmup, flush)
+    depth, _ = out["r"]
+    voxels = depth.size * 512
+    line = {
+        "metric": "height-map voxels/s", "value": voxels / (ms / 1e3), "unit": "voxels/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+        "filled_pixels": int(np.isfinite(depth).sum()),
+        "config": {"workload": "64-sphere union height map, 512^3 voxels",
+                   "clauses": tape.n_clauses}}
+    if rank == 0 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from oracle_ffi import OracleTape, render_heightmap as oracle_heightmap
+        ora = OracleTape(shape)
+        t0 = time.perf_counter()
+        oracle_heightmap(ora, lo, hi, 128 / 3.0, workers=1)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": 128 ** 3 / dt, "unit": "voxels/s", "cores": 1,
+                                "kind": "port", "sample": "128^3 grid of the same region"}
+    if rank == 0:
+        print(json.dumps(line))
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
@@ -552,6 +592,8 @@ def main():
         run_eval(args, world, rank, local)
     elif args.workload == "adjoint":
         run_adjoint(args, world, rank, local)
+    elif args.workload == "heightmap":
+        run_heightmap(args, world, rank, local)
     elif args.impl == "reference":
         run_reference(args, world, rank)
     else:

@@ -2657,8 +2657,9 @@ int render_in(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_fe
         cudaMemsetAsync(wL1, 0, scratch_warps * nw1 * 4, s);
     }
     const size_t wide_smem = sizeof(WideSmem) * 8;
-    cudaFuncSetAttribute(k_interval_wide, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         static_cast<int>(wide_smem));
+    if (!raise_smem_limit(reinterpret_cast<const void*>(k_interval_wide), wide_smem)) {
+        return LFB_E_CUDA;
+    }
     // Two list arenas, one per parity of depth: depth d reads the lists of
     // its groups from one and writes its children's lists to the other.
     const int list_key[2] = {K_LIST_A, K_LIST_B};
@@ -2678,8 +2679,9 @@ int render_in(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_fe
     uint8_t* glast = ws.get<uint8_t>(K_GLAST, static_cast<size_t>(group_warps) * 8 * kRenumberMax);
     if (!gdec || !glast) return LFB_E_CUDA;
     if (group_smem > 48 * 1024) {
-        cudaFuncSetAttribute(k_interval_group, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(group_smem));
+        if (!raise_smem_limit(reinterpret_cast<const void*>(k_interval_group), group_smem)) {
+            return LFB_E_CUDA;
+        }
     }
     bool group_mode = false;
 
@@ -2851,8 +2853,9 @@ int render_in(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_fe
         if (smem > 220 * 1024) {
             return set_error(LFB_E_UNSUPPORTED, "tape register file too large for the leaf kernel");
         }
-        cudaFuncSetAttribute(k_leaf_groups, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(smem));
+        if (!raise_smem_limit(reinterpret_cast<const void*>(k_leaf_groups), smem)) {
+            return LFB_E_CUDA;
+        }
         int per_sm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_leaf_groups, 32 * wpb, smem);
         per_sm = std::max(per_sm, 1);
@@ -2939,8 +2942,9 @@ int render_in(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_fe
         while (block > 32 && static_cast<size_t>(bt.n_regs) * block * 4 > 96 * 1024) block /= 2;
         const size_t smem = static_cast<size_t>(bt.n_regs) * block * 4;
         if (smem > 48 * 1024) {
-            cudaFuncSetAttribute(k_collapse_level, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem));
+            if (!raise_smem_limit(reinterpret_cast<const void*>(k_collapse_level), smem)) {
+                return LFB_E_CUDA;
+            }
         }
         for (int d = L - 1; d >= 0; --d) {
             const uint32_t n = o.lv[d].n_cells;

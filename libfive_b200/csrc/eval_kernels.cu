@@ -12,6 +12,7 @@
 //   IntervalEvaluator::eval      (libfive/src/eval/eval_interval.cpp:68-93)
 // which process at most 256 points per pass on one CPU thread.
 #include "eval_kernels.cuh"
+#include "runtime.hpp"
 
 namespace lfb {
 
@@ -222,12 +223,8 @@ cudaError_t launch_values(const DevTape& t, uint32_t n, const float* x,
     const int block = 128;
     const size_t smem = static_cast<size_t>(t.n_regs) * block * PTS * sizeof(float);
     if (smem > 200 * 1024) return cudaErrorInvalidConfiguration;
-    static size_t configured = 0;
-    if (smem > 48 * 1024 && smem > configured) {
-        cudaFuncSetAttribute(k_values<PTS>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(smem));
-        configured = smem;
+    if (!raise_smem_limit(reinterpret_cast<const void*>(k_values<PTS>), smem)) {
+        return cudaErrorInvalidValue;
     }
     const int grid = grid_for((n + PTS - 1) / PTS, block, device_sm_count(), 16);
     k_values<PTS><<<grid, block, smem, s>>>(t, n, x, y, z, out);
@@ -242,11 +239,8 @@ cudaError_t launch_derivs(const DevTape& t, uint32_t n, const float* x,
     const int block = 128;
     const size_t smem = static_cast<size_t>(t.n_regs) * block * 4 * sizeof(float);
     if (smem > 200 * 1024) return cudaErrorInvalidConfiguration;
-    static size_t configured = 0;
-    if (smem > 48 * 1024 && smem > configured) {
-        cudaFuncSetAttribute(k_derivs, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(smem));
-        configured = smem;
+    if (!raise_smem_limit(reinterpret_cast<const void*>(k_derivs), smem)) {
+        return cudaErrorInvalidValue;
     }
     const int grid = grid_for(n, block, device_sm_count(), 16);
     k_derivs<<<grid, block, smem, s>>>(t, n, x, y, z, v, dx, dy, dz);
@@ -263,12 +257,8 @@ cudaError_t launch_intervals(const DevTape& t, uint32_t n, const float* xlo,
     const int block = 128;
     const size_t smem = static_cast<size_t>(t.n_regs) * block * (2 * sizeof(float) + 1);
     if (smem > 200 * 1024) return cudaErrorInvalidConfiguration;
-    static size_t configured = 0;
-    if (smem > 48 * 1024 && smem > configured) {
-        cudaFuncSetAttribute(k_intervals,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(smem));
-        configured = smem;
+    if (!raise_smem_limit(reinterpret_cast<const void*>(k_intervals), smem)) {
+        return cudaErrorInvalidValue;
     }
     const int grid = grid_for(n, block, device_sm_count(), 16);
     k_intervals<<<grid, block, smem, s>>>(t, n, xlo, xhi, ylo, yhi, zlo, zhi,

@@ -208,10 +208,7 @@ constexpr int kBlock = 128;
 
 bool set_smem(const void* fn, size_t bytes)
 {
-    if (bytes <= 48 * 1024) return true;
-    return cuda_ok(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(bytes)),
-                   "shared memory size");
+    return raise_smem_limit(fn, bytes);
 }
 
 int jacobian_device(GpuTape& g, uint64_t n, const float* x, const float* y, const float* z,

@@ -16,10 +16,12 @@
 //   2. per tile, the highest filled slab sets a depth floor (its top
 //      sample) and the ambiguous slabs above it are the only ones that can
 //      raise it;
-//   3. those slabs are evaluated voxel by voxel, top slab first, one round
-//      per slab depth, skipping tiles whose pixels are all above the slab;
-//      each inside voxel raises its pixel's depth with an atomic max on an
-//      order-preserving integer key;
+//   3. those slabs are processed top slab first, one round per slab depth,
+//      skipping tiles whose pixels are all above the slab: each selected
+//      box is refined into 4 x 4 x 4 sub-boxes, classified by interval
+//      again (a filled sub-box raises its pixels to its top sample), and
+//      only the ambiguous sub-boxes are evaluated voxel by voxel; depths
+//      rise by an atomic max on an order-preserving integer key;
 //   4. normals are the normalised gradient at (x, y, depth) of each pixel
 //      (DerivArrayEvaluator, as NormalRenderer does, heightmap.cpp:35-53).
 //
@@ -164,45 +166,132 @@ __global__ void k_hm_select(Grid g, uint32_t s, const uint8_t* need, const uint3
     }
 }
 
-/// Sample points of boxes list[0..n): box i owns points [i * vpb, (i+1) * vpb),
-/// voxel (i, j, k) of the box at (k * 16 + j) * 16 + i; voxels past the
-/// image edge repeat the last row / column (their results are ignored).
-__global__ void k_hm_points(Grid g, const uint32_t* list, uint32_t n, float* x, float* y,
-                            float* z)
+/// Each selected box is refined into sub-boxes of 4 x 4 pixels x 4 z samples
+/// (fewer at the image edge and in short slabs) before any voxel is
+/// evaluated: sub-box j of a box covers pixel columns 4 (j % 4), rows
+/// 4 ((j / 4) % 4) of its tile and the j / 16-th group of 4 z samples from
+/// the top of its slab.
+constexpr uint32_t kSub = 4;
+
+struct SubRange {
+    uint32_t x0, x1, y0, y1, z0, z1;
+    bool valid;
+};
+
+__device__ __forceinline__ uint32_t sub_depth(const Grid& g)
 {
-    const uint64_t q = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const uint32_t vpb = kTile * kTile * g.tz;
-    if (q >= static_cast<uint64_t>(n) * vpb) return;
-    const uint32_t b = list[q / vpb], v = q % vpb;
+    return min(kSub, g.tz);
+}
+
+__device__ SubRange sub_range(const Grid& g, uint32_t b, uint32_t j)
+{
     const uint32_t s = b % g.ns, t = b / g.ns;
     const uint32_t tx = t % g.ntx, ty = t / g.ntx;
     uint32_t k0, k1;
     slab_range(g, s, &k0, &k1);
-    const uint32_t xi = min(g.W - 1, tx * kTile + v % kTile);
-    const uint32_t yi = min(g.H - 1, ty * kTile + (v / kTile) % kTile);
-    const uint32_t zi = min(k1 - 1, k0 + v / (kTile * kTile));
+    const uint32_t sd = sub_depth(g);
+    SubRange r;
+    r.x0 = tx * kTile + (j % 4) * kSub;
+    r.x1 = min(g.W, r.x0 + kSub);
+    r.y0 = ty * kTile + ((j / 4) % 4) * kSub;
+    r.y1 = min(g.H, r.y0 + kSub);
+    const uint32_t dz = (j / 16) * sd;
+    r.valid = r.x0 < r.x1 && r.y0 < r.y1 && dz < k1 - k0;
+    r.z1 = r.valid ? k1 - dz : k1;
+    r.z0 = (r.z1 - k0 > sd) ? r.z1 - sd : k0;
+    if (!r.valid) {
+        r.x0 = r.y0 = 0;
+        r.x1 = r.y1 = 1;
+    }
+    return r;
+}
+
+/// Bounds of the sub-boxes of boxes list[0..n), nsub per box (invalid
+/// sub-boxes get the first voxel's bounds; classification skips them).
+__global__ void k_hm_subboxes(Grid g, const uint32_t* list, uint32_t n, uint32_t nsub,
+                              float* xlo, float* xhi, float* ylo, float* yhi, float* zlo,
+                              float* zhi)
+{
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n * nsub) return;
+    const SubRange r = sub_range(g, list[q / nsub], q % nsub);
+    auto span = [](const float* p, uint32_t i0, uint32_t i1, float* lo, float* hi) {
+        const float a = p[i0], c = p[i1 - 1];
+        *lo = a < c ? a : c;
+        *hi = a < c ? c : a;
+    };
+    span(g.px, r.x0, r.x1, xlo + q, xhi + q);
+    span(g.py, r.y0, r.y1, ylo + q, yhi + q);
+    span(g.pz, r.z0, r.z1, zlo + q, zhi + q);
+}
+
+/// Filled sub-boxes raise their pixels to the sub-box's top sample; the
+/// ambiguous ones with a pixel still below that sample are listed for
+/// voxel evaluation (entry = q, the sub-box's index in this chunk).
+__global__ void k_hm_subclassify(Grid g, const uint32_t* list, uint32_t n, uint32_t nsub,
+                                 const float* lo, const float* hi, uint32_t* pix_key,
+                                 uint32_t* amb, uint32_t* n_amb)
+{
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n * nsub) return;
+    const SubRange r = sub_range(g, list[q / nsub], q % nsub);
+    if (!r.valid) return;
+    const uint32_t top = depth_key(g.pz[r.z1 - 1]);
+    if (hi[q] < 0) {
+        for (uint32_t y = r.y0; y < r.y1; ++y) {
+            for (uint32_t x = r.x0; x < r.x1; ++x) {
+                atomicMax(pix_key + static_cast<size_t>(y) * g.W + x, top);
+            }
+        }
+        return;
+    }
+    if (lo[q] > 0) return;
+    bool below = false;
+    for (uint32_t y = r.y0; y < r.y1; ++y) {
+        for (uint32_t x = r.x0; x < r.x1; ++x) {
+            below |= pix_key[static_cast<size_t>(y) * g.W + x] < top;
+        }
+    }
+    if (below) amb[atomicAdd(n_amb, 1u)] = q;
+}
+
+/// Voxel v of listed sub-box e: column v % 4, row (v / 4) % 4, z sample
+/// v / 16 from the sub-box's bottom; false past its edge.
+__device__ __forceinline__ bool sub_voxel(const Grid& g, const uint32_t* list, uint32_t nsub,
+                                          uint32_t e, uint32_t v, uint32_t* xi, uint32_t* yi,
+                                          uint32_t* zi)
+{
+    const SubRange r = sub_range(g, list[e / nsub], e % nsub);
+    const uint32_t x = r.x0 + v % kSub, y = r.y0 + (v / kSub) % kSub;
+    const uint32_t z = r.z0 + v / (kSub * kSub);
+    *xi = min(x, r.x1 - 1);
+    *yi = min(y, r.y1 - 1);
+    *zi = min(z, r.z1 - 1);
+    return x < r.x1 && y < r.y1 && z < r.z1;
+}
+
+/// Sample points of the listed sub-boxes amb[0..n), vps points each.
+__global__ void k_hm_points(Grid g, const uint32_t* list, uint32_t nsub, const uint32_t* amb,
+                            uint32_t n, uint32_t vps, float* x, float* y, float* z)
+{
+    const uint64_t q = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (q >= static_cast<uint64_t>(n) * vps) return;
+    uint32_t xi, yi, zi;
+    sub_voxel(g, list, nsub, amb[q / vps], q % vps, &xi, &yi, &zi);
     x[q] = g.px[xi];
     y[q] = g.py[yi];
     z[q] = g.pz[zi];
 }
 
 /// Raises each pixel's depth to every inside voxel's z.
-__global__ void k_hm_reduce(Grid g, const uint32_t* list, uint32_t n, const float* f,
-                            uint32_t* pix_key)
+__global__ void k_hm_reduce(Grid g, const uint32_t* list, uint32_t nsub, const uint32_t* amb,
+                            uint32_t n, uint32_t vps, const float* f, uint32_t* pix_key)
 {
     const uint64_t q = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const uint32_t vpb = kTile * kTile * g.tz;
-    if (q >= static_cast<uint64_t>(n) * vpb) return;
+    if (q >= static_cast<uint64_t>(n) * vps) return;
     if (!(f[q] < 0)) return;
-    const uint32_t b = list[q / vpb], v = q % vpb;
-    const uint32_t s = b % g.ns, t = b / g.ns;
-    const uint32_t tx = t % g.ntx, ty = t / g.ntx;
-    uint32_t k0, k1;
-    slab_range(g, s, &k0, &k1);
-    const uint32_t xi = tx * kTile + v % kTile;
-    const uint32_t yi = ty * kTile + (v / kTile) % kTile;
-    const uint32_t zi = k0 + v / (kTile * kTile);
-    if (xi >= g.W || yi >= g.H || zi >= k1) return;
+    uint32_t xi, yi, zi;
+    if (!sub_voxel(g, list, nsub, amb[q / vps], q % vps, &xi, &yi, &zi)) return;
     atomicMax(pix_key + static_cast<size_t>(yi) * g.W + xi, depth_key(g.pz[zi]));
 }
 
@@ -276,7 +365,7 @@ __global__ void k_hm_fill(uint32_t* p, uint64_t n, uint32_t v)
 /// Device buffers of the height-map driver, grow-only, reused across calls.
 struct HmBuffers {
     std::mutex mu;
-    DevBuf b[24];
+    DevBuf b[26];
     template <class T>
     T* get(int k, size_t count)
     {
@@ -319,9 +408,15 @@ int render_heightmap(GpuTape& g, const VoxelGrid& V, float* depth, uint32_t* nor
     const uint64_t n_tiles = static_cast<uint64_t>(gr.ntx) * gr.nty;
     const uint64_t nb = n_tiles * gr.ns;
     const uint64_t npix = W * H;
-    const uint32_t vpb = kTile * kTile * gr.tz;
-    const uint32_t chunk_boxes = std::max<uint32_t>(1, (1u << 22) / vpb);
-    const uint64_t chunk = static_cast<uint64_t>(chunk_boxes) * vpb;
+    // Sub-boxes per box and voxels per sub-box; boxes are refined 1024 at a
+    // time, ambiguous sub-boxes evaluated up to 2^22 voxels at a time.
+    const uint32_t sub_d = std::min(4u, gr.tz);
+    const uint32_t nsub = 16 * ((gr.tz + sub_d - 1) / sub_d);
+    const uint32_t vps = 16 * sub_d;
+    const uint32_t chunk_boxes = 1024;
+    const uint64_t n_sub = static_cast<uint64_t>(chunk_boxes) * nsub;
+    const uint32_t chunk_amb = (1u << 22) / vps;
+    const uint64_t chunk = static_cast<uint64_t>(chunk_amb) * vps;
 
     float* px = B.get<float>(0, W);
     float* py = B.get<float>(1, H);
@@ -334,18 +429,24 @@ int render_heightmap(GpuTape& g, const VoxelGrid& V, float* depth, uint32_t* nor
     uint32_t* floor_key = B.get<uint32_t>(8, n_tiles);
     uint32_t* pix_key = B.get<uint32_t>(9, npix);
     uint32_t* list = B.get<uint32_t>(10, std::max<uint64_t>(n_tiles, npix));
-    uint32_t* count = B.get<uint32_t>(11, 1);
+    uint32_t* count = B.get<uint32_t>(11, 2);
     float* cx = B.get<float>(12, std::max<uint64_t>(chunk, npix));
     float* cy = B.get<float>(13, std::max<uint64_t>(chunk, npix));
     float* cz = B.get<float>(14, std::max<uint64_t>(chunk, npix));
     float* cf = B.get<float>(15, std::max<uint64_t>(chunk, npix));
+    float* sbox = B.get<float>(21, 6 * n_sub);
+    float* slo = B.get<float>(22, n_sub);
+    float* shi = B.get<float>(23, n_sub);
+    uint8_t* snan = B.get<uint8_t>(24, n_sub);
+    uint32_t* amb = B.get<uint32_t>(25, n_sub);
     float* d_depth = B.get<float>(16, npix);
     uint32_t* d_norm = norm ? B.get<uint32_t>(17, npix) : nullptr;
     float* gdx = norm ? B.get<float>(18, npix) : nullptr;
     float* gdy = norm ? B.get<float>(19, npix) : nullptr;
     float* gdz = norm ? B.get<float>(20, npix) : nullptr;
     if (!px || !py || !pz || !box || !ilo || !ihi || !inan || !need || !floor_key ||
-        !pix_key || !list || !count || !cx || !cy || !cz || !cf || !d_depth ||
+        !pix_key || !list || !count || !cx || !cy || !cz || !cf || !d_depth || !sbox ||
+        !slo || !shi || !snan || !amb ||
         (norm && (!d_norm || !gdx || !gdy || !gdz))) {
         return LFB_E_CUDA;
     }
@@ -384,12 +485,33 @@ int render_heightmap(GpuTape& g, const VoxelGrid& V, float* depth, uint32_t* nor
         if (!cuda_ok(cudaStreamSynchronize(s), "height map slab selection")) return LFB_E_CUDA;
         for (uint32_t c0 = 0; c0 < n; c0 += chunk_boxes) {
             const uint32_t m = std::min(chunk_boxes, n - c0);
-            const uint64_t q = static_cast<uint64_t>(m) * vpb;
-            k_hm_points<<<blocks_for(q, 256), 256, 0, s>>>(gr, list + c0, m, cx, cy, cz);
-            rc = eval_values_device(g, q, cx, cy, cz, cf, s);
+            const uint32_t q = m * nsub;
+            const uint32_t* lc = list + c0;
+            k_hm_subboxes<<<blocks_for(q, 256), 256, 0, s>>>(gr, lc, m, nsub, sbox, sbox + n_sub,
+                                                             sbox + 2 * n_sub, sbox + 3 * n_sub,
+                                                             sbox + 4 * n_sub, sbox + 5 * n_sub);
+            rc = eval_intervals_device(g, q, sbox, sbox + n_sub, sbox + 2 * n_sub,
+                                       sbox + 3 * n_sub, sbox + 4 * n_sub, sbox + 5 * n_sub,
+                                       slo, shi, snan, s);
             if (rc) return rc;
-            k_hm_reduce<<<blocks_for(q, 256), 256, 0, s>>>(gr, list + c0, m, cf, pix_key);
+            cudaMemsetAsync(count + 1, 0, sizeof(uint32_t), s);
+            k_hm_subclassify<<<blocks_for(q, 256), 256, 0, s>>>(gr, lc, m, nsub, slo, shi,
+                                                                pix_key, amb, count + 1);
             launches += 2;
+            uint32_t na = 0;
+            cudaMemcpyAsync(&na, count + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+            if (!cuda_ok(cudaStreamSynchronize(s), "height map refinement")) return LFB_E_CUDA;
+            for (uint32_t a0 = 0; a0 < na; a0 += chunk_amb) {
+                const uint32_t ma = std::min(chunk_amb, na - a0);
+                const uint64_t nv = static_cast<uint64_t>(ma) * vps;
+                k_hm_points<<<blocks_for(nv, 256), 256, 0, s>>>(gr, lc, nsub, amb + a0, ma, vps,
+                                                                cx, cy, cz);
+                rc = eval_values_device(g, nv, cx, cy, cz, cf, s);
+                if (rc) return rc;
+                k_hm_reduce<<<blocks_for(nv, 256), 256, 0, s>>>(gr, lc, nsub, amb + a0, ma, vps,
+                                                                cf, pix_key);
+                launches += 2;
+            }
         }
     }
     k_hm_finalize<<<blocks_for(npix, 256), 256, 0, s>>>(gr, pix_key, floor_key, d_depth, d_norm);

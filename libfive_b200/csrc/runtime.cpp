@@ -1,5 +1,7 @@
 #include "runtime.hpp"
 
+#include <map>
+
 #include <atomic>
 #include <cstdio>
 
@@ -54,6 +56,25 @@ bool require_device()
                   "no CUDA device: libfive_b200 evaluates on the GPU only");
         return false;
     }
+    return true;
+}
+
+bool raise_smem_limit(const void* fn, size_t bytes)
+{
+    if (bytes <= 48 * 1024) return true;
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, size_t> limits;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    size_t& cur = limits[{dev, fn}];
+    if (bytes <= cur) return true;
+    if (!cuda_ok(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(bytes)),
+                 "shared memory size")) {
+        return false;
+    }
+    cur = bytes;
     return true;
 }
 

@@ -64,6 +64,12 @@ struct DevBuf {
     template <class T> T* as() const { return static_cast<T*>(ptr); }
 };
 
+/// Lets `fn` (a __global__ function) be launched with `bytes` of dynamic
+/// shared memory on the current device.  The limit only ever rises, under a
+/// lock, so that a thread that has raised it for its launch cannot have it
+/// lowered by another thread between the raise and the launch.
+bool raise_smem_limit(const void* fn, size_t bytes);
+
 /// Counts kernel launches of this library (reported by lfb_kernel_launches).
 void note_launches(uint64_t n);
 uint64_t launches();

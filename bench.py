@@ -532,12 +532,15 @@ def run_adjoint(args, world, rank, local):
         tape.grad(x, y, z, seed=seed, f=f, gx=gx, gy=gy, gz=gz, gvars=gv, stream=s)
 
     ms = _timed(step, args.steps, args.warmup, flush)
+    ms_fwd = _timed(lambda: tape.values(x, y, z, out=f, stream=torch.cuda.current_stream().cuda_stream),
+                    args.steps, args.warmup, flush)
     comps = n * (3 + tape.n_vars)
     if rank == 0:
         print(json.dumps({
             "metric": "grads/s", "value": comps / (ms / 1e3), "unit": "gradient components/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "higher_is_better": True, "loss_grads_per_s": 1e3 / ms, "dtype": "f32",
+            "higher_is_better": True, "loss_grads_per_s": 1e3 / ms,
+            "ms_forward": ms_fwd, "step_over_forward": ms / ms_fwd, "dtype": "f32",
             "data": "synthetic",
             "config": {"workload": "256 blended spheres, 1024 free variables, 2^22 surface points",
                        "points": n, "vars": tape.n_vars, "clauses": tape.n_clauses}}))

@@ -1,6 +1,9 @@
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "mesher.hpp"
 
@@ -29,18 +32,34 @@ bool save_stl(const char* path, const std::vector<libfive_mesh*>& meshes)
     uint32_t count = 0;
     for (auto m : meshes) count += m->tri_count;
     std::fwrite(&count, sizeof(count), 1, f);
+    // Records are packed into one buffer by a few threads and written with
+    // one call per mesh (a write per 50-byte record is the slow part of a
+    // large file).
+    std::vector<unsigned char> body;
     for (auto m : meshes) {
-        for (uint32_t i = 0; i < m->tri_count; ++i) {
-            unsigned char rec[50];
-            std::memset(rec, 0, sizeof(rec));
-            const uint32_t idx[3] = {m->tris[i].a, m->tris[i].b, m->tris[i].c};
-            for (int k = 0; k < 3; ++k) {
-                const libfive_vec3& v = m->verts[idx[k]];
-                const float xyz[3] = {v.x, v.y, v.z};
-                std::memcpy(rec + 12 + 12 * k, xyz, 12);
+        const size_t n = m->tri_count;
+        body.assign(n * 50, 0);
+        auto pack = [&](size_t lo, size_t hi) {
+            for (size_t i = lo; i < hi; ++i) {
+                unsigned char* rec = body.data() + 50 * i;
+                const uint32_t idx[3] = {m->tris[i].a, m->tris[i].b, m->tris[i].c};
+                for (int k = 0; k < 3; ++k) {
+                    const libfive_vec3& v = m->verts[idx[k]];
+                    const float xyz[3] = {v.x, v.y, v.z};
+                    std::memcpy(rec + 12 + 12 * k, xyz, 12);
+                }
             }
-            std::fwrite(rec, 1, sizeof(rec), f);
+        };
+        const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+        const size_t n_threads = std::min<size_t>(std::min(hw, 8u), std::max<size_t>(1, n >> 16));
+        const size_t part = (n + n_threads - 1) / n_threads;
+        std::vector<std::thread> pool;
+        for (size_t t = 1; t < n_threads; ++t) {
+            pool.emplace_back(pack, std::min(n, t * part), std::min(n, (t + 1) * part));
         }
+        pack(0, std::min(n, part));
+        for (auto& th : pool) th.join();
+        if (n) std::fwrite(body.data(), 1, body.size(), f);
     }
     const bool ok = std::ferror(f) == 0;
     std::fclose(f);

@@ -26,6 +26,10 @@ enum : uint32_t {
     ST_FEATURE_OVERFLOW = 1u << 3,
     ST_REGS = 1u << 4,
     ST_LIST_OVERFLOW = 1u << 5,
+    // which feature-evaluator capacity ST_FEATURE_OVERFLOW ran into
+    ST_FEAT_EPS = 1u << 6,    // epsilon directions of one feature
+    ST_FEAT_LIST = 1u << 7,   // features of one register
+    ST_FEAT_TMP = 1u << 8,    // candidate features of one clause
 };
 
 /// A level-ordered clause list (WideEntry) in a list arena, with the list

@@ -234,7 +234,7 @@ __device__ inline bool feat_push(const FeatCtx& C, float* f, const float* e_)
         if (!dup) {
             const int n = static_cast<int>(f[3]);
             if (n >= kMaxEps) {
-                atomicOr(C.status, ST_FEATURE_OVERFLOW);
+                atomicOr(C.status, ST_FEATURE_OVERFLOW | ST_FEAT_EPS);
                 return false;
             }
             f[4 + 3 * n] = e[0]; f[5 + 3 * n] = e[1]; f[6 + 3 * n] = e[2];
@@ -454,7 +454,7 @@ static __device__ __noinline__ void feat_eval(const FeatCtx& C, const DevTape& b
                         }
                         if (found) continue;
                         if (n >= kMaxEps) {
-                            atomicOr(C.status, ST_FEATURE_OVERFLOW);
+                            atomicOr(C.status, ST_FEATURE_OVERFLOW | ST_FEAT_EPS);
                             break;
                         }
 #pragma unroll
@@ -475,10 +475,10 @@ static __device__ __noinline__ void feat_eval(const FeatCtx& C, const DevTape& b
         }
 
         int nt = 0;
-        bool overflow = false;
+        bool overflow = false, tmp_over = false;
         auto emit = [&](const float* f) -> float* {
             if (nt >= kTmpFeat) {
-                overflow = true;
+                tmp_over = true;
                 return nullptr;
             }
             float* d = T->feats[nt++];
@@ -604,8 +604,10 @@ static __device__ __noinline__ void feat_eval(const FeatCtx& C, const DevTape& b
                 nt = 1;
             }
         }
-        if (nt > kMaxFeat || overflow) {
-            atomicOr(C.status, ST_FEATURE_OVERFLOW);
+        if (nt > kMaxFeat || overflow || tmp_over) {
+            atomicOr(C.status, ST_FEATURE_OVERFLOW | (overflow ? ST_FEAT_EPS : 0u) |
+                                   (tmp_over ? ST_FEAT_TMP : 0u) |
+                                   (nt > kMaxFeat ? ST_FEAT_LIST : 0u));
             if (nt > kMaxFeat) nt = kMaxFeat;
         }
         for (int i = 0; i < nt; ++i) feat_copy(out + i * kFeatFloats, T->feats[i]);

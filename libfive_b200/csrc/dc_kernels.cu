@@ -2969,8 +2969,18 @@ int render_in(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_fe
     if (!cuda_ok(cudaStreamSynchronize(s), "leaf/collapse")) return LFB_E_CUDA;
     if (st & ST_RECORD_OVERFLOW) return set_error(LFB_E_CAPACITY, "leaf record overflow");
     if (st & ST_FEATURE_OVERFLOW) {
+        std::string why;
+        if (st & ST_FEAT_EPS) {
+            why += " (more than " + std::to_string(kMaxEps) + " epsilon directions in a feature)";
+        }
+        if (st & ST_FEAT_LIST) {
+            why += " (more than " + std::to_string(kMaxFeat) + " features in a clause)";
+        }
+        if (st & ST_FEAT_TMP) {
+            why += " (more than " + std::to_string(kTmpFeat) + " candidate features in a clause)";
+        }
         return set_error(LFB_E_CAPACITY,
-                         "feature list overflow at a non-smooth sample point");
+                         "feature list overflow at a non-smooth sample point" + why);
     }
 
     // Dual walk.

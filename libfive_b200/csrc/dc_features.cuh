@@ -3,22 +3,23 @@
 // eval_feature.cpp:56-372, and Feature, libfive/src/eval/feature.cpp:14-284).
 //
 // These points are rare, so one lane of the warp runs the evaluator serially
-// while the others wait.  Its workspace is the warp's register-file slice in
-// shared memory (free at every call site) plus a small per-warp scratch
-// area: every register holds up to kMaxFeat features of up to kMaxEps
-// epsilon directions.  Capacity overflows are reported through the status
+// while the others wait.  Its workspace is a per-warp slice of global memory
+// (kRegBlock floats per tape register) plus a small per-warp scratch area:
+// every register holds up to kMaxFeat features of up to kMaxEps epsilon
+// directions.  Capacity overflows are reported through the status
 // word (ST_FEATURE_OVERFLOW), never silently truncated.
 #pragma once
 #include "dc_device.cuh"
 
 namespace lfb {
 
-constexpr int kMaxFeat = 7;          // per register
+constexpr int kMaxFeat = 15;         // per register
 constexpr int kMaxEps = 4;           // per feature
 constexpr int kFeatFloats = 16;      // deriv[3], neps, eps[4][3]
-constexpr int kRegBlock = 128;       // floats per register in the workspace
-constexpr int kValOff = kMaxFeat * kFeatFloats;          // 112
-constexpr int kCountOff = kValOff + 1;                   // 113
+constexpr int kRegBlock = 256;       // floats per register in the workspace
+constexpr int kValOff = kMaxFeat * kFeatFloats;          // 240
+constexpr int kCountOff = kValOff + 1;                   // 241
+static_assert(kCountOff < kRegBlock, "feature lists must fit a register block");
 constexpr int kTmpFeat = 64;         // candidate features of one clause
 constexpr int kTmpCorners = 168;     // plane triples in Feature::check: C(11, 3) = 165
 

@@ -1246,6 +1246,7 @@ struct LeafArgs {
     uint32_t* next_group;       // work counter (zero at launch)
     const uint32_t* order;      // processing order of the groups (or null)
     unsigned long long* prof;   // debug: 8 per group (cycles by section, feature calls, E)
+    float* featws;              // per warp: n_regs x kRegBlock floats of feature lists
 };
 
 __global__ void __launch_bounds__(256, 3)
@@ -1256,8 +1257,8 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
     const int lane = threadIdx.x & 31;
     const int wpb = blockDim.x >> 5;
     LeafWarpShared* S = reinterpret_cast<LeafWarpShared*>(lsmem) + warp;
-    // Register file of the tape interpreters and the feature evaluator
-    // (n_regs x 4 x 32 floats): in shared memory when the group's tape uses
+    // Register file of the tape interpreters (n_regs x 4 x 32 floats): in
+    // shared memory when the group's tape uses
     // at most A.smem_regs registers (leaf tapes are renumbered compactly, so
     // nearly all do), else in a per-warp slice of global memory.
     float* Rs = reinterpret_cast<float*>(lsmem + kLeafSmallBytes * wpb) +
@@ -1313,7 +1314,9 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
     float* R = rs ? Rs : Rgl;
     const uint32_t rsoff = static_cast<uint32_t>(reinterpret_cast<unsigned char*>(Rs) - lsmem);
 #define RF_CALL(fn, ...) (rs ? fn<true>(__VA_ARGS__) : fn<false>(__VA_ARGS__))
-    const FeatCtx fc{R, &W->fs, A.status};
+    const FeatCtx fc{A.featws + (static_cast<size_t>(blockIdx.x) * wpb + warp) *
+                                    A.bt.n_regs * kRegBlock,
+                     &W->fs, A.status};
 
     // --- corners (dc_tree.inl:156-239) ---------------------------------
     const int npts = n * n * n;
@@ -2314,7 +2317,7 @@ enum BufKey {
     K_CUBTMP, K_TASK_A, K_TASK_B, K_TRIS, K_USED, K_VSCAN, K_VERTS, K_FEAT,
     K_LIST_A, K_LIST_B, K_WIDE_S, K_WIDE_SN, K_WIDE_P, K_WIDE_LIVE, K_WIDE_NEW,
     K_WIDE_ST2, K_WIDE_L1, K_WIDE_WL, K_LEAF_RD, K_ORDER_K0, K_ORDER_K1,
-    K_ORDER_V0, K_ORDER_V1, K_SORTTMP, K_PROF, K_GDEC, K_GLAST,
+    K_ORDER_V0, K_ORDER_V1, K_SORTTMP, K_PROF, K_GDEC, K_GLAST, K_FEATWS,
     K_LEVEL = 100,
 };
 
@@ -2891,8 +2894,11 @@ int render_in(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_fe
         }
         unsigned long long* prof = nullptr;
         if (debug_levels()) prof = ws.get<unsigned long long>(K_PROF, 8ull * n_leaf_groups);
+        float* featws = ws.get<float>(K_FEATWS, static_cast<size_t>(grid) * wpb * bt.n_regs *
+                                                    kRegBlock);
+        if (!featws) return LFB_E_CUDA;
         LeafArgs A{o, bt, arena, recs, rec_top, static_cast<uint32_t>(rec_cap), status,
-                   evals, scratch, rd, smem_regs, next_group, order, prof};
+                   evals, scratch, rd, smem_regs, next_group, order, prof, featws};
         k_leaf_groups<<<grid, 32 * wpb, smem, s>>>(A, n_leaf_groups);
         if (!cuda_ok(cudaGetLastError(), "leaf kernel")) return LFB_E_CUDA;
         if (prof) {

@@ -129,7 +129,11 @@ __device__ __forceinline__ float warp_sum(float v)
 /// the start; X, Y, Z adjoints are registers 0-2 at the end.  With
 /// block_const_var, CONST_VAR stops the adjoint (variable gradients, as
 /// clear_vars does in the forward Jacobian); otherwise it passes through
-/// (point gradients, as in DerivArrayEvaluator).
+/// (point gradients, as in DerivArrayEvaluator).  Variable adjoints are
+/// summed over the warp, then (SV) over the block in shared memory, and
+/// reach gvars with one atomic add per variable and block; without SV
+/// (too many variables for shared memory) each warp adds to gvars.
+template <bool SV>
 __global__ void __launch_bounds__(128)
 k_grad_backward(DevTape t, uint32_t m, const float2* __restrict__ P,
                 const float* __restrict__ seed, float* __restrict__ gx,
@@ -143,13 +147,22 @@ k_grad_backward(DevTape t, uint32_t m, const float2* __restrict__ P,
     const uint32_t i = blockIdx.x * B + tid;
     const bool ok = i < m;
     float* A = smem;
+    float* Gv = smem + t.n_regs * B;
+    const uint32_t n_vars = t.n_cpool - t.n_const;
+    if (SV && gvars) {
+        for (uint32_t k = tid; k < n_vars; k += B) Gv[k] = 0.0f;
+        __syncthreads();
+    }
+    auto add_var = [&](uint32_t k, float g) {
+        const float w = warp_sum(g);
+        if (lane == 0 && w != 0.0f) atomicAdd((SV ? Gv : gvars) + k, w);
+    };
     for (uint32_t r = 0; r < t.n_regs; ++r) A[r * B + tid] = 0.0f;
     const float s0 = ok ? (seed ? seed[i] : 1.0f) : 0.0f;
     if (t.root_kind == OPND_REG) {
         A[t.root * B + tid] = s0;
     } else if (t.root_kind == OPND_VAR && gvars) {
-        const float w = warp_sum(s0);
-        if (lane == 0 && w != 0.0f) atomicAdd(gvars + (t.root - t.n_const), w);
+        add_var(t.root - t.n_const, s0);
     }
     for (int64_t c = static_cast<int64_t>(t.n) - 1; c >= 0; --c) {
         const uint2 raw = __ldg(reinterpret_cast<const uint2*>(t.clauses + c));
@@ -165,16 +178,14 @@ k_grad_backward(DevTape t, uint32_t m, const float2* __restrict__ P,
         if (ka == OPND_REG) {
             A[ra * B + tid] += ga;
         } else if (ka == OPND_VAR && gvars) {
-            const float w = warp_sum(ga);
-            if (lane == 0 && w != 0.0f) atomicAdd(gvars + (ra - t.n_const), w);
+            add_var(ra - t.n_const, ga);
         }
         if (dev_is_binary(o)) {
             const float gb = adj * pd.y;
             if (kb == OPND_REG) {
                 A[rb * B + tid] += gb;
             } else if (kb == OPND_VAR && gvars) {
-                const float w = warp_sum(gb);
-                if (lane == 0 && w != 0.0f) atomicAdd(gvars + (rb - t.n_const), w);
+                add_var(rb - t.n_const, gb);
             }
         }
     }
@@ -182,6 +193,12 @@ k_grad_backward(DevTape t, uint32_t m, const float2* __restrict__ P,
         if (gx) gx[i] = A[0 * B + tid];
         if (gy) gy[i] = A[1 * B + tid];
         if (gz) gz[i] = A[2 * B + tid];
+    }
+    if (SV && gvars) {
+        __syncthreads();
+        for (uint32_t k = tid; k < n_vars; k += B) {
+            if (Gv[k] != 0.0f) atomicAdd(gvars + k, Gv[k]);
+        }
     }
 }
 
@@ -242,20 +259,39 @@ int grad_device(GpuTape& g, uint64_t n, const float* x, const float* y, const fl
     if (n == 0) return 0;
     const size_t smem = static_cast<size_t>(t.n_regs) * kBlock * sizeof(float);
     if (smem > 200 * 1024) return set_error(LFB_E_UNSUPPORTED, "tape needs too many registers");
+    // Variable adjoints are gathered per block in shared memory when they fit.
+    const size_t smem_sv = smem + static_cast<size_t>(t.n_cpool - t.n_const) * sizeof(float);
+    const bool sv = smem_sv <= 200 * 1024;
     if (!set_smem(reinterpret_cast<const void*>(k_grad_forward), smem) ||
-        !set_smem(reinterpret_cast<const void*>(k_grad_backward), smem)) {
+        !set_smem(reinterpret_cast<const void*>(k_grad_backward<false>), smem) ||
+        (sv && !set_smem(reinterpret_cast<const void*>(k_grad_backward<true>), smem_sv))) {
         return LFB_E_CUDA;
     }
     // Partials take 8 bytes per clause and point: points per launch so that
-    // they stay within 1 GiB.
+    // they stay within 4 GiB (enough points to fill the GPU for tapes of
+    // tens of thousands of clauses).
     const uint64_t per_point = std::max<uint64_t>(8ull * t.n, 8);
     const uint64_t chunk = std::max<uint64_t>(kBlock, std::min<uint64_t>(
-        (1ull << 30) / per_point / kBlock * kBlock, uint64_t(1) << 22));
+        (4ull << 30) / per_point / kBlock * kBlock, uint64_t(1) << 22));
     auto& st = grad_staging();
     if (!st.partials.reserve(std::min(chunk, n) * per_point)) return LFB_E_CUDA;
     float2* P = st.partials.as<float2>();
     const bool has_cv = tape_has_const_var(g);
     const bool want_xyz = gx || gy || gz;
+    auto backward = [&](uint32_t m, unsigned blocks, const float* sd, uint64_t off, bool xyz,
+                        float* gv, int block_cv) {
+        float* ox = xyz && gx ? gx + off : nullptr;
+        float* oy = xyz && gy ? gy + off : nullptr;
+        float* oz = xyz && gz ? gz + off : nullptr;
+        if (gv && sv) {
+            k_grad_backward<true><<<blocks, kBlock, smem_sv, s>>>(t, m, P, sd, ox, oy, oz, gv,
+                                                                  block_cv);
+        } else {
+            k_grad_backward<false><<<blocks, kBlock, smem, s>>>(t, m, P, sd, ox, oy, oz, gv,
+                                                                block_cv);
+        }
+        note_launches(1);
+    };
     for (uint64_t off = 0; off < n; off += chunk) {
         const uint32_t m = static_cast<uint32_t>(std::min(chunk, n - off));
         const unsigned blocks = (m + kBlock - 1) / kBlock;
@@ -264,25 +300,11 @@ int grad_device(GpuTape& g, uint64_t n, const float* x, const float* y, const fl
         note_launches(1);
         const float* sd = seed ? seed + off : nullptr;
         if (!has_cv) {
-            if (want_xyz || gvars) {
-                k_grad_backward<<<blocks, kBlock, smem, s>>>(
-                    t, m, P, sd, gx ? gx + off : nullptr, gy ? gy + off : nullptr,
-                    gz ? gz + off : nullptr, gvars, 0);
-                note_launches(1);
-            }
+            if (want_xyz || gvars) backward(m, blocks, sd, off, true, gvars, 0);
         } else {
             // CONST_VAR passes point gradients but blocks variable ones.
-            if (want_xyz) {
-                k_grad_backward<<<blocks, kBlock, smem, s>>>(
-                    t, m, P, sd, gx ? gx + off : nullptr, gy ? gy + off : nullptr,
-                    gz ? gz + off : nullptr, nullptr, 0);
-                note_launches(1);
-            }
-            if (gvars) {
-                k_grad_backward<<<blocks, kBlock, smem, s>>>(
-                    t, m, P, sd, nullptr, nullptr, nullptr, gvars, 1);
-                note_launches(1);
-            }
+            if (want_xyz) backward(m, blocks, sd, off, true, nullptr, 0);
+            if (gvars) backward(m, blocks, sd, off, false, gvars, 1);
         }
         if (!cuda_ok(cudaGetLastError(), "gradient kernels")) return LFB_E_CUDA;
     }

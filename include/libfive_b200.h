@@ -150,8 +150,8 @@ int lfb_render_heightmap(lfb_tape t, const float lower[3], const float upper[3],
  * settings.  The reference has no such call (libfive_tree_save_meshes,
  * libfive.cpp:419-440, renders its trees one after another through
  * Mesh::render, mesh.cpp:35-125); here up to `workers` meshes are in flight
- * at once, each on its own CUDA stream with its own scratch buffers, longest
- * first (0 workers: 4).  meshes[i] receives tape i's mesh (free it with
+ * at once, each on its own CUDA stream with its own scratch buffers (0
+ * workers: 4); large meshes run one at a time beside the small ones.  meshes[i] receives tape i's mesh (free it with
  * libfive_mesh_delete), or NULL if that mesh failed; stats is NULL or an
  * array of n.  Returns 0 when every mesh succeeded, else the first failure's
  * LFB_E* code (message from lfb_last_error). */

@@ -3144,26 +3144,71 @@ int render_dc_meshes(MeshJob* jobs, size_t n, unsigned workers)
 
     workers = std::max(1u, std::min<unsigned>(workers, static_cast<unsigned>(
                                                            std::min<size_t>(n, 16))));
-    std::atomic<size_t> next{0};
-    auto work = [&](unsigned k) {
-        cudaSetDevice(dev);
-        Workspace* ws = stream_workspace(k);
-        if (!ws) return;
-        std::lock_guard<std::mutex> lock(ws->mu);
+    // Large meshes (tape length x 4^depth above kBigCost) fill the GPU on
+    // their own and need the most scratch memory: worker 0 renders them one
+    // after another while the other workers render the small ones side by
+    // side; worker 0 joins them when the large ones are done.
+    constexpr double kBigCost = 2e9;
+    std::vector<size_t> big, small;
+    for (size_t i : order) (cost[i] >= kBigCost && workers > 1 ? big : small).push_back(i);
+    std::atomic<size_t> next_big{0}, next_small{0};
+    auto run_queue = [&](Workspace* ws, const std::vector<size_t>& q, std::atomic<size_t>& next) {
         for (;;) {
             const size_t i = next.fetch_add(1);
-            if (i >= n) break;
-            MeshJob& j = jobs[order[i]];
+            if (i >= q.size()) break;
+            MeshJob& j = jobs[q[i]];
             clear_error();
             j.rc = render_in(*ws, *j.g, j.R, j.min_feature, j.max_err, j.out,
                              j.want_stats ? &j.stats : nullptr);
             if (j.rc != 0) last_error(&j.err);
         }
     };
+    auto work = [&](unsigned k) {
+        cudaSetDevice(dev);
+        Workspace* ws = stream_workspace(k);
+        if (!ws) return;
+        std::lock_guard<std::mutex> lock(ws->mu);
+        if (k == 0) run_queue(ws, big, next_big);
+        run_queue(ws, small, next_small);
+    };
     std::vector<std::thread> pool;
     for (unsigned k = 1; k < workers; ++k) pool.emplace_back(work, k);
     work(0);
     for (auto& t : pool) t.join();
+
+    // A mesh that ran out of device memory while others were in flight is
+    // rendered again alone, after the other contexts (and the single-call
+    // context, when idle) have given their buffers back.
+    std::vector<size_t> retry;
+    for (size_t i = 0; i < n; ++i) {
+        if (jobs[i].rc == LFB_E_CUDA && jobs[i].err.find("out of memory") != std::string::npos) {
+            retry.push_back(i);
+        }
+    }
+    if (!retry.empty()) {
+        cudaDeviceSynchronize();
+        cudaGetLastError();
+        for (unsigned k = 1; k < workers; ++k) {
+            Workspace* w = stream_workspace(k);
+            std::lock_guard<std::mutex> lock(w->mu);
+            w->bufs.clear();
+        }
+        {
+            Workspace& d = default_workspace();
+            std::unique_lock<std::mutex> lock(d.mu, std::try_to_lock);
+            if (lock.owns_lock()) d.bufs.clear();
+        }
+        Workspace* w = stream_workspace(0);
+        std::lock_guard<std::mutex> lock(w->mu);
+        for (size_t i : retry) {
+            MeshJob& j = jobs[i];
+            clear_error();
+            j.err.clear();
+            j.rc = render_in(*w, *j.g, j.R, j.min_feature, j.max_err, j.out,
+                             j.want_stats ? &j.stats : nullptr);
+            if (j.rc != 0) last_error(&j.err);
+        }
+    }
 
     clear_error();
     for (size_t i = 0; i < n; ++i) {

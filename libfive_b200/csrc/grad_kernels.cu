@@ -6,12 +6,15 @@
 //    and CONST_VAR clears tangents (clear_vars).  Each output is the same
 //    sequence of float operations as the reference's per-variable column.
 //  * k_grad_forward / k_grad_backward: reverse mode (the reference has none).
-//    The forward pass stores every clause's local partials (the forward
+//    The forward pass stores the clauses' local partials (the forward
 //    derivative rules of DerivArrayEvaluator, eval_deriv_array.cpp:119-256,
-//    applied to unit tangents, so min / max / abs pick the same branch); the
+//    applied to unit tangents, so min / max / abs pick the same branch),
+//    except those fixed by the opcode (partial_kind); the
 //    backward pass walks the register tape from the end, one adjoint per
 //    register, and sends variable adjoints to a warp-reduced atomic sum.
 #include <cfloat>
+#include <mutex>
+#include <vector>
 
 #include "eval_api.hpp"
 #include "eval_kernels.cuh"
@@ -81,18 +84,48 @@ k_jacobian(DevTape t, uint32_t n, uint32_t n_vars, const float* __restrict__ X,
     }
 }
 
+/// How a clause's local partials (d out / d a, d out / d b for unit
+/// tangents) reach the backward pass: PK_CONST ones are fixed by the opcode
+/// (ADD, SUB, NEG, CONST_VAR, COPY: exactly 1 or -1), PK_CHOICE (MIN, MAX)
+/// store d out / d a (0 or 1; the other is its complement), PK_ONE (other
+/// unary ops) store d out / d a, PK_TWO (other binary ops) store both.
+/// Slots are numbered per tape; a point's partials take n_pslot floats.
+enum : uint32_t { PK_CONST = 0, PK_CHOICE = 1, PK_ONE = 2, PK_TWO = 3 };
+
+uint32_t partial_kind(uint8_t o)
+{
+    switch (o) {
+        case op::ADD: case op::SUB: case op::NEG: case op::CONST_VAR: case OP_COPY:
+            return PK_CONST;
+        case op::MIN: case op::MAX:
+            return PK_CHOICE;
+        default:
+            return op::arity(o) == 2 ? PK_TWO : PK_ONE;
+    }
+}
+
+__device__ __forceinline__ float2 const_partials(uint8_t o)
+{
+    switch (o) {
+        case op::ADD: return make_float2(1.0f, 1.0f);
+        case op::SUB: return make_float2(1.0f, -1.0f);
+        case op::NEG: return make_float2(-1.0f, 0.0f);
+        default: return make_float2(1.0f, 0.0f);   // CONST_VAR, COPY
+    }
+}
+
 __device__ __forceinline__ float gv_fetch(uint8_t kind, uint16_t idx, const float* R, int tid,
                                           int B, const float* __restrict__ cp)
 {
     return kind == OPND_REG ? R[idx * B + tid] : __ldg(cp + idx);
 }
 
-/// Forward pass of the reverse mode: value of every clause, and its local
-/// partials d out / d a, d out / d b stored at P[c * m + i] (one float2).
+/// Forward pass of the reverse mode: value of every clause, and the local
+/// partials its kind keeps, at P[slot * m + i] (and slot + 1 for PK_TWO).
 __global__ void __launch_bounds__(128)
-k_grad_forward(DevTape t, uint32_t m, const float* __restrict__ X,
-               const float* __restrict__ Y, const float* __restrict__ Z,
-               float2* __restrict__ P, float* __restrict__ f)
+k_grad_forward(DevTape t, const uint32_t* __restrict__ pslot, uint32_t m,
+               const float* __restrict__ X, const float* __restrict__ Y,
+               const float* __restrict__ Z, float* __restrict__ P, float* __restrict__ f)
 {
     extern __shared__ float smem[];
     const int B = blockDim.x;
@@ -114,7 +147,12 @@ k_grad_forward(DevTape t, uint32_t m, const float* __restrict__ X,
         // variables).
         const D4 d = dv_deriv(o, D4{av, 1.0f, 0.0f, 0.0f}, D4{bv, 0.0f, 1.0f, 0.0f}, false);
         R[(raw.x >> 16) * B + tid] = d.v;
-        if (ok) P[static_cast<size_t>(c) * m + i] = make_float2(d.dx, d.dy);
+        const uint32_t ps = __ldg(pslot + c);
+        const uint32_t kind = ps >> 28, slot = ps & 0x0fffffffu;
+        if (ok && kind != PK_CONST) {
+            P[static_cast<size_t>(slot) * m + i] = d.dx;
+            if (kind == PK_TWO) P[static_cast<size_t>(slot + 1) * m + i] = d.dy;
+        }
     }
     if (ok && f) f[i] = gv_fetch(t.root_kind, t.root, R, tid, B, t.cpool);
 }
@@ -135,7 +173,8 @@ __device__ __forceinline__ float warp_sum(float v)
 /// (too many variables for shared memory) each warp adds to gvars.
 template <bool SV>
 __global__ void __launch_bounds__(128)
-k_grad_backward(DevTape t, uint32_t m, const float2* __restrict__ P,
+k_grad_backward(DevTape t, const uint32_t* __restrict__ pslot, uint32_t m,
+                const float* __restrict__ P,
                 const float* __restrict__ seed, float* __restrict__ gx,
                 float* __restrict__ gy, float* __restrict__ gz, float* __restrict__ gvars,
                 int block_const_var)
@@ -171,7 +210,17 @@ k_grad_backward(DevTape t, uint32_t m, const float2* __restrict__ P,
         const uint32_t ro = raw.x >> 16, ra = raw.y & 0xffff, rb = raw.y >> 16;
         const float adj = A[ro * B + tid];
         A[ro * B + tid] = 0.0f;
-        float2 pd = ok ? P[static_cast<size_t>(c) * m + i] : make_float2(0.0f, 0.0f);
+        const uint32_t ps = __ldg(pslot + c);
+        const uint32_t kind = ps >> 28, slot = ps & 0x0fffffffu;
+        float2 pd = make_float2(0.0f, 0.0f);
+        if (kind == PK_CONST) {
+            pd = const_partials(o);
+        } else if (ok) {
+            const float p0 = P[static_cast<size_t>(slot) * m + i];
+            pd = kind == PK_TWO ? make_float2(p0, P[static_cast<size_t>(slot + 1) * m + i])
+               : kind == PK_CHOICE ? make_float2(p0, 1.0f - p0)
+                                   : make_float2(p0, 0.0f);
+        }
         if (block_const_var && o == op::CONST_VAR) pd = make_float2(0.0f, 0.0f);
         const float ga = adj * pd.x;
         const uint8_t ka = kinds & 3, kb = (kinds >> 2) & 3;
@@ -200,6 +249,32 @@ k_grad_backward(DevTape t, uint32_t m, const float2* __restrict__ P,
             if (Gv[k] != 0.0f) atomicAdd(gvars + k, Gv[k]);
         }
     }
+}
+
+/// The tape's partial-slot table (partial_kind), uploaded on first use.
+bool ensure_pslots(GpuTape& g)
+{
+    std::lock_guard<std::mutex> lock(g.mu);
+    if (g.pslot_ready) return true;
+    std::vector<uint32_t> ps(std::max<size_t>(g.reg.clauses.size(), 1), 0);
+    uint32_t next = 0;
+    for (size_t c = 0; c < g.reg.clauses.size(); ++c) {
+        const uint32_t kind = partial_kind(g.reg.clauses[c].op);
+        ps[c] = next | (kind << 28);
+        next += kind == PK_CONST ? 0 : kind == PK_TWO ? 2 : 1;
+    }
+    if (next >= (1u << 28)) {
+        set_error(LFB_E_UNSUPPORTED, "tape too long for the reverse mode");
+        return false;
+    }
+    if (!cuda_ok(cudaMalloc(&g.d_pslot, ps.size() * sizeof(uint32_t)), "partial slots") ||
+        !cuda_ok(cudaMemcpy(g.d_pslot, ps.data(), ps.size() * sizeof(uint32_t),
+                            cudaMemcpyHostToDevice), "partial slots")) {
+        return false;
+    }
+    g.n_pslot = next;
+    g.pslot_ready = true;
+    return true;
 }
 
 bool tape_has_const_var(const GpuTape& g)
@@ -267,15 +342,17 @@ int grad_device(GpuTape& g, uint64_t n, const float* x, const float* y, const fl
         (sv && !set_smem(reinterpret_cast<const void*>(k_grad_backward<true>), smem_sv))) {
         return LFB_E_CUDA;
     }
-    // Partials take 8 bytes per clause and point: points per launch so that
+    if (!ensure_pslots(g)) return LFB_E_CUDA;
+    const uint32_t* pslot = g.d_pslot;
+    // Partials take 4 bytes per slot and point: points per launch so that
     // they stay within 4 GiB (enough points to fill the GPU for tapes of
     // tens of thousands of clauses).
-    const uint64_t per_point = std::max<uint64_t>(8ull * t.n, 8);
+    const uint64_t per_point = std::max<uint64_t>(4ull * g.n_pslot, 4);
     const uint64_t chunk = std::max<uint64_t>(kBlock, std::min<uint64_t>(
         (4ull << 30) / per_point / kBlock * kBlock, uint64_t(1) << 22));
     auto& st = grad_staging();
     if (!st.partials.reserve(std::min(chunk, n) * per_point)) return LFB_E_CUDA;
-    float2* P = st.partials.as<float2>();
+    float* P = st.partials.as<float>();
     const bool has_cv = tape_has_const_var(g);
     const bool want_xyz = gx || gy || gz;
     auto backward = [&](uint32_t m, unsigned blocks, const float* sd, uint64_t off, bool xyz,
@@ -284,18 +361,18 @@ int grad_device(GpuTape& g, uint64_t n, const float* x, const float* y, const fl
         float* oy = xyz && gy ? gy + off : nullptr;
         float* oz = xyz && gz ? gz + off : nullptr;
         if (gv && sv) {
-            k_grad_backward<true><<<blocks, kBlock, smem_sv, s>>>(t, m, P, sd, ox, oy, oz, gv,
-                                                                  block_cv);
+            k_grad_backward<true><<<blocks, kBlock, smem_sv, s>>>(t, pslot, m, P, sd, ox, oy, oz,
+                                                                  gv, block_cv);
         } else {
-            k_grad_backward<false><<<blocks, kBlock, smem, s>>>(t, m, P, sd, ox, oy, oz, gv,
-                                                                block_cv);
+            k_grad_backward<false><<<blocks, kBlock, smem, s>>>(t, pslot, m, P, sd, ox, oy, oz,
+                                                                gv, block_cv);
         }
         note_launches(1);
     };
     for (uint64_t off = 0; off < n; off += chunk) {
         const uint32_t m = static_cast<uint32_t>(std::min(chunk, n - off));
         const unsigned blocks = (m + kBlock - 1) / kBlock;
-        k_grad_forward<<<blocks, kBlock, smem, s>>>(t, m, x + off, y + off, z + off, P,
+        k_grad_forward<<<blocks, kBlock, smem, s>>>(t, pslot, m, x + off, y + off, z + off, P,
                                                     f ? f + off : nullptr);
         note_launches(1);
         const float* sd = seed ? seed + off : nullptr;

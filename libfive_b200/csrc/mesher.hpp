@@ -52,8 +52,10 @@ struct MeshJob {
 
 /// Renders n meshes with up to `workers` of them in flight at once, each on
 /// its own CUDA stream and scratch context, longest (tape length x 4^depth)
-/// first.  Returns 0 when every job succeeded, else the first failing job's
-/// code (with its message set as this thread's error).
+/// first; large meshes go one at a time through one context while the
+/// others render the small ones.  A mesh that runs out of device memory is
+/// rendered again alone.  Returns 0 when every job succeeded, else the first
+/// failing job's code (with its message set as this thread's error).
 int render_dc_meshes(MeshJob* jobs, size_t n, unsigned workers);
 
 /// Binary STL in the reference's layout (mesh.cpp:139-194): 80-byte header,

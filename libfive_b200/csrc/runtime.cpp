@@ -93,6 +93,7 @@ GpuTape::~GpuTape()
     if (d_clauses) cudaFree(d_clauses);
     if (d_cpool) cudaFree(d_cpool);
     if (d_wide) cudaFree(d_wide);
+    if (d_pslot) cudaFree(d_pslot);
 }
 
 bool GpuTape::ensure_wide()

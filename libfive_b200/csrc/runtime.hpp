@@ -42,6 +42,12 @@ struct GpuTape {
     bool wide_ready = false;
     bool ensure_wide();
 
+    // Reverse mode: where each clause's local partials are stored per point
+    // (slot | kind << 28, see grad_kernels.cu), built on first use.
+    uint32_t* d_pslot = nullptr;
+    uint32_t n_pslot = 0;
+    bool pslot_ready = false;
+
     ~GpuTape();
     DevTape dev() const;
     /// Sets variable values by tree id; returns true if any value changed.

@@ -394,7 +394,7 @@ def run_batch(args, world, rank, local):
     mesh is downloaded to the host.  Rank r meshes its own trees (seed 11 + r)."""
     import torch
     from libfive_b200 import ffi, workloads
-    from libfive_b200.shape import Tape, render_meshes
+    from libfive_b200.shape import Tape
     torch.cuda.set_device(local)
     lib = ffi.load()
     specs = workloads.batch_specs(args.trees, seed=11 + rank)
@@ -414,8 +414,23 @@ def run_batch(args, world, rank, local):
             tris += st.triangles
         return tris
 
+    n = len(jobs)
+    b_tapes = (ffi.tape_t * n)(*[t.ptr for t, *_ in jobs])
+    b_regions = (ffi.Region3 * n)(*[region] * n)
+    b_settings = (ffi.MeshSettings * n)(*[ffi.MeshSettings(mf, me) for _, _, _, mf, me in jobs])
+    b_stats = (ffi.MeshStats * n)()
+
     def batch():
-        return sum(len(t) for _, t in render_meshes(jobs, workers=args.workers))
+        # the same work as loop(): meshes downloaded to the host and freed
+        meshes = (ctypes.POINTER(ffi.Mesh) * n)()
+        rc = lib.lfb_render_meshes(b_tapes, n, b_regions, b_settings, args.workers, meshes,
+                                   b_stats)
+        for m in meshes:
+            if m:
+                lib.libfive_mesh_delete(m)
+        if rc != 0:
+            raise RuntimeError("lfb_render_meshes failed: " + ffi.last_error()[1])
+        return sum(st.triangles for st in b_stats)
 
     timings = {}
     for name, fn in (("loop", loop), ("batch", batch)):

@@ -2398,7 +2398,12 @@ struct PinnedPool {
     std::multimap<size_t, void*> free_blocks;   // capacity -> block
     std::map<void*, size_t> owned;              // every pool block
     size_t free_bytes = 0;
+    size_t owned_bytes = 0;
     static constexpr size_t kKeepBytes = size_t(1) << 30;   // cached when free
+    // Page-locked memory in use or cached at most; beyond it (many large
+    // meshes alive at once) blocks are pageable, since pinning is slow and
+    // takes memory from the rest of the host.
+    static constexpr size_t kMaxOwned = size_t(4) << 30;
 };
 
 PinnedPool& pinned_pool()
@@ -2424,11 +2429,19 @@ void* host_alloc(size_t bytes)
             return blk;
         }
     }
+    {
+        std::lock_guard<std::mutex> lock(P.mu);
+        if (P.owned_bytes + n > PinnedPool::kMaxOwned) {
+            return std::aligned_alloc(kGrain, n);   // pageable; same interface
+        }
+        P.owned_bytes += n;   // reserved before the (slow) pinning call
+    }
     void* blk = nullptr;
     if (cudaMallocHost(&blk, n) != cudaSuccess || !blk) {
         cudaGetLastError();
-        blk = std::aligned_alloc(kGrain, n);   // pageable fallback; same interface
-        return blk;
+        std::lock_guard<std::mutex> lock(P.mu);
+        P.owned_bytes -= n;
+        return std::aligned_alloc(kGrain, n);   // pageable fallback; same interface
     }
     std::lock_guard<std::mutex> lock(P.mu);
     P.owned[blk] = n;
@@ -2451,6 +2464,7 @@ void host_free(void* p)
     while (P.free_bytes > PinnedPool::kKeepBytes && !P.free_blocks.empty()) {
         auto last = std::prev(P.free_blocks.end());
         P.free_bytes -= last->first;
+        P.owned_bytes -= last->first;
         P.owned.erase(last->second);
         cudaFreeHost(last->second);
         P.free_blocks.erase(last);

@@ -120,8 +120,77 @@ __device__ __forceinline__ float gv_fetch(uint8_t kind, uint16_t idx, const floa
     return kind == OPND_REG ? R[idx * B + tid] : __ldg(cp + idx);
 }
 
-/// Forward pass of the reverse mode: value of every clause, and the local
-/// partials its kind keeps, at P[slot * m + i] (and slot + 1 for PK_TWO).
+/// Value and local partials (d out / d a, d out / d b) of one clause: the
+/// results of dv_deriv for unit tangents (a = (1, 0), b = (0, 1)), bit for
+/// bit, computed directly for the common opcodes (one transcendental call
+/// instead of two for EXP, one division instead of three for LOG / SQRT /
+/// RECIP / DIV) and through dv_deriv_all for the rest.
+__device__ __forceinline__ void dv_partials(uint8_t o, float av, float bv, float* v, float* pa,
+                                            float* pb)
+{
+    switch (o) {
+        case op::ADD: *v = __fadd_rn(av, bv); *pa = 1.0f; *pb = 1.0f; return;
+        case op::SUB: *v = __fsub_rn(av, bv); *pa = 1.0f; *pb = -1.0f; return;
+        case op::MUL:
+            *v = __fmul_rn(av, bv);
+            *pa = __fadd_rn(__fmul_rn(0.0f, av), __fmul_rn(1.0f, bv));
+            *pb = __fadd_rn(__fmul_rn(1.0f, av), __fmul_rn(0.0f, bv));
+            return;
+        case op::MIN:
+            *v = sc_min(av, bv);
+            *pa = av < bv ? 1.0f : 0.0f;
+            *pb = av < bv ? 0.0f : 1.0f;
+            return;
+        case op::MAX:
+            *v = sc_max(av, bv);
+            *pa = av < bv ? 0.0f : 1.0f;
+            *pb = av < bv ? 1.0f : 0.0f;
+            return;
+        case op::SQUARE: *v = __fmul_rn(av, av); *pa = __fmul_rn(av, 2.0f); *pb = 0.0f; return;
+        case op::NEG: *v = -av; *pa = -1.0f; *pb = 0.0f; return;
+        case op::ABS: *v = fabsf(av); *pa = av > 0 ? 1.0f : -1.0f; *pb = 0.0f; return;
+        case op::SQRT: {
+            const float ov = __fsqrt_rn(av);
+            *v = ov;
+            *pa = av < 0 ? 0.0f : __fdiv_rn(1.0f, __fmul_rn(2.0f, ov));
+            *pb = 0.0f;
+            return;
+        }
+        case op::LOG: *v = logf(av); *pa = __fdiv_rn(1.0f, av); *pb = 0.0f; return;
+        case op::EXP: {
+            const float e = expf(av);
+            *v = e;
+            *pa = __fmul_rn(1.0f, e);
+            *pb = 0.0f;
+            return;
+        }
+        case op::RECIP:
+            *v = __fdiv_rn(1.0f, av);
+            *pa = __fdiv_rn(1.0f, -__fmul_rn(av, av));
+            *pb = 0.0f;
+            return;
+        case op::DIV: {
+            const float den = __fmul_rn(bv, bv);
+            *v = __fdiv_rn(av, bv);
+            *pa = __fdiv_rn(__fsub_rn(__fmul_rn(1.0f, bv), __fmul_rn(0.0f, av)), den);
+            *pb = __fdiv_rn(__fsub_rn(__fmul_rn(0.0f, bv), __fmul_rn(1.0f, av)), den);
+            return;
+        }
+        default: {
+            const D4 d = dv_deriv_all(o, D4{av, 1.0f, 0.0f, 0.0f}, D4{bv, 0.0f, 1.0f, 0.0f},
+                                      false);
+            *v = d.v;
+            *pa = d.dx;
+            *pb = d.dy;
+        }
+    }
+}
+
+/// Forward pass of the reverse mode, PTS points per thread (points
+/// base + k * blockDim.x): value of every clause, and the local partials
+/// its kind keeps, at P[slot * m + i] (and slot + 1 for PK_TWO).  Register r
+/// of point k lives at R[(r * PTS + k) * blockDim.x + tid].
+template <int PTS>
 __global__ void __launch_bounds__(128)
 k_grad_forward(DevTape t, const uint32_t* __restrict__ pslot, uint32_t m,
                const float* __restrict__ X, const float* __restrict__ Y,
@@ -130,31 +199,49 @@ k_grad_forward(DevTape t, const uint32_t* __restrict__ pslot, uint32_t m,
     extern __shared__ float smem[];
     const int B = blockDim.x;
     const int tid = threadIdx.x;
-    const uint32_t i = blockIdx.x * B + tid;
     float* R = smem;
-    const bool ok = i < m;
-    R[0 * B + tid] = ok ? X[i] : 0.0f;
-    R[1 * B + tid] = ok ? Y[i] : 0.0f;
-    R[2 * B + tid] = ok ? Z[i] : 0.0f;
+    uint32_t idx[PTS];
+    bool ok[PTS];
+#pragma unroll
+    for (int k = 0; k < PTS; ++k) {
+        idx[k] = (blockIdx.x * PTS + k) * B + tid;
+        ok[k] = idx[k] < m;
+        R[(0 * PTS + k) * B + tid] = ok[k] ? X[idx[k]] : 0.0f;
+        R[(1 * PTS + k) * B + tid] = ok[k] ? Y[idx[k]] : 0.0f;
+        R[(2 * PTS + k) * B + tid] = ok[k] ? Z[idx[k]] : 0.0f;
+    }
     for (uint32_t c = 0; c < t.n; ++c) {
         const uint2 raw = __ldg(reinterpret_cast<const uint2*>(t.clauses + c));
         const uint8_t o = raw.x & 0xff;
         const uint8_t kinds = (raw.x >> 8) & 0xff;
-        const float av = gv_fetch(kinds & 3, raw.y & 0xffff, R, tid, B, t.cpool);
-        const float bv = gv_fetch((kinds >> 2) & 3, raw.y >> 16, R, tid, B, t.cpool);
-        // Unit tangents: dx slot = d/da, dy slot = d/db (CONST_VAR passes
-        // its argument's tangent here; the backward pass blocks it for
-        // variables).
-        const D4 d = dv_deriv(o, D4{av, 1.0f, 0.0f, 0.0f}, D4{bv, 0.0f, 1.0f, 0.0f}, false);
-        R[(raw.x >> 16) * B + tid] = d.v;
+        const uint32_t ra = raw.y & 0xffff, rb = raw.y >> 16, ro = raw.x >> 16;
         const uint32_t ps = __ldg(pslot + c);
         const uint32_t kind = ps >> 28, slot = ps & 0x0fffffffu;
-        if (ok && kind != PK_CONST) {
-            P[static_cast<size_t>(slot) * m + i] = d.dx;
-            if (kind == PK_TWO) P[static_cast<size_t>(slot + 1) * m + i] = d.dy;
+        const bool ra_reg = (kinds & 3) == OPND_REG, rb_reg = ((kinds >> 2) & 3) == OPND_REG;
+        const float ca = ra_reg ? 0.0f : __ldg(t.cpool + ra);
+        const float cb = rb_reg ? 0.0f : __ldg(t.cpool + rb);
+#pragma unroll
+        for (int k = 0; k < PTS; ++k) {
+            const float av = ra_reg ? R[(ra * PTS + k) * B + tid] : ca;
+            const float bv = rb_reg ? R[(rb * PTS + k) * B + tid] : cb;
+            float v, pa, pb;
+            dv_partials(o, av, bv, &v, &pa, &pb);
+            R[(ro * PTS + k) * B + tid] = v;
+            if (ok[k] && kind != PK_CONST) {
+                P[static_cast<size_t>(slot) * m + idx[k]] = pa;
+                if (kind == PK_TWO) P[static_cast<size_t>(slot + 1) * m + idx[k]] = pb;
+            }
         }
     }
-    if (ok && f) f[i] = gv_fetch(t.root_kind, t.root, R, tid, B, t.cpool);
+    if (f) {
+#pragma unroll
+        for (int k = 0; k < PTS; ++k) {
+            if (ok[k]) {
+                f[idx[k]] = t.root_kind == OPND_REG ? R[(t.root * PTS + k) * B + tid]
+                                                    : __ldg(t.cpool + t.root);
+            }
+        }
+    }
 }
 
 __device__ __forceinline__ float warp_sum(float v)
@@ -337,7 +424,10 @@ int grad_device(GpuTape& g, uint64_t n, const float* x, const float* y, const fl
     // Variable adjoints are gathered per block in shared memory when they fit.
     const size_t smem_sv = smem + static_cast<size_t>(t.n_cpool - t.n_const) * sizeof(float);
     const bool sv = smem_sv <= 200 * 1024;
-    if (!set_smem(reinterpret_cast<const void*>(k_grad_forward), smem) ||
+    constexpr int kFwdPts = 2;
+    const size_t smem_fwd = smem * kFwdPts;
+    if (smem_fwd > 200 * 1024) return set_error(LFB_E_UNSUPPORTED, "tape needs too many registers");
+    if (!set_smem(reinterpret_cast<const void*>(k_grad_forward<kFwdPts>), smem_fwd) ||
         !set_smem(reinterpret_cast<const void*>(k_grad_backward<false>), smem) ||
         (sv && !set_smem(reinterpret_cast<const void*>(k_grad_backward<true>), smem_sv))) {
         return LFB_E_CUDA;
@@ -372,8 +462,9 @@ int grad_device(GpuTape& g, uint64_t n, const float* x, const float* y, const fl
     for (uint64_t off = 0; off < n; off += chunk) {
         const uint32_t m = static_cast<uint32_t>(std::min(chunk, n - off));
         const unsigned blocks = (m + kBlock - 1) / kBlock;
-        k_grad_forward<<<blocks, kBlock, smem, s>>>(t, pslot, m, x + off, y + off, z + off, P,
-                                                    f ? f + off : nullptr);
+        const unsigned fwd_blocks = (m + kBlock * kFwdPts - 1) / (kBlock * kFwdPts);
+        k_grad_forward<kFwdPts><<<fwd_blocks, kBlock, smem_fwd, s>>>(
+            t, pslot, m, x + off, y + off, z + off, P, f ? f + off : nullptr);
         note_launches(1);
         const float* sd = seed ? seed + off : nullptr;
         if (!has_cv) {

@@ -258,7 +258,7 @@ __device__ __forceinline__ float warp_sum(float v)
 /// summed over the warp, then (SV) over the block in shared memory, and
 /// reach gvars with one atomic add per variable and block; without SV
 /// (too many variables for shared memory) each warp adds to gvars.
-template <bool SV>
+template <bool SV, int PTS>
 __global__ void __launch_bounds__(128)
 k_grad_backward(DevTape t, const uint32_t* __restrict__ pslot, uint32_t m,
                 const float* __restrict__ P,
@@ -270,10 +270,16 @@ k_grad_backward(DevTape t, const uint32_t* __restrict__ pslot, uint32_t m,
     const int B = blockDim.x;
     const int tid = threadIdx.x;
     const int lane = tid & 31;
-    const uint32_t i = blockIdx.x * B + tid;
-    const bool ok = i < m;
+    uint32_t idx[PTS];
+    bool ok[PTS];
+#pragma unroll
+    for (int k = 0; k < PTS; ++k) {
+        idx[k] = (blockIdx.x * PTS + k) * B + tid;
+        ok[k] = idx[k] < m;
+    }
+    // adjoint of register r, point k: A[(r * PTS + k) * B + tid]
     float* A = smem;
-    float* Gv = smem + t.n_regs * B;
+    float* Gv = smem + t.n_regs * PTS * B;
     const uint32_t n_vars = t.n_cpool - t.n_const;
     if (SV && gvars) {
         for (uint32_t k = tid; k < n_vars; k += B) Gv[k] = 0.0f;
@@ -283,52 +289,72 @@ k_grad_backward(DevTape t, const uint32_t* __restrict__ pslot, uint32_t m,
         const float w = warp_sum(g);
         if (lane == 0 && w != 0.0f) atomicAdd((SV ? Gv : gvars) + k, w);
     };
-    for (uint32_t r = 0; r < t.n_regs; ++r) A[r * B + tid] = 0.0f;
-    const float s0 = ok ? (seed ? seed[i] : 1.0f) : 0.0f;
+    for (uint32_t r = 0; r < t.n_regs * PTS; ++r) A[r * B + tid] = 0.0f;
+    float s0[PTS];
+#pragma unroll
+    for (int k = 0; k < PTS; ++k) s0[k] = ok[k] ? (seed ? seed[idx[k]] : 1.0f) : 0.0f;
     if (t.root_kind == OPND_REG) {
-        A[t.root * B + tid] = s0;
+#pragma unroll
+        for (int k = 0; k < PTS; ++k) A[(t.root * PTS + k) * B + tid] = s0[k];
     } else if (t.root_kind == OPND_VAR && gvars) {
-        add_var(t.root - t.n_const, s0);
+        float g = 0.0f;
+#pragma unroll
+        for (int k = 0; k < PTS; ++k) g += s0[k];
+        add_var(t.root - t.n_const, g);
     }
     for (int64_t c = static_cast<int64_t>(t.n) - 1; c >= 0; --c) {
         const uint2 raw = __ldg(reinterpret_cast<const uint2*>(t.clauses + c));
         const uint8_t o = raw.x & 0xff;
         const uint8_t kinds = (raw.x >> 8) & 0xff;
         const uint32_t ro = raw.x >> 16, ra = raw.y & 0xffff, rb = raw.y >> 16;
-        const float adj = A[ro * B + tid];
-        A[ro * B + tid] = 0.0f;
         const uint32_t ps = __ldg(pslot + c);
         const uint32_t kind = ps >> 28, slot = ps & 0x0fffffffu;
-        float2 pd = make_float2(0.0f, 0.0f);
-        if (kind == PK_CONST) {
-            pd = const_partials(o);
-        } else if (ok) {
-            const float p0 = P[static_cast<size_t>(slot) * m + i];
-            pd = kind == PK_TWO ? make_float2(p0, P[static_cast<size_t>(slot + 1) * m + i])
-               : kind == PK_CHOICE ? make_float2(p0, 1.0f - p0)
-                                   : make_float2(p0, 0.0f);
-        }
-        if (block_const_var && o == op::CONST_VAR) pd = make_float2(0.0f, 0.0f);
-        const float ga = adj * pd.x;
         const uint8_t ka = kinds & 3, kb = (kinds >> 2) & 3;
-        if (ka == OPND_REG) {
-            A[ra * B + tid] += ga;
-        } else if (ka == OPND_VAR && gvars) {
-            add_var(ra - t.n_const, ga);
-        }
-        if (dev_is_binary(o)) {
-            const float gb = adj * pd.y;
-            if (kb == OPND_REG) {
-                A[rb * B + tid] += gb;
-            } else if (kb == OPND_VAR && gvars) {
-                add_var(rb - t.n_const, gb);
+        const bool binary = dev_is_binary(o);
+        const bool blocked = block_const_var && o == op::CONST_VAR;
+        float va = 0.0f, vb = 0.0f;   // variable adjoints of this clause, summed over points
+#pragma unroll
+        for (int k = 0; k < PTS; ++k) {
+            float* ao = A + (ro * PTS + k) * B + tid;
+            const float adj = *ao;
+            *ao = 0.0f;
+            float2 pd = make_float2(0.0f, 0.0f);
+            if (kind == PK_CONST) {
+                pd = const_partials(o);
+            } else if (ok[k]) {
+                const float p0 = P[static_cast<size_t>(slot) * m + idx[k]];
+                pd = kind == PK_TWO ? make_float2(p0, P[static_cast<size_t>(slot + 1) * m + idx[k]])
+                   : kind == PK_CHOICE ? make_float2(p0, 1.0f - p0)
+                                       : make_float2(p0, 0.0f);
+            }
+            if (blocked) pd = make_float2(0.0f, 0.0f);
+            const float ga = adj * pd.x;
+            if (ka == OPND_REG) {
+                A[(ra * PTS + k) * B + tid] += ga;
+            } else {
+                va += ga;
+            }
+            if (binary) {
+                const float gb = adj * pd.y;
+                if (kb == OPND_REG) {
+                    A[(rb * PTS + k) * B + tid] += gb;
+                } else {
+                    vb += gb;
+                }
             }
         }
+        if (gvars) {
+            if (ka == OPND_VAR) add_var(ra - t.n_const, va);
+            if (binary && kb == OPND_VAR) add_var(rb - t.n_const, vb);
+        }
     }
-    if (ok) {
-        if (gx) gx[i] = A[0 * B + tid];
-        if (gy) gy[i] = A[1 * B + tid];
-        if (gz) gz[i] = A[2 * B + tid];
+#pragma unroll
+    for (int k = 0; k < PTS; ++k) {
+        if (ok[k]) {
+            if (gx) gx[idx[k]] = A[(0 * PTS + k) * B + tid];
+            if (gy) gy[idx[k]] = A[(1 * PTS + k) * B + tid];
+            if (gz) gz[idx[k]] = A[(2 * PTS + k) * B + tid];
+        }
     }
     if (SV && gvars) {
         __syncthreads();
@@ -419,17 +445,17 @@ int grad_device(GpuTape& g, uint64_t n, const float* x, const float* y, const fl
 {
     const DevTape t = g.dev();
     if (n == 0) return 0;
-    const size_t smem = static_cast<size_t>(t.n_regs) * kBlock * sizeof(float);
+    // Two points per thread in both passes: registers / adjoints of both
+    // points in shared memory, plus (when they fit) the block's variable
+    // adjoints.
+    constexpr int kPts = 2;
+    const size_t smem = static_cast<size_t>(t.n_regs) * kBlock * kPts * sizeof(float);
     if (smem > 200 * 1024) return set_error(LFB_E_UNSUPPORTED, "tape needs too many registers");
-    // Variable adjoints are gathered per block in shared memory when they fit.
     const size_t smem_sv = smem + static_cast<size_t>(t.n_cpool - t.n_const) * sizeof(float);
     const bool sv = smem_sv <= 200 * 1024;
-    constexpr int kFwdPts = 2;
-    const size_t smem_fwd = smem * kFwdPts;
-    if (smem_fwd > 200 * 1024) return set_error(LFB_E_UNSUPPORTED, "tape needs too many registers");
-    if (!set_smem(reinterpret_cast<const void*>(k_grad_forward<kFwdPts>), smem_fwd) ||
-        !set_smem(reinterpret_cast<const void*>(k_grad_backward<false>), smem) ||
-        (sv && !set_smem(reinterpret_cast<const void*>(k_grad_backward<true>), smem_sv))) {
+    if (!set_smem(reinterpret_cast<const void*>(k_grad_forward<kPts>), smem) ||
+        !set_smem(reinterpret_cast<const void*>(k_grad_backward<false, kPts>), smem) ||
+        (sv && !set_smem(reinterpret_cast<const void*>(k_grad_backward<true, kPts>), smem_sv))) {
         return LFB_E_CUDA;
     }
     if (!ensure_pslots(g)) return LFB_E_CUDA;
@@ -451,20 +477,19 @@ int grad_device(GpuTape& g, uint64_t n, const float* x, const float* y, const fl
         float* oy = xyz && gy ? gy + off : nullptr;
         float* oz = xyz && gz ? gz + off : nullptr;
         if (gv && sv) {
-            k_grad_backward<true><<<blocks, kBlock, smem_sv, s>>>(t, pslot, m, P, sd, ox, oy, oz,
-                                                                  gv, block_cv);
+            k_grad_backward<true, kPts><<<blocks, kBlock, smem_sv, s>>>(
+                t, pslot, m, P, sd, ox, oy, oz, gv, block_cv);
         } else {
-            k_grad_backward<false><<<blocks, kBlock, smem, s>>>(t, pslot, m, P, sd, ox, oy, oz,
-                                                                gv, block_cv);
+            k_grad_backward<false, kPts><<<blocks, kBlock, smem, s>>>(
+                t, pslot, m, P, sd, ox, oy, oz, gv, block_cv);
         }
         note_launches(1);
     };
     for (uint64_t off = 0; off < n; off += chunk) {
         const uint32_t m = static_cast<uint32_t>(std::min(chunk, n - off));
-        const unsigned blocks = (m + kBlock - 1) / kBlock;
-        const unsigned fwd_blocks = (m + kBlock * kFwdPts - 1) / (kBlock * kFwdPts);
-        k_grad_forward<kFwdPts><<<fwd_blocks, kBlock, smem_fwd, s>>>(
-            t, pslot, m, x + off, y + off, z + off, P, f ? f + off : nullptr);
+        const unsigned blocks = (m + kBlock * kPts - 1) / (kBlock * kPts);
+        k_grad_forward<kPts><<<blocks, kBlock, smem, s>>>(t, pslot, m, x + off, y + off, z + off,
+                                                          P, f ? f + off : nullptr);
         note_launches(1);
         const float* sd = seed ? seed + off : nullptr;
         if (!has_cv) {

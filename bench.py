@@ -73,6 +73,8 @@ def parse():
     p.add_argument("--trees", type=int, default=512, help="batch workload: tree count")
     p.add_argument("--workers", type=int, default=4,
                    help="batch workload: meshes in flight at once")
+    p.add_argument("--points", type=int, default=1 << 22,
+                   help="adjoint workload: points (smaller for profiling captures)")
     return p.parse_args()
 
 
@@ -528,7 +530,7 @@ def run_adjoint(args, world, rank, local):
     tri = v[t.astype(np.int64)].astype(np.float64)
     area = 0.5 * np.linalg.norm(np.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0]), axis=1)
     rng = np.random.Generator(np.random.PCG64(7 + rank))
-    n = 1 << 22
+    n = args.points
     k = rng.choice(len(tri), size=n, p=area / area.sum())
     u, w = rng.random(n), rng.random(n)
     flip = u + w > 1

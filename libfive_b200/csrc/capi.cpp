@@ -506,6 +506,13 @@ int lfb_tape_set_vars(lfb_tape t, libfive_vars vars)
     return changed ? 1 : 0;
 }
 
+int lfb_tape_compiled(lfb_tape t)
+{
+    if (!t) return 0;
+    std::lock_guard<std::mutex> lock(t->g->mu);
+    return t->g->jit_state == 1 ? 1 : 0;
+}
+
 int lfb_tape_info(lfb_tape t, uint32_t counts[6])
 {
     if (!t || !counts) return set_error(LFB_E_INVALID, "null argument");

@@ -3,6 +3,7 @@
 #include <vector>
 
 #include "eval_kernels.cuh"
+#include "jit.hpp"
 #include "libfive_b200.h"
 
 namespace lfb {
@@ -13,6 +14,7 @@ int eval_values_device(GpuTape& g, uint64_t n, const float* x, const float* y,
                        const float* z, float* out, cudaStream_t s)
 {
     if (!require_device()) return LFB_E_CUDA;
+    if (jit_values(g, n, x, y, z, out, s)) return 0;
     const DevTape t = g.dev();
     for (uint64_t off = 0; off < n; off += kChunk) {
         const uint32_t m = static_cast<uint32_t>(std::min(kChunk, n - off));

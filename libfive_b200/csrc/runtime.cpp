@@ -1,5 +1,7 @@
 #include "runtime.hpp"
 
+#include "jit.hpp"
+
 #include <map>
 
 #include <atomic>
@@ -94,6 +96,7 @@ GpuTape::~GpuTape()
     if (d_cpool) cudaFree(d_cpool);
     if (d_wide) cudaFree(d_wide);
     if (d_pslot) cudaFree(d_pslot);
+    jit_release(*this);
 }
 
 bool GpuTape::ensure_wide()

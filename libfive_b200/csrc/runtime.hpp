@@ -48,6 +48,11 @@ struct GpuTape {
     uint32_t n_pslot = 0;
     bool pslot_ready = false;
 
+    // Compiled value kernel (jit.cpp): 0 not tried, 1 ready, -1 none.
+    int jit_state = 0;
+    void* jit_module = nullptr;
+    void* jit_function = nullptr;
+
     ~GpuTape();
     DevTape dev() const;
     /// Sets variable values by tree id; returns true if any value changed.

@@ -135,6 +135,7 @@ SIGNATURES = [
     ("lfb_tape_delete", None, [tape_t]),
     ("lfb_tape_set_vars", ctypes.c_int, [tape_t, Vars]),
     ("lfb_tape_info", ctypes.c_int, [tape_t, u32p]),
+    ("lfb_tape_compiled", ctypes.c_int, [tape_t]),
     ("lfb_tape_var_ids", ctypes.c_int, [tape_t, ctypes.POINTER(vp), ctypes.c_uint32]),
     ("lfb_eval_derivs_static", ctypes.c_int, [tape_t, ctypes.c_uint64, vp, vp, vp, vp, vp, vp, vp]),
     ("lfb_eval_values", ctypes.c_int, [tape_t, ctypes.c_uint64, vp, vp, vp, vp, vp, ctypes.c_uint32]),

@@ -1,0 +1,93 @@
+"""Tapes compiled to straight-line kernels (jit.cpp) against the interpreter.
+
+The compiled kernel must give the interpreter's bits at every point,
+transcendental opcodes included (both call the same CUDA functions with
+contraction off).  The interpreter's values are computed in a child process
+with LFB_JIT=0; lfb_tape_compiled says which path a tape took."""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from libfive_b200 import ffi, workloads
+from libfive_b200.shape import Shape, Tape
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+X, Y, Z = Shape.X, Shape.Y, Shape.Z
+
+
+def shapes():
+    """name -> (shape, var values); every compiled opcode appears."""
+    out = {
+        "spheres": (workloads.spheres_union(64, seed=1), None),
+        "csg": (workloads.random_csg(60, seed=5), None),
+    }
+    blend, vals = workloads.blended_spheres_vars(16, seed=4)
+    out["blend_vars"] = (blend, vals)
+    x, y, z = X(), Y(), Z()
+    v = Shape.var()
+    recip = Shape.new("recip", (z * v).abs())
+    misc = ((x / (y.square() + 0.5)) - recip).max(-(x.with_constant_vars() * 0.25))
+    out["misc"] = (misc, {v: 1.75})
+    return out
+
+
+CHILD = r"""
+import sys, numpy as np
+sys.path.insert(0, sys.argv[1]); sys.path.insert(0, sys.argv[1] + "/tests")
+from test_gpu_jit import shapes, points
+from libfive_b200.shape import Tape
+from libfive_b200 import ffi
+name = sys.argv[2]
+s, vals = shapes()[name]
+t = Tape(s, vals)
+out = t.values(*points())
+assert ffi.load().lfb_tape_compiled(t.ptr) == 0
+np.save(sys.argv[3], out)
+"""
+
+
+def points():
+    x, y, z = workloads.uniform_points(50000, seed=9, lo=-1.6, hi=1.6)
+    # exact zeros and ties: lattice points too
+    lx, ly, lz = workloads.lattice(16, lo=-1.0, hi=1.0)
+    return (np.concatenate([x, lx]), np.concatenate([y, ly]), np.concatenate([z, lz]))
+
+
+@pytest.mark.parametrize("name", ["spheres", "csg", "blend_vars", "misc"])
+def test_compiled_matches_interpreter(gpu, name, tmp_path):
+    s, vals = shapes()[name]
+    t = Tape(s, vals)
+    got = t.values(*points())
+    assert ffi.load().lfb_tape_compiled(t.ptr) == 1
+    path = str(tmp_path / "interp.npy")
+    r = subprocess.run([sys.executable, "-c", CHILD, ROOT, name, path],
+                       env=dict(os.environ, LFB_JIT="0"), capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    want = np.load(path)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def test_variables_change_without_recompiling(gpu):
+    s, vals = shapes()["blend_vars"]
+    t = Tape(s, vals)
+    p = points()
+    a = t.values(*p)
+    t.set_vars({k: v + 0.1 for k, v in vals.items()})
+    b = t.values(*p)
+    assert ffi.load().lfb_tape_compiled(t.ptr) == 1
+    assert not np.array_equal(a, b)
+    t2 = Tape(s, {k: v + 0.1 for k, v in vals.items()})
+    assert np.array_equal(b.view(np.uint32), t2.values(*p).view(np.uint32))
+
+
+def test_unsupported_opcode_stays_interpreted(gpu):
+    t = Tape(X().sin() + Y())
+    t.values(*points())
+    assert ffi.load().lfb_tape_compiled(t.ptr) == 0

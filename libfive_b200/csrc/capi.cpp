@@ -510,7 +510,7 @@ int lfb_tape_compiled(lfb_tape t)
 {
     if (!t) return 0;
     std::lock_guard<std::mutex> lock(t->g->mu);
-    return t->g->jit_state == 1 ? 1 : 0;
+    return t->g->jit[0].state == 1 ? 1 : 0;
 }
 
 int lfb_tape_info(lfb_tape t, uint32_t counts[6])

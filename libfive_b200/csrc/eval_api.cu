@@ -68,6 +68,7 @@ int eval_derivs_device(GpuTape& g, uint64_t n, const float* x, const float* y,
                        float* dz, cudaStream_t s)
 {
     if (!require_device()) return LFB_E_CUDA;
+    if (jit_derivs(g, n, x, y, z, v, dx, dy, dz, s)) return 0;
     const DevTape t = g.dev();
     for (uint64_t off = 0; off < n; off += kChunk) {
         const uint32_t m = static_cast<uint32_t>(std::min(kChunk, n - off));

@@ -102,22 +102,33 @@ std::string operand(const RegTape& t, uint32_t kind, uint32_t idx)
     return buf;
 }
 
+/// Tangent c (0 = d/dx, 1 = d/dy, 2 = d/dz) of an operand: constants and
+/// free variables have none.
+std::string tangent(uint32_t kind, uint32_t idx, int c)
+{
+    if (kind != OPND_REG) return "0.0f";
+    return "r" + std::to_string(idx) + "_" + "xyz"[c];
+}
+
+const char* kHead =
+    "    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;\n"
+    "    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + "
+    "threadIdx.x;\n         i < n; i += stride) {\n";
+
 /// CUDA source of the tape's value kernel, or empty when an opcode has no
 /// compiled form.  Registers of the tape become local variables; constants
 /// are literals (bit patterns), free variables are read from the constant
 /// pool so that they can change without recompiling.
-std::string source(const RegTape& t)
+std::string values_source(const RegTape& t)
 {
     std::string s;
     s.reserve(64 * t.clauses.size() + 1024);
     s += "extern \"C\" __global__ void __launch_bounds__(256)\n"
          "lfb_tape_values(const float* __restrict__ X, const float* __restrict__ Y,\n"
          "                const float* __restrict__ Z, float* __restrict__ out,\n"
-         "                unsigned long long n, const float* __restrict__ cp)\n{\n"
-         "    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;\n"
-         "    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + "
-         "threadIdx.x;\n         i < n; i += stride) {\n"
-         "        float r0 = X[i], r1 = Y[i], r2 = Z[i];\n";
+         "                unsigned long long n, const float* __restrict__ cp)\n{\n";
+    s += kHead;
+    s += "        float r0 = X[i], r1 = Y[i], r2 = Z[i];\n";
     for (uint32_t r = 3; r < t.n_regs; ++r) {
         s += "        float r" + std::to_string(r) + " = 0.0f;\n";
     }
@@ -132,12 +143,141 @@ std::string source(const RegTape& t)
     return s;
 }
 
-bool build(GpuTape& g)
+/// One clause of the derivative kernel: value and the three tangents by the
+/// rules of dv_deriv (clear_vars off), through temporaries so that an output
+/// register may also be an operand.  Empty for opcodes without a compiled form.
+std::string deriv_clause(const RegTape& t, const RegClause& c)
+{
+    const uint32_t ka = c.kinds & 3, kb = (c.kinds >> 2) & 3;
+    std::string s = "        {\n            const float a = " + operand(t, ka, c.a) +
+                    ", b = " + operand(t, kb, c.b) + ";\n";
+    for (int k = 0; k < 3; ++k) {
+        s += std::string("            const float a") + "xyz"[k] + " = " + tangent(ka, c.a, k) +
+             ", b" + "xyz"[k] + " = " + tangent(kb, c.b, k) + ";\n";
+    }
+    std::string v, d[3];
+    std::string pre;
+    switch (c.op) {
+        case op::ADD:
+            v = "__fadd_rn(a, b)";
+            for (int k = 0; k < 3; ++k) d[k] = std::string("__fadd_rn(a") + "xyz"[k] + ", b" + "xyz"[k] + ")";
+            break;
+        case op::SUB:
+            v = "__fsub_rn(a, b)";
+            for (int k = 0; k < 3; ++k) d[k] = std::string("__fsub_rn(a") + "xyz"[k] + ", b" + "xyz"[k] + ")";
+            break;
+        case op::MUL:
+            v = "__fmul_rn(a, b)";
+            for (int k = 0; k < 3; ++k) {
+                d[k] = std::string("__fadd_rn(__fmul_rn(b") + "xyz"[k] + ", a), __fmul_rn(a" +
+                       "xyz"[k] + ", b))";
+            }
+            break;
+        case op::DIV:
+            pre = "            const float den = __fmul_rn(b, b);\n";
+            v = "__fdiv_rn(a, b)";
+            for (int k = 0; k < 3; ++k) {
+                d[k] = std::string("__fdiv_rn(__fsub_rn(__fmul_rn(a") + "xyz"[k] +
+                       ", b), __fmul_rn(b" + "xyz"[k] + ", a)), den)";
+            }
+            break;
+        case op::MIN:
+            v = "((b) < (a) ? (b) : (a))";
+            for (int k = 0; k < 3; ++k) d[k] = std::string("(a < b ? a") + "xyz"[k] + " : b" + "xyz"[k] + ")";
+            break;
+        case op::MAX:
+            v = "((a) < (b) ? (b) : (a))";
+            for (int k = 0; k < 3; ++k) d[k] = std::string("(a < b ? b") + "xyz"[k] + " : a" + "xyz"[k] + ")";
+            break;
+        case op::SQUARE:
+            v = "__fmul_rn(a, a)";
+            for (int k = 0; k < 3; ++k) d[k] = std::string("__fmul_rn(__fmul_rn(a") + "xyz"[k] + ", a), 2.0f)";
+            break;
+        case op::SQRT:
+            pre = "            const float ov = __fsqrt_rn(a);\n"
+                  "            const float den = __fmul_rn(2.0f, ov);\n";
+            v = "ov";
+            for (int k = 0; k < 3; ++k) {
+                const std::string t_ = std::string("a") + "xyz"[k];
+                d[k] = "((a < 0 || " + t_ + " == 0) ? 0.0f : __fdiv_rn(" + t_ + ", den))";
+            }
+            break;
+        case op::NEG:
+            v = "(-a)";
+            for (int k = 0; k < 3; ++k) d[k] = std::string("(-a") + "xyz"[k] + ")";
+            break;
+        case op::LOG:
+            v = "logf(a)";
+            for (int k = 0; k < 3; ++k) d[k] = std::string("__fdiv_rn(a") + "xyz"[k] + ", a)";
+            break;
+        case op::EXP:
+            pre = "            const float e = expf(a);\n";
+            v = "e";
+            for (int k = 0; k < 3; ++k) d[k] = std::string("__fmul_rn(a") + "xyz"[k] + ", e)";
+            break;
+        case op::ABS:
+            v = "fabsf(a)";
+            for (int k = 0; k < 3; ++k) d[k] = std::string("(a > 0 ? a") + "xyz"[k] + " : -a" + "xyz"[k] + ")";
+            break;
+        case op::RECIP:
+            pre = "            const float den = -__fmul_rn(a, a);\n";
+            v = "__fdiv_rn(1.0f, a)";
+            for (int k = 0; k < 3; ++k) d[k] = std::string("__fdiv_rn(a") + "xyz"[k] + ", den)";
+            break;
+        case op::CONST_VAR:
+            v = "a";
+            for (int k = 0; k < 3; ++k) d[k] = std::string("a") + "xyz"[k];
+            break;
+        default:
+            return std::string();
+    }
+    const std::string o = "r" + std::to_string(c.out);
+    s += pre;
+    s += "            " + o + " = " + v + ";\n";
+    for (int k = 0; k < 3; ++k) s += "            " + o + "_" + "xyz"[k] + " = " + d[k] + ";\n";
+    s += "        }\n";
+    return s;
+}
+
+/// CUDA source of the tape's value + derivative kernel (or empty).
+std::string derivs_source(const RegTape& t)
+{
+    std::string s;
+    s.reserve(400 * t.clauses.size() + 2048);
+    s += "extern \"C\" __global__ void __launch_bounds__(256)\n"
+         "lfb_tape_derivs(const float* __restrict__ X, const float* __restrict__ Y,\n"
+         "                const float* __restrict__ Z, float* __restrict__ ov,\n"
+         "                float* __restrict__ odx, float* __restrict__ ody,\n"
+         "                float* __restrict__ odz, unsigned long long n,\n"
+         "                const float* __restrict__ cp)\n{\n";
+    s += kHead;
+    s += "        float r0 = X[i], r0_x = 1.0f, r0_y = 0.0f, r0_z = 0.0f;\n"
+         "        float r1 = Y[i], r1_x = 0.0f, r1_y = 1.0f, r1_z = 0.0f;\n"
+         "        float r2 = Z[i], r2_x = 0.0f, r2_y = 0.0f, r2_z = 1.0f;\n";
+    for (uint32_t r = 3; r < t.n_regs; ++r) {
+        const std::string n = "r" + std::to_string(r);
+        s += "        float " + n + " = 0.0f, " + n + "_x = 0.0f, " + n + "_y = 0.0f, " + n +
+             "_z = 0.0f;\n";
+    }
+    for (const RegClause& c : t.clauses) {
+        const std::string cl = deriv_clause(t, c);
+        if (cl.empty()) return std::string();
+        s += cl;
+    }
+    const uint32_t rk = t.root_kind, ri = t.root;
+    s += "        ov[i] = " + operand(t, rk, ri) + ";\n";
+    s += "        if (odx) odx[i] = " + tangent(rk, ri, 0) + ";\n";
+    s += "        if (ody) ody[i] = " + tangent(rk, ri, 1) + ";\n";
+    s += "        if (odz) odz[i] = " + tangent(rk, ri, 2) + ";\n    }\n}\n";
+    return s;
+}
+
+/// Compiles `src` and loads its kernel `name` into slot k; false when
+/// anything is unavailable or fails.
+bool build(GpuTape& g, int k, const std::string& src, const char* name)
 {
     const Api& A = api();
-    if (!A.ok || g.reg.clauses.size() > kJitMaxClauses) return false;
-    const std::string src = source(g.reg);
-    if (src.empty()) return false;
+    if (!A.ok || src.empty()) return false;
     nvrtcProgram prog = nullptr;
     if (A.create(&prog, src.c_str(), "lfb_tape.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS) {
         return false;
@@ -156,12 +296,40 @@ bool build(GpuTape& g)
     CUmodule mod = nullptr;
     CUfunction fn = nullptr;
     if (A.load(&mod, cubin.data()) != CUDA_SUCCESS) return false;
-    if (A.function(&fn, mod, "lfb_tape_values") != CUDA_SUCCESS) {
+    if (A.function(&fn, mod, name) != CUDA_SUCCESS) {
         A.unload(mod);
         return false;
     }
-    g.jit_module = mod;
-    g.jit_function = fn;
+    g.jit[k].module = mod;
+    g.jit[k].function = fn;
+    return true;
+}
+
+/// The kernel of slot k (0 values, 1 derivatives), compiled on first use.
+void* kernel(GpuTape& g, int k)
+{
+    std::lock_guard<std::mutex> lock(g.mu);
+    GpuTape::JitKernel& j = g.jit[k];
+    if (j.state == 0) {
+        bool ok = api().ok && g.reg.clauses.size() <= kJitMaxClauses;
+        if (ok) {
+            ok = k == 0 ? build(g, 0, values_source(g.reg), "lfb_tape_values")
+                        : build(g, 1, derivs_source(g.reg), "lfb_tape_derivs");
+        }
+        j.state = ok ? 1 : -1;
+    }
+    return j.state == 1 ? j.function : nullptr;
+}
+
+bool launch(void* fn, uint64_t n, void** args, cudaStream_t s)
+{
+    const uint64_t blocks = std::min<uint64_t>((n + 255) / 256,
+                                               static_cast<uint64_t>(device_sm_count()) * 16);
+    if (api().launch(static_cast<CUfunction>(fn), static_cast<unsigned>(blocks), 1, 1, 256, 1,
+                     1, 0, reinterpret_cast<CUstream>(s), args, nullptr) != CUDA_SUCCESS) {
+        return false;
+    }
+    note_launches(1);
     return true;
 }
 
@@ -170,31 +338,34 @@ bool build(GpuTape& g)
 bool jit_values(GpuTape& g, uint64_t n, const float* x, const float* y, const float* z,
                 float* out, cudaStream_t s)
 {
-    {
-        std::lock_guard<std::mutex> lock(g.mu);
-        if (g.jit_state == 0) g.jit_state = build(g) ? 1 : -1;
-        if (g.jit_state != 1) return false;
-    }
+    void* fn = kernel(g, 0);
+    if (!fn) return false;
     if (n == 0) return true;
-    const uint64_t blocks = std::min<uint64_t>((n + 255) / 256,
-                                               static_cast<uint64_t>(device_sm_count()) * 16);
     unsigned long long nn = n;
     const float* cp = g.d_cpool;
     void* args[] = {&x, &y, &z, &out, &nn, &cp};
-    if (api().launch(static_cast<CUfunction>(g.jit_function), static_cast<unsigned>(blocks), 1,
-                     1, 256, 1, 1, 0, reinterpret_cast<CUstream>(s), args,
-                     nullptr) != CUDA_SUCCESS) {
-        return false;
-    }
-    note_launches(1);
-    return true;
+    return launch(fn, n, args, s);
+}
+
+bool jit_derivs(GpuTape& g, uint64_t n, const float* x, const float* y, const float* z,
+                float* v, float* dx, float* dy, float* dz, cudaStream_t s)
+{
+    void* fn = kernel(g, 1);
+    if (!fn) return false;
+    if (n == 0) return true;
+    unsigned long long nn = n;
+    const float* cp = g.d_cpool;
+    void* args[] = {&x, &y, &z, &v, &dx, &dy, &dz, &nn, &cp};
+    return launch(fn, n, args, s);
 }
 
 void jit_release(GpuTape& g)
 {
-    if (g.jit_module && api().ok) api().unload(static_cast<CUmodule>(g.jit_module));
-    g.jit_module = nullptr;
-    g.jit_function = nullptr;
+    for (auto& j : g.jit) {
+        if (j.module && api().ok) api().unload(static_cast<CUmodule>(j.module));
+        j.module = nullptr;
+        j.function = nullptr;
+    }
 }
 
 }  // namespace lfb

@@ -27,7 +27,13 @@ constexpr uint32_t kJitMaxClauses = 4096;
 bool jit_values(GpuTape& g, uint64_t n, const float* x, const float* y, const float* z,
                 float* out, cudaStream_t s);
 
-/// Releases a tape's compiled kernel (called when the tape is destroyed).
+/// Values and d/dx, d/dy, d/dz (dx / dy / dz may be null) through the
+/// tape's compiled derivative kernel; the same conditions as jit_values, and
+/// the same bits as DerivArrayEvaluator's rules in dv_deriv.
+bool jit_derivs(GpuTape& g, uint64_t n, const float* x, const float* y, const float* z,
+                float* v, float* dx, float* dy, float* dz, cudaStream_t s);
+
+/// Releases a tape's compiled kernels (called when the tape is destroyed).
 void jit_release(GpuTape& g);
 
 }  // namespace lfb

@@ -48,10 +48,14 @@ struct GpuTape {
     uint32_t n_pslot = 0;
     bool pslot_ready = false;
 
-    // Compiled value kernel (jit.cpp): 0 not tried, 1 ready, -1 none.
-    int jit_state = 0;
-    void* jit_module = nullptr;
-    void* jit_function = nullptr;
+    // Compiled kernels (jit.cpp), [0] values, [1] values + derivatives:
+    // state 0 not tried, 1 ready, -1 none.
+    struct JitKernel {
+        int state = 0;
+        void* module = nullptr;
+        void* function = nullptr;
+    };
+    JitKernel jit[2];
 
     ~GpuTape();
     DevTape dev() const;

@@ -1,6 +1,7 @@
 """Tapes compiled to straight-line kernels (jit.cpp) against the interpreter.
 
-The compiled kernel must give the interpreter's bits at every point,
+The compiled value and derivative kernels must give the interpreter's bits
+at every point,
 transcendental opcodes included (both call the same CUDA functions with
 contraction off).  The interpreter's values are computed in a child process
 with LFB_JIT=0; lfb_tape_compiled says which path a tape took."""
@@ -48,7 +49,8 @@ s, vals = shapes()[name]
 t = Tape(s, vals)
 out = t.values(*points())
 assert ffi.load().lfb_tape_compiled(t.ptr) == 0
-np.save(sys.argv[3], out)
+d = t.derivs(*points())
+np.save(sys.argv[3], np.stack([out] + list(d)))
 """
 
 
@@ -71,7 +73,10 @@ def test_compiled_matches_interpreter(gpu, name, tmp_path):
                        timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     want = np.load(path)
-    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    assert np.array_equal(got.view(np.uint32), want[0].view(np.uint32))
+    # values and d/dx, d/dy, d/dz of the compiled derivative kernel
+    d = np.stack(list(t.derivs(*points())))
+    assert np.array_equal(d.view(np.uint32), want[1:].view(np.uint32))
 
 
 def test_variables_change_without_recompiling(gpu):

@@ -18,6 +18,7 @@
 
 #include "eval_api.hpp"
 #include "eval_kernels.cuh"
+#include "jit.hpp"
 #include "libfive_b200.h"
 
 namespace lfb {
@@ -385,6 +386,7 @@ bool ensure_pslots(GpuTape& g)
                             cudaMemcpyHostToDevice), "partial slots")) {
         return false;
     }
+    g.h_pslot = std::move(ps);
     g.n_pslot = next;
     g.pslot_ready = true;
     return true;
@@ -485,20 +487,43 @@ int grad_device(GpuTape& g, uint64_t n, const float* x, const float* y, const fl
         }
         note_launches(1);
     };
+    // The tape's compiled reverse-mode kernels (jit.cpp) when it has them,
+    // else the interpreters; both do the same arithmetic.
+    const uint32_t* hs = g.h_pslot.data();
+    const bool jit = jit_partials(g, hs, 0, x, y, z, P, f, s) &&
+                     jit_backward(g, hs, 0, P, seed, gx, gy, gz, gvars, 0, s);
+    auto backward_any = [&](uint32_t m, unsigned blocks, const float* sd, uint64_t off, bool xyz,
+                            float* gv, int block_cv) {
+        if (jit) {
+            return jit_backward(g, hs, m, P, sd, xyz && gx ? gx + off : nullptr,
+                                xyz && gy ? gy + off : nullptr, xyz && gz ? gz + off : nullptr,
+                                gv, block_cv, s);
+        }
+        backward(m, blocks, sd, off, xyz, gv, block_cv);
+        return true;
+    };
     for (uint64_t off = 0; off < n; off += chunk) {
         const uint32_t m = static_cast<uint32_t>(std::min(chunk, n - off));
         const unsigned blocks = (m + kBlock * kPts - 1) / (kBlock * kPts);
-        k_grad_forward<kPts><<<blocks, kBlock, smem, s>>>(t, pslot, m, x + off, y + off, z + off,
-                                                          P, f ? f + off : nullptr);
-        note_launches(1);
+        if (jit) {
+            if (!jit_partials(g, hs, m, x + off, y + off, z + off, P, f ? f + off : nullptr, s)) {
+                return set_error(LFB_E_CUDA, "compiled gradient kernel launch failed");
+            }
+        } else {
+            k_grad_forward<kPts><<<blocks, kBlock, smem, s>>>(t, pslot, m, x + off, y + off,
+                                                              z + off, P, f ? f + off : nullptr);
+            note_launches(1);
+        }
         const float* sd = seed ? seed + off : nullptr;
+        bool ok = true;
         if (!has_cv) {
-            if (want_xyz || gvars) backward(m, blocks, sd, off, true, gvars, 0);
+            if (want_xyz || gvars) ok = backward_any(m, blocks, sd, off, true, gvars, 0);
         } else {
             // CONST_VAR passes point gradients but blocks variable ones.
-            if (want_xyz) backward(m, blocks, sd, off, true, nullptr, 0);
-            if (gvars) backward(m, blocks, sd, off, false, gvars, 1);
+            if (want_xyz) ok = backward_any(m, blocks, sd, off, true, nullptr, 0);
+            if (gvars && ok) ok = backward_any(m, blocks, sd, off, false, gvars, 1);
         }
+        if (!ok) return set_error(LFB_E_CUDA, "compiled gradient kernel launch failed");
         if (!cuda_ok(cudaGetLastError(), "gradient kernels")) return LFB_E_CUDA;
     }
     return 0;

@@ -272,6 +272,173 @@ std::string derivs_source(const RegTape& t)
     return s;
 }
 
+/// Reverse mode.  The slot table (slot | kind << 28) and the partial rules
+/// are those of grad_kernels.cu: kind 0 fixed by the opcode, 1 a min/max
+/// choice, 2 one partial, 3 two partials.
+enum : uint32_t { RK_CONST = 0, RK_CHOICE = 1, RK_ONE = 2, RK_TWO = 3 };
+
+/// Partials d out / d a, d out / d b of one clause as expressions of its
+/// operand values `a`, `b` (and temporaries declared in `pre`), the results
+/// of DerivArrayEvaluator's rules for unit tangents; false for opcodes
+/// without a compiled form.
+bool partial_exprs(uint8_t o, std::string* v, std::string* pa, std::string* pb, std::string* pre)
+{
+    *pb = "0.0f";
+    switch (o) {
+        case op::ADD: *v = "__fadd_rn(a, b)"; *pa = "1.0f"; *pb = "1.0f"; return true;
+        case op::SUB: *v = "__fsub_rn(a, b)"; *pa = "1.0f"; *pb = "-1.0f"; return true;
+        case op::NEG: *v = "(-a)"; *pa = "-1.0f"; return true;
+        case op::CONST_VAR: *v = "a"; *pa = "1.0f"; return true;
+        case op::MUL:
+            *v = "__fmul_rn(a, b)";
+            *pa = "__fadd_rn(__fmul_rn(0.0f, a), __fmul_rn(1.0f, b))";
+            *pb = "__fadd_rn(__fmul_rn(1.0f, a), __fmul_rn(0.0f, b))";
+            return true;
+        case op::MIN: *v = "((b) < (a) ? (b) : (a))"; *pa = "(a < b ? 1.0f : 0.0f)"; return true;
+        case op::MAX: *v = "((a) < (b) ? (b) : (a))"; *pa = "(a < b ? 0.0f : 1.0f)"; return true;
+        case op::SQUARE: *v = "__fmul_rn(a, a)"; *pa = "__fmul_rn(a, 2.0f)"; return true;
+        case op::ABS: *v = "fabsf(a)"; *pa = "(a > 0 ? 1.0f : -1.0f)"; return true;
+        case op::SQRT:
+            *pre = "const float ov = __fsqrt_rn(a); ";
+            *v = "ov";
+            *pa = "(a < 0 ? 0.0f : __fdiv_rn(1.0f, __fmul_rn(2.0f, ov)))";
+            return true;
+        case op::LOG: *v = "logf(a)"; *pa = "__fdiv_rn(1.0f, a)"; return true;
+        case op::EXP:
+            *pre = "const float e = expf(a); ";
+            *v = "e";
+            *pa = "__fmul_rn(1.0f, e)";
+            return true;
+        case op::RECIP:
+            *v = "__fdiv_rn(1.0f, a)";
+            *pa = "__fdiv_rn(1.0f, -__fmul_rn(a, a))";
+            return true;
+        case op::DIV:
+            *pre = "const float den = __fmul_rn(b, b); ";
+            *v = "__fdiv_rn(a, b)";
+            *pa = "__fdiv_rn(__fsub_rn(__fmul_rn(1.0f, b), __fmul_rn(0.0f, a)), den)";
+            *pb = "__fdiv_rn(__fsub_rn(__fmul_rn(0.0f, b), __fmul_rn(1.0f, a)), den)";
+            return true;
+        default:
+            return false;
+    }
+}
+
+/// Forward pass of the reverse mode: values in registers, the partials the
+/// slot table keeps written per point.
+std::string partials_source(const RegTape& t, const std::vector<uint32_t>& slots)
+{
+    std::string s;
+    s.reserve(160 * t.clauses.size() + 1024);
+    s += "extern \"C\" __global__ void __launch_bounds__(256)\n"
+         "lfb_tape_partials(const float* __restrict__ X, const float* __restrict__ Y,\n"
+         "                  const float* __restrict__ Z, float* __restrict__ P,\n"
+         "                  float* __restrict__ f, unsigned m, const float* __restrict__ cp)\n{\n"
+         "    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;\n"
+         "    if (i >= m) return;\n"
+         "    float* const Pi = P + i;\n"
+         "    float r0 = X[i], r1 = Y[i], r2 = Z[i];\n";
+    for (uint32_t r = 3; r < t.n_regs; ++r) s += "    float r" + std::to_string(r) + " = 0.0f;\n";
+    for (size_t c = 0; c < t.clauses.size(); ++c) {
+        const RegClause& cl = t.clauses[c];
+        std::string v, pa, pb, pre;
+        if (!partial_exprs(cl.op, &v, &pa, &pb, &pre)) return std::string();
+        const uint32_t kind = slots[c] >> 28, slot = slots[c] & 0x0fffffffu;
+        s += "    { const float a = " + operand(t, cl.kinds & 3, cl.a) + ", b = " +
+             operand(t, (cl.kinds >> 2) & 3, cl.b) + "; " + pre;
+        if (kind != RK_CONST) {
+            s += "Pi[(size_t)" + std::to_string(slot) + " * m] = " + pa + "; ";
+            if (kind == RK_TWO) s += "Pi[(size_t)" + std::to_string(slot + 1) + " * m] = " + pb + "; ";
+        }
+        s += "r" + std::to_string(cl.out) + " = " + v + "; }\n";
+    }
+    s += "    if (f) f[i] = " + operand(t, t.root_kind, t.root) + ";\n}\n";
+    return s;
+}
+
+/// Backward pass: one adjoint per tape register, clauses in reverse, the
+/// same products and sums as the interpreted backward pass; variable
+/// adjoints are summed over the warp, then over the block in shared memory.
+std::string backward_source(const RegTape& t, const std::vector<uint32_t>& slots)
+{
+    std::string s;
+    s.reserve(200 * t.clauses.size() + 2048);
+    s += "__device__ __forceinline__ void lfb_add_var(float* Gv, unsigned k, float g)\n{\n"
+         "    for (int o = 16; o > 0; o >>= 1) g += __shfl_xor_sync(0xffffffffu, g, o);\n"
+         "    if ((threadIdx.x & 31) == 0 && g != 0.0f) atomicAdd(Gv + k, g);\n}\n"
+         "extern \"C\" __global__ void __launch_bounds__(256)\n"
+         "lfb_tape_backward(const float* __restrict__ P, const float* __restrict__ seed,\n"
+         "                  float* __restrict__ gx, float* __restrict__ gy,\n"
+         "                  float* __restrict__ gz, float* __restrict__ gvars, unsigned m,\n"
+         "                  unsigned n_vars, int block_cv)\n{\n"
+         "    extern __shared__ float Gv[];\n"
+         "    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;\n"
+         "    const bool ok = i < m;\n"
+         "    const bool gv = gvars != nullptr;\n"
+         "    if (gv) {\n"
+         "        for (unsigned k = threadIdx.x; k < n_vars; k += blockDim.x) Gv[k] = 0.0f;\n"
+         "        __syncthreads();\n    }\n"
+         "    const float* const Pi = P + (ok ? i : 0);\n";
+    for (uint32_t r = 0; r < t.n_regs; ++r) s += "    float a" + std::to_string(r) + " = 0.0f;\n";
+    s += "    const float s0 = ok ? (seed ? seed[i] : 1.0f) : 0.0f;\n";
+    if (t.root_kind == OPND_REG) {
+        s += "    a" + std::to_string(t.root) + " = s0;\n";
+    } else if (t.root_kind == OPND_VAR) {
+        s += "    if (gv) lfb_add_var(Gv, " + std::to_string(t.root - t.n_const) + ", s0);\n";
+    }
+    auto contribution = [&](uint32_t kind, uint32_t idx, const std::string& g) {
+        if (kind == OPND_REG) return "a" + std::to_string(idx) + " += " + g + "; ";
+        if (kind == OPND_VAR) {
+            return "if (gv) lfb_add_var(Gv, " + std::to_string(idx - t.n_const) + ", " + g +
+                   "); ";
+        }
+        return std::string();
+    };
+    for (size_t c = t.clauses.size(); c-- > 0;) {
+        const RegClause& cl = t.clauses[c];
+        const uint32_t kind = slots[c] >> 28, slot = slots[c] & 0x0fffffffu;
+        const uint32_t ka = cl.kinds & 3, kb = (cl.kinds >> 2) & 3;
+        const bool binary = op::arity(cl.op) == 2;
+        const std::string o = "a" + std::to_string(cl.out);
+        std::string pdx, pdy = "0.0f";
+        switch (kind) {
+            case RK_CONST:
+                switch (cl.op) {
+                    case op::ADD: pdx = "1.0f"; pdy = "1.0f"; break;
+                    case op::SUB: pdx = "1.0f"; pdy = "-1.0f"; break;
+                    case op::NEG: pdx = "-1.0f"; break;
+                    case op::CONST_VAR: pdx = "(block_cv ? 0.0f : 1.0f)"; break;
+                    default: pdx = "1.0f"; break;
+                }
+                break;
+            case RK_CHOICE:
+                pdx = "p0";
+                pdy = "(ok ? 1.0f - p0 : 0.0f)";
+                break;
+            case RK_ONE: pdx = "p0"; break;
+            default: pdx = "p0"; pdy = "p1"; break;
+        }
+        s += "    { const float adj = " + o + "; " + o + " = 0.0f; ";
+        if (kind != RK_CONST) {
+            s += "const float p0 = ok ? Pi[(size_t)" + std::to_string(slot) + " * m] : 0.0f; ";
+            if (kind == RK_TWO) {
+                s += "const float p1 = ok ? Pi[(size_t)" + std::to_string(slot + 1) +
+                     " * m] : 0.0f; ";
+            }
+        }
+        s += contribution(ka, cl.a, "adj * " + pdx);
+        if (binary) s += contribution(kb, cl.b, "adj * " + pdy);
+        s += "}\n";
+    }
+    s += "    if (ok) {\n"
+         "        if (gx) gx[i] = a0;\n        if (gy) gy[i] = a1;\n        if (gz) gz[i] = a2;\n"
+         "    }\n"
+         "    if (gv) {\n        __syncthreads();\n"
+         "        for (unsigned k = threadIdx.x; k < n_vars; k += blockDim.x) {\n"
+         "            if (Gv[k] != 0.0f) atomicAdd(gvars + k, Gv[k]);\n        }\n    }\n}\n";
+    return s;
+}
+
 /// Compiles `src` and loads its kernel `name` into slot k; false when
 /// anything is unavailable or fails.
 bool build(GpuTape& g, int k, const std::string& src, const char* name)
@@ -305,20 +472,36 @@ bool build(GpuTape& g, int k, const std::string& src, const char* name)
     return true;
 }
 
-/// The kernel of slot k (0 values, 1 derivatives), compiled on first use.
-void* kernel(GpuTape& g, int k)
+/// The kernel of slot k (0 values, 1 derivatives, 2 reverse-mode
+/// partials, 3 reverse-mode backward pass), compiled on first use.
+void* kernel(GpuTape& g, int k, const std::vector<uint32_t>* slots = nullptr)
 {
     std::lock_guard<std::mutex> lock(g.mu);
     GpuTape::JitKernel& j = g.jit[k];
     if (j.state == 0) {
         bool ok = api().ok && g.reg.clauses.size() <= kJitMaxClauses;
         if (ok) {
-            ok = k == 0 ? build(g, 0, values_source(g.reg), "lfb_tape_values")
-                        : build(g, 1, derivs_source(g.reg), "lfb_tape_derivs");
+            switch (k) {
+                case 0: ok = build(g, 0, values_source(g.reg), "lfb_tape_values"); break;
+                case 1: ok = build(g, 1, derivs_source(g.reg), "lfb_tape_derivs"); break;
+                case 2: ok = build(g, 2, partials_source(g.reg, *slots), "lfb_tape_partials"); break;
+                default: ok = build(g, 3, backward_source(g.reg, *slots), "lfb_tape_backward"); break;
+            }
         }
         j.state = ok ? 1 : -1;
     }
     return j.state == 1 ? j.function : nullptr;
+}
+
+bool launch_1d(void* fn, uint32_t m, void** args, unsigned smem, cudaStream_t s)
+{
+    const unsigned blocks = (m + 255) / 256;
+    if (api().launch(static_cast<CUfunction>(fn), blocks, 1, 1, 256, 1, 1, smem,
+                     reinterpret_cast<CUstream>(s), args, nullptr) != CUDA_SUCCESS) {
+        return false;
+    }
+    note_launches(1);
+    return true;
 }
 
 bool launch(void* fn, uint64_t n, void** args, cudaStream_t s)
@@ -357,6 +540,41 @@ bool jit_derivs(GpuTape& g, uint64_t n, const float* x, const float* y, const fl
     const float* cp = g.d_cpool;
     void* args[] = {&x, &y, &z, &v, &dx, &dy, &dz, &nn, &cp};
     return launch(fn, n, args, s);
+}
+
+bool jit_partials(GpuTape& g, const uint32_t* slots, uint32_t m, const float* x,
+                  const float* y, const float* z, float* P, float* f, cudaStream_t s)
+{
+    std::vector<uint32_t> table;
+    {
+        std::lock_guard<std::mutex> lock(g.mu);
+        if (g.jit[2].state == 0) table.assign(slots, slots + g.reg.clauses.size());
+    }
+    void* fn = kernel(g, 2, &table);
+    if (!fn) return false;
+    if (m == 0) return true;
+    const float* cp = g.d_cpool;
+    void* args[] = {&x, &y, &z, &P, &f, &m, &cp};
+    return launch_1d(fn, m, args, 0, s);
+}
+
+bool jit_backward(GpuTape& g, const uint32_t* slots, uint32_t m, const float* P,
+                  const float* seed, float* gx, float* gy, float* gz, float* gvars,
+                  int block_cv, cudaStream_t s)
+{
+    uint32_t n_vars = g.reg.n_vars;
+    const unsigned smem = gvars ? n_vars * 4 : 0;
+    if (smem > 48 * 1024) return false;
+    std::vector<uint32_t> table;
+    {
+        std::lock_guard<std::mutex> lock(g.mu);
+        if (g.jit[3].state == 0) table.assign(slots, slots + g.reg.clauses.size());
+    }
+    void* fn = kernel(g, 3, &table);
+    if (!fn) return false;
+    if (m == 0) return true;
+    void* args[] = {&P, &seed, &gx, &gy, &gz, &gvars, &m, &n_vars, &block_cv};
+    return launch_1d(fn, m, args, smem, s);
 }
 
 void jit_release(GpuTape& g)

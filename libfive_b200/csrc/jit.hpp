@@ -33,6 +33,17 @@ bool jit_values(GpuTape& g, uint64_t n, const float* x, const float* y, const fl
 bool jit_derivs(GpuTape& g, uint64_t n, const float* x, const float* y, const float* z,
                 float* v, float* dx, float* dy, float* dz, cudaStream_t s);
 
+/// Reverse mode through compiled kernels: the forward pass storing the
+/// local partials at P[slot * m + i] (slot table of partial_slots), and the
+/// backward pass (block_cv: CONST_VAR blocks the adjoint).  Same
+/// arithmetic, clause by clause, as the interpreted reverse mode; false when
+/// the tape has no compiled form (then nothing was launched).
+bool jit_partials(GpuTape& g, const uint32_t* slots, uint32_t m, const float* x,
+                  const float* y, const float* z, float* P, float* f, cudaStream_t s);
+bool jit_backward(GpuTape& g, const uint32_t* slots, uint32_t m, const float* P,
+                  const float* seed, float* gx, float* gy, float* gz, float* gvars,
+                  int block_cv, cudaStream_t s);
+
 /// Releases a tape's compiled kernels (called when the tape is destroyed).
 void jit_release(GpuTape& g);
 

@@ -45,17 +45,19 @@ struct GpuTape {
     // Reverse mode: where each clause's local partials are stored per point
     // (slot | kind << 28, see grad_kernels.cu), built on first use.
     uint32_t* d_pslot = nullptr;
+    std::vector<uint32_t> h_pslot;
     uint32_t n_pslot = 0;
     bool pslot_ready = false;
 
-    // Compiled kernels (jit.cpp), [0] values, [1] values + derivatives:
+    // Compiled kernels (jit.cpp), [0] values, [1] values + derivatives,
+    // [2] reverse-mode partials, [3] reverse-mode backward pass:
     // state 0 not tried, 1 ready, -1 none.
     struct JitKernel {
         int state = 0;
         void* module = nullptr;
         void* function = nullptr;
     };
-    JitKernel jit[2];
+    JitKernel jit[4];
 
     ~GpuTape();
     DevTape dev() const;

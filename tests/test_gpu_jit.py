@@ -41,7 +41,7 @@ def shapes():
 CHILD = r"""
 import sys, numpy as np
 sys.path.insert(0, sys.argv[1]); sys.path.insert(0, sys.argv[1] + "/tests")
-from test_gpu_jit import shapes, points
+from test_gpu_jit import shapes, points, grad, grad_vars
 from libfive_b200.shape import Tape
 from libfive_b200 import ffi
 name = sys.argv[2]
@@ -51,7 +51,28 @@ out = t.values(*points())
 assert ffi.load().lfb_tape_compiled(t.ptr) == 0
 d = t.derivs(*points())
 np.save(sys.argv[3], np.stack([out] + list(d)))
+np.save(sys.argv[3] + ".grad.npy", np.stack(grad(t)))
+np.save(sys.argv[3] + ".gvars.npy", grad_vars(t))
 """
+
+
+def grad(t):
+    """f and the reverse-mode point gradients with a varying seed."""
+    x, y, z = points()
+    n = len(x)
+    seed = np.linspace(-1.0, 1.0, n).astype(np.float32)
+    f = np.empty(n, np.float32)
+    gx, gy, gz = (np.empty(n, np.float32) for _ in range(3))
+    t.grad(x, y, z, seed=seed, f=f, gx=gx, gy=gy, gz=gz)
+    return f, gx, gy, gz
+
+
+def grad_vars(t):
+    x, y, z = points()
+    gv = np.zeros(max(t.n_vars, 1), np.float32)
+    if t.n_vars:
+        t.grad(x, y, z, gvars=gv)
+    return gv
 
 
 def points():
@@ -77,6 +98,12 @@ def test_compiled_matches_interpreter(gpu, name, tmp_path):
     # values and d/dx, d/dy, d/dz of the compiled derivative kernel
     d = np.stack(list(t.derivs(*points())))
     assert np.array_equal(d.view(np.uint32), want[1:].view(np.uint32))
+    # reverse mode: f and point gradients bit for bit (same operations in the
+    # same order), variable gradients up to the order of the atomic sums
+    g = np.stack(grad(t))
+    assert np.array_equal(g.view(np.uint32), np.load(path + ".grad.npy").view(np.uint32))
+    gv, gw = grad_vars(t), np.load(path + ".gvars.npy")
+    assert np.allclose(gv, gw, rtol=1e-5, atol=1e-5 * max(1.0, float(np.abs(gw).max())))
 
 
 def test_variables_change_without_recompiling(gpu):

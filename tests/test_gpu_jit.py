@@ -103,7 +103,10 @@ def test_compiled_matches_interpreter(gpu, name, tmp_path):
     g = np.stack(grad(t))
     assert np.array_equal(g.view(np.uint32), np.load(path + ".grad.npy").view(np.uint32))
     gv, gw = grad_vars(t), np.load(path + ".gvars.npy")
-    assert np.allclose(gv, gw, rtol=1e-5, atol=1e-5 * max(1.0, float(np.abs(gw).max())))
+    finite = np.isfinite(gw)
+    scale = max(1.0, float(np.abs(gw[finite]).max())) if finite.any() else 1.0
+    assert np.array_equal(np.isfinite(gv), finite)
+    assert np.allclose(gv, gw, rtol=1e-5, atol=1e-5 * scale, equal_nan=True)
 
 
 def test_variables_change_without_recompiling(gpu):

@@ -483,10 +483,12 @@ def run_eval(args, world, rank, local):
     derivatives, points resident on the device; e2e passes host arrays."""
     import numpy as np
     import torch
-    from libfive_b200 import workloads
+    from libfive_b200 import ffi, workloads
     from libfive_b200.shape import Tape
     torch.cuda.set_device(local)
-    tape = Tape(workloads.spheres_union(64, seed=1 + rank))
+    shape = workloads.spheres_union(64, seed=1 + rank)
+    tape = Tape(shape)
+    wv, wg, _ = tape_weights(shape)
     pts = workloads.lattice(128)
     n = len(pts[0])
     x, y, z = (torch.from_numpy(a).cuda() for a in pts)
@@ -500,9 +502,18 @@ def run_eval(args, world, rank, local):
     hf = np.empty(n, np.float32)
     t_e2e = _timed(lambda: tape.values(hx, hy, hz, out=hf), args.steps, args.warmup, flush)
     ce = n * tape.n_clauses
+    sm = torch.cuda.get_device_properties(local).multi_processor_count
+    peak = sm * 128 * 1965e6 / 1e9   # G FP32 lane-ops/s at the maximum SM clock
+    achieved = ce * wv / (t_val / 1e3) / 1e9
     if rank == 0:
         print(json.dumps({
             "metric": "clause-evals/s", "value": ce / (t_val / 1e3), "unit": "clause-evals/s",
+            "compiled": bool(ffi.load().lfb_tape_compiled(tape.ptr)),
+            "roofline": {"kernel": "lfb_tape_values" if ffi.load().lfb_tape_compiled(tape.ptr)
+                         else "k_values", "bound": "fp32", "achieved": achieved,
+                         "peak": peak, "unit": "G lane-ops/s", "frac": achieved / peak,
+                         "peak_source": "derived: SMs x 128 FP32 lanes x 1965 MHz",
+                         "lane_ops_per_clause": wv},
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_val,
             "higher_is_better": True, "deriv_value": ce / (t_der / 1e3), "ms_deriv": t_der,
             "e2e": {"value": ce / (t_e2e / 1e3), "unit": "clause-evals/s",

@@ -47,6 +47,37 @@ def _headers():
         for n in os.listdir(os.path.join(ROOT, "include"))]
 
 
+# Headers that kernels compiled at run time (csrc/jit.cpp) include; their
+# text is built into the library.
+JIT_HEADERS = ["opcode_ids.h", "scalar_minmax.h", "dev_interval.cuh"]
+
+
+def _jit_headers_source():
+    """Writes _build/jit_headers.cpp (the JIT headers as string literals)
+    when a header is newer than it; returns its path."""
+    out = os.path.join(BUILD, "jit_headers.cpp")
+    srcs = [os.path.join(CSRC, h) for h in JIT_HEADERS]
+    if os.path.exists(out) and os.path.getmtime(out) >= max(os.path.getmtime(h) for h in srcs):
+        return out
+    delim = "lfbjit"
+    parts = []
+    for h in srcs:
+        text = open(h).read()
+        assert ")" + delim + '"' not in text
+        parts.append('R"%s(%s)%s"' % (delim, text, delim))
+    with open(out, "w") as f:
+        f.write("// Generated by libfive_b200/build.py from csrc/: the headers that\n"
+                "// kernels compiled at run time include.\n"
+                "namespace lfb {\n"
+                "extern const int kJitHeaderCount = %d;\n" % len(srcs) +
+                "extern const char* const kJitHeaderNames[] = {%s};\n"
+                % ", ".join('"%s"' % h for h in JIT_HEADERS) +
+                "extern const char* const kJitHeaderSources[] = {\n%s};\n"
+                % ",\n".join(parts) +
+                "}  // namespace lfb\n")
+    return out
+
+
 def _compile(src, force, newest_header):
     obj = os.path.join(BUILD, os.path.basename(src) + ".o")
     if (not force and os.path.exists(obj)
@@ -68,7 +99,7 @@ def build(force=False, verbose=True):
     os.makedirs(BUILD, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
     newest_header = max(os.path.getmtime(h) for h in _headers())
-    srcs = _sources()
+    srcs = _sources() + [_jit_headers_source()]
     objs = []
     errors = []
     with concurrent.futures.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:

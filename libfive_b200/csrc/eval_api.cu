@@ -121,6 +121,7 @@ int eval_intervals_device(GpuTape& g, uint64_t n, const float* xlo,
                           uint8_t* onan, cudaStream_t s)
 {
     if (!require_device()) return LFB_E_CUDA;
+    if (jit_intervals(g, n, xlo, xhi, ylo, yhi, zlo, zhi, olo, ohi, onan, s)) return 0;
     const DevTape t = g.dev();
     for (uint64_t off = 0; off < n; off += kChunk) {
         const uint32_t m = static_cast<uint32_t>(std::min(kChunk, n - off));

@@ -20,6 +20,11 @@ namespace lfb {
 
 int device_sm_count();   // eval_kernels.cu
 
+// The headers run-time compiled kernels include (generated by build.py).
+extern const int kJitHeaderCount;
+extern const char* const kJitHeaderNames[];
+extern const char* const kJitHeaderSources[];
+
 namespace {
 
 /// NVRTC and the driver's module calls, looked up at run time so that the
@@ -32,6 +37,8 @@ struct Api {
     nvrtcResult (*cubin_size)(nvrtcProgram, size_t*) = nullptr;
     nvrtcResult (*cubin)(nvrtcProgram, char*) = nullptr;
     nvrtcResult (*destroy)(nvrtcProgram*) = nullptr;
+    nvrtcResult (*log_size)(nvrtcProgram, size_t*) = nullptr;
+    nvrtcResult (*log)(nvrtcProgram, char*) = nullptr;
     CUresult (*load)(CUmodule*, const void*) = nullptr;
     CUresult (*function)(CUfunction*, CUmodule, const char*) = nullptr;
     CUresult (*unload)(CUmodule) = nullptr;
@@ -45,20 +52,28 @@ const Api& api()
         Api r;
         const char* e = std::getenv("LFB_JIT");
         if (e && e[0] == '0') return r;
-        void* rtc = dlopen("libnvrtc.so.12", RTLD_NOW | RTLD_LOCAL);
-        if (!rtc) rtc = dlopen("/usr/local/cuda/lib64/libnvrtc.so.12", RTLD_NOW | RTLD_LOCAL);
-        void* drv = dlopen("libcuda.so.1", RTLD_NOW | RTLD_LOCAL);
-        if (!rtc || !drv) return r;
         auto get = [](void* h, const char* name, auto& fn) {
             fn = reinterpret_cast<std::remove_reference_t<decltype(fn)>>(dlsym(h, name));
             return fn != nullptr;
         };
-        r.ok = get(rtc, "nvrtcCreateProgram", r.create) &&
-               get(rtc, "nvrtcCompileProgram", r.compile) &&
-               get(rtc, "nvrtcGetCUBINSize", r.cubin_size) &&
-               get(rtc, "nvrtcGetCUBIN", r.cubin) &&
-               get(rtc, "nvrtcDestroyProgram", r.destroy) &&
-               get(drv, "cuModuleLoadData", r.load) &&
+        void* rtc = dlopen("libnvrtc.so.12", RTLD_NOW | RTLD_LOCAL);
+        if (!rtc) rtc = dlopen("/usr/local/cuda/lib64/libnvrtc.so.12", RTLD_NOW | RTLD_LOCAL);
+        if (!rtc) return r;
+        const bool rtc_ok = get(rtc, "nvrtcCreateProgram", r.create) &&
+                            get(rtc, "nvrtcCompileProgram", r.compile) &&
+                            get(rtc, "nvrtcGetCUBINSize", r.cubin_size) &&
+                            get(rtc, "nvrtcGetCUBIN", r.cubin) &&
+                            get(rtc, "nvrtcDestroyProgram", r.destroy) &&
+                            get(rtc, "nvrtcGetProgramLogSize", r.log_size) &&
+                            get(rtc, "nvrtcGetProgramLog", r.log);
+        if (!rtc_ok) {
+            r.create = nullptr;
+            return r;
+        }
+        // The driver's module calls: only on a machine with a GPU driver
+        // (compilation alone works without one).
+        void* drv = dlopen("libcuda.so.1", RTLD_NOW | RTLD_LOCAL);
+        r.ok = drv && get(drv, "cuModuleLoadData", r.load) &&
                get(drv, "cuModuleGetFunction", r.function) &&
                get(drv, "cuModuleUnload", r.unload) &&
                get(drv, "cuLaunchKernel", r.launch);
@@ -439,27 +454,30 @@ std::string backward_source(const RegTape& t, const std::vector<uint32_t>& slots
     return s;
 }
 
+/// Interval operand: registers are kept as Iv values; constants and free
+/// variables become degenerate intervals as the interpreter's fetch does.
+std::string iv_operand(const RegTape& t, uint32_t kind, uint32_t idx)
+{
+    if (kind == OPND_REG) return "r" + std::to_string(idx);
+    const std::string v = operand(t, kind, idx);
+    return "iv_make(" + v + ", " + v + ")";
+}
+
+/// Opcodes the interval kernel compiles (the value kernel's set); the rest
+/// stay on the interpreter.
+bool iv_supported(uint8_t o)
+{
+    return !expr(o, "a", "b").empty();
+}
+
 /// Compiles `src` and loads its kernel `name` into slot k; false when
 /// anything is unavailable or fails.
 bool build(GpuTape& g, int k, const std::string& src, const char* name)
 {
     const Api& A = api();
     if (!A.ok || src.empty()) return false;
-    nvrtcProgram prog = nullptr;
-    if (A.create(&prog, src.c_str(), "lfb_tape.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS) {
-        return false;
-    }
-    const char* opts[] = {"--gpu-architecture=sm_100a", "-fmad=false", "--std=c++17"};
-    bool ok = A.compile(prog, 3, opts) == NVRTC_SUCCESS;
     std::vector<char> cubin;
-    size_t size = 0;
-    ok = ok && A.cubin_size(prog, &size) == NVRTC_SUCCESS && size > 0;
-    if (ok) {
-        cubin.resize(size);
-        ok = A.cubin(prog, cubin.data()) == NVRTC_SUCCESS;
-    }
-    A.destroy(&prog);
-    if (!ok) return false;
+    if (!jit_compile(src, &cubin, nullptr)) return false;
     CUmodule mod = nullptr;
     CUfunction fn = nullptr;
     if (A.load(&mod, cubin.data()) != CUDA_SUCCESS) return false;
@@ -485,7 +503,8 @@ void* kernel(GpuTape& g, int k, const std::vector<uint32_t>* slots = nullptr)
                 case 0: ok = build(g, 0, values_source(g.reg), "lfb_tape_values"); break;
                 case 1: ok = build(g, 1, derivs_source(g.reg), "lfb_tape_derivs"); break;
                 case 2: ok = build(g, 2, partials_source(g.reg, *slots), "lfb_tape_partials"); break;
-                default: ok = build(g, 3, backward_source(g.reg, *slots), "lfb_tape_backward"); break;
+                case 3: ok = build(g, 3, backward_source(g.reg, *slots), "lfb_tape_backward"); break;
+                default: ok = build(g, 4, jit_interval_source(g.reg), "lfb_tape_intervals"); break;
             }
         }
         j.state = ok ? 1 : -1;
@@ -575,6 +594,81 @@ bool jit_backward(GpuTape& g, const uint32_t* slots, uint32_t m, const float* P,
     if (m == 0) return true;
     void* args[] = {&P, &seed, &gx, &gy, &gz, &gvars, &m, &n_vars, &block_cv};
     return launch_1d(fn, m, args, smem, s);
+}
+
+bool jit_compile(const std::string& src, std::vector<char>* cubin, std::string* log)
+{
+    const Api& A = api();
+    if (!A.create) return false;
+    nvrtcProgram prog = nullptr;
+    if (A.create(&prog, src.c_str(), "lfb_tape.cu", kJitHeaderCount, kJitHeaderSources,
+                 kJitHeaderNames) != NVRTC_SUCCESS) {
+        return false;
+    }
+    const char* opts[] = {"--gpu-architecture=sm_100a", "-fmad=false", "--std=c++17"};
+    bool ok = A.compile(prog, 3, opts) == NVRTC_SUCCESS;
+    if (log && A.log_size && A.log) {
+        size_t n = 0;
+        if (A.log_size(prog, &n) == NVRTC_SUCCESS && n > 1) {
+            log->resize(n);
+            A.log(prog, &(*log)[0]);
+        }
+    }
+    size_t size = 0;
+    ok = ok && A.cubin_size(prog, &size) == NVRTC_SUCCESS && size > 0;
+    if (ok) {
+        cubin->resize(size);
+        ok = A.cubin(prog, cubin->data()) == NVRTC_SUCCESS;
+    }
+    A.destroy(&prog);
+    return ok;
+}
+
+std::string jit_interval_source(const RegTape& t)
+{
+    std::string s;
+    s.reserve(96 * t.clauses.size() + 1024);
+    s += "typedef unsigned char uint8_t;\ntypedef unsigned short uint16_t;\n"
+         "typedef unsigned int uint32_t;\ntypedef unsigned long long uint64_t;\n"
+         "#include \"dev_interval.cuh\"\nusing namespace lfb;\n"
+         "extern \"C\" __global__ void __launch_bounds__(256)\n"
+         "lfb_tape_intervals(const float* __restrict__ xlo, const float* __restrict__ xhi,\n"
+         "                   const float* __restrict__ ylo, const float* __restrict__ yhi,\n"
+         "                   const float* __restrict__ zlo, const float* __restrict__ zhi,\n"
+         "                   float* __restrict__ olo, float* __restrict__ ohi,\n"
+         "                   unsigned char* __restrict__ onan, unsigned long long n,\n"
+         "                   const float* __restrict__ cp)\n{\n";
+    s += kHead;
+    s += "        Iv r0 = iv_make(xlo[i], xhi[i]), r1 = iv_make(ylo[i], yhi[i]),\n"
+         "           r2 = iv_make(zlo[i], zhi[i]);\n";
+    for (uint32_t r = 3; r < t.n_regs; ++r) {
+        s += "        Iv r" + std::to_string(r) + " = {0.0f, 0.0f, false};\n";
+    }
+    for (const RegClause& c : t.clauses) {
+        if (!iv_supported(c.op)) return std::string();
+        const std::string a = iv_operand(t, c.kinds & 3, c.a);
+        const bool binary = op::arity(c.op) == 2;
+        const std::string b = binary ? iv_operand(t, (c.kinds >> 2) & 3, c.b) : "ia";
+        s += "        { const Iv ia = " + a + "; const Iv ib = " + b + "; r" +
+             std::to_string(c.out) + " = iv_apply(" + std::to_string(c.op) + ", ia, ib); }\n";
+    }
+    const std::string root = iv_operand(t, t.root_kind, t.root);
+    s += "        { const Iv r = " + root + "; olo[i] = r.lo; ohi[i] = r.hi; onan[i] = r.nan; }\n"
+         "    }\n}\n";
+    return s;
+}
+
+bool jit_intervals(GpuTape& g, uint64_t n, const float* xlo, const float* xhi,
+                   const float* ylo, const float* yhi, const float* zlo, const float* zhi,
+                   float* olo, float* ohi, uint8_t* onan, cudaStream_t s)
+{
+    void* fn = kernel(g, 4);
+    if (!fn) return false;
+    if (n == 0) return true;
+    unsigned long long nn = n;
+    const float* cp = g.d_cpool;
+    void* args[] = {&xlo, &xhi, &ylo, &yhi, &zlo, &zhi, &olo, &ohi, &onan, &nn, &cp};
+    return launch(fn, n, args, s);
 }
 
 void jit_release(GpuTape& g)

@@ -12,6 +12,8 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <string>
+#include <vector>
 
 #include "runtime.hpp"
 
@@ -43,6 +45,18 @@ bool jit_partials(GpuTape& g, const uint32_t* slots, uint32_t m, const float* x,
 bool jit_backward(GpuTape& g, const uint32_t* slots, uint32_t m, const float* P,
                   const float* seed, float* gx, float* gy, float* gz, float* gvars,
                   int block_cv, cudaStream_t s);
+
+/// Intervals of the tape over n boxes through its compiled interval kernel
+/// (the interval operations of dev_interval.cuh, written out per clause):
+/// the same bounds and NaN flags as the interval interpreter.
+bool jit_intervals(GpuTape& g, uint64_t n, const float* xlo, const float* xhi,
+                   const float* ylo, const float* yhi, const float* zlo, const float* zhi,
+                   float* olo, float* ohi, uint8_t* onan, cudaStream_t s);
+
+/// Source of the interval kernel (empty when the tape has no compiled form)
+/// and its compilation to a cubin, for checks that need no GPU.
+std::string jit_interval_source(const RegTape& t);
+bool jit_compile(const std::string& src, std::vector<char>* cubin, std::string* log);
 
 /// Releases a tape's compiled kernels (called when the tape is destroyed).
 void jit_release(GpuTape& g);

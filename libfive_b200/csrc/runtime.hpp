@@ -50,14 +50,15 @@ struct GpuTape {
     bool pslot_ready = false;
 
     // Compiled kernels (jit.cpp), [0] values, [1] values + derivatives,
-    // [2] reverse-mode partials, [3] reverse-mode backward pass:
+    // [2] reverse-mode partials, [3] reverse-mode backward pass,
+    // [4] intervals:
     // state 0 not tried, 1 ready, -1 none.
     struct JitKernel {
         int state = 0;
         void* module = nullptr;
         void* function = nullptr;
     };
-    JitKernel jit[4];
+    JitKernel jit[5];
 
     ~GpuTape();
     DevTape dev() const;

@@ -12,16 +12,10 @@
 #include <cmath>
 #include <cstdint>
 
-#ifdef __CUDACC__
-#define LF_HD __host__ __device__ __forceinline__
-#else
-#define LF_HD inline
-#endif
+#include "scalar_minmax.h"
 
 namespace lfb {
 
-LF_HD float sc_min(float a, float b) { return (b < a) ? b : a; }
-LF_HD float sc_max(float a, float b) { return (a < b) ? b : a; }
 LF_HD bool sc_isnan(float a) { return a != a; }
 
 /// Python-style modulo with the reference's clamping rules

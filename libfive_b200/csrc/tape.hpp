@@ -47,8 +47,6 @@ enum : uint8_t {
     OPND_VAR = 2,     // index into the constant pool (a free variable)
 };
 
-// Extra opcode used only inside pruned device tapes: out = a.
-enum : uint8_t { OP_COPY = 40 };
 
 struct RegClause {
     uint8_t op;

@@ -1,7 +1,7 @@
 """Tapes compiled to straight-line kernels (jit.cpp) against the interpreter.
 
-The compiled value and derivative kernels must give the interpreter's bits
-at every point,
+The compiled value, derivative, reverse-mode and interval kernels must give
+the interpreters' bits at every point and box,
 transcendental opcodes included (both call the same CUDA functions with
 contraction off).  The interpreter's values are computed in a child process
 with LFB_JIT=0; lfb_tape_compiled says which path a tape took."""
@@ -41,7 +41,7 @@ def shapes():
 CHILD = r"""
 import sys, numpy as np
 sys.path.insert(0, sys.argv[1]); sys.path.insert(0, sys.argv[1] + "/tests")
-from test_gpu_jit import shapes, points, grad, grad_vars
+from test_gpu_jit import shapes, points, grad, grad_vars, boxes
 from libfive_b200.shape import Tape
 from libfive_b200 import ffi
 name = sys.argv[2]
@@ -53,7 +53,18 @@ d = t.derivs(*points())
 np.save(sys.argv[3], np.stack([out] + list(d)))
 np.save(sys.argv[3] + ".grad.npy", np.stack(grad(t)))
 np.save(sys.argv[3] + ".gvars.npy", grad_vars(t))
+lo, hi, nan = t.intervals(*boxes())
+np.save(sys.argv[3] + ".iv.npy", np.stack([lo, hi, nan.astype(np.float32)]))
 """
+
+
+def boxes():
+    """Boxes of several sizes around random centres, a few degenerate."""
+    r = np.random.default_rng(4)
+    c = r.uniform(-1.5, 1.5, (3, 20000)).astype(np.float32)
+    h = (10.0 ** r.uniform(-4, 0, (1, 20000))).astype(np.float32)
+    h[:, :100] = 0
+    return c - h, c + h
 
 
 def grad(t):
@@ -107,6 +118,12 @@ def test_compiled_matches_interpreter(gpu, name, tmp_path):
     scale = max(1.0, float(np.abs(gw[finite]).max())) if finite.any() else 1.0
     assert np.array_equal(np.isfinite(gv), finite)
     assert np.allclose(gv, gw, rtol=1e-5, atol=1e-5 * scale, equal_nan=True)
+    # intervals: the same bounds and NaN flags
+    lo, hi, nan = t.intervals(*boxes())
+    iv = np.load(path + ".iv.npy")
+    assert np.array_equal(lo.view(np.uint32), iv[0].view(np.uint32))
+    assert np.array_equal(hi.view(np.uint32), iv[1].view(np.uint32))
+    assert np.array_equal(nan, iv[2].astype(bool))
 
 
 def test_variables_change_without_recompiling(gpu):

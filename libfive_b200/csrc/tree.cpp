@@ -462,7 +462,8 @@ std::vector<const Node*> Tree::walk() const
     if (p->flags & Node::HAS_REMAP) {
         return flatten().walk();
     }
-    FlatMap<const Node*, unsigned, PtrHash> count(1024);
+    static std::atomic<size_t> count_hint{1024};   // capacity hint, as in optimized()
+    FlatMap<const Node*, unsigned, PtrHash> count(count_hint.load(std::memory_order_relaxed));
     std::vector<const Node*> todo{p};
     auto nkids = [](const Node* n) {
         return n->kind == Kind::Unary ? 1 : n->kind == Kind::Binary ? 2 : 0;
@@ -489,6 +490,7 @@ std::vector<const Node*> Tree::walk() const
             }
         }
     }
+    count_hint.store(std::max<size_t>(1024, count.size()), std::memory_order_relaxed);
     std::reverse(flat.begin(), flat.end());
     return flat;
 }
@@ -641,7 +643,10 @@ Tree Tree::optimized() const
     // everything below it (the output stack, affine terms, commutative
     // lists) holds plain pointers, which stay valid because each of them
     // is either a node of the input tree or a canonical entry.
-    FlatMap<Key, Tree, KeyHash> canonical(1024);
+    // Sized from the previous call (a capacity hint only: trees built
+    // repeatedly from the same kind of model skip the rehashing).
+    static std::atomic<size_t> canon_hint{1024};
+    FlatMap<Key, Tree, KeyHash> canonical(canon_hint.load(std::memory_order_relaxed));
     auto uniq_new = [&canonical](Tree&& t) -> const Node* {
         const Key k = key_of(t.p);
         return canonical.emplace(k, std::move(t)).first->p;
@@ -929,6 +934,7 @@ Tree Tree::optimized() const
             deliver(self, task.scale);
         }
     }
+    canon_hint.store(std::max<size_t>(1024, canonical.size()), std::memory_order_relaxed);
     return Tree(out.back(), true, true);
 }
 

@@ -502,6 +502,25 @@ def run_eval(args, world, rank, local):
     hf = np.empty(n, np.float32)
     t_e2e = _timed(lambda: tape.values(hx, hy, hz, out=hf), args.steps, args.warmup, flush)
     ce = n * tape.n_clauses
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        # the oracle port (ArrayEvaluator / DerivArrayEvaluator restated,
+        # 256-point batches) on every host core, over the first 2^18 points
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from oracle_ffi import OracleTape
+        ora = OracleTape(shape)
+        m = 1 << 18
+        sub = [np.ascontiguousarray(a[:m]) for a in pts]
+        cores = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        ora.values(*sub, threads=cores)
+        tv = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        ora.derivs(*sub, threads=cores)
+        td = time.perf_counter() - t0
+        cpu = {"value": m * tape.n_clauses / tv, "unit": "clause-evals/s", "cores": cores,
+               "kind": "port", "sample": "first 2^18 lattice points",
+               "deriv_value": m * tape.n_clauses / td}
     sm = torch.cuda.get_device_properties(local).multi_processor_count
     peak = sm * 128 * 1965e6 / 1e9   # G FP32 lane-ops/s at the maximum SM clock
     achieved = ce * wv / (t_val / 1e3) / 1e9
@@ -518,7 +537,7 @@ def run_eval(args, world, rank, local):
             "higher_is_better": True, "deriv_value": ce / (t_der / 1e3), "ms_deriv": t_der,
             "e2e": {"value": ce / (t_e2e / 1e3), "unit": "clause-evals/s",
                     "h2d_bytes_per_step": 12 * n, "d2h_bytes_per_step": 4 * n},
-            "dtype": "f32", "data": "synthetic",
+            "cpu_baseline": cpu, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "64-sphere union, 128^3 lattice", "points": n,
                        "clauses": tape.n_clauses, "l2": "flushed before each step"}}))
 
@@ -563,9 +582,26 @@ def run_adjoint(args, world, rank, local):
     ms_fwd = _timed(lambda: tape.values(x, y, z, out=f, stream=torch.cuda.current_stream().cuda_stream),
                     args.steps, args.warmup, flush)
     comps = n * (3 + tape.n_vars)
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        # the oracle port: JacobianEvaluator::gradient (variables) and
+        # DerivArrayEvaluator (points) on every host core, first 16 points
+        # (each point takes 342 forward passes over the tape for 1024 variables)
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from oracle_ffi import OracleTape
+        ora = OracleTape(shape, vals)
+        m = 16
+        sub = [np.ascontiguousarray(t_.cpu().numpy()[:m]) for t_ in (x, y, z)]
+        cores = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        ora.jacobian(*sub, threads=cores)
+        ora.derivs(*sub, threads=cores)
+        dt = time.perf_counter() - t0
+        cpu = {"value": m * (3 + tape.n_vars) / dt, "unit": "gradient components/s",
+               "cores": cores, "kind": "port", "sample": "first 16 points"}
     if rank == 0:
         print(json.dumps({
-            "metric": "grads/s", "value": comps / (ms / 1e3), "unit": "gradient components/s",
+            "metric": "grads/s", "cpu_baseline": cpu, "value": comps / (ms / 1e3), "unit": "gradient components/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "loss_grads_per_s": 1e3 / ms,
             "ms_forward": ms_fwd, "step_over_forward": ms / ms_fwd, "dtype": "f32",

@@ -49,7 +49,8 @@ def _headers():
 
 # Headers that kernels compiled at run time (csrc/jit.cpp) include; their
 # text is built into the library.
-JIT_HEADERS = ["opcode_ids.h", "scalar_minmax.h", "dev_interval.cuh"]
+JIT_HEADERS = ["opcode_ids.h", "scalar_minmax.h", "scalar_ops.h", "dev_interval.cuh",
+               "dev_point.cuh"]
 
 
 def _jit_headers_source():

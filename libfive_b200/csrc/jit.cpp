@@ -102,12 +102,29 @@ std::string expr(uint8_t o, const std::string& a, const std::string& b)
         case op::ABS: return "fabsf(" + a + ")";
         case op::RECIP: return "__fdiv_rn(1.0f, " + a + ")";
         case op::CONST_VAR: return "(" + a + ")";
-        default: return std::string();
+        default:
+            // the remaining opcodes through the interpreter's own function
+            if (op::arity(o) < 1) return std::string();
+            return "dv_value(" + std::to_string(o) + ", " + a + ", " + b + ")";
     }
 }
 
+/// Common start of every generated source: the point and interval rules of
+/// the interpreters (dev_point.cuh, dev_interval.cuh), included from text
+/// built into the library.
+const char* kPrelude =
+    "typedef unsigned char uint8_t;\ntypedef unsigned short uint16_t;\n"
+    "typedef unsigned int uint32_t;\ntypedef unsigned long long uint64_t;\n"
+    "typedef int int32_t;\ntypedef long long int64_t;\n"
+    "#include \"dev_point.cuh\"\n#include \"dev_interval.cuh\"\nusing namespace lfb;\n";
+
+/// Second operand of a clause: unary clauses get a zero (their rules never
+/// read it).
+uint32_t b_kind(const RegClause& c) { return op::arity(c.op) == 2 ? (c.kinds >> 2) & 3 : 99u; }
+
 std::string operand(const RegTape& t, uint32_t kind, uint32_t idx)
 {
+    if (kind == 99u) return "0.0f";
     if (kind == OPND_REG) return "r" + std::to_string(idx);
     if (kind == OPND_VAR) return "__ldg(cp + " + std::to_string(idx) + ")";
     uint32_t bits;
@@ -138,6 +155,7 @@ std::string values_source(const RegTape& t)
 {
     std::string s;
     s.reserve(64 * t.clauses.size() + 1024);
+    s += kPrelude;
     s += "extern \"C\" __global__ void __launch_bounds__(256)\n"
          "lfb_tape_values(const float* __restrict__ X, const float* __restrict__ Y,\n"
          "                const float* __restrict__ Z, float* __restrict__ out,\n"
@@ -149,7 +167,7 @@ std::string values_source(const RegTape& t)
     }
     for (const RegClause& c : t.clauses) {
         const std::string a = operand(t, c.kinds & 3, c.a);
-        const std::string b = operand(t, (c.kinds >> 2) & 3, c.b);
+        const std::string b = operand(t, b_kind(c), c.b);
         const std::string e = expr(c.op, a, b);
         if (e.empty()) return std::string();
         s += "        r" + std::to_string(c.out) + " = " + e + ";\n";
@@ -163,7 +181,7 @@ std::string values_source(const RegTape& t)
 /// register may also be an operand.  Empty for opcodes without a compiled form.
 std::string deriv_clause(const RegTape& t, const RegClause& c)
 {
-    const uint32_t ka = c.kinds & 3, kb = (c.kinds >> 2) & 3;
+    const uint32_t ka = c.kinds & 3, kb = b_kind(c);
     std::string s = "        {\n            const float a = " + operand(t, ka, c.a) +
                     ", b = " + operand(t, kb, c.b) + ";\n";
     for (int k = 0; k < 3; ++k) {
@@ -244,7 +262,15 @@ std::string deriv_clause(const RegTape& t, const RegClause& c)
             for (int k = 0; k < 3; ++k) d[k] = std::string("a") + "xyz"[k];
             break;
         default:
-            return std::string();
+            // the remaining opcodes through the interpreter's own rules
+            if (op::arity(c.op) < 1) return std::string();
+            pre = "            const D4 dd = dv_deriv_all(" + std::to_string(c.op) +
+                  ", D4{a, ax, ay, az}, D4{b, bx, by, bz}, false);\n";
+            v = "dd.v";
+            d[0] = "dd.dx";
+            d[1] = "dd.dy";
+            d[2] = "dd.dz";
+            break;
     }
     const std::string o = "r" + std::to_string(c.out);
     s += pre;
@@ -259,6 +285,7 @@ std::string derivs_source(const RegTape& t)
 {
     std::string s;
     s.reserve(400 * t.clauses.size() + 2048);
+    s += kPrelude;
     s += "extern \"C\" __global__ void __launch_bounds__(256)\n"
          "lfb_tape_derivs(const float* __restrict__ X, const float* __restrict__ Y,\n"
          "                const float* __restrict__ Z, float* __restrict__ ov,\n"
@@ -335,7 +362,14 @@ bool partial_exprs(uint8_t o, std::string* v, std::string* pa, std::string* pb, 
             *pb = "__fdiv_rn(__fsub_rn(__fmul_rn(0.0f, b), __fmul_rn(1.0f, a)), den)";
             return true;
         default:
-            return false;
+            // the remaining opcodes through the interpreter's own rules
+            if (op::arity(o) < 1) return false;
+            *pre = "const D4 dd = dv_deriv_all(" + std::to_string(o) +
+                   ", D4{a, 1.0f, 0.0f, 0.0f}, D4{b, 0.0f, 1.0f, 0.0f}, false); ";
+            *v = "dd.v";
+            *pa = "dd.dx";
+            *pb = "dd.dy";
+            return true;
     }
 }
 
@@ -345,6 +379,7 @@ std::string partials_source(const RegTape& t, const std::vector<uint32_t>& slots
 {
     std::string s;
     s.reserve(160 * t.clauses.size() + 1024);
+    s += kPrelude;
     s += "extern \"C\" __global__ void __launch_bounds__(256)\n"
          "lfb_tape_partials(const float* __restrict__ X, const float* __restrict__ Y,\n"
          "                  const float* __restrict__ Z, float* __restrict__ P,\n"
@@ -360,7 +395,7 @@ std::string partials_source(const RegTape& t, const std::vector<uint32_t>& slots
         if (!partial_exprs(cl.op, &v, &pa, &pb, &pre)) return std::string();
         const uint32_t kind = slots[c] >> 28, slot = slots[c] & 0x0fffffffu;
         s += "    { const float a = " + operand(t, cl.kinds & 3, cl.a) + ", b = " +
-             operand(t, (cl.kinds >> 2) & 3, cl.b) + "; " + pre;
+             operand(t, b_kind(cl), cl.b) + "; " + pre;
         if (kind != RK_CONST) {
             s += "Pi[(size_t)" + std::to_string(slot) + " * m] = " + pa + "; ";
             if (kind == RK_TWO) s += "Pi[(size_t)" + std::to_string(slot + 1) + " * m] = " + pb + "; ";
@@ -463,11 +498,10 @@ std::string iv_operand(const RegTape& t, uint32_t kind, uint32_t idx)
     return "iv_make(" + v + ", " + v + ")";
 }
 
-/// Opcodes the interval kernel compiles (the value kernel's set); the rest
-/// stay on the interpreter.
+/// Opcodes the interval kernel compiles: every unary and binary one.
 bool iv_supported(uint8_t o)
 {
-    return !expr(o, "a", "b").empty();
+    return op::arity(o) >= 1;
 }
 
 /// Compiles `src` and loads its kernel `name` into slot k; false when
@@ -628,10 +662,8 @@ std::string jit_interval_source(const RegTape& t)
 {
     std::string s;
     s.reserve(96 * t.clauses.size() + 1024);
-    s += "typedef unsigned char uint8_t;\ntypedef unsigned short uint16_t;\n"
-         "typedef unsigned int uint32_t;\ntypedef unsigned long long uint64_t;\n"
-         "#include \"dev_interval.cuh\"\nusing namespace lfb;\n"
-         "extern \"C\" __global__ void __launch_bounds__(256)\n"
+    s += kPrelude;
+    s += "extern \"C\" __global__ void __launch_bounds__(256)\n"
          "lfb_tape_intervals(const float* __restrict__ xlo, const float* __restrict__ xhi,\n"
          "                   const float* __restrict__ ylo, const float* __restrict__ yhi,\n"
          "                   const float* __restrict__ zlo, const float* __restrict__ zhi,\n"

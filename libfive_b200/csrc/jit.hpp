@@ -5,9 +5,10 @@
 // is evaluated over many points, compiling it once into a kernel whose body
 // is the clause list itself (each clause one or two instructions, operands
 // in hardware registers) removes that overhead.  The generated code uses
-// the same separately rounded operations as the interpreter (dv_value), so
-// both give identical bits; tapes with opcodes outside the compiled set, or
-// longer than kJitMaxClauses, stay on the interpreter.
+// the same separately rounded operations as the interpreters (written out
+// for the common opcodes, the interpreters' own functions from
+// dev_point.cuh / dev_interval.cuh for the rest), so both give identical
+// bits; tapes longer than kJitMaxClauses stay on the interpreters.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -23,9 +24,8 @@ constexpr uint32_t kJitMaxClauses = 4096;
 
 /// Values of the tape at n points through its compiled kernel (compiled on
 /// first use).  Returns false, with no error set, when the tape has no
-/// compiled kernel (unsupported opcode, too long, NVRTC or the driver
-/// unavailable, or LFB_JIT=0 in the environment); the caller then uses the
-/// interpreter.
+/// compiled kernel (too long, NVRTC or the driver unavailable, or LFB_JIT=0
+/// in the environment); the caller then uses the interpreter.
 bool jit_values(GpuTape& g, uint64_t n, const float* x, const float* y, const float* z,
                 float* out, cudaStream_t s);
 

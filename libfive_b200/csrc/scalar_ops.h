@@ -9,8 +9,15 @@
 // an explicit, separately rounded IEEE operation; the translation units that
 // include this header are compiled without FMA contraction.
 #pragma once
+#ifdef __CUDACC_RTC__
+// kernels compiled at run time: math functions are built in
+#ifndef NAN
+#define NAN __int_as_float(0x7fc00000)
+#endif
+#else
 #include <cmath>
 #include <cstdint>
+#endif
 
 #include "scalar_minmax.h"
 

@@ -35,6 +35,11 @@ def shapes():
     recip = Shape.new("recip", (z * v).abs())
     misc = ((x / (y.square() + 0.5)) - recip).max(-(x.with_constant_vars() * 0.25))
     out["misc"] = (misc, {v: 1.75})
+    # opcodes compiled through the interpreters' own rules (dev_point.cuh)
+    trig = ((x.sin() * y.cos() + (z * 0.3).tan() - y.atan2(x) + (x * 0.5).asin()
+             + (y * 0.5).acos() + z.atan() + x ** 3 + y.nth_root(3) + z % 0.7
+             + x.sqrt().nanfill(y) + x.compare(y)) - 0.5)
+    out["trig"] = (trig, None)
     return out
 
 
@@ -93,7 +98,7 @@ def points():
     return (np.concatenate([x, lx]), np.concatenate([y, ly]), np.concatenate([z, lz]))
 
 
-@pytest.mark.parametrize("name", ["spheres", "csg", "blend_vars", "misc"])
+@pytest.mark.parametrize("name", ["spheres", "csg", "blend_vars", "misc", "trig"])
 def test_compiled_matches_interpreter(gpu, name, tmp_path):
     s, vals = shapes()[name]
     t = Tape(s, vals)
@@ -139,7 +144,8 @@ def test_variables_change_without_recompiling(gpu):
     assert np.array_equal(b.view(np.uint32), t2.values(*p).view(np.uint32))
 
 
-def test_unsupported_opcode_stays_interpreted(gpu):
-    t = Tape(X().sin() + Y())
+def test_long_tape_stays_interpreted(gpu):
+    # more clauses than the compiled kernels take (4096)
+    t = Tape(workloads.spheres_union(500, seed=2))
     t.values(*points())
     assert ffi.load().lfb_tape_compiled(t.ptr) == 0

@@ -19,6 +19,7 @@ import argparse
 import concurrent.futures
 import ctypes
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -67,12 +68,17 @@ def parse():
                    help="octree depth; 10 is the benchmark workload, smaller "
                         "depths are for profiling captures")
     p.add_argument("--workload", default="csg2000",
-                   choices=["csg2000", "batch", "eval", "adjoint", "heightmap"],
+                   choices=["csg2000", "batch", "eval", "adjoint", "heightmap", "fit"],
                    help="batch: many trees of mixed size and depth, meshed "
                         "one after another and through lfb_render_meshes")
     p.add_argument("--trees", type=int, default=512, help="batch workload: tree count")
     p.add_argument("--workers", type=int, default=4,
                    help="batch workload: meshes in flight at once")
+    p.add_argument("--shapes", type=int, default=64, help="fit workload: shapes")
+    p.add_argument("--fit-points", type=int, default=1 << 18,
+                   help="fit workload: surface points per shape")
+    p.add_argument("--no-remesh", action="store_true",
+                   help="fit workload: skip timing the remesh")
     p.add_argument("--points", type=int, default=1 << 22,
                    help="adjoint workload: points (smaller for profiling captures)")
     return p.parse_args()
@@ -610,6 +616,103 @@ def run_adjoint(args, world, rank, local):
                        "points": n, "vars": tape.n_vars, "clauses": tape.n_clauses}}))
 
 
+def run_fit(args, world, rank, local):
+    """Batched inverse fitting: `--shapes` (64) shapes, each a CSG of 128
+    primitives with 7 free variables each (896; workloads.fit_csg_vars, seed
+    21 + 1000 rank + 7 j), fitted to 2^18 points sampled from the surface of
+    a copy whose variables are perturbed by N(0, 0.05) (meshed at 128 voxels
+    per unit).  One step = one Adam step of every shape (lfb_fit_adam_step:
+    reverse-mode gradients of mean f^2, losses, update), points resident on
+    the device.  The DC remesh of all shapes at 128 voxels per unit, done
+    every 50 steps of the 500-step fit, is timed on its own (one
+    lfb_render_meshes call) and folded into the job estimate."""
+    import numpy as np
+    import torch
+    from libfive_b200 import shape as shape_mod
+    from libfive_b200 import workloads
+    from libfive_b200.fit import BatchedFit
+    from libfive_b200.shape import Tape
+    torch.cuda.set_device(local)
+    n_shapes, n_pts = args.shapes, args.fit_points
+    lo, hi = REGION
+    t0 = time.perf_counter()
+    shapes, vals, targets = [], [], []
+    for j in range(n_shapes):
+        seed = 21 + 1000 * rank + 7 * j
+        sh, v, _ = workloads.fit_csg_vars(128, seed=seed)
+        shapes.append(sh)
+        vals.append(v)
+        targets.append(Tape(sh, workloads.perturbed(v, 0.05, seed=seed + 1)))
+    meshes = shape_mod.render_meshes([(t, lo, hi, 1.0 / 128) for t in targets], workers=4)
+    pts = []
+    for j, (v, t) in enumerate(meshes):
+        if len(t) == 0:
+            raise RuntimeError("target %d has no surface" % j)
+        seed = 21 + 1000 * rank + 7 * j
+        pts.append(tuple(torch.from_numpy(a).cuda()
+                         for a in workloads.surface_points(v, t, n_pts, seed=seed + 2)))
+    del targets, meshes
+    tapes = [Tape(sh, v) for sh, v in zip(shapes, vals)]
+    setup_s = time.perf_counter() - t0
+    fit = BatchedFit(tapes, pts, lr=1e-3)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    first = fit.step().clone()
+    torch.cuda.synchronize()
+    first_s = time.perf_counter() - t0        # includes compiling the tapes' kernels
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    ms = _timed(fit.step, args.steps, args.warmup, flush)
+    last = fit.losses.clone()
+    torch.cuda.synchronize()
+    remesh_s = None
+    if not args.no_remesh:
+        jobs = [(t, lo, hi, 1.0 / 128) for t in tapes]
+        shape_mod.render_meshes(jobs, workers=4)   # warm
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        shape_mod.render_meshes(jobs, workers=4)
+        torch.cuda.synchronize()
+        remesh_s = time.perf_counter() - t0
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        # the oracle port: JacobianEvaluator::gradient (forward mode, one
+        # tape pass per three variables) on every host core, first 16 points
+        # of shape 0, extrapolated to one step's gradients of all shapes
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from oracle_ffi import OracleTape
+        ora = OracleTape(shapes[0], vals[0])
+        m = 16
+        sub = [np.ascontiguousarray(a.cpu().numpy()[:m]) for a in pts[0]]
+        cores = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        ora.jacobian(*sub, threads=cores)
+        ora.values(*sub, threads=cores)
+        dt = time.perf_counter() - t0
+        cpu = {"value": m / dt / fit.n_points, "unit": "Adam steps/s", "cores": cores,
+               "kind": "port", "sample": "16 points of shape 0 (values + 896-variable "
+                                         "gradients), extrapolated to %d points" % fit.n_points}
+    n_total = fit.n_points * world
+    step_s = ms / 1e3
+    job_s = 500 * step_s + (10 * remesh_s if remesh_s is not None else 0.0)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "Adam steps/s (64 shapes x 2^18 points, 896 variables each)",
+            "value": 1.0 / step_s, "unit": "Adam steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak",
+            "grads_per_s": n_total * tapes[0].n_vars / step_s,
+            "ms_remesh_all": remesh_s * 1e3 if remesh_s is not None else None,
+            "job_500_steps_s": job_s, "first_step_s": first_s, "setup_s": setup_s,
+            "loss_mean_first": float(first.mean()), "loss_mean_last": float(last.mean()),
+            "finite": bool(torch.isfinite(last).all()),
+            "cpu_baseline": cpu, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "%d CSG shapes x 128 primitives (7 vars each), "
+                                   "2^%d surface points each, Adam lr 1e-3"
+                                   % (n_shapes, int(round(math.log2(n_pts)))),
+                       "clauses": tapes[0].n_clauses, "vars_per_shape": tapes[0].n_vars,
+                       "points": fit.n_points, "l2": "flushed before each step"}}))
+
+
 def run_heightmap(args, world, rank, local):
     """Height maps: the 64-sphere union (seed 1 + rank) over [-1.5,1.5]^3 at
     512 / 3 voxels per unit (512^3 voxels: a 512 x 512 image with 512 z
@@ -663,6 +766,8 @@ def main():
         run_adjoint(args, world, rank, local)
     elif args.workload == "heightmap":
         run_heightmap(args, world, rank, local)
+    elif args.workload == "fit":
+        run_fit(args, world, rank, local)
     elif args.impl == "reference":
         run_reference(args, world, rank)
     else:

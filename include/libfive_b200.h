@@ -105,6 +105,44 @@ int lfb_eval_grad(lfb_tape t, uint64_t n, const float* x, const float* y,
                   float* gy, float* gz, float* gvars, void* stream,
                   uint32_t flags);
 
+/*  Current values of the tape's free variables (lfb_tape_var_ids order) in
+ *  a host array of len floats; after lfb_fit_adam_step this waits for the
+ *  device and reads the values it wrote.  Counterpart of reading
+ *  Evaluator's variable map (evaluator.hpp:35-44). */
+int lfb_tape_get_vars(lfb_tape t, float* values, uint32_t len);
+
+/*  Adam hyper-parameters (Kingma & Ba, 2015). */
+typedef struct lfb_adam_settings {
+    float lr;     /* step size */
+    float beta1;  /* first-moment decay, e.g. 0.9 */
+    float beta2;  /* second-moment decay, e.g. 0.999 */
+    float eps;    /* added to the root of the second moment, e.g. 1e-8 */
+} lfb_adam_settings;
+
+/*  Batched least-squares fitting (new; the reference has no optimiser).
+ *  One Adam step on every shape j of loss_j = mean_i f_j(p_i)^2 over its
+ *  points p_i = (x, y, z)[point_offsets[j] .. point_offsets[j + 1]), with
+ *  respect to the free variables of tapes[j]:
+ *    g   = (2 / n_j) * sum_i f_j(p_i) df_j(p_i)/dvar   (reverse mode, as
+ *          lfb_eval_grad with seed f)
+ *    m   = m + (1 - beta1) (g - m);   v = beta2 v + (1 - beta2) g g
+ *    var = var - lr / (1 - beta1^step) * m / (sqrt(v) / sqrt(1 - beta2^step) + eps)
+ *  The new values are written into the tapes' variables on the device
+ *  (later evaluations and meshes use them; lfb_tape_get_vars reads them).
+ *  x, y, z, m, v and losses are device arrays; point_offsets and
+ *  var_offsets are host arrays of n_shapes + 1 entries, and
+ *  var_offsets[j + 1] - var_offsets[j] must equal tapes[j]'s variable
+ *  count (m and v hold each shape's moments there; zero them before
+ *  step 1).  losses[j] receives loss_j at the values before the step.
+ *  step counts from 1.  Work is ordered on `stream`; calls on different
+ *  streams must not overlap, since they share scratch buffers. */
+int lfb_fit_adam_step(const lfb_tape* tapes, uint32_t n_shapes,
+                      const uint64_t* point_offsets, const float* x,
+                      const float* y, const float* z,
+                      const uint64_t* var_offsets, float* m, float* v,
+                      lfb_adam_settings adam, uint32_t step, float* losses,
+                      void* stream);
+
 /*  Mesh settings (BRepSettings, settings.hpp:27-74, minus the CPU-thread
  *  fields).  min_feature: subdivide until cells are smaller; max_err: QEF
  *  error below which cells collapse (negative disables collapsing). */

@@ -501,9 +501,42 @@ int lfb_tape_set_vars(lfb_tape t, libfive_vars vars)
 {
     if (!t) return set_error(LFB_E_INVALID, "null tape");
     std::lock_guard<std::mutex> lock(t->g->mu);
+    // variables that fit steps changed on the device keep their new values
+    if (!t->g->pull_vars()) return LFB_E_CUDA;
     const bool changed = t->g->set_vars(vars.vars, vars.values, vars.size);
     if (!t->g->upload_cpool()) return LFB_E_CUDA;
     return changed ? 1 : 0;
+}
+
+int lfb_tape_get_vars(lfb_tape t, float* values, uint32_t len)
+{
+    clear_error();
+    if (!t || (!values && len)) return set_error(LFB_E_INVALID, "null argument");
+    std::lock_guard<std::mutex> lock(t->g->mu);
+    if (!t->g->pull_vars()) return LFB_E_CUDA;
+    const auto& r = t->g->reg;
+    for (uint32_t i = 0; i < r.n_vars && i < len; ++i) {
+        values[i] = r.cpool[r.n_const + i];
+    }
+    return 0;
+}
+
+int lfb_fit_adam_step(const lfb_tape* tapes, uint32_t n_shapes,
+                      const uint64_t* point_offsets, const float* x,
+                      const float* y, const float* z,
+                      const uint64_t* var_offsets, float* m, float* v,
+                      lfb_adam_settings adam, uint32_t step, float* losses,
+                      void* stream)
+{
+    clear_error();
+    if (!tapes) return set_error(LFB_E_INVALID, "null tape list");
+    std::vector<GpuTape*> gs(n_shapes);
+    for (uint32_t j = 0; j < n_shapes; ++j) {
+        if (!tapes[j]) return set_error(LFB_E_INVALID, "null tape");
+        gs[j] = tapes[j]->g.get();
+    }
+    return fit_adam_step(gs.data(), n_shapes, point_offsets, x, y, z, var_offsets, m, v,
+                         adam, step, losses, static_cast<cudaStream_t>(stream));
 }
 
 int lfb_tape_compiled(lfb_tape t)

@@ -4,6 +4,7 @@
 
 #include <cstdint>
 
+#include "libfive_b200.h"
 #include "runtime.hpp"
 
 namespace lfb {
@@ -37,5 +38,18 @@ int eval_grad(GpuTape& g, uint64_t n, const float* x, const float* y,
               const float* z, const float* seed, float* f, float* gx,
               float* gy, float* gz, float* gvars, cudaStream_t s,
               bool device);
+
+/// Builds what the reverse mode needs for this tape (partial-slot table,
+/// compiled partials and backward kernels) without launching anything, so
+/// that many tapes can be prepared on several host threads at once.
+bool grad_prepare(GpuTape& g);
+/// True once grad_prepare (or a gradient call) has run for the tape.
+bool grad_prepared(GpuTape& g);
+
+/// lfb_fit_adam_step (fit.cu); every pointer as documented there.
+int fit_adam_step(GpuTape* const* tapes, uint32_t n_shapes, const uint64_t* point_offsets,
+                  const float* x, const float* y, const float* z, const uint64_t* var_offsets,
+                  float* m, float* v, const lfb_adam_settings& adam, uint32_t step,
+                  float* losses, cudaStream_t s);
 
 }  // namespace lfb

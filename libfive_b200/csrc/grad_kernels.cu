@@ -563,6 +563,22 @@ int eval_jacobian(GpuTape& g, uint64_t n, const float* x, const float* y, const 
     return cuda_ok(cudaStreamSynchronize(s0), "sync") ? 0 : LFB_E_CUDA;
 }
 
+bool grad_prepare(GpuTape& g)
+{
+    if (!ensure_pslots(g)) return false;
+    // m = 0: compile (or find that the tape has no compiled form), no launch
+    const uint32_t* hs = g.h_pslot.data();
+    jit_partials(g, hs, 0, nullptr, nullptr, nullptr, nullptr, nullptr, 0);
+    jit_backward(g, hs, 0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0);
+    return true;
+}
+
+bool grad_prepared(GpuTape& g)
+{
+    std::lock_guard<std::mutex> lock(g.mu);
+    return g.pslot_ready && g.jit[2].state != 0 && g.jit[3].state != 0;
+}
+
 int eval_grad(GpuTape& g, uint64_t n, const float* x, const float* y, const float* z,
               const float* seed, float* f, float* gx, float* gy, float* gz, float* gvars,
               cudaStream_t s, bool device)

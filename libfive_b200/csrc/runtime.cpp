@@ -144,6 +144,20 @@ bool GpuTape::upload_cpool()
                    "upload constants");
 }
 
+bool GpuTape::pull_vars()
+{
+    if (!vars_on_device) return true;
+    if (reg.n_vars &&
+        (!cuda_ok(cudaDeviceSynchronize(), "variable download") ||
+         !cuda_ok(cudaMemcpy(reg.cpool.data() + reg.n_const, d_cpool + reg.n_const,
+                             reg.n_vars * sizeof(float), cudaMemcpyDeviceToHost),
+                  "variable download"))) {
+        return false;
+    }
+    vars_on_device = false;
+    return true;
+}
+
 bool GpuTape::set_vars(const void* const* ids, const float* values,
                        uint32_t n)
 {

@@ -60,11 +60,18 @@ struct GpuTape {
     };
     JitKernel jit[5];
 
+    // Set when a kernel (the fit step, fit.cu) has written the variable
+    // slots of d_cpool, so that the host copy in reg.cpool is out of date.
+    bool vars_on_device = false;
+
     ~GpuTape();
     DevTape dev() const;
     /// Sets variable values by tree id; returns true if any value changed.
     bool set_vars(const void* const* ids, const float* values, uint32_t n);
     bool upload_cpool();
+    /// Copies the device's variable values into reg.cpool when a kernel has
+    /// changed them (waits for the device).  Call with `mu` held.
+    bool pull_vars();
 };
 
 std::shared_ptr<GpuTape> make_tape(const Tree& t);

@@ -53,6 +53,11 @@ class Vars(ctypes.Structure):
                 ("size", ctypes.c_uint32)]
 
 
+class AdamSettings(ctypes.Structure):
+    _fields_ = [("lr", ctypes.c_float), ("beta1", ctypes.c_float),
+                ("beta2", ctypes.c_float), ("eps", ctypes.c_float)]
+
+
 class MeshSettings(ctypes.Structure):
     _fields_ = [("min_feature", ctypes.c_double), ("max_err", ctypes.c_double)]
 
@@ -143,6 +148,11 @@ SIGNATURES = [
     ("lfb_eval_intervals", ctypes.c_int, [tape_t, ctypes.c_uint64, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_uint32]),
     ("lfb_eval_jacobian", ctypes.c_int, [tape_t, ctypes.c_uint64, vp, vp, vp, vp, vp, ctypes.c_uint32]),
     ("lfb_eval_grad", ctypes.c_int, [tape_t, ctypes.c_uint64, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_uint32]),
+    ("lfb_tape_get_vars", ctypes.c_int, [tape_t, fp, ctypes.c_uint32]),
+    ("lfb_fit_adam_step", ctypes.c_int, [ctypes.POINTER(tape_t), ctypes.c_uint32,
+                                         ctypes.POINTER(ctypes.c_uint64), vp, vp, vp,
+                                         ctypes.POINTER(ctypes.c_uint64), vp, vp, AdamSettings,
+                                         ctypes.c_uint32, vp, vp]),
     ("lfb_render_mesh", ctypes.POINTER(Mesh), [tape_t, Region3, MeshSettings, ctypes.POINTER(MeshStats)]),
     ("lfb_render_heightmap", ctypes.c_int, [tape_t, fp, fp, fp, u32p, fp, u32p]),
     ("lfb_render_meshes", ctypes.c_int, [ctypes.POINTER(tape_t), ctypes.c_uint32,

@@ -225,6 +225,15 @@ class Tape:
         ffi.check(_lib().lfb_tape_var_ids(self.ptr, arr, self.n_vars))
         return [arr[i] for i in range(self.n_vars)]
 
+    def get_vars(self):
+        """Current variable values in var_ids() order (after fit steps on
+        the device, the values they wrote)."""
+        out = np.zeros(max(1, self.n_vars), np.float32)
+        ffi.check(_lib().lfb_tape_get_vars(
+            self.ptr, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), self.n_vars),
+            "get_vars")
+        return out[:self.n_vars]
+
     def _flags(self, arrays):
         devs = {_ptr(a)[1] for a in arrays if a is not None}
         if len(devs) != 1:

@@ -72,6 +72,18 @@ def blend(a, b, m=0.05):
     return -((ea + eb).log()) / k
 
 
+def blend_stable(a, b, m=0.05):
+    """The same smooth union as `blend`, -log(exp(-k a) + exp(-k b)) / k
+    with k = 2.75 / m^2, written as min(a, b) - log(1 + exp(-k |a - b|)) / k:
+    equal in exact arithmetic, but its exp never overflows, while `blend`'s
+    exp(-k a) overflows float32 once a < -88 / k (-0.08 for m = 0.05) and
+    its value becomes -inf (or +inf when both terms underflow)."""
+    mt = Shape.constant(m)
+    k = Shape.constant(2.75) / (mt ** Shape.constant(2))
+    e = ((-k) * (a - b).abs()).exp()
+    return a.min(b) - (e + 1.0).log() / k
+
+
 def spheres_union(n=64, seed=1):
     """Union (min) of n spheres, centres U[-1,1]^3, radii U[0.1,0.35]."""
     rng = SplitMix64(seed)
@@ -161,6 +173,91 @@ def blended_spheres_vars(n=256, seed=4, m=0.05):
             nxt.append(level[-1])
         level = nxt
     return level[0], values
+
+
+def fit_csg_vars(n_prims=128, seed=21, m=0.05, size=(0.1, 0.35)):
+    """CSG of n primitives with 7 free variables each (the fitting
+    workload): spheres sqrt((ax (x-cx))^2 + (ay (y-cy))^2 + (az (z-cz))^2) - r,
+    boxes max(|x-cx| - sx, |y-cy| - sy, |z-cz| - sz) - d and z-cylinders
+    max(sqrt((ax (x-cx))^2 + (ay (y-cy))^2) - r, |z-cz| - h), in rotation,
+    centres U[-1,1]^3, sizes U[size], axis scales 1, box offsets 0; combined
+    by a random binary tree with the CSG_WEIGHTS operators (smooth unions of
+    radius m, in the overflow-free form of blend_stable, so that f and its
+    gradient stay finite everywhere).  Returns (shape, {var: value}, [vars
+    in creation order])."""
+    rng = SplitMix64(seed)
+    x, y, z = X(), Y(), Z()
+    values, order, prims = {}, [], []
+
+    def var(v):
+        s = Shape.var()
+        values[s] = v
+        order.append(s)
+        return s
+
+    for i in range(n_prims):
+        cx, cy, cz = (var(rng.uniform(-1, 1)) for _ in range(3))
+        kind = i % 3
+        if kind == 0:
+            r = var(rng.uniform(*size))
+            ax, ay, az = var(1.0), var(1.0), var(1.0)
+            prims.append(((ax * (x - cx)).square() + (ay * (y - cy)).square()
+                          + (az * (z - cz)).square()).sqrt() - r)
+        elif kind == 1:
+            sx, sy, sz = (var(rng.uniform(*size)) for _ in range(3))
+            d = var(0.0)
+            prims.append(((x - cx).abs() - sx).max(((y - cy).abs() - sy).max(
+                (z - cz).abs() - sz)) - d)
+        else:
+            r, h = var(rng.uniform(*size)), var(rng.uniform(*size))
+            ax, ay = var(1.0), var(1.0)
+            radial = ((ax * (x - cx)).square() + (ay * (y - cy)).square()).sqrt() - r
+            prims.append(radial.max((z - cz).abs() - h))
+    level = prims
+    while len(level) > 1:
+        nxt = []
+        for i in range(0, len(level) - 1, 2):
+            u = rng.uniform()
+            a, b = level[i], level[i + 1]
+            w = CSG_WEIGHTS
+            if u < w[0]:
+                nxt.append(union(a, b))
+            elif u < w[0] + w[1]:
+                nxt.append(blend_stable(a, b, m))
+            elif u < w[0] + w[1] + w[2]:
+                nxt.append(difference(a, b))
+            else:
+                nxt.append(intersection(a, b))
+        if len(level) % 2:
+            nxt.append(level[-1])
+        level = nxt
+    return level[0], values, order
+
+
+def perturbed(values, sigma=0.05, seed=0):
+    """The variable values plus N(0, sigma) noise (Box-Muller over SplitMix64
+    uniforms), in the dict's order."""
+    rng = SplitMix64(seed)
+    out = {}
+    for k, v in values.items():
+        u1 = max(rng.uniform(), 1e-300)
+        u2 = rng.uniform()
+        out[k] = v + sigma * math.sqrt(-2.0 * math.log(u1)) * math.cos(2.0 * math.pi * u2)
+    return out
+
+
+def surface_points(verts, tris, n, seed=7):
+    """n points sampled area-uniformly from a triangle mesh, as float32
+    x, y, z arrays."""
+    tri = verts[tris.astype(np.int64)].astype(np.float64)
+    area = 0.5 * np.linalg.norm(np.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0]), axis=1)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    k = rng.choice(len(tri), size=n, p=area / area.sum())
+    u, w = rng.random(n), rng.random(n)
+    flip = u + w > 1
+    u[flip], w[flip] = 1 - u[flip], 1 - w[flip]
+    p = tri[k, 0] + u[:, None] * (tri[k, 1] - tri[k, 0]) + w[:, None] * (tri[k, 2] - tri[k, 0])
+    return tuple(np.ascontiguousarray(p[:, a], np.float32) for a in range(3))
 
 
 def lattice(n=128, lo=-1.5, hi=1.5):

@@ -636,22 +636,28 @@ def run_fit(args, world, rank, local):
     n_shapes, n_pts = args.shapes, args.fit_points
     lo, hi = REGION
     t0 = time.perf_counter()
-    shapes, vals, targets = [], [], []
-    for j in range(n_shapes):
-        seed = 21 + 1000 * rank + 7 * j
-        sh, v, _ = workloads.fit_csg_vars(128, seed=seed)
-        shapes.append(sh)
-        vals.append(v)
-        targets.append(Tape(sh, workloads.perturbed(v, 0.05, seed=seed + 1)))
-    meshes = shape_mod.render_meshes([(t, lo, hi, 1.0 / 128) for t in targets], workers=4)
-    pts = []
-    for j, (v, t) in enumerate(meshes):
-        if len(t) == 0:
-            raise RuntimeError("target %d has no surface" % j)
-        seed = 21 + 1000 * rank + 7 * j
-        pts.append(tuple(torch.from_numpy(a).cuda()
-                         for a in workloads.surface_points(v, t, n_pts, seed=seed + 2)))
-    del targets, meshes
+    # seeds 21 + 1000 rank, +7, +14, ...; a seed whose perturbed copy meshes
+    # to nothing (a random intersection at the top can leave no solid) is
+    # skipped
+    shapes, vals, pts, seeds = [], [], [], []
+    seed, skipped = 21 + 1000 * rank, 0
+    while len(shapes) < n_shapes:
+        cand = []
+        for _ in range(n_shapes - len(shapes)):
+            sh, v, _ = workloads.fit_csg_vars(128, seed=seed)
+            cand.append((seed, sh, v, Tape(sh, workloads.perturbed(v, 0.05, seed=seed + 1))))
+            seed += 7
+        meshes = shape_mod.render_meshes([(c[3], lo, hi, 1.0 / 128) for c in cand], workers=4)
+        for (sd, sh, v, _), (mv, mt) in zip(cand, meshes):
+            if len(mt) == 0:
+                skipped += 1
+                continue
+            shapes.append(sh)
+            vals.append(v)
+            seeds.append(sd)
+            pts.append(tuple(torch.from_numpy(a).cuda()
+                             for a in workloads.surface_points(mv, mt, n_pts, seed=sd + 2)))
+        del cand, meshes
     tapes = [Tape(sh, v) for sh, v in zip(shapes, vals)]
     setup_s = time.perf_counter() - t0
     fit = BatchedFit(tapes, pts, lr=1e-3)
@@ -710,7 +716,8 @@ def run_fit(args, world, rank, local):
                                    "2^%d surface points each, Adam lr 1e-3"
                                    % (n_shapes, int(round(math.log2(n_pts)))),
                        "clauses": tapes[0].n_clauses, "vars_per_shape": tapes[0].n_vars,
-                       "points": fit.n_points, "l2": "flushed before each step"}}))
+                       "points": fit.n_points, "seeds_skipped_empty": skipped,
+                       "l2": "flushed before each step"}}))
 
 
 def run_heightmap(args, world, rank, local):

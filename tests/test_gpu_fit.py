@@ -15,6 +15,7 @@ from adam_ref import adam_step
 from libfive_b200 import ffi, workloads
 from libfive_b200.fit import BatchedFit
 from libfive_b200.shape import Tape
+from mesh_compare import same_mesh
 
 pytestmark = pytest.mark.gpu
 
@@ -96,9 +97,10 @@ def test_fitted_values_reach_evaluation_and_meshing(gpu, problems):
     for t, (shape, _, pts) in zip(tapes, problems):
         fresh = Tape(shape, dict(zip(t.var_ids(), t.get_vars().tolist())))
         assert np.array_equal(t.values(*pts), fresh.values(*pts))
+        # vertex numbering varies from run to run: compare triangle sets
         va, ta = t.render_mesh(*REGION, 1.0 / 16)
         vb, tb = fresh.render_mesh(*REGION, 1.0 / 16)
-        assert np.array_equal(va, vb) and np.array_equal(ta, tb)
+        assert len(ta) > 0 and len(va) == len(vb) and same_mesh(va, ta, vb, tb)
 
 
 def test_set_vars_after_fit_keeps_fitted_values(gpu, problems):

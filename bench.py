@@ -68,7 +68,8 @@ def parse():
                    help="octree depth; 10 is the benchmark workload, smaller "
                         "depths are for profiling captures")
     p.add_argument("--workload", default="csg2000",
-                   choices=["csg2000", "batch", "eval", "adjoint", "heightmap", "fit"],
+                   choices=["csg2000", "batch", "eval", "adjoint", "heightmap", "fit",
+                            "spheres64"],
                    help="batch: many trees of mixed size and depth, meshed "
                         "one after another and through lfb_render_meshes")
     p.add_argument("--trees", type=int, default=512, help="batch workload: tree count")
@@ -720,6 +721,67 @@ def run_fit(args, world, rank, local):
                        "l2": "flushed before each step"}}))
 
 
+def run_spheres_mesh(args, world, rank, local):
+    """The plain configuration's meshes: the union of 64 spheres (centres
+    U[-1,1]^3, radii U[0.1,0.35], seed 1 + rank) over [-1.5,1.5]^3, meshed
+    at 64 voxels per unit (min_feature 1/64: octree depth 8) and at
+    min_feature 0.1 (depth 5), max_err 1e-8.  Device time per mesh with the
+    tape resident (mesh downloaded to the host), e2e from the host tree
+    (flatten + upload + mesh + download), the oracle mesher on the whole
+    region on every host core, and whether the two meshes have the same
+    triangle set."""
+    import torch
+    from libfive_b200 import workloads
+    from libfive_b200.shape import Tape
+    torch.cuda.set_device(local)
+    shape = workloads.spheres_union(64, seed=1 + rank)
+    tape = Tape(shape)
+    lo, hi = REGION
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from mesh_compare import oracle_mesh, same_mesh
+    from oracle_ffi import OracleTape
+    ora = OracleTape(shape)
+    cores = os.cpu_count() or 1
+    lines = {}
+    for name, mf in (("res64", 1.0 / 64), ("min_feature_0.1", 0.1)):
+        holder = {}
+
+        def once(t=None):
+            v, tr, st = (t or tape).render_mesh(lo, hi, mf, MAX_ERR, stats=True)
+            holder["mesh"], holder["stats"] = (v, tr), st
+
+        ms = _timed(once, args.steps, args.warmup, flush)
+        ms_e2e = _timed(lambda: once(Tape(shape)), args.steps, args.warmup, flush)
+        v, tr = holder["mesh"]
+        st = holder["stats"]
+        entry = {"ms_per_mesh": ms, "meshes_per_s": 1e3 / ms, "e2e_meshes_per_s": 1e3 / ms_e2e,
+                 "octree_depth": st.levels, "triangles": int(len(tr)),
+                 "stages_ms": {"interval": st.ms_interval, "leaf": st.ms_leaf,
+                               "collapse": st.ms_collapse, "dual": st.ms_dual}}
+        if rank == 0 and not args.no_cpu_baseline:
+            t0 = time.perf_counter()
+            ov, ot = oracle_mesh(ora, lo, hi, mf, MAX_ERR, threads=cores)
+            dt = time.perf_counter() - t0
+            entry["cpu_baseline"] = {"value": 1.0 / dt, "unit": "meshes/s", "cores": cores,
+                                     "kind": "port", "sample": "the whole mesh"}
+            entry["same_triangles_as_oracle"] = bool(len(ov) == len(v) and
+                                                     same_mesh(v, tr, ov, ot))
+        lines[name] = entry
+    if rank == 0:
+        main_ = lines["res64"]
+        print(json.dumps({
+            "metric": "DC meshes/s", "value": main_["meshes_per_s"], "unit": "meshes/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": main_["ms_per_mesh"], "higher_is_better": True, "scaling": "weak",
+            "dtype": "f32", "data": "synthetic",
+            "e2e": {"value": main_["e2e_meshes_per_s"], "unit": "meshes/s"},
+            "cpu_baseline": main_.get("cpu_baseline"), "resolutions": lines,
+            "config": {"workload": "64-sphere union, [-1.5,1.5]^3, 64 voxels per unit "
+                                   "and min_feature 0.1", "clauses": tape.n_clauses,
+                       "max_err": MAX_ERR, "l2": "flushed before each mesh"}}))
+
+
 def run_heightmap(args, world, rank, local):
     """Height maps: the 64-sphere union (seed 1 + rank) over [-1.5,1.5]^3 at
     512 / 3 voxels per unit (512^3 voxels: a 512 x 512 image with 512 z
@@ -775,6 +837,8 @@ def main():
         run_heightmap(args, world, rank, local)
     elif args.workload == "fit":
         run_fit(args, world, rank, local)
+    elif args.workload == "spheres64":
+        run_spheres_mesh(args, world, rank, local)
     elif args.impl == "reference":
         run_reference(args, world, rank)
     else:

@@ -531,7 +531,8 @@ void* kernel(GpuTape& g, int k, const std::vector<uint32_t>* slots = nullptr)
     std::lock_guard<std::mutex> lock(g.mu);
     GpuTape::JitKernel& j = g.jit[k];
     if (j.state == 0) {
-        bool ok = api().ok && g.reg.clauses.size() <= kJitMaxClauses;
+        bool ok = api().ok && g.reg.clauses.size() <= (k == 4 ? kJitMaxIntervalClauses
+                                                                 : kJitMaxClauses);
         if (ok) {
             switch (k) {
                 case 0: ok = build(g, 0, values_source(g.reg), "lfb_tape_values"); break;

@@ -21,6 +21,11 @@
 namespace lfb {
 
 constexpr uint32_t kJitMaxClauses = 4096;
+/// The interval kernel's limit is lower: its compile time grows much faster
+/// than the tape (NVRTC for sm_100a on a development host: 5 s for 703
+/// clauses, 69 s for 1924), while the interval interpreter gives the same
+/// bounds and takes milliseconds for a height map's boxes.
+constexpr uint32_t kJitMaxIntervalClauses = 1024;
 
 /// Values of the tape at n points through its compiled kernel (compiled on
 /// first use).  Returns false, with no error set, when the tape has no

@@ -92,6 +92,36 @@ def dist_setup(args):
     return world, rank, local
 
 
+# Process group of an auxiliary workload under torchrun (set by main; None
+# on one GPU).  Its only traffic is rank_max.
+_AUX_PG = None
+
+
+def aux_group(world, local):
+    """NCCL group for an auxiliary workload when WORLD_SIZE > 1, else None."""
+    if world <= 1:
+        return None
+    import datetime
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return dist
+
+
+def rank_max(x, pg=None):
+    """Max over ranks of a device-timed figure (identity on one GPU); every
+    rank calls it at the same points."""
+    pg = pg or _AUX_PG
+    if pg is None:
+        return x
+    import torch
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return t.item()
+
+
 def rank_seed(rank):
     """Weak scaling: every rank meshes its own seeded shape."""
     return SEED_BASE + rank
@@ -449,15 +479,17 @@ def run_batch(args, world, rank, local):
         t0 = time.perf_counter()
         tris = [fn() for _ in range(args.steps)]
         torch.cuda.synchronize()
-        timings[name] = (time.perf_counter() - t0) / args.steps
+        timings[name] = rank_max((time.perf_counter() - t0) / args.steps)
         assert len(set(tris)) == 1
     if rank == 0:
         n = len(jobs)
         print(json.dumps({
-            "metric": "meshes/s (many trees)", "value": n / timings["batch"], "unit": "meshes/s",
+            "metric": "meshes/s (many trees)", "value": world * n / timings["batch"],
+            "unit": "meshes/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": timings["batch"] * 1e3, "higher_is_better": True,
-            "loop_value": n / timings["loop"], "batch_over_loop": timings["loop"] / timings["batch"],
+            "loop_value": world * n / timings["loop"],
+            "batch_over_loop": timings["loop"] / timings["batch"],
             "triangles_per_step": tris[0], "dtype": "f32", "data": "synthetic",
             "config": {"workload": "batch of %d random CSG trees, 8-4000 primitives, "
                                    "depth 8-11" % n, "workers": args.workers}}))
@@ -508,7 +540,8 @@ def run_eval(args, world, rank, local):
     hx, hy, hz = (np.ascontiguousarray(a) for a in pts)
     hf = np.empty(n, np.float32)
     t_e2e = _timed(lambda: tape.values(hx, hy, hz, out=hf), args.steps, args.warmup, flush)
-    ce = n * tape.n_clauses
+    t_val, t_der, t_e2e = rank_max(t_val), rank_max(t_der), rank_max(t_e2e)
+    ce = n * tape.n_clauses * world      # clause evaluations of all ranks per step
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         # the oracle port (ArrayEvaluator / DerivArrayEvaluator restated,
@@ -530,7 +563,7 @@ def run_eval(args, world, rank, local):
                "deriv_value": m * tape.n_clauses / td}
     sm = torch.cuda.get_device_properties(local).multi_processor_count
     peak = sm * 128 * 1965e6 / 1e9   # G FP32 lane-ops/s at the maximum SM clock
-    achieved = ce * wv / (t_val / 1e3) / 1e9
+    achieved = ce / world * wv / (t_val / 1e3) / 1e9      # one GPU's kernel
     if rank == 0:
         print(json.dumps({
             "metric": "clause-evals/s", "value": ce / (t_val / 1e3), "unit": "clause-evals/s",
@@ -543,7 +576,7 @@ def run_eval(args, world, rank, local):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_val,
             "higher_is_better": True, "deriv_value": ce / (t_der / 1e3), "ms_deriv": t_der,
             "e2e": {"value": ce / (t_e2e / 1e3), "unit": "clause-evals/s",
-                    "h2d_bytes_per_step": 12 * n, "d2h_bytes_per_step": 4 * n},
+                    "h2d_bytes_per_step": 12 * n * world, "d2h_bytes_per_step": 4 * n * world},
             "cpu_baseline": cpu, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "64-sphere union, 128^3 lattice", "points": n,
                        "clauses": tape.n_clauses, "l2": "flushed before each step"}}))
@@ -588,7 +621,8 @@ def run_adjoint(args, world, rank, local):
     ms = _timed(step, args.steps, args.warmup, flush)
     ms_fwd = _timed(lambda: tape.values(x, y, z, out=f, stream=torch.cuda.current_stream().cuda_stream),
                     args.steps, args.warmup, flush)
-    comps = n * (3 + tape.n_vars)
+    ms, ms_fwd = rank_max(ms), rank_max(ms_fwd)
+    comps = n * (3 + tape.n_vars) * world     # gradient components of all ranks per step
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         # the oracle port: JacobianEvaluator::gradient (variables) and
@@ -668,7 +702,7 @@ def run_fit(args, world, rank, local):
     torch.cuda.synchronize()
     first_s = time.perf_counter() - t0        # includes compiling the tapes' kernels
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
-    ms = _timed(fit.step, args.steps, args.warmup, flush)
+    ms = rank_max(_timed(fit.step, args.steps, args.warmup, flush))
     last = fit.losses.clone()
     torch.cuda.synchronize()
     remesh_s = None
@@ -679,7 +713,7 @@ def run_fit(args, world, rank, local):
         t0 = time.perf_counter()
         shape_mod.render_meshes(jobs, workers=4)
         torch.cuda.synchronize()
-        remesh_s = time.perf_counter() - t0
+        remesh_s = rank_max(time.perf_counter() - t0)
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         # the oracle port: JacobianEvaluator::gradient (forward mode, one
@@ -753,9 +787,11 @@ def run_spheres_mesh(args, world, rank, local):
 
         ms = _timed(once, args.steps, args.warmup, flush)
         ms_e2e = _timed(lambda: once(Tape(shape)), args.steps, args.warmup, flush)
+        ms, ms_e2e = rank_max(ms), rank_max(ms_e2e)
         v, tr = holder["mesh"]
         st = holder["stats"]
-        entry = {"ms_per_mesh": ms, "meshes_per_s": 1e3 / ms, "e2e_meshes_per_s": 1e3 / ms_e2e,
+        entry = {"ms_per_mesh": ms, "meshes_per_s": world * 1e3 / ms,
+                 "e2e_meshes_per_s": world * 1e3 / ms_e2e,
                  "octree_depth": st.levels, "triangles": int(len(tr)),
                  "stages_ms": {"interval": st.ms_interval, "leaf": st.ms_leaf,
                                "collapse": st.ms_collapse, "dual": st.ms_dual}}
@@ -801,10 +837,12 @@ def run_heightmap(args, world, rank, local):
     out = {}
     ms = _timed(lambda: out.update(r=render_heightmap(tape, lo, hi, res)), args.steps,
                 args.warmup, flush)
+    ms = rank_max(ms)
     depth, _ = out["r"]
     voxels = depth.size * 512
     line = {
-        "metric": "height-map voxels/s", "value": voxels / (ms / 1e3), "unit": "voxels/s",
+        "metric": "height-map voxels/s", "value": world * voxels / (ms / 1e3),
+        "unit": "voxels/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "dtype": "f32", "data": "synthetic",
         "filled_pixels": int(np.isfinite(depth).sum()),
@@ -827,18 +865,16 @@ def run_heightmap(args, world, rank, local):
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
-    if args.workload == "batch":
-        run_batch(args, world, rank, local)
-    elif args.workload == "eval":
-        run_eval(args, world, rank, local)
-    elif args.workload == "adjoint":
-        run_adjoint(args, world, rank, local)
-    elif args.workload == "heightmap":
-        run_heightmap(args, world, rank, local)
-    elif args.workload == "fit":
-        run_fit(args, world, rank, local)
-    elif args.workload == "spheres64":
-        run_spheres_mesh(args, world, rank, local)
+    aux = {"batch": run_batch, "eval": run_eval, "adjoint": run_adjoint,
+           "heightmap": run_heightmap, "fit": run_fit, "spheres64": run_spheres_mesh}
+    if args.workload in aux:
+        global _AUX_PG
+        _AUX_PG = aux_group(world, local)
+        try:
+            aux[args.workload](args, world, rank, local)
+        finally:
+            if _AUX_PG is not None:
+                _AUX_PG.destroy_process_group()
     elif args.impl == "reference":
         run_reference(args, world, rank)
     else:

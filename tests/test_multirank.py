@@ -47,3 +47,33 @@ def test_two_gloo_ranks():
         assert total_ms == 200.0 and e2e_ms == 100.0          # slowest rank
         assert value == pytest.approx(world * 3 / 0.2)         # whole-job meshes/s
         assert e2e_value == pytest.approx(world * 3 / 0.1)
+
+
+def _rank_aux(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, ROOT)
+    import bench
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        # the auxiliary workloads' timing reduction: every rank reports the
+        # slowest rank's time
+        q.put((rank, bench.rank_max(10.0 * (rank + 1), dist), bench.rank_max(3.5 - rank, dist)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_auxiliary_workloads_take_the_slowest_rank():
+    world = 2
+    port = 30600 + os.getpid() % 1000
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_rank_aux, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=300)
+        assert p.exitcode == 0
+    got = sorted(q.get(timeout=10) for _ in range(world))
+    assert [g[1:] for g in got] == [(20.0, 3.5), (20.0, 3.5)]
+    import bench
+    assert bench.rank_max(7.25) == 7.25      # one process: unchanged

@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <new>
 #include <thread>
 #include <vector>
 
@@ -581,9 +582,10 @@ int ora_render_mesh(void* h, float xl, float yl, float zl, float xu, float yu,
     std::vector<uint32_t> tr;
     const float lo[3] = {xl, yl, zl}, hi[3] = {xu, yu, zu};
     const int L = ora::render_mesh(t, lo, hi, min_feature, max_err, threads, v, tr);
-    float* vo = new float[v.size()];
+    // raw storage, released by ora_free whatever the element type
+    void* vo = ::operator new[](std::max<size_t>(v.size(), 1) * sizeof(float));
     std::memcpy(vo, v.data(), v.size() * sizeof(float));
-    uint32_t* to = new uint32_t[tr.size() ? tr.size() : 1];
+    void* to = ::operator new[](std::max<size_t>(tr.size(), 1) * sizeof(uint32_t));
     std::memcpy(to, tr.data(), tr.size() * sizeof(uint32_t));
     *verts_out = vo;
     *tris_out = to;
@@ -592,6 +594,6 @@ int ora_render_mesh(void* h, float xl, float yl, float zl, float xu, float yu,
     return L;
 }
 
-void ora_free(void* p) { delete[] static_cast<char*>(p); }
+void ora_free(void* p) { ::operator delete[](p); }
 
 }  // extern "C"

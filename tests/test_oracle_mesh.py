@@ -80,3 +80,20 @@ def test_edges_pair_up():
                       (workloads.random_csg(30, seed=6), 0.05)):
         _, t = _mesh(shape, (-1.5,) * 3, (1.5,) * 3, mf)
         assert len(t) > 0 and edge_pairs_ok(t)
+
+
+def test_region_levels():
+    # region.cpp:160-167: Region<3>({-1,-1,-1}, {1,1,1}).withResolution(r).level
+    import ctypes
+
+    import oracle_ffi
+    lib = oracle_ffi.load()
+    ora = OracleTape(workloads.sphere((0, 0, 0), 0.5))
+    for res, level in ((5, 0), (1, 1), (1.2, 1), (0.9, 2)):
+        vp, tp = ctypes.c_void_p(), ctypes.c_void_p()
+        nv, nt = ctypes.c_uint32(), ctypes.c_uint32()
+        got = lib.ora_render_mesh(ora.h, -1, -1, -1, 1, 1, 1, res, 1e-8, 1, ctypes.byref(vp),
+                                  ctypes.byref(nv), ctypes.byref(tp), ctypes.byref(nt))
+        lib.ora_free(vp)
+        lib.ora_free(tp)
+        assert got == level

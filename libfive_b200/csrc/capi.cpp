@@ -530,13 +530,18 @@ int lfb_fit_adam_step(const lfb_tape* tapes, uint32_t n_shapes,
 {
     clear_error();
     if (!tapes) return set_error(LFB_E_INVALID, "null tape list");
-    std::vector<GpuTape*> gs(n_shapes);
-    for (uint32_t j = 0; j < n_shapes; ++j) {
-        if (!tapes[j]) return set_error(LFB_E_INVALID, "null tape");
-        gs[j] = tapes[j]->g.get();
+    try {
+        std::vector<GpuTape*> gs(n_shapes);
+        for (uint32_t j = 0; j < n_shapes; ++j) {
+            if (!tapes[j]) return set_error(LFB_E_INVALID, "null tape");
+            gs[j] = tapes[j]->g.get();
+        }
+        return fit_adam_step(gs.data(), n_shapes, point_offsets, x, y, z, var_offsets, m, v,
+                             adam, step, losses, static_cast<cudaStream_t>(stream));
+    } catch (const std::exception& e) {
+        // nothing may unwind through the C ABI
+        return set_error(LFB_E_INVALID, std::string("lfb_fit_adam_step: ") + e.what());
     }
-    return fit_adam_step(gs.data(), n_shapes, point_offsets, x, y, z, var_offsets, m, v,
-                         adam, step, losses, static_cast<cudaStream_t>(stream));
 }
 
 int lfb_tape_compiled(lfb_tape t)

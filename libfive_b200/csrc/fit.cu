@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <exception>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -151,7 +152,12 @@ int prepare_all(GpuTape* const* tapes, uint32_t n)
         work();
     } else {
         std::vector<std::thread> pool;
-        for (size_t t = 0; t < n_threads; ++t) pool.emplace_back(work);
+        try {
+            for (size_t t = 0; t < n_threads; ++t) pool.emplace_back(work);
+        } catch (const std::exception&) {
+            // fewer threads than asked for: this thread helps below
+        }
+        if (pool.size() < n_threads) work();
         for (auto& t : pool) t.join();
     }
     return err_code ? set_error(err_code, err_msg) : 0;

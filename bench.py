@@ -646,9 +646,52 @@ def run_adjoint(args, world, rank, local):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "loss_grads_per_s": 1e3 / ms,
             "ms_forward": ms_fwd, "step_over_forward": ms / ms_fwd, "dtype": "f32",
+            "roofline": reverse_mode_roofline(shape, n, ms),
             "data": "synthetic",
             "config": {"workload": "256 blended spheres, 1024 free variables, 2^22 surface points",
                        "points": n, "vars": tape.n_vars, "clauses": tape.n_clauses}}))
+
+
+def hbm_peak():
+    """(measured HBM GB/s, source): the copy bandwidth in MEASURED_PEAKS.json
+    when present, else the earlier measurement on this kind of GPU."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback: earlier B200 copy measurement"
+
+
+def reverse_mode_bytes_per_point(shape):
+    """Algorithmic HBM bytes per point of one reverse-mode pass (forward pass
+    storing the local partials, backward pass reading them): 12 B of
+    coordinates, f written once and read twice (as the seed, and by the
+    loss) = 12 B, and each stored partial written and read once = 8 B.
+    Stored partials per clause follow the opcode: none for add / sub / neg
+    (fixed +-1), one for min / max (0 or 1) and unary ops, two for other
+    binary ops."""
+    from libfive_b200 import ffi
+    from libfive_b200.shape import slot_tape
+    lib = ffi.load()
+    fixed = {lib.libfive_opcode_enum(n.encode()) for n in ("add", "sub", "neg", "const-var")}
+    choice = {lib.libfive_opcode_enum(n.encode()) for n in ("min", "max")}
+    stored = 0
+    for c in slot_tape(shape)["clauses"]:
+        o = c[0]
+        stored += 0 if o in fixed else 1 if o in choice else lib.libfive_opcode_args(o)
+    return 24 + 8 * stored, stored
+
+
+def reverse_mode_roofline(shape, points, ms):
+    """roofline object of a reverse-mode step over `points` points in `ms`."""
+    per_point, stored = reverse_mode_bytes_per_point(shape)
+    peak, src = hbm_peak()
+    achieved = per_point * points / (ms / 1e3) / 1e9
+    return {"kernel": "lfb_tape_partials + lfb_tape_backward", "bound": "hbm",
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": src, "traffic": None,
+            "algorithmic_bytes_per_point": per_point, "stored_partials_per_point": stored}
 
 
 def run_fit(args, world, rank, local):
@@ -744,6 +787,7 @@ def run_fit(args, world, rank, local):
             "grads_per_s": n_total * tapes[0].n_vars / step_s,
             "ms_remesh_all": remesh_s * 1e3 if remesh_s is not None else None,
             "job_500_steps_s": job_s, "first_step_s": first_s, "setup_s": setup_s,
+            "roofline": reverse_mode_roofline(shapes[0], fit.n_points, ms),
             "loss_mean_first": float(first.mean()), "loss_mean_last": float(last.mean()),
             "finite": bool(torch.isfinite(last).all()),
             "cpu_baseline": cpu, "dtype": "f32", "data": "synthetic",

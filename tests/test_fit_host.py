@@ -49,3 +49,14 @@ def test_surface_points_lie_on_the_mesh():
     assert np.all((x >= 0) & (x <= 1) & (y >= 0) & (y <= 1))
     # area-uniform: both triangles get about half the points
     assert abs(np.mean(y < x) - 0.5) < 0.05
+
+
+def test_reverse_mode_bytes_follow_the_stored_partials():
+    # sqrt(x^2 + y^2) - 0.5: square, square and sqrt store one partial each,
+    # add and sub none: 24 B of coordinates and f traffic + 3 x 8 B
+    import bench
+    from libfive_b200.shape import X, Y
+    shape = (X().square() + Y().square()).sqrt() - 0.5
+    assert bench.reverse_mode_bytes_per_point(shape) == (48, 3)
+    # min stores one (a choice), mul two
+    assert bench.reverse_mode_bytes_per_point(X().min(Y() * X()))[1] == 3

@@ -834,8 +834,17 @@ def run_spheres_mesh(args, world, rank, local):
         ms, ms_e2e = rank_max(ms), rank_max(ms_e2e)
         v, tr = holder["mesh"]
         st = holder["stats"]
+        # the leaf kernel's FP32 roofline, as on the main mesh line
+        wv, wg, _ = tape_weights(shape)
+        sms = torch.cuda.get_device_properties(local).multi_processor_count
+        peak = sms * 128 * 1965e6 / 1e9
+        leaf_ops = st.clause_evals * wv + st.clause_evals_grad * wg
+        achieved = leaf_ops / (st.ms_leaf / 1e3) / 1e9 if st.ms_leaf > 0 else 0.0
         entry = {"ms_per_mesh": ms, "meshes_per_s": world * 1e3 / ms,
                  "e2e_meshes_per_s": world * 1e3 / ms_e2e,
+                 "roofline": {"kernel": "k_leaf_groups", "bound": "fp32", "achieved": achieved,
+                              "peak": peak, "unit": "G lane-ops/s", "frac": achieved / peak,
+                              "peak_source": "derived: SMs x 128 FP32 lanes x 1965 MHz"},
                  "octree_depth": st.levels, "triangles": int(len(tr)),
                  "stages_ms": {"interval": st.ms_interval, "leaf": st.ms_leaf,
                                "collapse": st.ms_collapse, "dual": st.ms_dual}}
@@ -856,7 +865,8 @@ def run_spheres_mesh(args, world, rank, local):
             "ms_per_step": main_["ms_per_mesh"], "higher_is_better": True, "scaling": "weak",
             "dtype": "f32", "data": "synthetic",
             "e2e": {"value": main_["e2e_meshes_per_s"], "unit": "meshes/s"},
-            "cpu_baseline": main_.get("cpu_baseline"), "resolutions": lines,
+            "cpu_baseline": main_.get("cpu_baseline"), "roofline": main_["roofline"],
+            "resolutions": lines,
             "config": {"workload": "64-sphere union, [-1.5,1.5]^3, 64 voxels per unit "
                                    "and min_feature 0.1", "clauses": tape.n_clauses,
                        "max_err": MAX_ERR, "l2": "flushed before each mesh"}}))

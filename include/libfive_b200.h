@@ -78,6 +78,17 @@ int lfb_eval_derivs(lfb_tape t, uint64_t n, const float* x, const float* y,
                     const float* z, float* v, float* dx, float* dy, float* dz,
                     void* stream, uint32_t flags);
 
+/* FeatureEvaluator at n host points (the path the mesher takes at samples
+ * whose value is exactly zero): inside[i] = isInside (eval_feature.cpp:
+ * 56-116); when n_feats is not NULL, n_feats[i] = the number of distinct
+ * feature gradients at point i (features, eval_feature.cpp:125-169) and, when
+ * feats is not NULL, feats[(i * max_feats + k) * 3 + 0..2] the first
+ * max_feats of them.  LFB_E_CAPACITY when a feature list outgrows the
+ * device evaluator's fixed capacity (15 features of 4 epsilons per clause). */
+int lfb_eval_features(lfb_tape t, uint64_t n, const float* x, const float* y,
+                      const float* z, uint8_t* inside, float* feats,
+                      uint32_t max_feats, uint32_t* n_feats);
+
 /* IntervalEvaluator::eval (eval_interval.cpp:68-93) over n boxes; out_nan
  * receives the "may be NaN" flag (0/1). */
 int lfb_eval_intervals(lfb_tape t, uint64_t n,

@@ -599,6 +599,15 @@ int lfb_eval_derivs(lfb_tape t, uint64_t n, const float* x, const float* y,
     return eval_derivs_host(*t->g, n, x, y, z, v, dx, dy, dz);
 }
 
+int lfb_eval_features(lfb_tape t, uint64_t n, const float* x, const float* y,
+                      const float* z, uint8_t* inside, float* feats, uint32_t max_feats,
+                      uint32_t* n_feats)
+{
+    clear_error();
+    if (!t) return set_error(LFB_E_INVALID, "null tape");
+    return eval_features_host(*t->g, n, x, y, z, inside, feats, max_feats, n_feats);
+}
+
 int lfb_eval_intervals(lfb_tape t, uint64_t n, const float* xlo,
                        const float* xhi, const float* ylo, const float* yhi,
                        const float* zlo, const float* zhi, float* out_lo,

@@ -31,6 +31,10 @@ int eval_intervals_host(GpuTape& g, uint64_t n, const float* xlo,
                         const float* zlo, const float* zhi, float* olo,
                         float* ohi, uint8_t* onan);
 
+/// lfb_eval_features (feature_api.cu); host arrays.
+int eval_features_host(GpuTape& g, uint64_t n, const float* x, const float* y, const float* z,
+                       uint8_t* inside, float* feats, uint32_t max_feats, uint32_t* n_feats);
+
 int eval_jacobian(GpuTape& g, uint64_t n, const float* x, const float* y,
                   const float* z, float* out, cudaStream_t s, bool device);
 

@@ -269,6 +269,19 @@ class Tape:
             olo.ctypes.data, ohi.ctypes.data, onan.ctypes.data, stream, 0), "intervals")
         return olo, ohi, onan.astype(bool)
 
+    def features(self, x, y, z, max_feats=16):
+        """FeatureEvaluator at host points: (inside [n] bool, list of
+        [k, 3] arrays of the distinct feature gradients at each point)."""
+        x, y, z = (np.ascontiguousarray(a, np.float32) for a in (x, y, z))
+        n = len(x)
+        inside = np.zeros(n, np.uint8)
+        feats = np.zeros((n, max_feats, 3), np.float32)
+        counts = np.zeros(n, np.uint32)
+        ffi.check(_lib().lfb_eval_features(
+            self.ptr, n, x.ctypes.data, y.ctypes.data, z.ctypes.data, inside.ctypes.data,
+            feats.ctypes.data, max_feats, counts.ctypes.data), "features")
+        return inside.astype(bool), [feats[i, :min(int(c), max_feats)] for i, c in enumerate(counts)]
+
     def jacobian(self, x, y, z, out=None, stream=None):
         out = np.zeros((len(x), self.n_vars), np.float32) if out is None else out
         fl = self._flags([x, y, z, out])

@@ -198,3 +198,61 @@ void ora_render_heightmap(void* h_, const float lower[3], const float upper[3],
 }
 
 }  // extern "C"
+
+// Library-call record / replay (see libm in oracle_eval.cpp).
+extern "C" {
+void ora_libm_mode(int mode) { ora::libm_set_mode(mode); }
+void ora_libm_table(const uint64_t* keys, const uint32_t* vals, uint64_t n)
+{
+    ora::libm_set_table(keys, vals, n);
+}
+uint64_t ora_libm_take(uint64_t* out, uint64_t max) { return ora::libm_take(out, max); }
+uint64_t ora_libm_misses() { return ora::libm_misses(); }
+}
+
+// The mesher's FP64 QEF routines (qef.h), for checks against an independent
+// eigensolver.
+#include "qef.h"
+extern "C" {
+void ora_sym3_eigen(const double s[6], double eval[3], double evec[9])
+{
+    double U[3][3];
+    lfb::sym3_eigen(s, eval, U);
+    for (int r = 0; r < 3; ++r) {
+        for (int c = 0; c < 3; ++c) evec[3 * r + c] = U[r][c];
+    }
+}
+int ora_qef_rank(const double ata[6])
+{
+    lfb::Qef q;
+    lfb::qef_zero(q);
+    for (int i = 0; i < 6; ++i) q.ata[i] = ata[i];
+    return lfb::qef_rank(q);
+}
+double ora_qef_vertex(const double ata[6], const double atb[3], double btb,
+                      const double mass[4], double v[3], int* rank)
+{
+    lfb::Qef q;
+    for (int i = 0; i < 6; ++i) q.ata[i] = ata[i];
+    for (int i = 0; i < 3; ++i) q.atb[i] = atb[i];
+    q.btb = btb;
+    for (int i = 0; i < 4; ++i) q.mass[i] = mass[i];
+    return lfb::qef_vertex(q, v, rank);
+}
+}
+
+// The mesher's constant tables (dc_tables.hpp), for checks against the
+// reference's own table tests.
+#include "dc_tables.hpp"
+extern "C" {
+const void* ora_dc_tables(uint64_t* bytes)
+{
+    static const lfb::DcTables* t = [] {
+        auto* p = new lfb::DcTables;
+        lfb::build_dc_tables(*p);
+        return p;
+    }();
+    if (bytes) *bytes = sizeof(lfb::DcTables);
+    return t;
+}
+}

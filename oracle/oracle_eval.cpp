@@ -1,10 +1,13 @@
 // CPU oracle evaluators (TEST INFRASTRUCTURE ONLY; see oracle.hpp).
 #include <algorithm>
+#include <atomic>
 #include <cfenv>
 #include <cmath>
 #include <cstring>
 #include <limits>
 #include <memory>
+#include <mutex>
+#include <unordered_set>
 
 #include "oracle_eval.hpp"
 
@@ -17,6 +20,116 @@ namespace ora {
 
 static inline float fmin_std(float a, float b) { return (b < a) ? b : a; }   // std::min
 static inline float fmax_std(float a, float b) { return (a < b) ? b : a; }   // std::max
+
+////////////////////////////////////////////////////////////////////////////////
+// Library calls of the point evaluators (sin, cos, tan, asin, acos, atan, exp,
+// log).  By default they call the host C library.  For parity checks of whole
+// tapes the caller can instead supply the results of another implementation
+// (the GPU's) for given inputs: in record mode every (opcode, input) pair is
+// collected; in replay mode results come from the supplied table, and inputs
+// missing from it fall back to the C library, are counted and recorded, so a
+// caller can iterate until nothing is missing.  Every other operation is
+// exactly rounded, so with the same library results the oracle and the GPU
+// must agree bit for bit.
+
+static float host_libm(int op, float a)
+{
+    switch (op) {
+        case OP_SIN: return sinf(a);
+        case OP_COS: return cosf(a);
+        case OP_TAN: return tanf(a);
+        case OP_ASIN: return asinf(a);
+        case OP_ACOS: return acosf(a);
+        case OP_ATAN: return atanf(a);
+        case OP_LOG: return logf(a);
+        case OP_EXP: return expf(a);
+    }
+    return NAN;
+}
+
+namespace {
+struct LibmHook {
+    std::atomic<int> mode{0};   // 0 host, 1 record, 2 replay
+    std::mutex mu;
+    std::vector<std::unordered_set<uint64_t>*> sets;   // one per recording thread
+    std::vector<uint64_t> keys;                        // replay table, sorted
+    std::vector<uint32_t> vals;
+    std::atomic<uint64_t> misses{0};
+    std::atomic<uint64_t> generation{1};
+};
+LibmHook g_hook;
+
+std::unordered_set<uint64_t>& record_set()
+{
+    thread_local std::unordered_set<uint64_t>* set = nullptr;
+    thread_local uint64_t gen = 0;
+    const uint64_t now = g_hook.generation.load();
+    if (!set || gen != now) {
+        std::lock_guard<std::mutex> lk(g_hook.mu);
+        set = new std::unordered_set<uint64_t>();
+        g_hook.sets.push_back(set);
+        gen = now;
+    }
+    return *set;
+}
+}  // namespace
+
+static float libm(int op, float a)
+{
+    const int mode = g_hook.mode.load(std::memory_order_relaxed);
+    if (mode == 0) return host_libm(op, a);
+    uint32_t bits;
+    std::memcpy(&bits, &a, 4);
+    const uint64_t key = (static_cast<uint64_t>(op) << 32) | bits;
+    if (mode == 2) {
+        auto it = std::lower_bound(g_hook.keys.begin(), g_hook.keys.end(), key);
+        if (it != g_hook.keys.end() && *it == key) {
+            float r;
+            std::memcpy(&r, &g_hook.vals[it - g_hook.keys.begin()], 4);
+            return r;
+        }
+        g_hook.misses.fetch_add(1, std::memory_order_relaxed);
+    }
+    record_set().insert(key);
+    return host_libm(op, a);
+}
+
+// Mode changes and table updates must not overlap evaluations.
+void libm_set_mode(int mode)
+{
+    std::lock_guard<std::mutex> lk(g_hook.mu);
+    for (auto* s : g_hook.sets) delete s;
+    g_hook.sets.clear();
+    g_hook.generation.fetch_add(1);
+    g_hook.misses = 0;
+    g_hook.mode = mode;
+}
+
+void libm_set_table(const uint64_t* keys, const uint32_t* vals, uint64_t n)
+{
+    std::vector<std::pair<uint64_t, uint32_t>> kv(n);
+    for (uint64_t i = 0; i < n; ++i) kv[i] = {keys[i], vals[i]};
+    std::sort(kv.begin(), kv.end());
+    g_hook.keys.resize(n);
+    g_hook.vals.resize(n);
+    for (uint64_t i = 0; i < n; ++i) {
+        g_hook.keys[i] = kv[i].first;
+        g_hook.vals[i] = kv[i].second;
+    }
+}
+
+uint64_t libm_take(uint64_t* out, uint64_t max)
+{
+    std::lock_guard<std::mutex> lk(g_hook.mu);
+    std::unordered_set<uint64_t> all;
+    for (auto* s : g_hook.sets) all.insert(s->begin(), s->end());
+    std::vector<uint64_t> v(all.begin(), all.end());
+    std::sort(v.begin(), v.end());
+    if (out) std::copy(v.begin(), v.begin() + std::min<uint64_t>(max, v.size()), out);
+    return v.size();
+}
+
+uint64_t libm_misses() { return g_hook.misses.load(); }
 
 float value_op(int op, float a, float b)
 {
@@ -52,14 +165,14 @@ float value_op(int op, float a, float b)
         case OP_SQUARE: return a * a;
         case OP_SQRT: return std::sqrt(a);
         case OP_NEG: return -a;
-        case OP_SIN: return sinf(a);
-        case OP_COS: return cosf(a);
-        case OP_TAN: return tanf(a);
-        case OP_ASIN: return asinf(a);
-        case OP_ACOS: return acosf(a);
-        case OP_ATAN: return atanf(a);
-        case OP_LOG: return logf(a);
-        case OP_EXP: return expf(a);
+        case OP_SIN: return libm(OP_SIN, a);
+        case OP_COS: return libm(OP_COS, a);
+        case OP_TAN: return libm(OP_TAN, a);
+        case OP_ASIN: return libm(OP_ASIN, a);
+        case OP_ACOS: return libm(OP_ACOS, a);
+        case OP_ATAN: return libm(OP_ATAN, a);
+        case OP_LOG: return libm(OP_LOG, a);
+        case OP_EXP: return libm(OP_EXP, a);
         case OP_ABS: return std::fabs(a);
         case OP_RECIP: return 1.0f / a;
         case OP_CONST_VAR: return a;
@@ -112,14 +225,14 @@ void deriv_op(int op, float av, float bv, float ov, const float* ad,
                 break;
             }
             case OP_NEG: r = -a; break;
-            case OP_SIN: r = a * cosf(av); break;
-            case OP_COS: r = a * -sinf(av); break;
-            case OP_TAN: { const float s = 1 / cosf(av); const float s2 = s * s; r = a * s2; break; }
+            case OP_SIN: r = a * libm(OP_COS, av); break;
+            case OP_COS: r = a * -libm(OP_SIN, av); break;
+            case OP_TAN: { const float s = 1 / libm(OP_COS, av); const float s2 = s * s; r = a * s2; break; }
             case OP_ASIN: { const float q = av * av; r = a / std::sqrt(1 - q); break; }
             case OP_ACOS: { const float q = av * av; r = a / -std::sqrt(1 - q); break; }
             case OP_ATAN: { const float q = av * av; r = a / (q + 1); break; }
             case OP_LOG: r = a / av; break;
-            case OP_EXP: r = a * expf(av); break;
+            case OP_EXP: r = a * libm(OP_EXP, av); break;
             case OP_ABS: r = (av > 0) ? a : -a; break;
             case OP_RECIP: { const float q = av * av; r = a / -q; break; }
             case OP_CONST_VAR: r = clear_vars ? 0.0f : a; break;

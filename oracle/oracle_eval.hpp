@@ -21,6 +21,15 @@ enum {
 constexpr int NB = 256;   // LIBFIVE_EVAL_ARRAY_SIZE
 
 int op_arity(int op);
+
+// Library-call results of the point evaluators: 0 = host C library,
+// 1 = host library and record every (opcode << 32 | input bits) key,
+// 2 = replay from the table of libm_set_table (misses use the host library
+// and are recorded).  Switching mode clears what was recorded.
+void libm_set_mode(int mode);
+void libm_set_table(const uint64_t* keys, const uint32_t* vals, uint64_t n);
+uint64_t libm_take(uint64_t* out, uint64_t max);
+uint64_t libm_misses();
 float value_op(int op, float a, float b);
 void deriv_op(int op, float av, float bv, float ov, const float* ad,
               const float* bd, float* od, bool clear_vars);

@@ -41,6 +41,18 @@ def load():
                 ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(vp),
                 ctypes.POINTER(ctypes.c_uint32)]
             _lib.ora_free.argtypes = [vp]
+        _lib.ora_libm_mode.argtypes = [ctypes.c_int]
+        _lib.ora_libm_table.argtypes = [vp, vp, ctypes.c_uint64]
+        _lib.ora_libm_take.restype = ctypes.c_uint64
+        _lib.ora_libm_take.argtypes = [vp, ctypes.c_uint64]
+        _lib.ora_libm_misses.restype = ctypes.c_uint64
+        _lib.ora_sym3_eigen.argtypes = [vp, vp, vp]
+        _lib.ora_dc_tables.restype = vp
+        _lib.ora_dc_tables.argtypes = [ctypes.POINTER(ctypes.c_uint64)]
+        _lib.ora_qef_rank.restype = ctypes.c_int
+        _lib.ora_qef_rank.argtypes = [vp]
+        _lib.ora_qef_vertex.restype = ctypes.c_double
+        _lib.ora_qef_vertex.argtypes = [vp, vp, ctypes.c_double, vp, vp, vp]
     return _lib
 
 

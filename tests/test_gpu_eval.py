@@ -11,6 +11,7 @@ import pytest
 
 from libfive_b200 import workloads
 from libfive_b200.shape import Shape, Tape
+from libm_replay import with_gpu_libm
 from oracle_ffi import OracleTape
 from sexpr import parse
 
@@ -163,13 +164,24 @@ def test_spheres_lattice_parity(gpu):
         assert np.array_equal(a, b)
 
 
-def test_random_csg_parity(gpu):
-    """Random CSG with blends: exact ops bit-exact, exp/log within bounds."""
-    t = workloads.random_csg(200, seed=5)
+@pytest.mark.parametrize("n,seed", [(200, 5), (2000, 2)])
+def test_random_csg_parity(gpu, n, seed):
+    """Random CSG with exp / log blends (the 2000-primitive case is the
+    benchmark tree).  Each library-call opcode is held to its ULP bound
+    against the C library by test_every_opcode_matches_oracle; every other
+    opcode is exactly rounded.  So given the GPU's exp / log results for the
+    inputs it meets, the oracle must reproduce the GPU's values and
+    derivatives bit for bit: no tolerance on the composition."""
+    t = workloads.random_csg(n, seed=seed)
     P = workloads.uniform_points(20000, seed=9)
     g, o = Tape(t), OracleTape(t)
-    d = ulp_diff(g.values(*P), o.values(*P, threads=8))
-    assert np.percentile(d, 99) == 0 and d.max() <= 64
+    gv = g.values(*P)
+    ov = with_gpu_libm(lambda: o.values(*P, threads=8))
+    assert ulp_diff(gv, ov).max() == 0
+    gd = g.derivs(*P)
+    od = with_gpu_libm(lambda: o.derivs(*P, threads=8))
+    for a, b in zip(gd, od):
+        assert ulp_diff(a, b).max() == 0
 
 
 def test_vars_and_update(gpu):

@@ -9,6 +9,7 @@ import pytest
 
 from libfive_b200 import workloads
 from libfive_b200.shape import Shape, Tape
+from libm_replay import with_gpu_libm
 from oracle_ffi import OracleTape
 from sexpr import parse
 
@@ -101,6 +102,11 @@ def test_jacobian_matches_oracle_blends(gpu):
     assert np.array_equal(ok, np.isfinite(j))
     # CUDA's expf/logf differ from the C library's by a few ULPs
     assert np.allclose(j[ok], o[ok], rtol=1e-4, atol=1e-5)
+    # with the GPU's exp / log results, the oracle's forward Jacobian is the
+    # GPU's bit for bit
+    ora = OracleTape(s, vals)
+    o2 = with_gpu_libm(lambda: ora.jacobian(x, y, z))
+    assert np.array_equal(j, o2, equal_nan=True)
 
 
 @pytest.mark.parametrize("maker", ["spheres", "blends"])
@@ -123,12 +129,54 @@ def test_reverse_gradient_matches_forward(gpu, maker):
     keep = np.isfinite(odx) & np.isfinite(ody) & np.isfinite(odz)
     for g, od in ((gx, odx), (gy, ody), (gz, odz)):
         assert np.allclose(g[keep], seed[keep] * od[keep], rtol=1e-4, atol=1e-5)
+    # Variable gradients: points whose Jacobian row is finite (blends
+    # overflow deep inside a shape, and a non-finite local partial makes the
+    # whole sum non-finite), run again on their own.
     jac = ora.jacobian(x, y, z).astype(np.float64)
-    rows = np.isfinite(jac).all(axis=1)
-    want = seed[rows].astype(np.float64) @ jac[rows]
-    if rows.all():
-        scale = np.abs(seed[:, None] * jac).sum(axis=0) + 1e-6
-        assert np.all(np.abs(gvars - want) <= 1e-4 * scale)
+    rows = np.isfinite(jac).all(axis=1) & np.isfinite(ov)
+    assert rows.mean() > 0.5
+    xs, ys, zs, ss = (np.ascontiguousarray(a[rows]) for a in (x, y, z, seed))
+    gvars = np.zeros(tape.n_vars, np.float32)
+    tape.grad(xs, ys, zs, seed=ss, gvars=gvars)
+    want = ss.astype(np.float64) @ jac[rows]
+    scale = np.abs(ss[:, None] * jac[rows]).sum(axis=0) + 1e-6
+    assert np.all(np.abs(gvars - want) <= 1e-4 * scale)
+
+
+def test_reverse_gradient_blended_spheres_256_chunked(gpu):
+    """The adjoint configuration's shape (256 spheres blended pairwise,
+    1024 free variables, 4094 clauses) over more points than one partials
+    chunk holds (about 380 k points per 4 GiB chunk at this tape's 2815
+    stored partials per point): 2048 points with finite Jacobian rows, each
+    repeated, so the summed variable gradient is 512 times that of the 2048
+    and the per-point gradients repeat the oracle's derivatives."""
+    s, vals = workloads.blended_spheres_vars(256, seed=4)
+    tape = Tape(s, vals)
+    assert tape.n_vars == 1024
+    ora = OracleTape(s, vals)
+    cx, cy, cz = workloads.uniform_points(8192, seed=21, lo=-1.2, hi=1.2)
+    ov, odx, ody, odz = ora.derivs(cx, cy, cz, threads=8)
+    fin = np.isfinite(ov) & np.isfinite(odx) & np.isfinite(ody) & np.isfinite(odz)
+    idx = np.flatnonzero(fin)[:2048]
+    assert len(idx) == 2048
+    bx, by, bz = (np.ascontiguousarray(a[idx]) for a in (cx, cy, cz))
+    jac = ora.jacobian(bx, by, bz, threads=8).astype(np.float64)
+    assert np.isfinite(jac).all()
+    bseed = np.random.default_rng(5).uniform(-1, 1, 2048).astype(np.float32)
+    reps = 512
+    x, y, z, seed = (np.ascontiguousarray(np.tile(a, reps)) for a in (bx, by, bz, bseed))
+    n = len(x)
+    f = np.empty(n, np.float32)
+    gx, gy, gz = (np.empty(n, np.float32) for _ in range(3))
+    gvars = np.zeros(1024, np.float32)
+    tape.grad(x, y, z, seed=seed, f=f, gx=gx, gy=gy, gz=gz, gvars=gvars)
+    assert np.array_equal(f, np.tile(tape.values(bx, by, bz), reps))
+    for g, od in ((gx, odx), (gy, ody), (gz, odz)):
+        w = np.tile(bseed * od[idx], reps)
+        assert np.allclose(g, w, rtol=1e-4, atol=1e-5)
+    want = reps * (bseed.astype(np.float64) @ jac)
+    scale = reps * np.abs(bseed[:, None] * jac).sum(axis=0) + 1e-6
+    assert np.all(np.abs(gvars - want) <= 1e-4 * scale)
 
 
 def test_reverse_gradient_const_var(gpu):

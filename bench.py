@@ -41,7 +41,6 @@ def min_feature_for(depth):
     """min_feature giving `depth` levels over the 3-unit region."""
     return 3.0 / (2 ** depth - 24) if depth >= 6 else 3.0 / (2 ** depth - 0.5)
 MAX_ERR = 1e-8
-SUBDIV = 8                       # CPU sample: sub-boxes of a 8x8x8 split
 
 # FP32 lane-ops per clause evaluation (value mode / value+gradient mode),
 # fixed per opcode; library calls count as 20.
@@ -59,8 +58,6 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--cpu-sample", type=int, default=24,
-                   help="sub-boxes meshed per CPU baseline step")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true",
                    help="skip the end-to-end pass (profiling runs)")
@@ -211,80 +208,100 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_sample_boxes(step_seed, count):
-    """`count` distinct sub-boxes of the SUBDIV^3 split of the region."""
-    import numpy as np
-    rng = np.random.default_rng(step_seed)
-    ids = rng.choice(SUBDIV ** 3, size=count, replace=False)
-    lo, hi = REGION
-    w = [(hi[a] - lo[a]) / SUBDIV for a in range(3)]
-    boxes = []
-    for i in ids:
-        c = (int(i) % SUBDIV, (int(i) // SUBDIV) % SUBDIV, int(i) // (SUBDIV * SUBDIV))
-        blo = tuple(lo[a] + c[a] * w[a] for a in range(3))
-        bhi = tuple(lo[a] + (c[a] + 1) * w[a] for a in range(3))
-        boxes.append((blo, bhi))
-    return boxes
-
-
-def cpu_mesh_rate(shape, count, step_seed, cores):
-    """CPU oracle (restatement of the reference mesher) on `count` sub-boxes
-    at the benchmark's cell size, one box per thread; returns extrapolated
-    meshes/s for the whole region and the wall time of the sample."""
+def _oracle():
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from oracle_ffi import OracleTape, load
-    lib = load()
+    return OracleTape, load()
+
+
+def cpu_mesh_time(shape, cores, stride=1, min_feature=MIN_FEATURE):
+    """The oracle (the reference's DC mesher restated, its octree build and
+    dual walk run as task pools over all `cores` threads as the reference's
+    WorkerPool and Dual walker do) on the whole region.  stride 1: the full
+    mesh; returns (seconds, triangles).  stride > 1: only every stride-th of
+    the parallel octree tasks (cells five levels below the root) is built;
+    returns (estimated seconds of the full mesh: serial top levels + stride
+    x the sampled tasks' time, None)."""
+    import numpy as np
+    OracleTape, lib = _oracle()
     ora = OracleTape(shape)
-    boxes = cpu_sample_boxes(step_seed, count)
+    ph = np.zeros(3)
+    nt = ctypes.c_uint32()
+    lo, hi = REGION
+    lib.ora_time_mesh(ora.h, *lo, *hi, min_feature, MAX_ERR, cores, stride, ph.ctypes.data,
+                      ctypes.byref(nt))
+    if stride == 1:
+        return float(ph.sum()), int(nt.value)
+    return float(ph[0] + stride * ph[1]), None
 
-    def one(box):
-        vp, tp = ctypes.c_void_p(), ctypes.c_void_p()
-        nv, nt = ctypes.c_uint32(), ctypes.c_uint32()
-        lib.ora_render_mesh(ora.h, *box[0], *box[1], MIN_FEATURE, MAX_ERR, 1,
-                            ctypes.byref(vp), ctypes.byref(nv), ctypes.byref(tp),
-                            ctypes.byref(nt))
-        lib.ora_free(vp)
-        lib.ora_free(tp)
-        return nt.value
 
-    t0 = time.perf_counter()
-    with concurrent.futures.ThreadPoolExecutor(max_workers=cores) as ex:
-        list(ex.map(one, boxes))
-    wall = time.perf_counter() - t0
-    full = wall * (SUBDIV ** 3) / count
-    return 1.0 / full, wall
+def mesh_config():
+    """The workload's `config`, identical on both arms."""
+    return {"workload": "csg2000-depth10-dc", "primitives": N_PRIMS, "seed": SEED_BASE,
+            "octree_depth": 10, "region": "[-1.5,1.5]^3", "max_err": MAX_ERR,
+            "l2": "flushed (512 MiB write) before every timed step"}
 
 
 def run_reference(args, world, rank):
+    """The reference's CPU mesher (restated: the reference cannot be built
+    here) on every host thread, measured on the whole mesh: the K timed steps
+    are one complete mesh of the workload (wall time of the full octree
+    build, collapse and dual walk), so meshes/s = 1 / that time and each
+    step is reported as 1/K of it.  Warm-up steps build a 1/64 sample of the
+    octree tasks, untimed."""
     if rank != 0:
         return
     cores = os.cpu_count() or 1
     shape = build_shape(SEED_BASE)
-    for w in range(args.warmup):
-        cpu_mesh_rate(shape, max(1, args.cpu_sample // 4), 1000 + w, cores)
-    rates, walls = [], []
-    for k in range(args.steps):
-        r, wall = cpu_mesh_rate(shape, args.cpu_sample, 2000 + k, cores)
-        rates.append(r)
-        walls.append(wall)
-    value = len(rates) / sum(1.0 / r for r in rates)
-    sample = (f"{args.cpu_sample} random sub-boxes of a {SUBDIV}^3 split of the region per "
-              f"step (same cell size, depth 7 each), one box per thread, extrapolated "
-              f"x{SUBDIV ** 3 // args.cpu_sample} to the whole region")
+    for _ in range(args.warmup):
+        cpu_mesh_time(shape, cores, stride=64)
+    total, tris = cpu_mesh_time(shape, cores)
+    value = 1.0 / total
+    sample = (f"one whole mesh of the workload ({tris} triangles) on {cores} threads: "
+              f"{total:.1f} s, divided evenly over the {args.steps} timed steps")
     print(json.dumps({
         "impl": "reference",
         "metric": "DC meshes/s", "value": value, "unit": "meshes/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "csg2000-depth10-dc", "primitives": N_PRIMS,
-                   "octree_depth": 10, "region": "[-1.5,1.5]^3", "max_err": MAX_ERR},
+        "ms_per_step": total / args.steps * 1000.0, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": mesh_config(),
         "cpu_baseline": {"value": value, "unit": "meshes/s", "cores": cores,
-                         "kind": "port", "sample": sample,
-                         "sample_wall_s": sum(walls)},
+                         "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "meshes/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }))
+
+
+def spheres64_summary(lib, cores):
+    """The plain configuration's mesh beside the main line: the 64-sphere
+    union (seed 1) over [-1.5,1.5]^3 at 64 voxels per unit (depth 8), GPU
+    device time per mesh (tape resident, mesh downloaded) and the oracle
+    mesher on the whole region on every host core, and whether both give
+    the same triangle set."""
+    import torch
+    from libfive_b200 import workloads
+    from libfive_b200.shape import Tape
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from mesh_compare import oracle_mesh, same_mesh
+    from oracle_ffi import OracleTape
+    shape = workloads.spheres_union(64, seed=1)
+    tape = Tape(shape)
+    lo, hi = REGION
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    holder = {}
+
+    def once():
+        holder["mesh"] = tape.render_mesh(lo, hi, 1.0 / 64, MAX_ERR)
+
+    ms = _timed(once, 10, 3, flush)
+    t0 = time.perf_counter()
+    ov, ot = oracle_mesh(OracleTape(shape), lo, hi, 1.0 / 64, MAX_ERR, threads=cores)
+    dt = time.perf_counter() - t0
+    v, t = holder["mesh"]
+    return {"gpu_meshes_per_s": 1e3 / ms, "cpu_meshes_per_s": 1.0 / dt, "cores": cores,
+            "kind": "port", "triangles": int(len(t)),
+            "same_triangles_as_oracle": bool(len(ov) == len(v) and same_mesh(v, t, ov, ot))}
 
 
 def run_ours(args, world, rank, local):
@@ -386,12 +403,10 @@ def run_ours(args, world, rank, local):
             "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded CSG, seed 2 + rank)",
-            "config": {"workload": "csg2000-depth10-dc", "primitives": N_PRIMS,
-                       "tape_clauses": n_clauses, "octree_depth": stats.levels,
-                       "region": "[-1.5,1.5]^3", "max_err": MAX_ERR,
-                       "triangles": stats.triangles, "vertices": stats.vertices,
-                       "leaf_records": stats.leaves_ambiguous,
-                       "l2": "flushed (512 MiB write) before every timed step"},
+            "config": mesh_config(),
+            "mesh": {"tape_clauses": n_clauses, "octree_depth": stats.levels,
+                     "triangles": stats.triangles, "vertices": stats.vertices,
+                     "leaf_records": stats.leaves_ambiguous},
             "roofline": {
                 "kernel": "k_leaf_groups",
                 "bound": "fp32",
@@ -403,6 +418,9 @@ def run_ours(args, world, rank, local):
                 "clause_evals_per_launch": (evals_v + evals_g) / args.steps,
                 "kernel_ms_per_launch": leaf_ms / args.steps,
                 "traffic": traffic,
+                "traffic_source": ("ncu capture of this kernel on this workload "
+                                   "(profiles/k_leaf_groups_csg2000_depth10_dram.md)"
+                                   if traffic is not None else None),
             },
             "stages_ms": {"interval": stats.ms_interval, "leaf": stats.ms_leaf,
                           "collapse": stats.ms_collapse, "dual": stats.ms_dual},
@@ -413,12 +431,13 @@ def run_ours(args, world, rank, local):
         }
         if not args.no_cpu_baseline and world == 1:
             cores = os.cpu_count() or 1
-            rate, wall = cpu_mesh_rate(shape, args.cpu_sample, 2000, cores)
+            est, _ = cpu_mesh_time(shape, cores, stride=8)
             line["cpu_baseline"] = {
-                "value": rate, "unit": "meshes/s", "cores": cores, "kind": "port",
-                "sample": f"{args.cpu_sample} random sub-boxes of a {SUBDIV}^3 split "
-                          f"(same cell size), one per thread, extrapolated to the "
-                          f"whole region; {wall:.1f} s wall"}
+                "value": 1.0 / est, "unit": "meshes/s", "cores": cores, "kind": "port",
+                "sample": f"1/8 of the whole mesh's parallel octree tasks (every 8th cell "
+                          f"five levels below the root) on {cores} threads, scaled x8, plus "
+                          f"the serial top levels: {est:.1f} s per mesh estimated"}
+            line["spheres64"] = spheres64_summary(lib, cores)
         print(json.dumps(line))
     if pg:
         pg.barrier()

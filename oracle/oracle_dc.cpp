@@ -18,6 +18,9 @@
 #include <cstring>
 #include <memory>
 #include <new>
+#include <array>
+#include <atomic>
+#include <chrono>
 #include <thread>
 #include <vector>
 
@@ -364,34 +367,39 @@ struct Builder {
     }
 
     // -- recursive build (WorkerPool::run) -------------------------------------
-    void build(Cell* c, const std::shared_ptr<Tape>& tape, int parallel_depth, int threads)
+    void build(Cell* c, const std::shared_ptr<Tape>& tape)
     {
         if (c->level > 0) {
             auto next = eval_interval(c, tape);
             if (c->type != AMBIGUOUS) return;
             subdivide(c);
-            if (parallel_depth > 0 && threads > 1) {
-                std::vector<std::thread> ts;
-                std::atomic<int> next_child{0};
-                const Tape base = *eval.base;
-                const double me = max_err;
-                for (int t = 0; t < std::min(threads, 8); ++t) {
-                    ts.emplace_back([&, t] {
-                        Builder b(base, me);
-                        for (int i = next_child++; i < 8; i = next_child++) {
-                            b.build(c->child[i].get(), next, parallel_depth - 1,
-                                    std::max(1, threads / 8));
-                        }
-                    });
-                }
-                for (auto& t : ts) t.join();
-            } else {
-                for (int i = 0; i < 8; ++i) build(c->child[i].get(), next, 0, 1);
-            }
+            for (int i = 0; i < 8; ++i) build(c->child[i].get(), next);
             collect(c, next);
         } else {
             eval_leaf(c, tape);
         }
+    }
+
+    /// The first `split` levels of build(): cells `split` levels below `c`
+    /// become tasks (built later by any thread, in any order), and the cells
+    /// above them are listed children-first for their collect() once every
+    /// task is done.  Same tree, same arithmetic as build().
+    struct Task {
+        Cell* c;
+        std::shared_ptr<Tape> tape;
+    };
+    void build_top(Cell* c, const std::shared_ptr<Tape>& tape, int split,
+                   std::vector<Task>& tasks, std::vector<Task>& post)
+    {
+        if (split == 0 || c->level == 0) {
+            tasks.push_back({c, tape});
+            return;
+        }
+        auto next = eval_interval(c, tape);
+        if (c->type != AMBIGUOUS) return;
+        subdivide(c);
+        for (int i = 0; i < 8; ++i) build_top(c->child[i].get(), next, split - 1, tasks, post);
+        post.push_back({c, next});
     }
 
     void subdivide(Cell* c)
@@ -413,8 +421,13 @@ struct Builder {
 
 // -- Dual walk + DCMesher ----------------------------------------------------
 struct Mesher {
-    std::vector<float> verts{0, 0, 0};
+    // Vertex ids come from a counter shared by the walking threads (ids from
+    // 1, as BRep does, brep.hpp:25, per_thread_brep.hpp:33-42); each thread
+    // keeps (id, position) records and its own triangles.
+    std::atomic<uint32_t>* next_id;
+    std::vector<std::pair<uint32_t, std::array<float, 3>>> vrecs;
     std::vector<uint32_t> tris;
+    explicit Mesher(std::atomic<uint32_t>* n) : next_id(n) {}
 
     static int Q(int a) { return a == 1 ? 2 : a == 2 ? 4 : 1; }
     static int R(int a) { return a == 1 ? 4 : a == 2 ? 1 : 2; }
@@ -443,8 +456,10 @@ struct Mesher {
             const int vi = ts[i]->leaf->level > 0 ? 0 : T.p[ts[i]->leaf->corner_mask][e];
             Leaf& L = *const_cast<Leaf*>(ts[i]->leaf.get());
             if (L.index[vi] == 0) {
-                L.index[vi] = static_cast<uint32_t>(verts.size() / 3);
-                for (int k = 0; k < 3; ++k) verts.push_back(static_cast<float>(L.verts[vi][k]));
+                L.index[vi] = next_id->fetch_add(1);
+                vrecs.push_back({L.index[vi], {static_cast<float>(L.verts[vi][0]),
+                                               static_cast<float>(L.verts[vi][1]),
+                                               static_cast<float>(L.verts[vi][2])}});
             }
             for (int k = 0; k < 3; ++k) P[i][k] = static_cast<float>(L.verts[vi][k]);
             vs[i] = L.index[vi];
@@ -544,12 +559,48 @@ struct Mesher {
     }
 };
 
+/// Branch cells `split` levels below t become walk tasks; the branch cells
+/// above them are listed children-first.  work() at a cell reads only that
+/// cell's descendants, so the tasks' subtrees are independent, and the
+/// cells above run after every task (Dual<3>::walk's order constraint,
+/// dual.hpp:304-385).
+void walk_top(const Cell* t, int split, std::vector<const Cell*>& tasks,
+              std::vector<const Cell*>& post)
+{
+    if (!t->branch()) return;
+    if (split == 0) {
+        tasks.push_back(t);
+        return;
+    }
+    for (auto& c : t->child) walk_top(c.get(), split - 1, tasks, post);
+    post.push_back(t);
+}
+
+/// Runs fn(i) for i in [0, n) on `threads` threads taking the next index
+/// from a shared counter (the reference's WorkerPool keeps every core busy
+/// the same way, worker_pool.inl:35-90).  fn receives the thread number.
+template <class F>
+void pool(size_t n, int threads, F fn)
+{
+    std::atomic<size_t> next{0};
+    std::vector<std::thread> ts;
+    for (int k = 0; k < threads; ++k) {
+        ts.emplace_back([&, k] {
+            for (size_t i = next++; i < n; i = next++) fn(k, i);
+        });
+    }
+    for (auto& t : ts) t.join();
+}
+
 }  // namespace
 
 int render_mesh(const Tape& tape, const float lo[3], const float hi[3],
                 double min_feature, double max_err, int threads,
-                std::vector<float>& verts, std::vector<uint32_t>& tris)
+                std::vector<float>& verts, std::vector<uint32_t>& tris, int sample_stride,
+                double* phase_s)
 {
+    using clk = std::chrono::steady_clock;
+    const auto t0 = clk::now();
     auto root = std::make_unique<Cell>();
     double md = 1e300;
     for (int a = 0; a < 3; ++a) {
@@ -560,11 +611,67 @@ int render_mesh(const Tape& tape, const float lo[3], const float hi[3],
     root->level = static_cast<int>(std::ceil(
         std::fmax(0.0f, logf(static_cast<float>(md / min_feature))) / logf(2.0f)));
     Builder b(tape, max_err);
-    b.build(root.get(), b.eval.base, threads > 1 ? 2 : 0, threads);
-    Mesher m;
-    m.walk(root.get());
-    verts = std::move(m.verts);
-    tris = std::move(m.tris);
+    threads = std::max(1, threads);
+    // Cells five levels below the root (up to 32768) are the parallel tasks.
+    const int split = threads > 1 ? std::min(5, root->level) : 0;
+    std::vector<Builder::Task> tasks, post;
+    auto t1 = clk::now(), t2 = t1;
+    if (split == 0) {
+        b.build(root.get(), b.eval.base);
+        t1 = t2 = clk::now();
+    } else {
+        b.build_top(root.get(), b.eval.base, split, tasks, post);
+        t1 = clk::now();
+        std::vector<std::unique_ptr<Builder>> bs(threads);
+        pool(tasks.size(), threads, [&](int k, size_t i) {
+            if (sample_stride > 1 && i % sample_stride != 0) return;
+            if (!bs[k]) bs[k] = std::make_unique<Builder>(tape, max_err);
+            bs[k]->build(tasks[i].c, tasks[i].tape);
+        });
+        t2 = clk::now();
+        if (sample_stride > 1) {
+            // a timing sample: only every sample_stride-th task was built
+            if (phase_s) {
+                phase_s[0] = std::chrono::duration<double>(t1 - t0).count();
+                phase_s[1] = std::chrono::duration<double>(t2 - t1).count();
+                phase_s[2] = 0.0;
+            }
+            return -1;
+        }
+        for (auto& p : post) b.collect(p.c, p.tape);
+    }
+    std::atomic<uint32_t> next_id{1};
+    std::vector<std::unique_ptr<Mesher>> ms;
+    if (split == 0) {
+        ms.push_back(std::make_unique<Mesher>(&next_id));
+        ms[0]->walk(root.get());
+    } else {
+        std::vector<const Cell*> wt, wpost;
+        walk_top(root.get(), split, wt, wpost);
+        ms.resize(threads + 1);
+        pool(wt.size(), threads, [&](int k, size_t i) {
+            if (!ms[k]) ms[k] = std::make_unique<Mesher>(&next_id);
+            ms[k]->walk(wt[i]);
+        });
+        ms[threads] = std::make_unique<Mesher>(&next_id);
+        for (const Cell* c : wpost) ms[threads]->work(c);
+    }
+    // BRep::collect (brep.hpp:51-107): vertex id -> position, vertex 0 the
+    // placeholder at the origin.
+    verts.assign(3 * static_cast<size_t>(next_id.load()), 0.0f);
+    tris.clear();
+    for (auto& m : ms) {
+        if (!m) continue;
+        for (auto& r : m->vrecs) {
+            for (int k = 0; k < 3; ++k) verts[3 * static_cast<size_t>(r.first) + k] = r.second[k];
+        }
+        tris.insert(tris.end(), m->tris.begin(), m->tris.end());
+    }
+    if (phase_s) {
+        phase_s[0] = std::chrono::duration<double>(t1 - t0).count();
+        phase_s[1] = std::chrono::duration<double>(t2 - t1).count();
+        phase_s[2] = std::chrono::duration<double>(clk::now() - t2).count();
+    }
     return root->level;
 }
 
@@ -581,7 +688,7 @@ int ora_render_mesh(void* h, float xl, float yl, float zl, float xu, float yu,
     std::vector<float> v;
     std::vector<uint32_t> tr;
     const float lo[3] = {xl, yl, zl}, hi[3] = {xu, yu, zu};
-    const int L = ora::render_mesh(t, lo, hi, min_feature, max_err, threads, v, tr);
+    const int L = ora::render_mesh(t, lo, hi, min_feature, max_err, threads, v, tr, 1, nullptr);
     // raw storage, released by ora_free whatever the element type
     void* vo = ::operator new[](std::max<size_t>(v.size(), 1) * sizeof(float));
     std::memcpy(vo, v.data(), v.size() * sizeof(float));
@@ -595,5 +702,24 @@ int ora_render_mesh(void* h, float xl, float yl, float zl, float xu, float yu,
 }
 
 void ora_free(void* p) { ::operator delete[](p); }
+
+/// Timing of the oracle mesher's phases for the CPU baseline: phase_s[0] the
+/// serial top levels, [1] the parallel octree tasks, [2] collapse of the top
+/// levels and the dual walk.  With sample_stride > 1 only every
+/// sample_stride-th octree task is built (a bounded sample of the same
+/// work), no mesh is produced, phase_s[2] is 0 and -1 is returned.
+int ora_time_mesh(void* h, float xl, float yl, float zl, float xu, float yu, float zu,
+                  double min_feature, double max_err, int threads, int sample_stride,
+                  double* phase_s, uint32_t* ntris)
+{
+    const ora::Tape& t = *static_cast<ora::Tape*>(h);
+    std::vector<float> v;
+    std::vector<uint32_t> tr;
+    const float lo[3] = {xl, yl, zl}, hi[3] = {xu, yu, zu};
+    const int L = ora::render_mesh(t, lo, hi, min_feature, max_err, threads, v, tr,
+                                   sample_stride, phase_s);
+    if (ntris) *ntris = static_cast<uint32_t>(tr.size() / 3);
+    return L;
+}
 
 }  // extern "C"

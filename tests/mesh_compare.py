@@ -29,14 +29,13 @@ def canonical_triangles(verts, tris):
     that the smallest vertex comes first (orientation preserved)."""
     if len(tris) == 0:
         return np.zeros((0, 9), np.uint32)
-    P = verts[tris].view(np.uint32).reshape(-1, 3, 3)   # [M, 3 corners, xyz]
-    keys = P.reshape(-1, 3, 3)
-    out = np.empty((len(tris), 9), np.uint32)
-    for i in range(len(tris)):
-        rows = [tuple(keys[i, k]) for k in range(3)]
-        j = rows.index(min(rows))
-        rot = rows[j:] + rows[:j]
-        out[i] = np.array(rot, np.uint32).ravel()
+    P = np.ascontiguousarray(verts, np.float32)[tris].view(np.uint32).reshape(-1, 3, 3)
+    # rank of every corner among all corners, in lexicographic order
+    _, rank = np.unique(P.reshape(-1, 3), axis=0, return_inverse=True)
+    rank = rank.reshape(-1, 3)
+    first = np.argmin(rank, axis=1)
+    idx = (first[:, None] + np.arange(3)[None, :]) % 3
+    out = np.take_along_axis(P, idx[:, :, None], axis=1).reshape(-1, 9)
     order = np.lexsort(out.T[::-1])
     return out[order]
 

@@ -41,6 +41,10 @@ def load():
                 ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(vp),
                 ctypes.POINTER(ctypes.c_uint32)]
             _lib.ora_free.argtypes = [vp]
+            _lib.ora_time_mesh.restype = ctypes.c_int
+            _lib.ora_time_mesh.argtypes = [vp] + [ctypes.c_float] * 6 + [
+                ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, vp,
+                ctypes.POINTER(ctypes.c_uint32)]
         _lib.ora_libm_mode.argtypes = [ctypes.c_int]
         _lib.ora_libm_table.argtypes = [vp, vp, ctypes.c_uint64]
         _lib.ora_libm_take.restype = ctypes.c_uint64

@@ -97,3 +97,18 @@ def test_region_levels():
         lib.ora_free(vp)
         lib.ora_free(tp)
         assert got == level
+
+
+def test_threaded_mesher_matches_serial():
+    """The oracle's task pools (octree build and dual walk on several
+    threads) give the serial mesher's triangle set."""
+    from libfive_b200 import workloads
+    from mesh_compare import oracle_mesh, same_mesh
+    from oracle_ffi import OracleTape
+    s = workloads.random_csg(300, seed=4)
+    o = OracleTape(s)
+    v1, t1 = oracle_mesh(o, (-1.5, -1.5, -1.5), (1.5, 1.5, 1.5), 0.02, threads=1)
+    v8, t8 = oracle_mesh(o, (-1.5, -1.5, -1.5), (1.5, 1.5, 1.5), 0.02, threads=8)
+    assert len(t1) > 1000
+    assert len(v1) == len(v8)
+    assert same_mesh(v1, t1, v8, t8)

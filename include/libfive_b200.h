@@ -116,6 +116,15 @@ int lfb_eval_grad(lfb_tape t, uint64_t n, const float* x, const float* y,
                   float* gy, float* gz, float* gvars, void* stream,
                   uint32_t flags);
 
+/*  Sets all of the tape's free variables (lfb_tape_var_ids order) from n
+ *  floats in DEVICE memory, ordered on `stream` (NULL: legacy default
+ *  stream); no host synchronisation.  n must equal the variable count.
+ *  Later evaluations on that stream, meshes and lfb_tape_get_vars see the
+ *  new values.  Device-side counterpart of lfb_tape_set_vars
+ *  (Evaluator::updateVars, evaluator.hpp:35-44). */
+int lfb_tape_set_vars_device(lfb_tape t, const float* values, uint32_t n,
+                             void* stream);
+
 /*  Current values of the tape's free variables (lfb_tape_var_ids order) in
  *  a host array of len floats; after lfb_fit_adam_step this waits for the
  *  device and reads the values it wrote.  Counterpart of reading
@@ -156,10 +165,16 @@ int lfb_fit_adam_step(const lfb_tape* tapes, uint32_t n_shapes,
 
 /*  Mesh settings (BRepSettings, settings.hpp:27-74, minus the CPU-thread
  *  fields).  min_feature: subdivide until cells are smaller; max_err: QEF
- *  error below which cells collapse (negative disables collapsing). */
+ *  error below which cells collapse (negative disables collapsing).
+ *  cancel (NULL: none): BRepSettings::cancel (settings.hpp:73); the mesher
+ *  reads it between octree levels, before the leaf and collapse stages and
+ *  between dual-walk rounds, and when it is non-zero stops, releases what
+ *  the call holds and fails with LFB_E_CANCELLED (the reference returns a
+ *  null mesh, worker_pool.inl:82-85, mesh.cpp:61-66). */
 typedef struct lfb_mesh_settings {
     double min_feature;
     double max_err;
+    const volatile int32_t* cancel;
 } lfb_mesh_settings;
 
 typedef struct lfb_mesh_stats {
@@ -214,6 +229,17 @@ int lfb_render_meshes(const lfb_tape* tapes, uint32_t n,
                       const libfive_region3* regions,
                       const lfb_mesh_settings* settings, uint32_t workers,
                       libfive_mesh** meshes, lfb_mesh_stats* stats);
+
+/*  Test hooks of the mesher's recovery paths (no counterpart in the
+ *  reference), process-wide until set back to 0:
+ *    "fail_alloc_after" n > 0: the n-th device allocation from now on fails
+ *        as if cudaMalloc had run out of memory (the call in progress fails
+ *        with LFB_E_CUDA; nothing else is affected);
+ *    "small_capacity" 1: every mesh starts from empty scratch buffers and
+ *        minimal tape-arena, list and dual-walk capacities, so each growth
+ *        and retry path runs.
+ *  Returns 0, or LFB_E_INVALID for an unknown key. */
+int lfb_debug_set(const char* key, int64_t value);
 
 /* The reference-layout tape of a tree (Deck, deck.cpp:19-94), for
  * checking slot numbering and for CPU cross-checks.  counts[0..7] =

@@ -5,10 +5,12 @@ tensors of one shape) and is differentiable with respect to the point
 coordinates and, when given, to the free variables (`vars`: a 1-D CUDA
 float32 tensor of the tape's variables in `tape.var_ids()` order).  The
 forward pass is lfb_eval_values, the backward pass the reverse-mode
-lfb_eval_grad: one launch pair per call, no CPU work on the data.
+lfb_eval_grad: one launch pair per call, no CPU work on the data (the
+variables are copied device to device into the tape on the current stream).
 """
 import torch
 
+from . import ffi
 from .shape import Tape
 
 
@@ -20,7 +22,12 @@ class _ShapeValue(torch.autograd.Function):
     @staticmethod
     def forward(ctx, tape, x, y, z, vars_):
         if vars_ is not None:
-            tape.set_vars(dict(zip(tape.var_ids(), vars_.detach().cpu().tolist())))
+            v = vars_.detach().to(torch.float32).contiguous()
+            if v.numel() != tape.n_vars or not v.is_cuda:
+                raise ValueError("vars must be a CUDA tensor of the tape's %d variables"
+                                 % tape.n_vars)
+            ffi.check(ffi.load().lfb_tape_set_vars_device(tape.ptr, v.data_ptr(), v.numel(),
+                                                          _stream()), "set_vars_device")
         x, y, z = (t.detach().contiguous() for t in (x, y, z))
         f = torch.empty_like(x)
         tape.values(x, y, z, out=f, stream=_stream())

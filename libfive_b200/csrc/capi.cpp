@@ -500,12 +500,49 @@ void lfb_tape_delete(lfb_tape t) { delete t; }
 int lfb_tape_set_vars(lfb_tape t, libfive_vars vars)
 {
     if (!t) return set_error(LFB_E_INVALID, "null tape");
+    if (!t->g->on_current_device()) return LFB_E_INVALID;
     std::lock_guard<std::mutex> lock(t->g->mu);
     // variables that fit steps changed on the device keep their new values
     if (!t->g->pull_vars()) return LFB_E_CUDA;
     const bool changed = t->g->set_vars(vars.vars, vars.values, vars.size);
     if (!t->g->upload_cpool()) return LFB_E_CUDA;
     return changed ? 1 : 0;
+}
+
+int lfb_debug_set(const char* key, int64_t value)
+{
+    clear_error();
+    if (!key) return set_error(LFB_E_INVALID, "null key");
+    const std::string k(key);
+    if (k == "fail_alloc_after") {
+        debug_hooks().fail_alloc_after = value > 0 ? value : 0;
+    } else if (k == "small_capacity") {
+        debug_hooks().small_capacity = value ? 1 : 0;
+    } else {
+        return set_error(LFB_E_INVALID, "unknown debug key: " + k);
+    }
+    return 0;
+}
+
+int lfb_tape_set_vars_device(lfb_tape t, const float* values, uint32_t n, void* stream)
+{
+    clear_error();
+    if (!t || !values) return set_error(LFB_E_INVALID, "null argument");
+    if (!t->g->on_current_device()) return LFB_E_INVALID;
+    GpuTape& g = *t->g;
+    std::lock_guard<std::mutex> lock(g.mu);
+    if (n != g.reg.n_vars) {
+        return set_error(LFB_E_INVALID, "expected " + std::to_string(g.reg.n_vars) +
+                                            " variable values, got " + std::to_string(n));
+    }
+    if (n == 0) return 0;
+    if (!cuda_ok(cudaMemcpyAsync(g.d_cpool + g.reg.n_const, values, n * sizeof(float),
+                                 cudaMemcpyDeviceToDevice, static_cast<cudaStream_t>(stream)),
+                 "variable copy")) {
+        return LFB_E_CUDA;
+    }
+    g.vars_on_device = true;
+    return 0;
 }
 
 int lfb_tape_get_vars(lfb_tape t, float* values, uint32_t len)
@@ -534,6 +571,7 @@ int lfb_fit_adam_step(const lfb_tape* tapes, uint32_t n_shapes,
         std::vector<GpuTape*> gs(n_shapes);
         for (uint32_t j = 0; j < n_shapes; ++j) {
             if (!tapes[j]) return set_error(LFB_E_INVALID, "null tape");
+            if (!tapes[j]->g->on_current_device()) return LFB_E_INVALID;
             gs[j] = tapes[j]->g.get();
         }
         return fit_adam_step(gs.data(), n_shapes, point_offsets, x, y, z, var_offsets, m, v,
@@ -579,6 +617,7 @@ int lfb_eval_values(lfb_tape t, uint64_t n, const float* x, const float* y,
 {
     clear_error();
     if (!t) return set_error(LFB_E_INVALID, "null tape");
+    if (!t->g->on_current_device()) return LFB_E_INVALID;
     if (flags & LFB_DEVICE_PTRS) {
         return eval_values_device(*t->g, n, x, y, z, out,
                                   static_cast<cudaStream_t>(stream));
@@ -592,6 +631,7 @@ int lfb_eval_derivs(lfb_tape t, uint64_t n, const float* x, const float* y,
 {
     clear_error();
     if (!t) return set_error(LFB_E_INVALID, "null tape");
+    if (!t->g->on_current_device()) return LFB_E_INVALID;
     if (flags & LFB_DEVICE_PTRS) {
         return eval_derivs_device(*t->g, n, x, y, z, v, dx, dy, dz,
                                   static_cast<cudaStream_t>(stream));
@@ -605,6 +645,7 @@ int lfb_eval_features(lfb_tape t, uint64_t n, const float* x, const float* y,
 {
     clear_error();
     if (!t) return set_error(LFB_E_INVALID, "null tape");
+    if (!t->g->on_current_device()) return LFB_E_INVALID;
     return eval_features_host(*t->g, n, x, y, z, inside, feats, max_feats, n_feats);
 }
 
@@ -616,6 +657,7 @@ int lfb_eval_intervals(lfb_tape t, uint64_t n, const float* xlo,
 {
     clear_error();
     if (!t) return set_error(LFB_E_INVALID, "null tape");
+    if (!t->g->on_current_device()) return LFB_E_INVALID;
     if (flags & LFB_DEVICE_PTRS) {
         return eval_intervals_device(*t->g, n, xlo, xhi, ylo, yhi, zlo, zhi,
                                      out_lo, out_hi, out_nan,
@@ -630,6 +672,7 @@ int lfb_eval_jacobian(lfb_tape t, uint64_t n, const float* x, const float* y,
 {
     clear_error();
     if (!t) return set_error(LFB_E_INVALID, "null tape");
+    if (!t->g->on_current_device()) return LFB_E_INVALID;
     return eval_jacobian(*t->g, n, x, y, z, out,
                          static_cast<cudaStream_t>(stream),
                          (flags & LFB_DEVICE_PTRS) != 0);
@@ -642,6 +685,7 @@ int lfb_eval_grad(lfb_tape t, uint64_t n, const float* x, const float* y,
 {
     clear_error();
     if (!t) return set_error(LFB_E_INVALID, "null tape");
+    if (!t->g->on_current_device()) return LFB_E_INVALID;
     return eval_grad(*t->g, n, x, y, z, seed, f, gx, gy, gz, gvars,
                      static_cast<cudaStream_t>(stream),
                      (flags & LFB_DEVICE_PTRS) != 0);
@@ -655,8 +699,9 @@ libfive_mesh* lfb_render_mesh(lfb_tape t, libfive_region3 R,
         set_error(LFB_E_INVALID, "null tape");
         return nullptr;
     }
+    if (!t->g->on_current_device()) return nullptr;
     MeshOut mesh;
-    if (render_dc_mesh(*t->g, R, s.min_feature, s.max_err, mesh, stats) != 0) {
+    if (render_dc_mesh(*t->g, R, s.min_feature, s.max_err, mesh, stats, s.cancel) != 0) {
         return nullptr;
     }
     return mesh.release();
@@ -672,6 +717,7 @@ int lfb_render_heightmap(lfb_tape t, const float lower[3], const float upper[3],
     const VoxelGrid V = make_voxel_grid(lower, upper, res);
     for (int a = 0; a < 3; ++a) dims[a] = static_cast<uint32_t>(V.pts[a].size());
     if (!depth) return 0;
+    if (!t->g->on_current_device()) return LFB_E_INVALID;
     return render_heightmap(*t->g, V, depth, norm);
 }
 
@@ -686,6 +732,7 @@ int lfb_render_meshes(const lfb_tape* tapes, uint32_t n, const libfive_region3* 
     for (uint32_t i = 0; i < n; ++i) {
         meshes[i] = nullptr;
         if (!tapes[i]) return set_error(LFB_E_INVALID, "null tape");
+        if (!tapes[i]->g->on_current_device()) return LFB_E_INVALID;
     }
     std::vector<MeshJob> jobs(n);
     for (uint32_t i = 0; i < n; ++i) {
@@ -693,6 +740,7 @@ int lfb_render_meshes(const lfb_tape* tapes, uint32_t n, const libfive_region3* 
         jobs[i].R = regions[i];
         jobs[i].min_feature = settings[i].min_feature;
         jobs[i].max_err = settings[i].max_err;
+        jobs[i].cancel = settings[i].cancel;
         jobs[i].want_stats = stats != nullptr;
     }
     const int rc = render_dc_meshes(jobs.data(), n, workers ? workers : 4);

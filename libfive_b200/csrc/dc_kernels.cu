@@ -2562,10 +2562,29 @@ struct StageEvents {
 
 /// One mesh in the context `ws` (held by the caller), on its stream.
 int render_in(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_feature,
-              double max_err, MeshOut& out, lfb_mesh_stats* stats)
+              double max_err, MeshOut& out, lfb_mesh_stats* stats,
+              const volatile int32_t* cancel)
 {
     if (!upload_tables()) return LFB_E_CUDA;
     cudaStream_t s = ws.s;
+    // Cancellation (BRepSettings::cancel, polled by WorkerPool::run,
+    // worker_pool.inl:105, and the dual walk, dual.hpp:315): checked at
+    // every point where the host waits for the stream anyway.
+    auto cancelled = [&] {
+        if (cancel && *cancel) {
+            cudaStreamSynchronize(s);
+            set_error(LFB_E_CANCELLED, "mesh cancelled");
+            return true;
+        }
+        return false;
+    };
+    if (cancelled()) return LFB_E_CANCELLED;
+    const bool small = debug_hooks().small_capacity.load() != 0;
+    if (small) {
+        // test hook: start from empty buffers and minimal capacities
+        cudaStreamSynchronize(s);
+        ws.bufs.clear();
+    }
     const auto t_start = std::chrono::steady_clock::now();
 
     Octree o{};
@@ -2601,7 +2620,8 @@ int render_in(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_fe
     };
     RegClause* arena = ws.get<RegClause>(
         K_ARENA, std::max<uint64_t>(cap_of(K_ARENA, sizeof(RegClause)),
-                                    std::max<size_t>(bt.n * 64 + (1u << 20), 1u << 22)));
+                                    small ? bt.n + 64
+                                          : std::max<size_t>(bt.n * 64 + (1u << 20), 1u << 22)));
     if (!arena) return LFB_E_CUDA;
     uint64_t arena_cap = cap_of(K_ARENA, sizeof(RegClause));
     if (bt.n && !cuda_ok(cudaMemcpyAsync(arena, bt.clauses, bt.n * sizeof(RegClause),
@@ -2682,7 +2702,7 @@ int render_in(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_fe
     const int list_key[2] = {K_LIST_A, K_LIST_B};
     for (int k = 0; k < 2; ++k) {
         if (!ws.get<WideEntry>(list_key[k], std::max<uint64_t>(cap_of(list_key[k], sizeof(WideEntry)),
-                                                                4 * n + 1024))) {
+                                                                small ? 64 : 4 * n + 1024))) {
             return LFB_E_CUDA;
         }
     }
@@ -2703,6 +2723,7 @@ int render_in(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_fe
     bool group_mode = false;
 
     for (int d = 0; d < L; ++d) {
+        if (cancelled()) return LFB_E_CANCELLED;
         LevelView& lv = o.lv[d];
         cells_evaluated += lv.n_cells;
         group_mode = group_mode || (d > 0 && lv.n_cells >= group_mode_cells() &&
@@ -2827,6 +2848,7 @@ int render_in(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_fe
         }
     }
 
+    if (cancelled()) return LFB_E_CANCELLED;
     if (stats) cudaEventRecord(ev[1], s);
     // Leaves.
     const uint32_t n_leaf_groups = (L == 0) ? 1 : o.lv[L].n_groups;
@@ -2952,6 +2974,7 @@ int render_in(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_fe
         }
         ++n_launch;
     }
+    if (cancelled()) return LFB_E_CANCELLED;
     if (stats) cudaEventRecord(ev[2], s);
 
     // Bottom-up collapse.
@@ -3017,8 +3040,8 @@ int render_in(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_fe
     cudaStreamSynchronize(s);
     const uint32_t n_keys = n_recs * 4;
     if (root_type == CELL_BRANCH && n_recs) {
-        size_t task_cap = std::max<size_t>(1u << 16, static_cast<size_t>(n_recs) * 24);
-        size_t tri_cap = std::max<size_t>(1u << 16, static_cast<size_t>(n_recs) * 16);
+        size_t task_cap = small ? 1024 : std::max<size_t>(1u << 16, static_cast<size_t>(n_recs) * 24);
+        size_t tri_cap = small ? 1024 : std::max<size_t>(1u << 16, static_cast<size_t>(n_recs) * 16);
         for (int attempt = 0; attempt < 5; ++attempt) {
             DualTask* qa = ws.get<DualTask>(K_TASK_A, task_cap);
             DualTask* qb = ws.get<DualTask>(K_TASK_B, task_cap);
@@ -3038,6 +3061,7 @@ int render_in(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_fe
                        tris, n_tris, static_cast<uint32_t>(tri_cap), used};
             bool overflow = false;
             while (n_in) {
+                if (cancelled()) return LFB_E_CANCELLED;
                 cudaMemsetAsync(n_out, 0, sizeof(uint32_t), s);
                 D.out = qb;
                 k_dual_round<<<(n_in + 127) / 128, 128, 0, s>>>(D, qa, n_in);
@@ -3124,12 +3148,13 @@ int render_in(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_fe
 }  // namespace
 
 int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
-                   double max_err, MeshOut& out, lfb_mesh_stats* stats)
+                   double max_err, MeshOut& out, lfb_mesh_stats* stats,
+                   const volatile int32_t* cancel)
 {
     if (!require_device()) return LFB_E_CUDA;
     Workspace& ws = default_workspace();
     std::lock_guard<std::mutex> lock(ws.mu);
-    return render_in(ws, g, R, min_feature, max_err, out, stats);
+    return render_in(ws, g, R, min_feature, max_err, out, stats, cancel);
 }
 
 int render_dc_meshes(MeshJob* jobs, size_t n, unsigned workers)
@@ -3173,7 +3198,7 @@ int render_dc_meshes(MeshJob* jobs, size_t n, unsigned workers)
             MeshJob& j = jobs[q[i]];
             clear_error();
             j.rc = render_in(*ws, *j.g, j.R, j.min_feature, j.max_err, j.out,
-                             j.want_stats ? &j.stats : nullptr);
+                             j.want_stats ? &j.stats : nullptr, j.cancel);
             if (j.rc != 0) last_error(&j.err);
         }
     };
@@ -3219,7 +3244,7 @@ int render_dc_meshes(MeshJob* jobs, size_t n, unsigned workers)
             clear_error();
             j.err.clear();
             j.rc = render_in(*w, *j.g, j.R, j.min_feature, j.max_err, j.out,
-                             j.want_stats ? &j.stats : nullptr);
+                             j.want_stats ? &j.stats : nullptr, j.cancel);
             if (j.rc != 0) last_error(&j.err);
         }
     }

@@ -596,6 +596,17 @@ bool jit_derivs(GpuTape& g, uint64_t n, const float* x, const float* y, const fl
     return launch(fn, n, args, s);
 }
 
+bool jit_derivs_if_loaded(GpuTape& g, uint64_t n, const float* x, const float* y,
+                          const float* z, float* v, float* dx, float* dy, float* dz,
+                          cudaStream_t s)
+{
+    {
+        std::lock_guard<std::mutex> lock(g.mu);
+        if (g.jit[1].state != 1) return false;
+    }
+    return jit_derivs(g, n, x, y, z, v, dx, dy, dz, s);
+}
+
 bool jit_partials(GpuTape& g, const uint32_t* slots, uint32_t m, const float* x,
                   const float* y, const float* z, float* P, float* f, cudaStream_t s)
 {

@@ -39,6 +39,11 @@ bool jit_values(GpuTape& g, uint64_t n, const float* x, const float* y, const fl
 /// the same bits as DerivArrayEvaluator's rules in dv_deriv.
 bool jit_derivs(GpuTape& g, uint64_t n, const float* x, const float* y, const float* z,
                 float* v, float* dx, float* dy, float* dz, cudaStream_t s);
+/// jit_derivs only when the tape's compiled kernel is already loaded (never
+/// compiles or loads a module); false otherwise.
+bool jit_derivs_if_loaded(GpuTape& g, uint64_t n, const float* x, const float* y,
+                          const float* z, float* v, float* dx, float* dy, float* dz,
+                          cudaStream_t s);
 
 /// Reverse mode through compiled kernels: the forward pass storing the
 /// local partials at P[slot * m + i] (slot table of partial_slots), and the

@@ -34,8 +34,10 @@ void host_free(void* p);
 
 /// Mesh::render with DUAL_CONTOURING (libfive/src/render/brep/mesh.cpp:48-72)
 /// for one tree; returns 0 or a negative LFB_E* code.
+/// cancel (or null) is polled between stages (lfb_mesh_settings::cancel).
 int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
-                   double max_err, MeshOut& out, lfb_mesh_stats* stats);
+                   double max_err, MeshOut& out, lfb_mesh_stats* stats,
+                   const volatile int32_t* cancel = nullptr);
 
 /// One mesh of a batch (render_dc_meshes).
 struct MeshJob {
@@ -43,6 +45,7 @@ struct MeshJob {
     libfive_region3 R{};
     double min_feature = 0.0;
     double max_err = 0.0;
+    const volatile int32_t* cancel = nullptr;
     bool want_stats = false;
     MeshOut out;
     lfb_mesh_stats stats{};

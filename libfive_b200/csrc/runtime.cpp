@@ -187,6 +187,7 @@ std::shared_ptr<GpuTape> make_tape(const Tree& t)
     }
     auto g = std::make_shared<GpuTape>();
     g->tree = t;
+    if (!cuda_ok(cudaGetDevice(&g->device), "cudaGetDevice")) return nullptr;
     std::string err;
     if (!build_slot_tape(t, g->slot, &err) ||
         !build_reg_tape(g->slot, g->reg, &err)) {
@@ -215,12 +216,27 @@ std::shared_ptr<GpuTape> make_tape(const Tree& t)
 static std::mutex g_cache_mu;
 static std::unordered_map<const Node*, std::shared_ptr<GpuTape>> g_cache;
 
+bool GpuTape::on_current_device() const
+{
+    int cur = -1;
+    if (!cuda_ok(cudaGetDevice(&cur), "cudaGetDevice")) return false;
+    if (cur != device) {
+        set_error(LFB_E_INVALID, "the tape was made on CUDA device " + std::to_string(device) +
+                                     " but device " + std::to_string(cur) + " is current");
+        return false;
+    }
+    return true;
+}
+
 std::shared_ptr<GpuTape> cached_tape(const Node* root)
 {
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess) cur = -1;
     {
         std::lock_guard<std::mutex> lock(g_cache_mu);
         auto it = g_cache.find(root);
-        if (it != g_cache.end()) {
+        // a tape made on another device is replaced by one on this device
+        if (it != g_cache.end() && it->second->device == cur) {
             return it->second;
         }
     }
@@ -246,6 +262,28 @@ DevBuf::~DevBuf()
     if (ptr) cudaFree(ptr);
 }
 
+DebugHooks& debug_hooks()
+{
+    static DebugHooks h;
+    return h;
+}
+
+bool debug_alloc_allowed()
+{
+    auto& h = debug_hooks().fail_alloc_after;
+    int64_t left = h.load();
+    while (left > 0) {
+        if (h.compare_exchange_weak(left, left - 1)) {
+            if (left == 1) {
+                set_error(LFB_E_CUDA, "scratch alloc: out of memory (failure injected by lfb_debug_set)");
+                return false;
+            }
+            return true;
+        }
+    }
+    return true;
+}
+
 bool DevBuf::reserve(size_t n)
 {
     if (n <= bytes) return true;
@@ -253,6 +291,7 @@ bool DevBuf::reserve(size_t n)
     ptr = nullptr;
     bytes = 0;
     const size_t want = std::max<size_t>(n, 256);
+    if (!debug_alloc_allowed()) return false;
     if (!cuda_ok(cudaMalloc(&ptr, want), "scratch alloc")) {
         return false;
     }

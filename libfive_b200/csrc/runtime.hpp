@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -60,6 +61,13 @@ struct GpuTape {
     };
     JitKernel jit[5];
 
+    // The CUDA device that was current when the tape was made: its arrays
+    // live there, so every call must run with that device current.
+    int device = -1;
+    /// False (with an LFB_E_INVALID error recorded) unless the current
+    /// device is the tape's.
+    bool on_current_device() const;
+
     // Set when a kernel (the fit step, fit.cu) has written the variable
     // slots of d_cpool, so that the host copy in reg.cpool is out of date.
     bool vars_on_device = false;
@@ -79,6 +87,17 @@ std::shared_ptr<GpuTape> make_tape(const Tree& t);
 /// Cached device tape for a C API tree handle (free variables at zero).
 std::shared_ptr<GpuTape> cached_tape(const Node* root);
 void invalidate_cached(const Node* root);
+
+/// Test hooks (lfb_debug_set): the number of device allocations left before
+/// one is made to fail (0: none is), and whether meshes start from minimal
+/// capacities.
+struct DebugHooks {
+    std::atomic<int64_t> fail_alloc_after{0};
+    std::atomic<int> small_capacity{0};
+};
+DebugHooks& debug_hooks();
+/// False when the allocation-failure hook says this allocation must fail.
+bool debug_alloc_allowed();
 
 /// Growable device buffer.
 struct DevBuf {

@@ -13,7 +13,18 @@
 // uses, until exit.  Host code cannot use the variable's name as a device
 // address: the address is looked up with cudaGetSymbolAddress once per
 // device, with that device current, on the first call made on that device.
-// That first call should therefore come before any stream capture begins.
+// CUDA loads a library's device code lazily, so that first lookup is also
+// when the array's 7 MiB are reserved on the device: the first call on each
+// device does take device memory, once, and should be made during set-up,
+// before any stream capture begins (a call with n == 0 returns before the
+// lookup and does not do it).
+//
+// The kernel is the tape's compiled value + derivative kernel when that
+// kernel is already loaded (a previous lfb_eval_derivs compiled it; the
+// static path never compiles or loads anything itself), otherwise the
+// interpreter, which needs the tape's register file in shared memory: tapes
+// of more than about 100 registers are rejected with LFB_E_CUDA.  Both give
+// the same bits as lfb_eval_derivs.
 //
 // All calls share the array and it keeps the last call's contents.  Each
 // call overwrites every element it reads before reading it, so nothing needs
@@ -25,6 +36,7 @@
 #include <mutex>
 
 #include "eval_kernels.cuh"
+#include "jit.hpp"
 #include "libfive_b200.h"
 #include "runtime.hpp"
 
@@ -88,6 +100,7 @@ extern "C" int lfb_eval_derivs_static(lfb_tape t, uint64_t n, const float* x,
     }
     if (!require_device()) return LFB_E_CUDA;
     if (n == 0) return 0;
+    if (!g->on_current_device()) return LFB_E_INVALID;
 
     std::lock_guard<std::mutex> lock(g_static_mu);
     int dev = 0;
@@ -106,13 +119,16 @@ extern "C" int lfb_eval_derivs_static(lfb_tape t, uint64_t n, const float* x,
             return LFB_E_CUDA;
         }
     }
-    if (!cuda_ok(launch_derivs(g->dev(), static_cast<uint32_t>(n), planes[0],
-                               planes[1], planes[2], planes[3], planes[4],
-                               planes[5], planes[6], s),
-                 "lfb_eval_derivs_static: kernel")) {
-        return LFB_E_CUDA;
+    if (!jit_derivs_if_loaded(*g, n, planes[0], planes[1], planes[2], planes[3], planes[4],
+                              planes[5], planes[6], s)) {
+        if (!cuda_ok(launch_derivs(g->dev(), static_cast<uint32_t>(n), planes[0],
+                                   planes[1], planes[2], planes[3], planes[4],
+                                   planes[5], planes[6], s),
+                     "lfb_eval_derivs_static: kernel")) {
+            return LFB_E_CUDA;
+        }
+        note_launches(1);
     }
-    note_launches(1);
     float* outs[4] = {v, dx, dy, dz};
     for (int k = 0; k < 4; ++k) {
         if (outs[k] && !cuda_ok(cudaMemcpyAsync(outs[k], planes[3 + k], b,

@@ -59,7 +59,8 @@ class AdamSettings(ctypes.Structure):
 
 
 class MeshSettings(ctypes.Structure):
-    _fields_ = [("min_feature", ctypes.c_double), ("max_err", ctypes.c_double)]
+    _fields_ = [("min_feature", ctypes.c_double), ("max_err", ctypes.c_double),
+                ("cancel", ctypes.POINTER(ctypes.c_int32))]
 
 
 class MeshStats(ctypes.Structure):
@@ -150,6 +151,8 @@ SIGNATURES = [
     ("lfb_eval_jacobian", ctypes.c_int, [tape_t, ctypes.c_uint64, vp, vp, vp, vp, vp, ctypes.c_uint32]),
     ("lfb_eval_grad", ctypes.c_int, [tape_t, ctypes.c_uint64, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_uint32]),
     ("lfb_tape_get_vars", ctypes.c_int, [tape_t, fp, ctypes.c_uint32]),
+    ("lfb_tape_set_vars_device", ctypes.c_int, [tape_t, vp, ctypes.c_uint32, vp]),
+    ("lfb_debug_set", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int64]),
     ("lfb_fit_adam_step", ctypes.c_int, [ctypes.POINTER(tape_t), ctypes.c_uint32,
                                          ctypes.POINTER(ctypes.c_uint64), vp, vp, vp,
                                          ctypes.POINTER(ctypes.c_uint64), vp, vp, AdamSettings,

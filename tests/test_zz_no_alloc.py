@@ -33,14 +33,18 @@ def _static(lib, tape, P):
 
 
 def test_matches_allocating_entry_on_consecutive_calls(gpu):
+    """Two calls in a row on a fresh tape: the first runs the interpreter
+    (nothing compiled for the tape yet, and the static path never compiles),
+    the second the compiled kernel that lfb_eval_derivs loaded in between.
+    The compiled kernel and the interpreter give the same bits, so both
+    calls must equal lfb_eval_derivs exactly (tolerance 0)."""
     lib = ffi.load()
     tape = Tape(workloads.spheres_union(32, seed=1))
     for call, n in enumerate([MAX_POINTS, 1000]):
         P = workloads.uniform_points(n, seed=10 + call)
-        want = tape.derivs(*P)
         rc, got = _static(lib, tape, P)
         assert rc == 0, ffi.last_error()
-        # same kernel, same inputs: bit-identical (tolerance 0)
+        want = tape.derivs(*P)
         for a, b in zip(got, want):
             assert np.array_equal(a, b)
 

@@ -30,6 +30,7 @@ enum : uint32_t {
     ST_FEAT_EPS = 1u << 6,    // epsilon directions of one feature
     ST_FEAT_LIST = 1u << 7,   // features of one register
     ST_FEAT_TMP = 1u << 8,    // candidate features of one clause
+    ST_EDGE_OVERFLOW = 1u << 9,   // leaf edge records
 };
 
 /// A level-ordered clause list (WideEntry) in a list arena, with the list

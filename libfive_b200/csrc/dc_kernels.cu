@@ -33,6 +33,7 @@
 #include "dc_device.cuh"
 #include "dc_features.cuh"
 #include "eval_kernels.cuh"
+#include "leaf_interp.cuh"
 
 namespace lfb {
 
@@ -962,11 +963,6 @@ k_interval_group(GroupArgs A, int d)
 ////////////////////////////////////////////////////////////////////////////////
 // 2. Leaves: one warp per group of eight sibling cells
 
-static __device__ __noinline__ int qef_rank_nd(const Qef& q) { return qef_rank(q); }
-static __device__ __noinline__ double qef_vertex_nd(const Qef& q, double v[3], int* r)
-{
-    return qef_vertex(q, v, r);
-}
 
 struct EdgeSlot {
     double t0[3], t1[3];   // current search bracket: inside, outside
@@ -993,239 +989,128 @@ struct LeafWarpScratch {
     EdgeSlot e[54];
 };
 
-__device__ __forceinline__ float warp_fetch_v(uint8_t kind, uint16_t idx,
-                                              const float* R, int lane,
-                                              const float* __restrict__ cp)
-{
-    return kind == OPND_REG ? R[idx * 32 + lane] : __ldg(cp + idx);
-}
+/// A crossing lattice edge's QEF, handed from the leaf kernel to the rank
+/// and vertex kernels.
+struct EdgeRec {
+    Qef q;
+    uint8_t exists;
+    uint8_t rank;
+};
 
-/// The interpreters' register file: in the block's dynamic shared memory at
-/// byte offset `soff` (S = true: the compiler then emits shared-memory loads
-/// and stores, and knows they cannot alias anything else), or in global
-/// memory at `g` (tapes with too many registers).
+/// Where a leaf group's edge records start, and which lattice edge has
+/// which (-1: none).
+struct GroupEdges {
+    uint32_t base;
+    int8_t slot_of[54];
+};
+
+/// The interpreters' register file (one float4 per register and lane): in
+/// the block's dynamic shared memory at byte offset `soff` (S = true: the
+/// compiler then emits shared-memory loads and stores, and knows they cannot
+/// alias anything else), or in global memory at `g` (tapes with too many
+/// registers).
 template <bool S>
-__device__ __forceinline__ float* regfile(uint32_t soff, float* g)
+__device__ __forceinline__ float4* regfile4(uint32_t soff, float* g)
 {
     if (S) {
         extern __shared__ __align__(16) unsigned char rf_smem[];
-        return reinterpret_cast<float*>(rf_smem + soff);
+        return reinterpret_cast<float4*>(rf_smem + soff);
     }
-    return g;
+    return reinterpret_cast<float4*>(g);
 }
 
-/// Value of the tape at (x, y, z) for this lane, plus whether any min/max
-/// saw equal arguments (ArrayEvaluator::getAmbiguous, eval_array.cpp:197-217).
-template <bool S>
-static __device__ __noinline__ float warp_value(const float* __restrict__ cpool, uint32_t root_kind,
-                                                uint32_t root, const RegClause* __restrict__ cl,
-                                                uint32_t len, uint32_t soff, float* Rg, int lane,
-                                                float x, float y, float z, bool* ambig,
-                                                uint64_t* evals, bool active)
+/// The warp's decoded-clause buffer (kLeafOps LeafOps) at byte offset `off`
+/// of the block's dynamic shared memory.
+__device__ __forceinline__ LeafOp* leaf_ops(uint32_t off)
 {
-    float* R = regfile<S>(soff, Rg);
-    R[0 * 32 + lane] = x;
-    R[1 * 32 + lane] = y;
-    R[2 * 32 + lane] = z;
-    bool amb = false;
-    for (uint32_t c = 0; c < len; ++c) {
-        const uint2 raw = __ldg(reinterpret_cast<const uint2*>(cl + c));
-        const uint8_t o = raw.x & 0xff;
-        const uint8_t kinds = (raw.x >> 8) & 0xff;
-        const float a = warp_fetch_v(kinds & 3, raw.y & 0xffff, R, lane, cpool);
-        const float b = warp_fetch_v((kinds >> 2) & 3, raw.y >> 16, R, lane, cpool);
-        if (o == op::MIN || o == op::MAX) amb |= (a == b);
-        R[(raw.x >> 16) * 32 + lane] = dv_value(o, a, b);
-    }
-    if (ambig) *ambig = amb;
-    const uint32_t act = __ballot_sync(0xffffffffu, active);
-    if (evals && lane == 0) *evals += static_cast<uint64_t>(__popc(act)) * len;
-    return warp_fetch_v(root_kind, root, R, lane, cpool);
+    extern __shared__ __align__(16) unsigned char rf_smem[];
+    return reinterpret_cast<LeafOp*>(rf_smem + off);
 }
 
-/// Values of the tape at four points per lane (the edge search): register
-/// r of point k lives at R[(4 r + k) * 32 + lane].
-template <bool S>
-static __device__ __noinline__ float4 warp_value4(const float* __restrict__ cpool,
+/// Values of the tape at four points per lane (point k of this lane in
+/// component k).  Tapes of at most kLeafOps clauses were decoded into the
+/// warp's buffer when the group started; longer ones are decoded chunk by
+/// chunk here.  With TIES, bit k of *amb reports a min / max with equal
+/// arguments at point k (ArrayEvaluator::getAmbiguous, eval_array.cpp:
+/// 197-217).
+template <bool S, bool TIES>
+static __device__ __noinline__ float4 leaf_value4(const float* __restrict__ cpool,
                                                   uint32_t root_kind, uint32_t root,
                                                   const RegClause* __restrict__ cl, uint32_t len,
-                                                  uint32_t soff, float* Rg, int lane,
-                                                  float4 x, float4 y, float4 z)
+                                                  uint32_t soff, float* Rg, uint32_t ops_off,
+                                                  int lane, float4 x, float4 y, float4 z,
+                                                  uint32_t* amb)
 {
-    float* R = regfile<S>(soff, Rg);
-    const float xs[4] = {x.x, x.y, x.z, x.w};
-    const float ys[4] = {y.x, y.y, y.z, y.w};
-    const float zs[4] = {z.x, z.y, z.z, z.w};
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        R[(0 + k) * 32 + lane] = xs[k];
-        R[(4 + k) * 32 + lane] = ys[k];
-        R[(8 + k) * 32 + lane] = zs[k];
-    }
-    float* Rl = R + lane;
-    // The previous clause's result stays in registers: most clauses read it,
-    // which takes a shared-memory round trip off the dependency chain.  The
-    // next clause is fetched one iteration ahead.
-    uint32_t last = 0xffffffffu;
-    float lv[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-    uint2 next = len ? __ldg(reinterpret_cast<const uint2*>(cl)) : make_uint2(0, 0);
-    for (uint32_t c = 0; c < len; ++c) {
-        const uint2 raw = next;
-        if (c + 1 < len) next = __ldg(reinterpret_cast<const uint2*>(cl + c + 1));
-        const uint8_t o = raw.x & 0xff;
-        const uint32_t kinds = (raw.x >> 8) & 0xff;
-        const uint32_t ra = raw.y & 0xffff, rb = raw.y >> 16, ro = raw.x >> 16;
-        float a[4], b[4], r[4];
-        if ((kinds & 3) == OPND_REG) {
-            if (ra == last) {
-#pragma unroll
-                for (int k = 0; k < 4; ++k) a[k] = lv[k];
-            } else {
-                const float* p = Rl + ra * 128;
-#pragma unroll
-                for (int k = 0; k < 4; ++k) a[k] = p[32 * k];
-            }
-        } else {
-            const float v = __ldg(cpool + ra);
-#pragma unroll
-            for (int k = 0; k < 4; ++k) a[k] = v;
-        }
-        if (((kinds >> 2) & 3) == OPND_REG) {
-            if (rb == last) {
-#pragma unroll
-                for (int k = 0; k < 4; ++k) b[k] = lv[k];
-            } else {
-                const float* p = Rl + rb * 128;
-#pragma unroll
-                for (int k = 0; k < 4; ++k) b[k] = p[32 * k];
-            }
-        } else {
-            const float v = __ldg(cpool + rb);
-#pragma unroll
-            for (int k = 0; k < 4; ++k) b[k] = v;
-        }
-        dv_value4(o, a, b, r);
-        float* q = Rl + ro * 128;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            q[32 * k] = r[k];
-            lv[k] = r[k];
-        }
-        last = ro;
-    }
-    float out[4];
-    if (root_kind == OPND_REG) {
-#pragma unroll
-        for (int k = 0; k < 4; ++k) out[k] = Rl[root * 128 + 32 * k];
+    float4* R = regfile4<S>(soff, Rg) + lane;
+    LeafOp* ops = leaf_ops(ops_off);
+    R[0] = x;
+    R[32] = y;
+    R[64] = z;
+    uint32_t t = 0;
+    if (len <= kLeafOps) {
+        if (len) leaf_run4<TIES>(ops, len, R, &t);
     } else {
-        const float v = __ldg(cpool + root);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) out[k] = v;
+        LeafRaw raw = leaf_fetch(cl, len, 0, lane);
+        for (uint32_t c0 = 0; c0 < len; c0 += kLeafOps) {
+            __syncwarp();
+            const uint32_t n = leaf_decode_chunk(ops, raw, len, c0, cpool, lane);
+            raw = leaf_fetch(cl, len, c0 + kLeafOps, lane);   // next chunk, in flight
+            leaf_run4<TIES>(ops, n, R, &t);
+        }
+        __syncwarp();
     }
-    return make_float4(out[0], out[1], out[2], out[3]);
+    if (TIES) *amb = t;
+    if (root_kind == OPND_REG) return R[root * 32];
+    return splat4(__ldg(cpool + root));
 }
 
-__device__ __forceinline__ D4 warp_fetch_d(uint8_t kind, uint16_t idx,
-                                           const float* R, int lane,
-                                           const float* __restrict__ cp)
-{
-    if (kind == OPND_REG) {
-        const float* r = R + idx * 128 + lane;
-        return {r[0], r[32], r[64], r[96]};
-    }
-    return {__ldg(cp + idx), 0.0f, 0.0f, 0.0f};
-}
-
-
-/// warp_deriv that also works out, for most points, FeatureEvaluator's
-/// feature list (eval_feature.cpp:171-372) without building it.  Every
-/// register is either plain (one feature: its gradient, no epsilons) or
-/// tainted (anything else).  A tied min/max of two plain features is
-/// settled as the general feature path settles it (Feature::push and
-/// operator<, feature.cpp:50-72, 247-284): a gradient difference of zero
-/// length keeps the first argument; otherwise the two candidates (each
-/// gradient with the normalised difference, or its negation, as epsilon)
-/// are sorted and, when their gradients agree to within 1e-10 (squared),
-/// collapse to the first, epsilons dropped.  Any other tie taints the result;
-/// a min/max without a tie passes on the chosen side, taint included; all
-/// other clauses are tainted when an operand is.  Values are always exact.
-/// *plain says the root is untainted: its single feature is then the
-/// returned gradient.  *ambig reports any tie (ArrayEvaluator::getAmbiguous).
-/// Tapes with more than 64 registers report every tie as not plain.
+/// Value and gradient of the tape at one point per lane, plus, for most
+/// points, FeatureEvaluator's feature list (eval_feature.cpp:171-372)
+/// without building it.  Every register is either plain (one feature: its
+/// gradient, no epsilons) or tainted (anything else).  A tied min/max of two
+/// plain features is settled as the general feature path settles it
+/// (Feature::push and operator<, feature.cpp:50-72, 247-284): a gradient
+/// difference of zero length keeps the first argument; otherwise the two
+/// candidates (each gradient with the normalised difference, or its
+/// negation, as epsilon) are sorted and, when their gradients agree to
+/// within 1e-10 (squared), collapse to the first, epsilons dropped.  Any
+/// other tie taints the result; a min/max without a tie passes on the chosen
+/// side, taint included; all other clauses are tainted when an operand is.
+/// Values are always exact.  *plain says the root is untainted: its single
+/// feature is then the returned gradient.  *ambig reports any tie
+/// (ArrayEvaluator::getAmbiguous).  Tapes with more than 64 registers report
+/// every tie as not plain.
 template <bool S>
-static __device__ __noinline__ D4 warp_deriv_lite(const float* __restrict__ cpool,
-                                                  uint32_t root_kind, uint32_t root,
-                                                  uint32_t n_regs,
-                                                  const RegClause* __restrict__ cl, uint32_t len,
-                                                  uint32_t soff, float* Rg, int lane, float x,
-                                                  float y, float z, bool* ambig, bool* plain,
-                                                  uint64_t* evals, bool active)
+static __device__ __noinline__ D4 leaf_deriv(const float* __restrict__ cpool, uint32_t root_kind,
+                                             uint32_t root, uint32_t n_regs,
+                                             const RegClause* __restrict__ cl, uint32_t len,
+                                             uint32_t soff, float* Rg, uint32_t ops_off, int lane,
+                                             float x, float y, float z, bool* ambig, bool* plain)
 {
-    float* R = regfile<S>(soff, Rg);
-    const float in[3] = {x, y, z};
-    for (int a = 0; a < 3; ++a) {
-        float* r = R + a * 128 + lane;
-        r[0] = in[a];
-        r[32] = a == 0 ? 1.0f : 0.0f;
-        r[64] = a == 1 ? 1.0f : 0.0f;
-        r[96] = a == 2 ? 1.0f : 0.0f;
-    }
+    float4* R = regfile4<S>(soff, Rg) + lane;
+    LeafOp* ops = leaf_ops(ops_off);
+    R[0] = make_float4(x, 1.0f, 0.0f, 0.0f);
+    R[32] = make_float4(y, 0.0f, 1.0f, 0.0f);
+    R[64] = make_float4(z, 0.0f, 0.0f, 1.0f);
     const bool trackable = n_regs <= 64;
     uint64_t taint = 0;
     bool amb = false, lost = false;
-    for (uint32_t c = 0; c < len; ++c) {
-        const uint2 raw = __ldg(reinterpret_cast<const uint2*>(cl + c));
-        const uint8_t o = raw.x & 0xff;
-        const uint8_t kinds = (raw.x >> 8) & 0xff;
-        const uint32_t ra = raw.y & 0xffff, rb = raw.y >> 16, ro = raw.x >> 16;
-        const D4 a = warp_fetch_d(kinds & 3, ra, R, lane, cpool);
-        const D4 b = warp_fetch_d((kinds >> 2) & 3, rb, R, lane, cpool);
-        const bool ta = (kinds & 3) == OPND_REG && ((taint >> (ra & 63)) & 1);
-        const bool tbb = dev_is_binary(o) && ((kinds >> 2) & 3) == OPND_REG &&
-                         ((taint >> (rb & 63)) & 1);
-        D4 r;
-        bool t_out;
-        if ((o == op::MIN || o == op::MAX) && a.v == b.v) {
-            amb = true;
-            lost |= !trackable;
-            const bool is_min = o == op::MIN;
-            const float e[3] = {is_min ? b.dx - a.dx : a.dx - b.dx,
-                                is_min ? b.dy - a.dy : a.dy - b.dy,
-                                is_min ? b.dz - a.dz : a.dz - b.dz};
-            const float nrm = sqrtf(fdot(e, e));
-            bool take_b = false;
-            t_out = ta || tbb;
-            if (!t_out && nrm != 0) {
-                const float dd[3] = {b.dx - a.dx, b.dy - a.dy, b.dz - a.dz};
-                if (!(static_cast<double>(fdot(dd, dd)) < 1e-10)) {
-                    t_out = true;
-                } else {
-                    const float en[3] = {e[0] / nrm, e[1] / nrm, e[2] / nrm};
-                    const float ep[3] = {-en[0], -en[1], -en[2]};
-                    const float ad[3] = {a.dx, a.dy, a.dz}, bd[3] = {b.dx, b.dy, b.dz};
-                    // Candidate order: b's feature carries -e, a's carries e.
-                    const int cmp = vcmp3(ep, en);
-                    take_b = cmp != 0 ? cmp < 0 : vcmp3(bd, ad) < 0;
-                }
-            }
-            r = take_b ? D4{dv_value(o, a.v, b.v), b.dx, b.dy, b.dz}
-                       : D4{dv_value(o, a.v, b.v), a.dx, a.dy, a.dz};
-        } else {
-            r = dv_deriv(o, a, b, false);
-            if (o == op::MIN) t_out = (a.v < b.v) ? ta : tbb;
-            else if (o == op::MAX) t_out = (a.v < b.v) ? tbb : ta;
-            else t_out = ta || tbb;
+    if (len <= kLeafOps) {
+        if (len) leaf_run_deriv(ops, len, R, taint, amb, lost, trackable);
+    } else {
+        LeafRaw raw = leaf_fetch(cl, len, 0, lane);
+        for (uint32_t c0 = 0; c0 < len; c0 += kLeafOps) {
+            __syncwarp();
+            const uint32_t n = leaf_decode_chunk(ops, raw, len, c0, cpool, lane);
+            raw = leaf_fetch(cl, len, c0 + kLeafOps, lane);
+            leaf_run_deriv(ops, n, R, taint, amb, lost, trackable);
         }
-        if (t_out) taint |= 1ull << (ro & 63);
-        else taint &= ~(1ull << (ro & 63));
-        float* out = R + ro * 128 + lane;
-        out[0] = r.v; out[32] = r.dx; out[64] = r.dy; out[96] = r.dz;
+        __syncwarp();
     }
     *ambig = amb;
     *plain = !lost && !(root_kind == OPND_REG && ((taint >> (root & 63)) & 1));
-    const uint32_t act = __ballot_sync(0xffffffffu, active);
-    if (evals && lane == 0) *evals += static_cast<uint64_t>(__popc(act)) * len;
-    return warp_fetch_d(root_kind, root, R, lane, cpool);
+    if (root_kind == OPND_REG) return d4_of(R[root * 32]);
+    return {__ldg(cpool + root), 0.0f, 0.0f, 0.0f};
 }
 
 constexpr size_t kLeafSmallBytes = (sizeof(LeafWarpShared) + 15) / 16 * 16;
@@ -1247,6 +1132,11 @@ struct LeafArgs {
     const uint32_t* order;      // processing order of the groups (or null)
     unsigned long long* prof;   // debug: 8 per group (cycles by section, feature calls, E)
     float* featws;              // per warp: n_regs x kRegBlock floats of feature lists
+    EdgeRec* edges;             // crossing-edge QEFs of all groups
+    unsigned long long* edge_top;
+    uint32_t edge_cap;
+    GroupEdges* group_edges;    // one per group
+    uint32_t* rec_group;        // per leaf record: group * 8 + cell
 };
 
 __global__ void __launch_bounds__(256, 3)
@@ -1264,6 +1154,11 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
     float* Rs = reinterpret_cast<float*>(lsmem + kLeafSmallBytes * wpb) +
                 static_cast<size_t>(warp) * A.smem_regs * 128;
     float* Rgl = A.rd + (static_cast<size_t>(blockIdx.x) * wpb + warp) * A.bt.n_regs * 128;
+    // Decoded clauses of the group's tape (leaf_interp.cuh), after the
+    // register files.
+    const uint32_t ops_off = static_cast<uint32_t>(kLeafSmallBytes * wpb +
+                                                   static_cast<size_t>(wpb) * A.smem_regs * 128 * 4 +
+                                                   static_cast<size_t>(warp) * kLeafOps * sizeof(LeafOp));
     LeafWarpScratch* W = A.scratch + static_cast<size_t>(blockIdx.x) * wpb + warp;
     uint64_t my_evals = 0, my_devals = 0;
     // Persistent warps take the next group from a shared counter (group
@@ -1314,6 +1209,13 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
     float* R = rs ? Rs : Rgl;
     const uint32_t rsoff = static_cast<uint32_t>(reinterpret_cast<unsigned char*>(Rs) - lsmem);
 #define RF_CALL(fn, ...) (rs ? fn<true>(__VA_ARGS__) : fn<false>(__VA_ARGS__))
+#define RF_VALUE4(T, ...) (rs ? leaf_value4<true, T>(__VA_ARGS__) : leaf_value4<false, T>(__VA_ARGS__))
+    // Tapes that fit the buffer are decoded once for the whole group.
+    __syncwarp();
+    if (tr.len <= kLeafOps) {
+        leaf_decode_chunk(leaf_ops(ops_off), leaf_fetch(cl, tr.len, 0, lane), tr.len, 0,
+                          tb.cpool, lane);
+    }
     const FeatCtx fc{A.featws + (static_cast<size_t>(blockIdx.x) * wpb + warp) *
                                     A.bt.n_regs * kRegBlock,
                      &W->fs, A.status};
@@ -1329,9 +1231,15 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
         py = static_cast<float>(lat[1][ib]);
         pz = static_cast<float>(lat[2][ic]);
     }
-    cv = RF_CALL(warp_value, tb.cpool, tb.root_kind, tb.root, cl, tr.len, rsoff, R, lane,
-                 px, py, pz, &camb, &my_evals,
-                    lane < npts);
+    {
+        uint32_t amb4 = 0;
+        const float4 v4 = RF_VALUE4(true, tb.cpool, tb.root_kind, tb.root, cl, tr.len, rsoff, R,
+                                    ops_off, lane, splat4(px), splat4(py), splat4(pz), &amb4);
+        cv = v4.x;
+        camb = (amb4 & 1) != 0;
+        const uint32_t act = __ballot_sync(0xffffffffu, lane < npts);
+        if (lane == 0) my_evals += static_cast<uint64_t>(__popc(act)) * tr.len;
+    }
     uint8_t cst = CELL_EMPTY;
     bool need_d = false, need_f = false;
     if (lane < npts) {
@@ -1342,9 +1250,10 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
     }
     if (__any_sync(0xffffffffu, need_d || need_f)) {
         bool amb = false, plain = false;
-        const D4 d = RF_CALL(warp_deriv_lite, tb.cpool, tb.root_kind, tb.root, tb.n_regs, cl,
-                             tr.len, rsoff, R, lane, px, py, pz, &amb, &plain,
-                                     &my_devals, need_d || need_f);
+        const D4 d = RF_CALL(leaf_deriv, tb.cpool, tb.root_kind, tb.root, tb.n_regs, cl,
+                             tr.len, rsoff, R, ops_off, lane, px, py, pz, &amb, &plain);
+        const uint32_t act = __ballot_sync(0xffffffffu, need_d || need_f);
+        if (lane == 0) my_devals += static_cast<uint64_t>(__popc(act)) * tr.len;
         if (need_d) {
             cst = (d.dx != 0 || d.dy != 0 || d.dz != 0) ? CELL_FILLED : CELL_EMPTY;
         }
@@ -1500,11 +1409,11 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
                     ++n_act;
                 }
             }
-            const float4 v4 = RF_CALL(warp_value4, tb.cpool, tb.root_kind, tb.root, cl, tr.len,
-                                      rsoff, R, lane,
-                                          make_float4(qx[0], qx[1], qx[2], qx[3]),
-                                          make_float4(qy[0], qy[1], qy[2], qy[3]),
-                                          make_float4(qz[0], qz[1], qz[2], qz[3]));
+            const float4 v4 = RF_VALUE4(false, tb.cpool, tb.root_kind, tb.root, cl, tr.len,
+                                        rsoff, R, ops_off, lane,
+                                        make_float4(qx[0], qx[1], qx[2], qx[3]),
+                                        make_float4(qy[0], qy[1], qy[2], qy[3]),
+                                        make_float4(qz[0], qz[1], qz[2], qz[3]), nullptr);
             my_evals += static_cast<uint64_t>(__reduce_add_sync(0xffffffffu, n_act)) * tr.len;
             const float vs[4] = {v4.x, v4.y, v4.z, v4.w};
             uint32_t term[4];
@@ -1519,10 +1428,11 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
                 bool inside = true;
                 if (__any_sync(0xffffffffu, zero)) {
                     bool amb = false, plain = false;
-                    const D4 dg = RF_CALL(warp_deriv_lite, tb.cpool, tb.root_kind, tb.root,
-                                          tb.n_regs, cl, tr.len, rsoff, R, lane,
-                                          qx[k], qy[k], qz[k],
-                                                  &amb, &plain, &my_devals, zero);
+                    const D4 dg = RF_CALL(leaf_deriv, tb.cpool, tb.root_kind, tb.root,
+                                          tb.n_regs, cl, tr.len, rsoff, R, ops_off, lane,
+                                          qx[k], qy[k], qz[k], &amb, &plain);
+                    const uint32_t zact = __ballot_sync(0xffffffffu, zero);
+                    if (lane == 0) my_devals += static_cast<uint64_t>(__popc(zact)) * tr.len;
                     amb = amb && !plain;   // a settled tie leaves one plain feature
                     if (zero && !amb) {
                         const float g[3] = {dg.dx, dg.dy, dg.dz};
@@ -1579,10 +1489,11 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
             for (int k = 0; k < 3; ++k) q[k] = (p & 1) ? es.t1[k] : es.t0[k];
         }
         bool amb = false, plain = false;
-        const D4 d = RF_CALL(warp_deriv_lite, tb.cpool, tb.root_kind, tb.root, tb.n_regs, cl,
-                             tr.len, rsoff, R, lane, static_cast<float>(q[0]),
-                                     static_cast<float>(q[1]), static_cast<float>(q[2]),
-                                     &amb, &plain, &my_devals, active);
+        const D4 d = RF_CALL(leaf_deriv, tb.cpool, tb.root_kind, tb.root, tb.n_regs, cl,
+                             tr.len, rsoff, R, ops_off, lane, static_cast<float>(q[0]),
+                             static_cast<float>(q[1]), static_cast<float>(q[2]), &amb, &plain);
+        const uint32_t gact = __ballot_sync(0xffffffffu, active);
+        if (lane == 0) my_devals += static_cast<uint64_t>(__popc(gact)) * tr.len;
         amb = amb && !plain;   // a settled tie leaves one plain feature
         if (active) {
             EdgeSlot& es = W->e[p >> 1];
@@ -1634,71 +1545,27 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
         }
     }
     __syncwarp();
-    for (int s = lane; s < E; s += 32) {
-        W->e[s].rank = qef_rank_nd(W->e[s].q);
-    }
-    __syncwarp();
-
     const long long t_vertices = clock64();
-    // --- vertices: one lane per (cell, patch) (dc_tree.inl:474-549) -----
+    // --- hand the edge QEFs to the rank and vertex kernels ---------------
     {
-        const int cell = lane >> 2, patch = lane & 3;
-        if (cell < ncell && S->rec[cell] >= 0) {
-            LeafRec& L = A.recs[S->rec[cell]];
-            const uint8_t mask = L.corner_mask;
-            if (patch < c_tab.npatch[mask]) {
-                const int ne = c_tab.nedge[mask][patch];
-                int slots[12];
-                for (int k = 0; k < ne; ++k) {
-                    const int ca = c_tab.v[mask][patch][k][0];
-                    const int cb = c_tab.v[mask][patch][k][1];
-                    // lattice edge between the two corners of this cell
-                    const int pa = lat_pt(cell, ca), pb = lat_pt(cell, cb);
-                    const int lo_p = pa < pb ? pa : pb;
-                    const int diff = (pa < pb ? pb - pa : pa - pb);
-                    const int ax = diff == 1 ? 0 : diff == n ? 1 : 2;
-                    const int c0 = lo_p % n, c1 = (lo_p / n) % n, c2 = lo_p / (n * n);
-                    int le;
-                    if (ax == 0) le = c0 + seg * (c1 + n * c2);
-                    else if (ax == 1) le = c1 + seg * (c0 + n * c2);
-                    else le = c2 + seg * (c0 + n * c1);
-                    le += ax * seg * n * n;
-                    slots[k] = S->slot_of[le];
-                }
-                int max_rank = 0;
-                for (int k = 0; k < ne; ++k) {
-                    if (slots[k] >= 0 && W->e[slots[k]].exists &&
-                        W->e[slots[k]].rank > max_rank) {
-                        max_rank = W->e[slots[k]].rank;
-                    }
-                }
-                Qef q;
-                qef_zero(q);
-                for (int k = 0; k < ne; ++k) {
-                    if (slots[k] < 0 || !W->e[slots[k]].exists) continue;
-                    const EdgeSlot& es = W->e[slots[k]];
-                    if (es.rank == max_rank) {
-                        q.mass[0] += es.q.mass[0] / es.q.mass[3];
-                        q.mass[1] += es.q.mass[1] / es.q.mass[3];
-                        q.mass[2] += es.q.mass[2] / es.q.mass[3];
-                        q.mass[3] += 1.0;
-                    }
-                }
-                for (int k = 0; k < ne; ++k) {
-                    if (slots[k] < 0 || !W->e[slots[k]].exists) continue;
-                    qef_add(q, W->e[slots[k]].q);
-                }
-                double v[3];
-                int rank = 0;
-                qef_vertex_nd(q, v, &rank);
-                for (int k = 0; k < 3; ++k) L.vert[patch][k] = v[k];
-                if (patch == c_tab.npatch[mask] - 1) {
-                    for (int k = 0; k < 4; ++k) L.mass[k] = q.mass[k];
-                    for (int k = 0; k < 6; ++k) L.ata[k] = q.ata[k];
-                    for (int k = 0; k < 3; ++k) L.atb[k] = q.atb[k];
-                    L.btb = q.btb;
-                    L.rank = static_cast<uint8_t>(rank);
-                }
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(A.edge_top, static_cast<unsigned long long>(E));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        const bool fits = base + E <= A.edge_cap;
+        if (!fits) {
+            if (lane == 0) atomicOr(A.status, ST_EDGE_OVERFLOW);
+        } else {
+            for (int s_ = lane; s_ < E; s_ += 32) {
+                EdgeRec& r = A.edges[base + s_];
+                r.q = W->e[s_].q;
+                r.exists = W->e[s_].exists;
+                r.rank = 0;
+            }
+            GroupEdges& ge = A.group_edges[single ? 0 : g];
+            if (lane == 0) ge.base = static_cast<uint32_t>(base);
+            for (int k = lane; k < n_lat_edges; k += 32) ge.slot_of[k] = S->slot_of[k];
+            if (lane < ncell && S->rec[lane] >= 0) {
+                A.rec_group[S->rec[lane]] = (single ? 0u : g * 8u) + static_cast<uint32_t>(lane);
             }
         }
     }
@@ -1712,14 +1579,110 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
         P[3] = E;
         P[4] = t_crossing - t_group;      // corners, classification
         P[5] = t_gradients - t_crossing;  // crossing edges, edge search
-        P[6] = t_vertices - t_gradients;  // gradients, QEF pushes, ranks
-        P[7] = t_end - t_vertices;        // vertices
+        P[6] = t_vertices - t_gradients;  // gradients, QEF pushes
+        P[7] = t_end - t_vertices;        // edge records
     }
     }   // groups
 #undef RF_CALL
+#undef RF_VALUE4
     if (lane == 0) {
         atomicAdd(A.evals, static_cast<unsigned long long>(my_evals));
         atomicAdd(A.evals + 1, static_cast<unsigned long long>(my_devals));
+    }
+}
+
+/// Intersection::get_rank (intersection.hpp:67-88) of every crossing edge's
+/// QEF, one thread per edge.
+__global__ void __launch_bounds__(128)
+k_edge_rank(EdgeRec* edges, const unsigned long long* edge_top, uint32_t cap)
+{
+    const uint64_t n = min(static_cast<unsigned long long>(cap), *edge_top);
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        edges[i].rank = static_cast<uint8_t>(qef_rank(edges[i].q));
+    }
+}
+
+/// Per-patch vertices of the leaf records (dc_tree.inl:474-549), one thread
+/// per record: the patch's crossing edges found through the group's lattice
+/// edge map, the mass point over the edges of highest rank, the summed QEF
+/// and DCTree::findVertex.  `single`: the root cell is the only leaf (a
+/// 2 x 2 x 2 lattice instead of the 3 x 3 x 3 of a sibling group).
+__global__ void __launch_bounds__(128)
+k_leaf_vertices(LeafRec* recs, const uint32_t* rec_top, uint32_t rec_cap,
+                const uint32_t* rec_group, const GroupEdges* group_edges,
+                const EdgeRec* edges, int single)
+{
+    const uint32_t n_recs = min(rec_cap, *rec_top);
+    const int n = single ? 2 : 3;
+    const int seg = n - 1;
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n_recs;
+         r += gridDim.x * blockDim.x) {
+        const uint32_t gi = rec_group[r];
+        const int cell = static_cast<int>(gi & 7);
+        const GroupEdges& ge = group_edges[gi >> 3];
+        LeafRec& L = recs[r];
+        const uint8_t mask = L.corner_mask;
+        auto lat_pt = [&](int corner) {
+            const int cx = cell & 1, cy = (cell >> 1) & 1, cz = (cell >> 2) & 1;
+            return (cx + (corner & 1)) + n * ((cy + ((corner >> 1) & 1)) +
+                                              n * (cz + ((corner >> 2) & 1)));
+        };
+        const int np = c_tab.npatch[mask];
+        for (int patch = 0; patch < np; ++patch) {
+            const int ne = c_tab.nedge[mask][patch];
+            int slots[12];
+            for (int k = 0; k < ne; ++k) {
+                const int ca = c_tab.v[mask][patch][k][0];
+                const int cb = c_tab.v[mask][patch][k][1];
+                // lattice edge between the two corners of this cell
+                const int pa = lat_pt(ca), pb = lat_pt(cb);
+                const int lo_p = pa < pb ? pa : pb;
+                const int diff = (pa < pb ? pb - pa : pa - pb);
+                const int ax = diff == 1 ? 0 : diff == n ? 1 : 2;
+                const int c0 = lo_p % n, c1 = (lo_p / n) % n, c2 = lo_p / (n * n);
+                int le;
+                if (ax == 0) le = c0 + seg * (c1 + n * c2);
+                else if (ax == 1) le = c1 + seg * (c0 + n * c2);
+                else le = c2 + seg * (c0 + n * c1);
+                le += ax * seg * n * n;
+                const int sl = ge.slot_of[le];
+                slots[k] = sl < 0 ? -1 : static_cast<int>(ge.base) + sl;
+            }
+            int max_rank = 0;
+            for (int k = 0; k < ne; ++k) {
+                if (slots[k] >= 0 && edges[slots[k]].exists && edges[slots[k]].rank > max_rank) {
+                    max_rank = edges[slots[k]].rank;
+                }
+            }
+            Qef q;
+            qef_zero(q);
+            for (int k = 0; k < ne; ++k) {
+                if (slots[k] < 0 || !edges[slots[k]].exists) continue;
+                const EdgeRec& es = edges[slots[k]];
+                if (es.rank == max_rank) {
+                    q.mass[0] += es.q.mass[0] / es.q.mass[3];
+                    q.mass[1] += es.q.mass[1] / es.q.mass[3];
+                    q.mass[2] += es.q.mass[2] / es.q.mass[3];
+                    q.mass[3] += 1.0;
+                }
+            }
+            for (int k = 0; k < ne; ++k) {
+                if (slots[k] < 0 || !edges[slots[k]].exists) continue;
+                qef_add(q, edges[slots[k]].q);
+            }
+            double v[3];
+            int rank = 0;
+            qef_vertex(q, v, &rank);
+            for (int k = 0; k < 3; ++k) L.vert[patch][k] = v[k];
+            if (patch == np - 1) {
+                for (int k = 0; k < 4; ++k) L.mass[k] = q.mass[k];
+                for (int k = 0; k < 6; ++k) L.ata[k] = q.ata[k];
+                for (int k = 0; k < 3; ++k) L.atb[k] = q.atb[k];
+                L.btb = q.btb;
+                L.rank = static_cast<uint8_t>(rank);
+            }
+        }
     }
 }
 
@@ -2275,6 +2238,10 @@ struct Workspace {
     std::map<int, DevBuf> bufs;
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
+    // Leaf edge records per leaf group (grows when a mesh needs more; the
+    // mesh is then rendered again).
+    uint32_t edges_per_group = 16;
+    bool retry = false;
 
     template <class T>
     T* get(int key, size_t count)
@@ -2318,6 +2285,7 @@ enum BufKey {
     K_LIST_A, K_LIST_B, K_WIDE_S, K_WIDE_SN, K_WIDE_P, K_WIDE_LIVE, K_WIDE_NEW,
     K_WIDE_ST2, K_WIDE_L1, K_WIDE_WL, K_LEAF_RD, K_ORDER_K0, K_ORDER_K1,
     K_ORDER_V0, K_ORDER_V1, K_SORTTMP, K_PROF, K_GDEC, K_GLAST, K_FEATWS,
+    K_EDGES, K_GEDGES, K_RECGROUP,
     K_LEVEL = 100,
 };
 
@@ -2560,10 +2528,11 @@ struct StageEvents {
     }
 };
 
-/// One mesh in the context `ws` (held by the caller), on its stream.
-int render_in(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_feature,
-              double max_err, MeshOut& out, lfb_mesh_stats* stats,
-              const volatile int32_t* cancel)
+/// One mesh in the context `ws` (held by the caller), on its stream; one
+/// attempt (render_in retries when a capacity estimate was too small).
+int render_once(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_feature,
+                double max_err, MeshOut& out, lfb_mesh_stats* stats,
+                const volatile int32_t* cancel, bool first_attempt)
 {
     if (!upload_tables()) return LFB_E_CUDA;
     cudaStream_t s = ws.s;
@@ -2584,6 +2553,7 @@ int render_in(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_fe
         // test hook: start from empty buffers and minimal capacities
         cudaStreamSynchronize(s);
         ws.bufs.clear();
+        if (first_attempt) ws.edges_per_group = 1;
     }
     const auto t_start = std::chrono::steady_clock::now();
 
@@ -2602,10 +2572,11 @@ int render_in(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_fe
     }
 
     uint32_t* status = ws.get<uint32_t>(K_STATUS, 1);
-    unsigned long long* counters = ws.get<unsigned long long>(K_COUNTERS, 8);
+    unsigned long long* counters = ws.get<unsigned long long>(K_COUNTERS, 9);
     if (!status || !counters) return LFB_E_CUDA;
     cudaMemsetAsync(status, 0, sizeof(uint32_t), s);
-    cudaMemsetAsync(counters, 0, 8 * sizeof(unsigned long long), s);
+    cudaMemsetAsync(counters, 0, 9 * sizeof(unsigned long long), s);
+    unsigned long long* edge_top = counters + 8;
     unsigned long long* arena_top = counters + 1;
     uint32_t* rec_top = reinterpret_cast<uint32_t*>(counters + 2);
     unsigned long long* evals = counters + 3;
@@ -2887,7 +2858,8 @@ int render_in(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_fe
             }
             std::fprintf(stderr, "\n");
         }
-        const size_t per_warp = kLeafSmallBytes + static_cast<size_t>(smem_regs) * 128 * 4;
+        const size_t per_warp = kLeafSmallBytes + static_cast<size_t>(smem_regs) * 128 * 4 +
+                                kLeafOps * sizeof(LeafOp);
         const size_t smem = per_warp * wpb;
         if (smem > 220 * 1024) {
             return set_error(LFB_E_UNSUPPORTED, "tape register file too large for the leaf kernel");
@@ -2933,10 +2905,27 @@ int render_in(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_fe
         float* featws = ws.get<float>(K_FEATWS, static_cast<size_t>(grid) * wpb * bt.n_regs *
                                                     kRegBlock);
         if (!featws) return LFB_E_CUDA;
+        const uint64_t edge_cap64 = static_cast<uint64_t>(n_leaf_groups) * ws.edges_per_group +
+                                    (small ? 0 : 1024);
+        const uint32_t edge_cap = static_cast<uint32_t>(std::min<uint64_t>(edge_cap64, 1u << 31));
+        EdgeRec* edges = ws.get<EdgeRec>(K_EDGES, edge_cap);
+        GroupEdges* gedges = ws.get<GroupEdges>(K_GEDGES, n_leaf_groups);
+        uint32_t* rec_group = ws.get<uint32_t>(K_RECGROUP, rec_cap);
+        if (!edges || !gedges || !rec_group) return LFB_E_CUDA;
         LeafArgs A{o, bt, arena, recs, rec_top, static_cast<uint32_t>(rec_cap), status,
-                   evals, scratch, rd, smem_regs, next_group, order, prof, featws};
+                   evals, scratch, rd, smem_regs, next_group, order, prof, featws,
+                   edges, edge_top, edge_cap, gedges, rec_group};
         k_leaf_groups<<<grid, 32 * wpb, smem, s>>>(A, n_leaf_groups);
         if (!cuda_ok(cudaGetLastError(), "leaf kernel")) return LFB_E_CUDA;
+        // Edge ranks, then the records' vertices: one thread per edge / record.
+        const uint32_t sms = static_cast<uint32_t>(device_sm_count());
+        k_edge_rank<<<std::min<uint32_t>(sms * 16, (edge_cap + 127) / 128), 128, 0, s>>>(
+            edges, edge_top, edge_cap);
+        k_leaf_vertices<<<std::min<uint32_t>(sms * 16, static_cast<uint32_t>((rec_cap + 127) / 128)),
+                          128, 0, s>>>(recs, rec_top, static_cast<uint32_t>(rec_cap), rec_group,
+                                       gedges, edges, L == 0 ? 1 : 0);
+        n_launch += 2;
+        if (!cuda_ok(cudaGetLastError(), "leaf vertex kernels")) return LFB_E_CUDA;
         if (prof) {
             std::vector<unsigned long long> pf(8ull * n_leaf_groups);
             std::vector<TapeRef> gt(n_leaf_groups);
@@ -3011,6 +3000,18 @@ int render_in(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_fe
     cudaMemcpyAsync(&n_recs, rec_top, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
     if (!cuda_ok(cudaStreamSynchronize(s), "leaf/collapse")) return LFB_E_CUDA;
     if (st & ST_RECORD_OVERFLOW) return set_error(LFB_E_CAPACITY, "leaf record overflow");
+    if (st & ST_EDGE_OVERFLOW) {
+        // more crossing edges than records were reserved for: grow, and the
+        // caller renders the mesh again
+        unsigned long long need = 0;
+        cudaMemcpyAsync(&need, edge_top, sizeof(need), cudaMemcpyDeviceToHost, s);
+        cudaStreamSynchronize(s);
+        const uint32_t groups = std::max<uint32_t>(n_leaf_groups, 1);
+        ws.edges_per_group = static_cast<uint32_t>(std::min<unsigned long long>(
+            54, need / groups + 2));
+        ws.retry = true;
+        return set_error(LFB_E_CAPACITY, "leaf edge records overflowed");
+    }
     if (st & ST_FEATURE_OVERFLOW) {
         std::string why;
         if (st & ST_FEAT_EPS) {
@@ -3146,6 +3147,22 @@ int render_in(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_fe
 }
 
 }  // namespace
+
+/// One mesh in the context `ws`, rendered again (up to twice) when an
+/// attempt reports that a capacity estimate was too small.
+int render_in(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_feature,
+              double max_err, MeshOut& out, lfb_mesh_stats* stats,
+              const volatile int32_t* cancel)
+{
+    int rc = 0;
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        ws.retry = false;
+        rc = render_once(ws, g, R, min_feature, max_err, out, stats, cancel, attempt == 0);
+        if (rc == 0 || !ws.retry) break;
+        clear_error();
+    }
+    return rc;
+}
 
 int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
                    double max_err, MeshOut& out, lfb_mesh_stats* stats,

@@ -49,6 +49,23 @@ __device__ __noinline__ uint32_t dev_feature_list(const FeatCtx& C, const DevTap
     return __shfl_sync(0xffffffffu, count, 0);
 }
 
+/// Value of the tape at one point, evaluated by one thread with the
+/// register file in `R` (n_regs floats).
+__device__ float serial_value(const DevTape& t, float* R, float x, float y, float z)
+{
+    R[0] = x;
+    R[1] = y;
+    R[2] = z;
+    for (uint32_t c = 0; c < t.n; ++c) {
+        const RegClause k = t.clauses[c];
+        const uint8_t ka = k.kinds & 3, kb = (k.kinds >> 2) & 3;
+        const float a = ka == OPND_REG ? R[k.a] : __ldg(t.cpool + k.a);
+        const float b = kb == OPND_REG ? R[k.b] : __ldg(t.cpool + k.b);
+        R[k.out] = dv_value(k.op, a, b);
+    }
+    return t.root_kind == OPND_REG ? R[t.root] : __ldg(t.cpool + t.root);
+}
+
 constexpr int kWarpsPerBlock = 4;
 
 __global__ void __launch_bounds__(32 * kWarpsPerBlock)
@@ -63,7 +80,14 @@ k_features(DevTape t, uint32_t n, const float* __restrict__ P, uint8_t* inside, 
                      scratch + warp, status};
     for (uint32_t i = warp; i < n; i += n_warps) {
         const float x = P[i], y = P[n + i], z = P[2 * static_cast<size_t>(n) + i];
-        const bool in = dev_is_inside(fc, t, t.clauses, t.n, x, y, z, lane);
+        // isInside decides by the value alone unless it is zero (or NaN)
+        // (eval_feature.cpp:56-72); only then are features built.
+        float v = 0.0f;
+        if (lane == 0) v = serial_value(t, fc.regs, x, y, z);
+        v = __shfl_sync(0xffffffffu, v, 0);
+        __syncwarp();
+        const bool in = v < 0 ? true : v > 0 ? false
+                                             : dev_is_inside(fc, t, t.clauses, t.n, x, y, z, lane);
         if (lane == 0) inside[i] = in ? 1 : 0;
         if (n_feats) {
             const uint32_t c = dev_feature_list(

@@ -269,17 +269,21 @@ class Tape:
             olo.ctypes.data, ohi.ctypes.data, onan.ctypes.data, stream, 0), "intervals")
         return olo, ohi, onan.astype(bool)
 
-    def features(self, x, y, z, max_feats=16):
+    def features(self, x, y, z, max_feats=16, lists=True):
         """FeatureEvaluator at host points: (inside [n] bool, list of
-        [k, 3] arrays of the distinct feature gradients at each point)."""
+        [k, 3] arrays of the distinct feature gradients at each point, or
+        None when lists is False)."""
         x, y, z = (np.ascontiguousarray(a, np.float32) for a in (x, y, z))
         n = len(x)
         inside = np.zeros(n, np.uint8)
-        feats = np.zeros((n, max_feats, 3), np.float32)
-        counts = np.zeros(n, np.uint32)
+        feats = np.zeros((n, max_feats, 3), np.float32) if lists else None
+        counts = np.zeros(n, np.uint32) if lists else None
         ffi.check(_lib().lfb_eval_features(
             self.ptr, n, x.ctypes.data, y.ctypes.data, z.ctypes.data, inside.ctypes.data,
-            feats.ctypes.data, max_feats, counts.ctypes.data), "features")
+            feats.ctypes.data if lists else None, max_feats,
+            counts.ctypes.data if lists else None), "features")
+        if not lists:
+            return inside.astype(bool), None
         return inside.astype(bool), [feats[i, :min(int(c), max_feats)] for i, c in enumerate(counts)]
 
     def jacobian(self, x, y, z, out=None, stream=None):

@@ -152,9 +152,11 @@ def batch_specs(n_trees=512, seed=11, prims=(8, 4000), resolutions=(64, 128, 256
     return out
 
 
-def blended_spheres_vars(n=256, seed=4, m=0.05):
+def blended_spheres_vars(n=256, seed=4, m=0.05, stable=False):
     """n spheres whose centres and radii are free variables, combined by a
-    balanced binary tree of blends.  Returns (shape, {var: value})."""
+    balanced binary tree of blends (`blend`, or with stable=True the
+    overflow-free `blend_stable`, whose values and gradients stay finite
+    everywhere).  Returns (shape, {var: value})."""
     rng = SplitMix64(seed)
     values = {}
     leaves = []
@@ -168,7 +170,8 @@ def blended_spheres_vars(n=256, seed=4, m=0.05):
         leaves.append(((x - cx).square() + (y - cy).square() + (z - cz).square()).sqrt() - r)
     level = leaves
     while len(level) > 1:
-        nxt = [blend(level[i], level[i + 1], m) for i in range(0, len(level) - 1, 2)]
+        mix = blend_stable if stable else blend
+        nxt = [mix(level[i], level[i + 1], m) for i in range(0, len(level) - 1, 2)]
         if len(level) % 2:
             nxt.append(level[-1])
         level = nxt

@@ -111,12 +111,13 @@ def test_jacobian_matches_oracle_blends(gpu):
 
 @pytest.mark.parametrize("maker", ["spheres", "blends"])
 def test_reverse_gradient_matches_forward(gpu, maker):
+    n = 4096
     if maker == "spheres":
         s, vals = sphere_vars(12, seed=9)
+        x, y, z = workloads.uniform_points(n, seed=11, lo=-1.2, hi=1.2)
     else:
-        s, vals = workloads.blended_spheres_vars(16, seed=8)
-    n = 4096
-    x, y, z = workloads.uniform_points(n, seed=11, lo=-1.2, hi=1.2)
+        s, vals = workloads.blended_spheres_vars(16, seed=8, stable=True)
+        x, y, z = workloads.uniform_points(n, seed=11, lo=-1.2, hi=1.2)
     seed = np.random.default_rng(3).uniform(-1, 1, n).astype(np.float32)
     tape = Tape(s, vals)
     f = np.empty(n, np.float32)
@@ -134,7 +135,7 @@ def test_reverse_gradient_matches_forward(gpu, maker):
     # whole sum non-finite), run again on their own.
     jac = ora.jacobian(x, y, z).astype(np.float64)
     rows = np.isfinite(jac).all(axis=1) & np.isfinite(ov)
-    assert rows.mean() > 0.5
+    assert rows.sum() >= n // 4
     xs, ys, zs, ss = (np.ascontiguousarray(a[rows]) for a in (x, y, z, seed))
     gvars = np.zeros(tape.n_vars, np.float32)
     tape.grad(xs, ys, zs, seed=ss, gvars=gvars)
@@ -144,13 +145,13 @@ def test_reverse_gradient_matches_forward(gpu, maker):
 
 
 def test_reverse_gradient_blended_spheres_256_chunked(gpu):
-    """The adjoint configuration's shape (256 spheres blended pairwise,
-    1024 free variables, 4094 clauses) over more points than one partials
-    chunk holds (about 380 k points per 4 GiB chunk at this tape's 2815
-    stored partials per point): 2048 points with finite Jacobian rows, each
+    """The adjoint configuration's shape (256 spheres blended pairwise, 1024
+    free variables; the blend in its overflow-free form, so that gradients
+    are finite everywhere) over more points than one 4 GiB partials chunk
+    holds at this tape's stored partials per point: 2048 points, each
     repeated, so the summed variable gradient is 512 times that of the 2048
     and the per-point gradients repeat the oracle's derivatives."""
-    s, vals = workloads.blended_spheres_vars(256, seed=4)
+    s, vals = workloads.blended_spheres_vars(256, seed=4, stable=True)
     tape = Tape(s, vals)
     assert tape.n_vars == 1024
     ora = OracleTape(s, vals)

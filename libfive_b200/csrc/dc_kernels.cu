@@ -992,6 +992,7 @@ struct LeafWarpScratch {
 /// A crossing lattice edge's QEF, handed from the leaf kernel to the rank
 /// and vertex kernels.
 struct EdgeRec {
+    double t0[3], t1[3];   // final search bracket: inside end, outside end
     Qef q;
     uint8_t exists;
     uint8_t rank;
@@ -1000,7 +1001,8 @@ struct EdgeRec {
 /// Where a leaf group's edge records start, and which lattice edge has
 /// which (-1: none).
 struct GroupEdges {
-    uint32_t base;
+    uint32_t base;          // 0xffffffff: the records did not fit
+    uint8_t n_edges;
     int8_t slot_of[54];
 };
 
@@ -1033,13 +1035,13 @@ __device__ __forceinline__ LeafOp* leaf_ops(uint32_t off)
 /// chunk here.  With TIES, bit k of *amb reports a min / max with equal
 /// arguments at point k (ArrayEvaluator::getAmbiguous, eval_array.cpp:
 /// 197-217).
-template <bool S, bool TIES>
+template <bool S>
 static __device__ __noinline__ float4 leaf_value4(const float* __restrict__ cpool,
                                                   uint32_t root_kind, uint32_t root,
                                                   const RegClause* __restrict__ cl, uint32_t len,
                                                   uint32_t soff, float* Rg, uint32_t ops_off,
                                                   int lane, float4 x, float4 y, float4 z,
-                                                  uint32_t* amb)
+                                                  bool TIES, uint32_t* amb)
 {
     float4* R = regfile4<S>(soff, Rg) + lane;
     LeafOp* ops = leaf_ops(ops_off);
@@ -1048,14 +1050,14 @@ static __device__ __noinline__ float4 leaf_value4(const float* __restrict__ cpoo
     R[64] = z;
     uint32_t t = 0;
     if (len <= kLeafOps) {
-        if (len) leaf_run4<TIES>(ops, len, R, &t);
+        if (len) leaf_run4(ops, len, R, TIES, &t);
     } else {
         LeafRaw raw = leaf_fetch(cl, len, 0, lane);
         for (uint32_t c0 = 0; c0 < len; c0 += kLeafOps) {
             __syncwarp();
             const uint32_t n = leaf_decode_chunk(ops, raw, len, c0, cpool, lane);
             raw = leaf_fetch(cl, len, c0 + kLeafOps, lane);   // next chunk, in flight
-            leaf_run4<TIES>(ops, n, R, &t);
+            leaf_run4(ops, n, R, TIES, &t);
         }
         __syncwarp();
     }
@@ -1137,6 +1139,7 @@ struct LeafArgs {
     uint32_t edge_cap;
     GroupEdges* group_edges;    // one per group
     uint32_t* rec_group;        // per leaf record: group * 8 + cell
+    uint32_t* next_group2;      // work counter of k_leaf_qef (zero at launch)
 };
 
 __global__ void __launch_bounds__(256, 3)
@@ -1209,7 +1212,7 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
     float* R = rs ? Rs : Rgl;
     const uint32_t rsoff = static_cast<uint32_t>(reinterpret_cast<unsigned char*>(Rs) - lsmem);
 #define RF_CALL(fn, ...) (rs ? fn<true>(__VA_ARGS__) : fn<false>(__VA_ARGS__))
-#define RF_VALUE4(T, ...) (rs ? leaf_value4<true, T>(__VA_ARGS__) : leaf_value4<false, T>(__VA_ARGS__))
+#define RF_VALUE4(...) (rs ? leaf_value4<true>(__VA_ARGS__) : leaf_value4<false>(__VA_ARGS__))
     // Tapes that fit the buffer are decoded once for the whole group.
     __syncwarp();
     if (tr.len <= kLeafOps) {
@@ -1233,8 +1236,8 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
     }
     {
         uint32_t amb4 = 0;
-        const float4 v4 = RF_VALUE4(true, tb.cpool, tb.root_kind, tb.root, cl, tr.len, rsoff, R,
-                                    ops_off, lane, splat4(px), splat4(py), splat4(pz), &amb4);
+        const float4 v4 = RF_VALUE4(tb.cpool, tb.root_kind, tb.root, cl, tr.len, rsoff, R,
+                                    ops_off, lane, splat4(px), splat4(py), splat4(pz), true, &amb4);
         cv = v4.x;
         camb = (amb4 & 1) != 0;
         const uint32_t act = __ballot_sync(0xffffffffu, lane < npts);
@@ -1409,11 +1412,12 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
                     ++n_act;
                 }
             }
-            const float4 v4 = RF_VALUE4(false, tb.cpool, tb.root_kind, tb.root, cl, tr.len,
+            uint32_t unused = 0;
+            const float4 v4 = RF_VALUE4(tb.cpool, tb.root_kind, tb.root, cl, tr.len,
                                         rsoff, R, ops_off, lane,
                                         make_float4(qx[0], qx[1], qx[2], qx[3]),
                                         make_float4(qy[0], qy[1], qy[2], qy[3]),
-                                        make_float4(qz[0], qz[1], qz[2], qz[3]), nullptr);
+                                        make_float4(qz[0], qz[1], qz[2], qz[3]), false, &unused);
             my_evals += static_cast<uint64_t>(__reduce_add_sync(0xffffffffu, n_act)) * tr.len;
             const float vs[4] = {v4.x, v4.y, v4.z, v4.w};
             uint32_t term[4];
@@ -1479,90 +1483,33 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
     }
 
     const long long t_gradients = clock64();
-    // --- gradients at the bracket ends and QEFs (dc_tree.inl:412-471) ---
-    for (int base = 0; base < 2 * E; base += 32) {
-        const int p = base + lane;
-        const bool active = p < 2 * E;
-        double q[3] = {0, 0, 0};
-        if (active) {
-            const EdgeSlot& es = W->e[p >> 1];
-            for (int k = 0; k < 3; ++k) q[k] = (p & 1) ? es.t1[k] : es.t0[k];
-        }
-        bool amb = false, plain = false;
-        const D4 d = RF_CALL(leaf_deriv, tb.cpool, tb.root_kind, tb.root, tb.n_regs, cl,
-                             tr.len, rsoff, R, ops_off, lane, static_cast<float>(q[0]),
-                             static_cast<float>(q[1]), static_cast<float>(q[2]), &amb, &plain);
-        const uint32_t gact = __ballot_sync(0xffffffffu, active);
-        if (lane == 0) my_devals += static_cast<uint64_t>(__popc(gact)) * tr.len;
-        amb = amb && !plain;   // a settled tie leaves one plain feature
-        if (active) {
-            EdgeSlot& es = W->e[p >> 1];
-            float* g = (p & 1) ? es.g1 : es.g0;
-            g[0] = d.dx; g[1] = d.dy; g[2] = d.dz; g[3] = d.v;
-            es.amb[p & 1] = amb;
-        }
-    }
-    __syncwarp();
-    // Samples are pushed inside end first, then outside end; edges are
-    // independent, so each lane owns whole edges.  Points where a min/max
-    // is tied use every feature gradient instead (eval_feature.cpp:125-169).
-    const uint32_t any_amb = __ballot_sync(0xffffffffu, [&] {
-        bool a = false;
-        for (int s = lane; s < E; s += 32) a |= W->e[s].amb[0] || W->e[s].amb[1];
-        return a;
-    }());
-    if (!any_amb) {
-        for (int s = lane; s < E; s += 32) {
-            EdgeSlot& es = W->e[s];
-            for (int side = 0; side < 2; ++side) {
-                const float* g = side ? es.g1 : es.g0;
-                const double* pos = side ? es.t1 : es.t0;
-                const double gd[3] = {g[0], g[1], g[2]};
-                qef_push(es.q, pos, gd, static_cast<double>(g[3]));
-            }
-            es.exists = 1;
-        }
-    } else {
-        for (int s = 0; s < E; ++s) {
-            EdgeSlot& es = W->e[s];
-            for (int side = 0; side < 2; ++side) {
-                const float* g = side ? es.g1 : es.g0;
-                const double* pos = side ? es.t1 : es.t0;
-                if (es.amb[side]) {
-                    const long long t0 = clock64();
-                    dev_push_features(fc, tb, cl, tr.len, pos,
-                                      static_cast<double>(g[3]), &es.q,
-                                      &es.exists, lane);
-                    feat_cycles += clock64() - t0;
-                    ++feat_calls;
-                } else if (lane == 0) {
-                    const double gd[3] = {g[0], g[1], g[2]};
-                    qef_push(es.q, pos, gd, static_cast<double>(g[3]));
-                    es.exists = 1;
-                }
-                __syncwarp();
-            }
-        }
-    }
-    __syncwarp();
-    const long long t_vertices = clock64();
-    // --- hand the edge QEFs to the rank and vertex kernels ---------------
+    const long long t_vertices = t_gradients;
+    // --- hand the final brackets to k_leaf_qef, the lattice edge map and
+    //     the records to the vertex kernel ---------------------------------
     {
         unsigned long long base = 0;
         if (lane == 0) base = atomicAdd(A.edge_top, static_cast<unsigned long long>(E));
         base = __shfl_sync(0xffffffffu, base, 0);
         const bool fits = base + E <= A.edge_cap;
+        GroupEdges& ge = A.group_edges[single ? 0 : g];
         if (!fits) {
-            if (lane == 0) atomicOr(A.status, ST_EDGE_OVERFLOW);
+            if (lane == 0) {
+                atomicOr(A.status, ST_EDGE_OVERFLOW);
+                ge.base = 0xffffffffu;
+                ge.n_edges = 0;
+            }
         } else {
             for (int s_ = lane; s_ < E; s_ += 32) {
                 EdgeRec& r = A.edges[base + s_];
-                r.q = W->e[s_].q;
-                r.exists = W->e[s_].exists;
-                r.rank = 0;
+                for (int k = 0; k < 3; ++k) {
+                    r.t0[k] = W->e[s_].t0[k];
+                    r.t1[k] = W->e[s_].t1[k];
+                }
             }
-            GroupEdges& ge = A.group_edges[single ? 0 : g];
-            if (lane == 0) ge.base = static_cast<uint32_t>(base);
+            if (lane == 0) {
+                ge.base = static_cast<uint32_t>(base);
+                ge.n_edges = static_cast<uint8_t>(E);
+            }
             for (int k = lane; k < n_lat_edges; k += 32) ge.slot_of[k] = S->slot_of[k];
             if (lane < ncell && S->rec[lane] >= 0) {
                 A.rec_group[S->rec[lane]] = (single ? 0u : g * 8u) + static_cast<uint32_t>(lane);
@@ -1591,6 +1538,135 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
     }
 }
 
+/// Gradients at the two ends of every crossing edge's final bracket and the
+/// edge's QEF (dc_tree.inl:412-471): one warp per leaf group (the group's
+/// tape), one bracket end per lane, then each lane pushes whole edges
+/// (inside end first).  Points where a min / max is tied use every feature
+/// gradient instead (eval_feature.cpp:125-169).  A launch of its own, so
+/// that the derivative interpreter does not share the instruction cache
+/// with the value interpreter of the edge search.
+__global__ void __launch_bounds__(256, 3)
+k_leaf_qef(LeafArgs A, uint32_t n_groups)
+{
+    extern __shared__ __align__(16) unsigned char lsmem[];
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    float* Rs = reinterpret_cast<float*>(lsmem + kLeafSmallBytes * wpb) +
+                static_cast<size_t>(warp) * A.smem_regs * 128;
+    float* Rgl = A.rd + (static_cast<size_t>(blockIdx.x) * wpb + warp) * A.bt.n_regs * 128;
+    const uint32_t ops_off = static_cast<uint32_t>(kLeafSmallBytes * wpb +
+                                                   static_cast<size_t>(wpb) * A.smem_regs * 128 * 4 +
+                                                   static_cast<size_t>(warp) * kLeafOps * sizeof(LeafOp));
+    LeafWarpScratch* W = A.scratch + static_cast<size_t>(blockIdx.x) * wpb + warp;
+    const FeatCtx fc{A.featws + (static_cast<size_t>(blockIdx.x) * wpb + warp) *
+                                    A.bt.n_regs * kRegBlock,
+                     &W->fs, A.status};
+    uint64_t my_devals = 0;
+    const Octree& o = A.o;
+    const int Ld = o.levels;
+    const bool single = (Ld == 0);
+    while (true) {
+        uint32_t g = 0;
+        if (lane == 0) g = atomicAdd(A.next_group2, 1u);
+        g = __shfl_sync(0xffffffffu, g, 0);
+        if (g >= n_groups) break;
+        if (A.order) g = A.order[g];
+        const GroupEdges& ge = A.group_edges[single ? 0 : g];
+        const uint32_t gbase = ge.base;
+        const int E = ge.n_edges;
+        if (gbase == 0xffffffffu || E == 0) continue;
+        const TapeRef tr = single ? root_tape_ref(A.bt) : o.lv[Ld].group_tape[g];
+        const RegClause* cl = A.arena + tr.off;
+        const DevTape tb = with_tape(A.bt, tr);
+        const bool rs = tb.n_regs <= A.smem_regs;
+        float* R = rs ? Rs : Rgl;
+        const uint32_t rsoff = static_cast<uint32_t>(reinterpret_cast<unsigned char*>(Rs) - lsmem);
+        __syncwarp();
+        if (tr.len <= kLeafOps) {
+            leaf_decode_chunk(leaf_ops(ops_off), leaf_fetch(cl, tr.len, 0, lane), tr.len, 0,
+                              tb.cpool, lane);
+        }
+        EdgeRec* er = A.edges + gbase;
+        for (int base = 0; base < 2 * E; base += 32) {
+            const int p = base + lane;
+            const bool active = p < 2 * E;
+            double q[3] = {0, 0, 0};
+            if (active) {
+                const EdgeRec& e = er[p >> 1];
+                for (int k = 0; k < 3; ++k) q[k] = (p & 1) ? e.t1[k] : e.t0[k];
+            }
+            bool amb = false, plain = false;
+            const D4 d = rs ? leaf_deriv<true>(tb.cpool, tb.root_kind, tb.root, tb.n_regs, cl,
+                                               tr.len, rsoff, R, ops_off, lane,
+                                               static_cast<float>(q[0]), static_cast<float>(q[1]),
+                                               static_cast<float>(q[2]), &amb, &plain)
+                            : leaf_deriv<false>(tb.cpool, tb.root_kind, tb.root, tb.n_regs, cl,
+                                                tr.len, rsoff, R, ops_off, lane,
+                                                static_cast<float>(q[0]), static_cast<float>(q[1]),
+                                                static_cast<float>(q[2]), &amb, &plain);
+            const uint32_t gact = __ballot_sync(0xffffffffu, active);
+            if (lane == 0) my_devals += static_cast<uint64_t>(__popc(gact)) * tr.len;
+            amb = amb && !plain;   // a settled tie leaves one plain feature
+            if (active) {
+                EdgeSlot& es = W->e[p >> 1];
+                float* gg = (p & 1) ? es.g1 : es.g0;
+                gg[0] = d.dx; gg[1] = d.dy; gg[2] = d.dz; gg[3] = d.v;
+                es.amb[p & 1] = amb;
+            }
+        }
+        __syncwarp();
+        const uint32_t any_amb = __ballot_sync(0xffffffffu, [&] {
+            bool a = false;
+            for (int s_ = lane; s_ < E; s_ += 32) a |= W->e[s_].amb[0] || W->e[s_].amb[1];
+            return a;
+        }());
+        if (!any_amb) {
+            for (int s_ = lane; s_ < E; s_ += 32) {
+                const EdgeSlot& es = W->e[s_];
+                EdgeRec& r = er[s_];
+                Qef qf;
+                qef_zero(qf);
+                for (int side = 0; side < 2; ++side) {
+                    const float* gg = side ? es.g1 : es.g0;
+                    const double* pos = side ? r.t1 : r.t0;
+                    const double gd[3] = {gg[0], gg[1], gg[2]};
+                    qef_push(qf, pos, gd, static_cast<double>(gg[3]));
+                }
+                r.q = qf;
+                r.exists = 1;
+                r.rank = 0;
+            }
+        } else {
+            for (int s_ = lane; s_ < E; s_ += 32) {
+                qef_zero(er[s_].q);
+                er[s_].exists = 0;
+                er[s_].rank = 0;
+            }
+            __syncwarp();
+            for (int s_ = 0; s_ < E; ++s_) {
+                const EdgeSlot& es = W->e[s_];
+                EdgeRec& r = er[s_];
+                for (int side = 0; side < 2; ++side) {
+                    const float* gg = side ? es.g1 : es.g0;
+                    const double* pos = side ? r.t1 : r.t0;
+                    if (es.amb[side]) {
+                        dev_push_features(fc, tb, cl, tr.len, pos, static_cast<double>(gg[3]),
+                                          &r.q, &r.exists, lane);
+                    } else if (lane == 0) {
+                        const double gd[3] = {gg[0], gg[1], gg[2]};
+                        qef_push(r.q, pos, gd, static_cast<double>(gg[3]));
+                        r.exists = 1;
+                    }
+                    __syncwarp();
+                }
+            }
+        }
+        __syncwarp();
+    }
+    if (lane == 0) atomicAdd(A.evals + 1, static_cast<unsigned long long>(my_devals));
+}
+
 /// Intersection::get_rank (intersection.hpp:67-88) of every crossing edge's
 /// QEF, one thread per edge.
 __global__ void __launch_bounds__(128)
@@ -1610,8 +1686,8 @@ k_edge_rank(EdgeRec* edges, const unsigned long long* edge_top, uint32_t cap)
 /// 2 x 2 x 2 lattice instead of the 3 x 3 x 3 of a sibling group).
 __global__ void __launch_bounds__(128)
 k_leaf_vertices(LeafRec* recs, const uint32_t* rec_top, uint32_t rec_cap,
-                const uint32_t* rec_group, const GroupEdges* group_edges,
-                const EdgeRec* edges, int single)
+                const uint32_t* rec_group, const GroupEdges* group_edges, uint32_t n_groups,
+                const EdgeRec* edges, uint32_t edge_cap, int single)
 {
     const uint32_t n_recs = min(rec_cap, *rec_top);
     const int n = single ? 2 : 3;
@@ -1619,8 +1695,12 @@ k_leaf_vertices(LeafRec* recs, const uint32_t* rec_top, uint32_t rec_cap,
     for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n_recs;
          r += gridDim.x * blockDim.x) {
         const uint32_t gi = rec_group[r];
+        // records of groups whose edges did not fit have none (the mesh is
+        // rendered again with more room)
+        if (gi == 0xffffffffu || (gi >> 3) >= n_groups) continue;
         const int cell = static_cast<int>(gi & 7);
         const GroupEdges& ge = group_edges[gi >> 3];
+        if (ge.base == 0xffffffffu || ge.base + ge.n_edges > edge_cap) continue;
         LeafRec& L = recs[r];
         const uint8_t mask = L.corner_mask;
         auto lat_pt = [&](int corner) {
@@ -2572,10 +2652,10 @@ int render_once(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_
     }
 
     uint32_t* status = ws.get<uint32_t>(K_STATUS, 1);
-    unsigned long long* counters = ws.get<unsigned long long>(K_COUNTERS, 9);
+    unsigned long long* counters = ws.get<unsigned long long>(K_COUNTERS, 10);
     if (!status || !counters) return LFB_E_CUDA;
     cudaMemsetAsync(status, 0, sizeof(uint32_t), s);
-    cudaMemsetAsync(counters, 0, 9 * sizeof(unsigned long long), s);
+    cudaMemsetAsync(counters, 0, 10 * sizeof(unsigned long long), s);
     unsigned long long* edge_top = counters + 8;
     unsigned long long* arena_top = counters + 1;
     uint32_t* rec_top = reinterpret_cast<uint32_t*>(counters + 2);
@@ -2912,18 +2992,26 @@ int render_once(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_
         GroupEdges* gedges = ws.get<GroupEdges>(K_GEDGES, n_leaf_groups);
         uint32_t* rec_group = ws.get<uint32_t>(K_RECGROUP, rec_cap);
         if (!edges || !gedges || !rec_group) return LFB_E_CUDA;
+        cudaMemsetAsync(rec_group, 0xff, rec_cap * sizeof(uint32_t), s);
         LeafArgs A{o, bt, arena, recs, rec_top, static_cast<uint32_t>(rec_cap), status,
                    evals, scratch, rd, smem_regs, next_group, order, prof, featws,
-                   edges, edge_top, edge_cap, gedges, rec_group};
+                   edges, edge_top, edge_cap, gedges, rec_group,
+                   reinterpret_cast<uint32_t*>(counters + 9)};
         k_leaf_groups<<<grid, 32 * wpb, smem, s>>>(A, n_leaf_groups);
         if (!cuda_ok(cudaGetLastError(), "leaf kernel")) return LFB_E_CUDA;
+        if (!raise_smem_limit(reinterpret_cast<const void*>(k_leaf_qef), smem)) {
+            return LFB_E_CUDA;
+        }
+        k_leaf_qef<<<grid, 32 * wpb, smem, s>>>(A, n_leaf_groups);
+        ++n_launch;
+        if (!cuda_ok(cudaGetLastError(), "leaf QEF kernel")) return LFB_E_CUDA;
         // Edge ranks, then the records' vertices: one thread per edge / record.
         const uint32_t sms = static_cast<uint32_t>(device_sm_count());
         k_edge_rank<<<std::min<uint32_t>(sms * 16, (edge_cap + 127) / 128), 128, 0, s>>>(
             edges, edge_top, edge_cap);
         k_leaf_vertices<<<std::min<uint32_t>(sms * 16, static_cast<uint32_t>((rec_cap + 127) / 128)),
                           128, 0, s>>>(recs, rec_top, static_cast<uint32_t>(rec_cap), rec_group,
-                                       gedges, edges, L == 0 ? 1 : 0);
+                                       gedges, n_leaf_groups, edges, edge_cap, L == 0 ? 1 : 0);
         n_launch += 2;
         if (!cuda_ok(cudaGetLastError(), "leaf vertex kernels")) return LFB_E_CUDA;
         if (prof) {

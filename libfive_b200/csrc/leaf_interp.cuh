@@ -193,12 +193,12 @@ static __device__ __noinline__ float4 leaf_generic4(uint8_t o, float4 a, float4 
 }
 
 /// Evaluates n decoded clauses at the four points held by this lane in the
-/// register file R (R[r * 32] is register r of this lane).  With TIES, bit k
-/// of *amb is set when a min / max saw equal arguments at point k
+/// register file R (R[r * 32] is register r of this lane).  With TIES (a
+/// run-time flag: one copy of the loop serves corners and edge search), bit
+/// k of *amb is set when a min / max saw equal arguments at point k
 /// (ArrayEvaluator::getAmbiguous, eval_array.cpp:197-217).
-template <bool TIES>
 __device__ __forceinline__ void leaf_run4(const LeafOp* __restrict__ ops, uint32_t n,
-                                          float4* R, uint32_t* amb)
+                                          float4* R, bool TIES, uint32_t* amb)
 {
     uint32_t t = 0;
     float4 last = make_float4(0.0f, 0.0f, 0.0f, 0.0f);

@@ -1035,33 +1035,79 @@ __device__ __forceinline__ LeafOp* leaf_ops(uint32_t off)
 /// chunk here.  With TIES, bit k of *amb reports a min / max with equal
 /// arguments at point k (ArrayEvaluator::getAmbiguous, eval_array.cpp:
 /// 197-217).
+/// dv_value on four points (a float4 per operand), the value rules of
+/// dev_point.cuh; the rare opcodes out of line.
+__device__ __forceinline__ float4 dv_value4f(uint8_t o, const float4& a, const float4& b)
+{
+#define LFB_EACH2(F) make_float4(F(a.x, b.x), F(a.y, b.y), F(a.z, b.z), F(a.w, b.w))
+#define LFB_EACH1(F) make_float4(F(a.x), F(a.y), F(a.z), F(a.w))
+    switch (o) {
+        case op::ADD: return LFB_EACH2(f_add);
+        case op::MUL: return LFB_EACH2(f_mul);
+        case op::MIN: return LFB_EACH2(sc_min);
+        case op::MAX: return LFB_EACH2(sc_max);
+        case op::SUB: return LFB_EACH2(f_sub);
+        case op::SQUARE: return LFB_EACH1(f_square);
+        case op::SQRT: return LFB_EACH1(f_sqrt);
+        case op::NEG: return LFB_EACH1(f_neg);
+        case op::ABS: return LFB_EACH1(f_abs);
+        case op::CONST_VAR:
+        case OP_COPY: return a;
+        default: return leaf_generic4(o, a, b);
+    }
+#undef LFB_EACH1
+#undef LFB_EACH2
+}
+
+/// Values of the tape at four points per lane (point k of this lane in
+/// component k), streaming the tape's clauses (one clause fetched ahead) with
+/// the register file as one float4 per register and lane; the previous
+/// clause's result stays in registers (most clauses read it).  With ties
+/// (a run-time flag, so that one copy of the loop serves corners and edge
+/// search), bit k of *amb reports a min / max with equal arguments at point
+/// k (ArrayEvaluator::getAmbiguous, eval_array.cpp:197-217).
 template <bool S>
-static __device__ __noinline__ float4 leaf_value4(const float* __restrict__ cpool,
+static __device__ __noinline__ float4 warp_value4(const float* __restrict__ cpool,
                                                   uint32_t root_kind, uint32_t root,
                                                   const RegClause* __restrict__ cl, uint32_t len,
-                                                  uint32_t soff, float* Rg, uint32_t ops_off,
-                                                  int lane, float4 x, float4 y, float4 z,
-                                                  bool TIES, uint32_t* amb)
+                                                  uint32_t soff, float* Rg, int lane, float4 x,
+                                                  float4 y, float4 z, bool ties, uint32_t* amb)
 {
     float4* R = regfile4<S>(soff, Rg) + lane;
-    LeafOp* ops = leaf_ops(ops_off);
     R[0] = x;
     R[32] = y;
     R[64] = z;
+    uint32_t last = 0xffffffffu;
+    float4 lv = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     uint32_t t = 0;
-    if (len <= kLeafOps) {
-        if (len) leaf_run4(ops, len, R, TIES, &t);
-    } else {
-        LeafRaw raw = leaf_fetch(cl, len, 0, lane);
-        for (uint32_t c0 = 0; c0 < len; c0 += kLeafOps) {
-            __syncwarp();
-            const uint32_t n = leaf_decode_chunk(ops, raw, len, c0, cpool, lane);
-            raw = leaf_fetch(cl, len, c0 + kLeafOps, lane);   // next chunk, in flight
-            leaf_run4(ops, n, R, TIES, &t);
+    uint2 next = len ? __ldg(reinterpret_cast<const uint2*>(cl)) : make_uint2(0, 0);
+#pragma unroll 1
+    for (uint32_t c = 0; c < len; ++c) {
+        const uint2 raw = next;
+        if (c + 1 < len) next = __ldg(reinterpret_cast<const uint2*>(cl + c + 1));
+        const uint8_t o = raw.x & 0xff;
+        const uint32_t kinds = (raw.x >> 8) & 0xff;
+        const uint32_t ra = raw.y & 0xffff, rb = raw.y >> 16, ro = raw.x >> 16;
+        float4 a, b;
+        if ((kinds & 3) == OPND_REG) {
+            if (ra == last) a = lv;
+            else a = R[ra * 32];
+        } else {
+            a = splat4(__ldg(cpool + ra));
         }
-        __syncwarp();
+        if (((kinds >> 2) & 3) == OPND_REG) {
+            if (rb == last) b = lv;
+            else b = R[rb * 32];
+        } else {
+            b = splat4(__ldg(cpool + rb));
+        }
+        if (ties && (o == op::MIN || o == op::MAX)) t |= tie4(a, b);
+        const float4 r = dv_value4f(o, a, b);
+        R[ro * 32] = r;
+        lv = r;
+        last = ro;
     }
-    if (TIES) *amb = t;
+    *amb = t;
     if (root_kind == OPND_REG) return R[root * 32];
     return splat4(__ldg(cpool + root));
 }
@@ -1087,7 +1133,8 @@ static __device__ __noinline__ D4 leaf_deriv(const float* __restrict__ cpool, ui
                                              uint32_t root, uint32_t n_regs,
                                              const RegClause* __restrict__ cl, uint32_t len,
                                              uint32_t soff, float* Rg, uint32_t ops_off, int lane,
-                                             float x, float y, float z, bool* ambig, bool* plain)
+                                             float x, float y, float z, bool* ambig, bool* plain,
+                                             bool predecoded)
 {
     float4* R = regfile4<S>(soff, Rg) + lane;
     LeafOp* ops = leaf_ops(ops_off);
@@ -1097,7 +1144,7 @@ static __device__ __noinline__ D4 leaf_deriv(const float* __restrict__ cpool, ui
     const bool trackable = n_regs <= 64;
     uint64_t taint = 0;
     bool amb = false, lost = false;
-    if (len <= kLeafOps) {
+    if (len <= kLeafOps && predecoded) {
         if (len) leaf_run_deriv(ops, len, R, taint, amb, lost, trackable);
     } else {
         LeafRaw raw = leaf_fetch(cl, len, 0, lane);
@@ -1212,13 +1259,9 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
     float* R = rs ? Rs : Rgl;
     const uint32_t rsoff = static_cast<uint32_t>(reinterpret_cast<unsigned char*>(Rs) - lsmem);
 #define RF_CALL(fn, ...) (rs ? fn<true>(__VA_ARGS__) : fn<false>(__VA_ARGS__))
-#define RF_VALUE4(...) (rs ? leaf_value4<true>(__VA_ARGS__) : leaf_value4<false>(__VA_ARGS__))
+#define RF_VALUE4(...) (rs ? warp_value4<true>(__VA_ARGS__) : warp_value4<false>(__VA_ARGS__))
     // Tapes that fit the buffer are decoded once for the whole group.
     __syncwarp();
-    if (tr.len <= kLeafOps) {
-        leaf_decode_chunk(leaf_ops(ops_off), leaf_fetch(cl, tr.len, 0, lane), tr.len, 0,
-                          tb.cpool, lane);
-    }
     const FeatCtx fc{A.featws + (static_cast<size_t>(blockIdx.x) * wpb + warp) *
                                     A.bt.n_regs * kRegBlock,
                      &W->fs, A.status};
@@ -1237,7 +1280,7 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
     {
         uint32_t amb4 = 0;
         const float4 v4 = RF_VALUE4(tb.cpool, tb.root_kind, tb.root, cl, tr.len, rsoff, R,
-                                    ops_off, lane, splat4(px), splat4(py), splat4(pz), true, &amb4);
+                                    lane, splat4(px), splat4(py), splat4(pz), true, &amb4);
         cv = v4.x;
         camb = (amb4 & 1) != 0;
         const uint32_t act = __ballot_sync(0xffffffffu, lane < npts);
@@ -1254,7 +1297,7 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
     if (__any_sync(0xffffffffu, need_d || need_f)) {
         bool amb = false, plain = false;
         const D4 d = RF_CALL(leaf_deriv, tb.cpool, tb.root_kind, tb.root, tb.n_regs, cl,
-                             tr.len, rsoff, R, ops_off, lane, px, py, pz, &amb, &plain);
+                             tr.len, rsoff, R, ops_off, lane, px, py, pz, &amb, &plain, false);
         const uint32_t act = __ballot_sync(0xffffffffu, need_d || need_f);
         if (lane == 0) my_devals += static_cast<uint64_t>(__popc(act)) * tr.len;
         if (need_d) {
@@ -1414,7 +1457,7 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
             }
             uint32_t unused = 0;
             const float4 v4 = RF_VALUE4(tb.cpool, tb.root_kind, tb.root, cl, tr.len,
-                                        rsoff, R, ops_off, lane,
+                                        rsoff, R, lane,
                                         make_float4(qx[0], qx[1], qx[2], qx[3]),
                                         make_float4(qy[0], qy[1], qy[2], qy[3]),
                                         make_float4(qz[0], qz[1], qz[2], qz[3]), false, &unused);
@@ -1434,7 +1477,7 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
                     bool amb = false, plain = false;
                     const D4 dg = RF_CALL(leaf_deriv, tb.cpool, tb.root_kind, tb.root,
                                           tb.n_regs, cl, tr.len, rsoff, R, ops_off, lane,
-                                          qx[k], qy[k], qz[k], &amb, &plain);
+                                          qx[k], qy[k], qz[k], &amb, &plain, false);
                     const uint32_t zact = __ballot_sync(0xffffffffu, zero);
                     if (lane == 0) my_devals += static_cast<uint64_t>(__popc(zact)) * tr.len;
                     amb = amb && !plain;   // a settled tie leaves one plain feature
@@ -1600,11 +1643,11 @@ k_leaf_qef(LeafArgs A, uint32_t n_groups)
             const D4 d = rs ? leaf_deriv<true>(tb.cpool, tb.root_kind, tb.root, tb.n_regs, cl,
                                                tr.len, rsoff, R, ops_off, lane,
                                                static_cast<float>(q[0]), static_cast<float>(q[1]),
-                                               static_cast<float>(q[2]), &amb, &plain)
+                                               static_cast<float>(q[2]), &amb, &plain, true)
                             : leaf_deriv<false>(tb.cpool, tb.root_kind, tb.root, tb.n_regs, cl,
                                                 tr.len, rsoff, R, ops_off, lane,
                                                 static_cast<float>(q[0]), static_cast<float>(q[1]),
-                                                static_cast<float>(q[2]), &amb, &plain);
+                                                static_cast<float>(q[2]), &amb, &plain, true);
             const uint32_t gact = __ballot_sync(0xffffffffu, active);
             if (lane == 0) my_devals += static_cast<uint64_t>(__popc(gact)) * tr.len;
             amb = amb && !plain;   // a settled tie leaves one plain feature

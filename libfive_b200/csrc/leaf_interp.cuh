@@ -192,93 +192,6 @@ static __device__ __noinline__ float4 leaf_generic4(uint8_t o, float4 a, float4 
                        dv_value(o, a.w, b.w));
 }
 
-/// Evaluates n decoded clauses at the four points held by this lane in the
-/// register file R (R[r * 32] is register r of this lane).  With TIES (a
-/// run-time flag: one copy of the loop serves corners and edge search), bit
-/// k of *amb is set when a min / max saw equal arguments at point k
-/// (ArrayEvaluator::getAmbiguous, eval_array.cpp:197-217).
-__device__ __forceinline__ void leaf_run4(const LeafOp* __restrict__ ops, uint32_t n,
-                                          float4* R, bool TIES, uint32_t* amb)
-{
-    uint32_t t = 0;
-    float4 last = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    LeafOp L = ops[0];
-#define LFB_A (L.flags & 8 ? last : R[L.a * 32])
-#define LFB_B (L.flags & 16 ? last : R[L.b * 32])
-#pragma unroll 1
-    for (uint32_t c = 0; c < n; ++c) {
-        const LeafOp next = ops[c + 1 < n ? c + 1 : c];
-        float4 r;
-        switch (L.h) {
-            case H_ADD_RR: r = LFB_MAP2(f_add, LFB_A, LFB_B); break;
-            case H_ADD_RI: r = LFB_MAP2(f_add, LFB_A, splat4(L.imm)); break;
-            case H_MUL_RR: r = LFB_MAP2(f_mul, LFB_A, LFB_B); break;
-            case H_MUL_RI: r = LFB_MAP2(f_mul, LFB_A, splat4(L.imm)); break;
-            case H_SUB_RR: r = LFB_MAP2(f_sub, LFB_A, LFB_B); break;
-            case H_SUB_RI: r = LFB_MAP2(f_sub, LFB_A, splat4(L.imm)); break;
-            case H_SUB_IR: r = LFB_MAP2(f_sub, splat4(L.imm), LFB_B); break;
-            case H_MIN_RR: {
-                const float4 a = LFB_A, b = LFB_B;
-                if (TIES) t |= tie4(a, b);
-                r = LFB_MAP2(sc_min, a, b);
-                break;
-            }
-            case H_MIN_RI: {
-                const float4 a = LFB_A, b = splat4(L.imm);
-                if (TIES) t |= tie4(a, b);
-                r = LFB_MAP2(sc_min, a, b);
-                break;
-            }
-            case H_MIN_IR: {
-                const float4 a = splat4(L.imm), b = LFB_B;
-                if (TIES) t |= tie4(a, b);
-                r = LFB_MAP2(sc_min, a, b);
-                break;
-            }
-            case H_MAX_RR: {
-                const float4 a = LFB_A, b = LFB_B;
-                if (TIES) t |= tie4(a, b);
-                r = LFB_MAP2(sc_max, a, b);
-                break;
-            }
-            case H_MAX_RI: {
-                const float4 a = LFB_A, b = splat4(L.imm);
-                if (TIES) t |= tie4(a, b);
-                r = LFB_MAP2(sc_max, a, b);
-                break;
-            }
-            case H_MAX_IR: {
-                const float4 a = splat4(L.imm), b = LFB_B;
-                if (TIES) t |= tie4(a, b);
-                r = LFB_MAP2(sc_max, a, b);
-                break;
-            }
-            case H_SQUARE: r = LFB_MAP1(f_square, LFB_A); break;
-            case H_SQRT: r = LFB_MAP1(f_sqrt, LFB_A); break;
-            case H_NEG: r = LFB_MAP1(f_neg, LFB_A); break;
-            case H_ABS: r = LFB_MAP1(f_abs, LFB_A); break;
-            case H_COPY: r = LFB_A; break;
-            case H_SET:
-                if (TIES && (L.flags & 4)) t |= 15u;
-                r = splat4(L.imm);
-                break;
-            default: {
-                const float4 a = (L.flags & 1) ? splat4(L.imm) : LFB_A;
-                const float4 b = (L.flags & 2) ? splat4(L.imm)
-                                               : dev_is_binary(L.op) ? LFB_B : splat4(0.0f);
-                r = leaf_generic4(L.op, a, b);
-                break;
-            }
-        }
-        R[L.o * 32] = r;
-        last = r;
-        L = next;
-    }
-#undef LFB_A
-#undef LFB_B
-    if (TIES) *amb |= t;
-}
-
 #undef LFB_MAP1
 #undef LFB_MAP2
 

@@ -799,7 +799,7 @@ struct GroupArgs {
     uint8_t* dec;                  // [warps][8][dec_cap] min/max decisions
     uint32_t dec_cap;
     uint8_t* lastuse;              // [warps][8][kRenumberMax] renumbering flags
-    uint32_t nregs_max;            // register file size (the unpruned tape's)
+    uint32_t nregs_max;            // register file size (this depth's largest group tape)
     uint32_t* status;
     uint32_t* next_group;          // work counter (zero at launch)
 };
@@ -2285,12 +2285,18 @@ __global__ void k_branch_flags(const uint8_t* type, uint32_t n, uint32_t* flags)
 
 /// For each branch cell at depth d: its group index at d + 1, and the
 /// group's parent, tapes and child coordinates.
-__global__ void k_build_groups(Octree o, int d, const uint32_t* scan)
+__global__ void k_build_groups(Octree o, int d, const uint32_t* scan, uint32_t* nregs_next)
 {
     const LevelView& lv = o.lv[d];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool branch = i < lv.n_cells && lv.type[i] == CELL_BRANCH;
+    // largest register count of the next depth's group tapes (sizes the
+    // group-mode interval kernel's shared memory for that depth)
+    const uint32_t nr = branch ? lv.cell_tape[i].nregs : 0u;
+    const uint32_t wmax = __reduce_max_sync(0xffffffffu, nr);
+    if ((threadIdx.x & 31) == 0 && wmax) atomicMax(nregs_next, wmax);
     if (i >= lv.n_cells) return;
-    if (lv.type[i] != CELL_BRANCH) {
+    if (!branch) {
         lv.child_group[i] = -1;
         return;
     }
@@ -2408,7 +2414,7 @@ enum BufKey {
     K_LIST_A, K_LIST_B, K_WIDE_S, K_WIDE_SN, K_WIDE_P, K_WIDE_LIVE, K_WIDE_NEW,
     K_WIDE_ST2, K_WIDE_L1, K_WIDE_WL, K_LEAF_RD, K_ORDER_K0, K_ORDER_K1,
     K_ORDER_V0, K_ORDER_V1, K_SORTTMP, K_PROF, K_GDEC, K_GLAST, K_FEATWS,
-    K_EDGES, K_GEDGES, K_RECGROUP,
+    K_EDGES, K_GEDGES, K_RECGROUP, K_NREGS,
     K_LEVEL = 100,
 };
 
@@ -2805,29 +2811,39 @@ int render_once(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_
     // group over register tapes; every level below stays in that mode.
     const uint32_t group_warps = static_cast<uint32_t>(device_sm_count()) * 32;
     const uint32_t gdec_cap = std::max<uint32_t>(bt.n_choices, 1);
-    const size_t group_smem = group_smem_per_warp(bt.n_regs) * 4;
     uint8_t* gdec = ws.get<uint8_t>(K_GDEC, static_cast<size_t>(group_warps) * 8 * gdec_cap);
     uint8_t* glast = ws.get<uint8_t>(K_GLAST, static_cast<size_t>(group_warps) * 8 * kRenumberMax);
-    if (!gdec || !glast) return LFB_E_CUDA;
-    if (group_smem > 48 * 1024) {
-        if (!raise_smem_limit(reinterpret_cast<const void*>(k_interval_group), group_smem)) {
-            return LFB_E_CUDA;
-        }
-    }
+    // per depth: the largest register count of its group tapes
+    uint32_t* level_nregs = ws.get<uint32_t>(K_NREGS, kMaxLevels + 2);
+    if (!gdec || !glast || !level_nregs) return LFB_E_CUDA;
+    cudaMemsetAsync(level_nregs, 0, (kMaxLevels + 2) * sizeof(uint32_t), s);
     bool group_mode = false;
 
     for (int d = 0; d < L; ++d) {
         if (cancelled()) return LFB_E_CANCELLED;
         LevelView& lv = o.lv[d];
         cells_evaluated += lv.n_cells;
-        group_mode = group_mode || (d > 0 && lv.n_cells >= group_mode_cells() &&
-                                    group_smem <= 200 * 1024);
-        const bool write_lists = d + 1 < L && !group_mode;
-        const int out_key = list_key[(d + 1) & 1];
         const auto t_level = std::chrono::steady_clock::now();
         unsigned long long arena_before = 0;
+        uint32_t nregs_d = bt.n_regs;
         cudaMemcpyAsync(&arena_before, arena_top, sizeof(arena_before), cudaMemcpyDeviceToHost, s);
+        if (d > 0) {
+            cudaMemcpyAsync(&nregs_d, level_nregs + d, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+        }
         if (!cuda_ok(cudaStreamSynchronize(s), "interval stage")) return LFB_E_CUDA;
+        // The group-mode register file holds this depth's largest tape (the
+        // pruned tapes of deep levels need far fewer registers than the
+        // unpruned tape, so more warps fit on an SM).
+        nregs_d = std::min<uint32_t>(std::max<uint32_t>(nregs_d, 3), bt.n_regs);
+        const size_t group_smem = group_smem_per_warp(nregs_d) * 4;
+        group_mode = group_mode || (d > 0 && lv.n_cells >= group_mode_cells() &&
+                                    group_smem <= 200 * 1024);
+        if (group_mode && group_smem > 48 * 1024 &&
+            !raise_smem_limit(reinterpret_cast<const void*>(k_interval_group), group_smem)) {
+            return LFB_E_CUDA;
+        }
+        const bool write_lists = d + 1 < L && !group_mode;
+        const int out_key = list_key[(d + 1) & 1];
         for (int attempt = 0; attempt < 4; ++attempt) {
             WideArgs W;
             W.o = o;
@@ -2856,7 +2872,7 @@ int render_once(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_
             cudaMemsetAsync(list_top, 0, sizeof(unsigned long long), s);
             if (group_mode) {
                 GroupArgs G{o, bt, arena, arena_top, arena_cap, gdec, gdec_cap, glast,
-                            bt.n_regs, status, W.next_cell};
+                            nregs_d, status, W.next_cell};
                 const uint32_t blocks = std::min<uint32_t>(group_warps / 4, (lv.n_groups + 3) / 4);
                 k_interval_group<<<std::max<uint32_t>(blocks, 1), 128, group_smem, s>>>(G, d);
             } else if (lv.n_cells <= block_mode_cells()) {
@@ -2930,7 +2946,7 @@ int render_once(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_
             return set_error(LFB_E_CAPACITY, "more than 2^27 cells on one octree level");
         }
         if (!alloc_level(d + 1, n_groups * 8, n_groups)) return LFB_E_CUDA;
-        k_build_groups<<<(lv.n_cells + 255) / 256, 256, 0, s>>>(o, d, scan);
+        k_build_groups<<<(lv.n_cells + 255) / 256, 256, 0, s>>>(o, d, scan, level_nregs + d + 1);
         n_launch += 2;   // k_branch_flags + k_build_groups
         if (n_groups == 0) {
             // Nothing ambiguous below this depth: no leaves, no faces.

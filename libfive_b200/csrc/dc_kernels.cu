@@ -1061,8 +1061,7 @@ __device__ __forceinline__ float4 dv_value4f(uint8_t o, const float4& a, const f
 
 /// Values of the tape at four points per lane (point k of this lane in
 /// component k), streaming the tape's clauses (one clause fetched ahead) with
-/// the register file as one float4 per register and lane; the previous
-/// clause's result stays in registers (most clauses read it).  With ties
+/// the register file as one float4 per register and lane.  With ties
 /// (a run-time flag, so that one copy of the loop serves corners and edge
 /// search), bit k of *amb reports a min / max with equal arguments at point
 /// k (ArrayEvaluator::getAmbiguous, eval_array.cpp:197-217).
@@ -1077,8 +1076,6 @@ static __device__ __noinline__ float4 warp_value4(const float* __restrict__ cpoo
     R[0] = x;
     R[32] = y;
     R[64] = z;
-    uint32_t last = 0xffffffffu;
-    float4 lv = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     uint32_t t = 0;
     uint2 next = len ? __ldg(reinterpret_cast<const uint2*>(cl)) : make_uint2(0, 0);
 #pragma unroll 1
@@ -1088,24 +1085,10 @@ static __device__ __noinline__ float4 warp_value4(const float* __restrict__ cpoo
         const uint8_t o = raw.x & 0xff;
         const uint32_t kinds = (raw.x >> 8) & 0xff;
         const uint32_t ra = raw.y & 0xffff, rb = raw.y >> 16, ro = raw.x >> 16;
-        float4 a, b;
-        if ((kinds & 3) == OPND_REG) {
-            if (ra == last) a = lv;
-            else a = R[ra * 32];
-        } else {
-            a = splat4(__ldg(cpool + ra));
-        }
-        if (((kinds >> 2) & 3) == OPND_REG) {
-            if (rb == last) b = lv;
-            else b = R[rb * 32];
-        } else {
-            b = splat4(__ldg(cpool + rb));
-        }
+        const float4 a = (kinds & 3) == OPND_REG ? R[ra * 32] : splat4(__ldg(cpool + ra));
+        const float4 b = ((kinds >> 2) & 3) == OPND_REG ? R[rb * 32] : splat4(__ldg(cpool + rb));
         if (ties && (o == op::MIN || o == op::MAX)) t |= tie4(a, b);
-        const float4 r = dv_value4f(o, a, b);
-        R[ro * 32] = r;
-        lv = r;
-        last = ro;
+        R[ro * 32] = dv_value4f(o, a, b);
     }
     *amb = t;
     if (root_kind == OPND_REG) return R[root * 32];

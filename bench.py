@@ -687,35 +687,37 @@ def hbm_peak():
         return 6650.0, "fallback: earlier B200 copy measurement"
 
 
-def reverse_mode_bytes_per_point(shape):
-    """Algorithmic HBM bytes per point of one reverse-mode pass (forward pass
-    storing the local partials, backward pass reading them): 12 B of
-    coordinates, f written once and read twice (as the seed, and by the
-    loss) = 12 B, and each stored partial written and read once = 8 B.
-    Stored partials per clause follow the opcode: none for add / sub / neg
-    (fixed +-1), one for min / max (0 or 1) and unary ops, two for other
-    binary ops."""
+def reverse_mode_ops_per_point(shape):
+    """Algorithmic FP32 lane-ops per point of one loss + gradient step: the
+    forward pass (W_VALUE per clause, library calls 20) and the reverse sweep
+    (per clause: its local partials, counted as one more W_VALUE, and one
+    multiply and one add per operand)."""
     from libfive_b200 import ffi
     from libfive_b200.shape import slot_tape
     lib = ffi.load()
-    fixed = {lib.libfive_opcode_enum(n.encode()) for n in ("add", "sub", "neg", "const-var")}
-    choice = {lib.libfive_opcode_enum(n.encode()) for n in ("min", "max")}
-    stored = 0
+    names = {}
+    for cand in list(W_VALUE) + ["atan2", "pow", "sin", "cos"]:
+        names[lib.libfive_opcode_enum(cand.encode())] = cand
+    ops = 0
     for c in slot_tape(shape)["clauses"]:
-        o = c[0]
-        stored += 0 if o in fixed else 1 if o in choice else lib.libfive_opcode_args(o)
-    return 24 + 8 * stored, stored
+        w = W_VALUE.get(names.get(c[0]), 20)
+        ops += 2 * w + 2 * lib.libfive_opcode_args(c[0])
+    return ops
 
 
-def reverse_mode_roofline(shape, points, ms):
-    """roofline object of a reverse-mode step over `points` points in `ms`."""
-    per_point, stored = reverse_mode_bytes_per_point(shape)
-    peak, src = hbm_peak()
+def reverse_mode_roofline(shape, points, ms, sm_mhz=1965.0):
+    """FP32 roofline object of a loss + gradient step over `points` points in
+    `ms` (the checkpointed reverse mode recomputes instead of storing, so the
+    step is bound by arithmetic, not memory)."""
+    import torch
+    per_point = reverse_mode_ops_per_point(shape)
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    peak = sms * 128 * sm_mhz * 1e6 / 1e9
     achieved = per_point * points / (ms / 1e3) / 1e9
-    return {"kernel": "lfb_tape_partials + lfb_tape_backward", "bound": "hbm",
-            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "peak_source": src, "traffic": None,
-            "algorithmic_bytes_per_point": per_point, "stored_partials_per_point": stored}
+    return {"kernel": "lfb_tape_values + lfb_tape_ckpt_fwd + lfb_tape_ckpt_bwd", "bound": "fp32",
+            "achieved": achieved, "peak": peak, "unit": "G lane-ops/s", "frac": achieved / peak,
+            "peak_source": f"derived: {sms} SMs x 128 FP32 lanes x {sm_mhz:.0f} MHz",
+            "traffic": None, "algorithmic_ops_per_point": per_point}
 
 
 def run_fit(args, world, rank, local):

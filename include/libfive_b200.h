@@ -47,9 +47,10 @@ int lfb_tape_set_vars(lfb_tape t, libfive_vars vars);
 int lfb_tape_info(lfb_tape t, uint32_t counts[6]);
 /* 1 when the tape's values (lfb_eval_values and the callers built on it)
  * run through the kernel compiled for this tape at its first evaluation
- * (straight-line code: tapes of at most 4096 clauses, NVRTC present,
- * LFB_JIT not set to 0); 0 when they run through the interpreter or
- * nothing was evaluated yet.  Both give identical values. */
+ * (straight-line code for tapes of at most 4096 clauses, segments of a few
+ * hundred clauses up to 65536; NVRTC present, LFB_JIT not set to 0); 0 when
+ * they run through the interpreter or nothing was evaluated yet.  Both give
+ * identical values. */
 int lfb_tape_compiled(lfb_tape t);
 /* Variable order used by the gradient calls: var_ids[i] receives the
  * libfive_tree_id of variable i (ascending reference slot order, as

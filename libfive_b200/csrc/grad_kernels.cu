@@ -460,6 +460,44 @@ int grad_device(GpuTape& g, uint64_t n, const float* x, const float* y, const fl
         (sv && !set_smem(reinterpret_cast<const void*>(k_grad_backward<true, kPts>), smem_sv))) {
         return LFB_E_CUDA;
     }
+    // Checkpointed reverse mode when the tape compiles: per point it stores
+    // only the registers each tape segment reads from earlier segments, and
+    // the backward kernel recomputes the segment from them (jit.cpp).
+    if (const uint32_t ckf = jit_ckpt_prepare(g)) {
+        const uint64_t per_point = 4ull * ckf;
+        const uint64_t cchunk = std::max<uint64_t>(kBlock, std::min<uint64_t>(
+            (4ull << 30) / per_point / kBlock * kBlock, uint64_t(1) << 22));
+        auto& cst = grad_staging();
+        if (!cst.partials.reserve(std::min(cchunk, n) * per_point)) return LFB_E_CUDA;
+        float* C = cst.partials.as<float>();
+        const bool has_cv = tape_has_const_var(g);
+        const bool want_xyz = gx || gy || gz;
+        for (uint64_t off = 0; off < n; off += cchunk) {
+            const uint32_t m = static_cast<uint32_t>(std::min(cchunk, n - off));
+            if (!jit_ckpt_forward(g, m, x + off, y + off, z + off, C, f ? f + off : nullptr, s)) {
+                return set_error(LFB_E_CUDA, "checkpointed gradient kernel launch failed");
+            }
+            const float* sd = seed ? seed + off : nullptr;
+            float* ox = gx ? gx + off : nullptr;
+            float* oy = gy ? gy + off : nullptr;
+            float* oz = gz ? gz + off : nullptr;
+            bool ok = true;
+            if (!has_cv) {
+                if (want_xyz || gvars) {
+                    ok = jit_ckpt_backward(g, m, C, sd, ox, oy, oz, gvars, 0, s);
+                }
+            } else {
+                // CONST_VAR passes point gradients but blocks variable ones.
+                if (want_xyz) ok = jit_ckpt_backward(g, m, C, sd, ox, oy, oz, nullptr, 0, s);
+                if (gvars && ok) {
+                    ok = jit_ckpt_backward(g, m, C, sd, nullptr, nullptr, nullptr, gvars, 1, s);
+                }
+            }
+            if (!ok) return set_error(LFB_E_CUDA, "checkpointed gradient kernel launch failed");
+            if (!cuda_ok(cudaGetLastError(), "gradient kernels")) return LFB_E_CUDA;
+        }
+        return 0;
+    }
     if (!ensure_pslots(g)) return LFB_E_CUDA;
     const uint32_t* pslot = g.d_pslot;
     // Partials take 4 bytes per slot and point: points per launch so that

@@ -489,6 +489,315 @@ std::string backward_source(const RegTape& t, const std::vector<uint32_t>& slots
     return s;
 }
 
+////////////////////////////////////////////////////////////////////////////////
+// Segmented kernels for long tapes, and the checkpointed reverse mode.
+//
+// A straight-line kernel's compile time grows much faster than its length
+// (register allocation over one huge function), so long tapes are cut into
+// segments of kJitSegClauses clauses, each a function of its own; the tape
+// registers pass between segments through a per-thread array in local
+// memory.  Inside a segment every clause result gets its own name (single
+// assignment), so that the reverse pass of a segment can use all of them.
+//
+// Checkpointed reverse mode: the forward kernel stores, per point, only the
+// registers each segment reads from earlier segments (its checkpoint); the
+// backward kernel runs the segments last to first, each recomputing its
+// clauses from its checkpoint and sweeping their adjoints back, so the
+// stored data per point is the checkpoints instead of every clause's local
+// partials.  The recomputed values, partials and products are the same
+// expressions as the partials / backward kernels', in the same order.
+
+constexpr uint32_t kJitSegClauses = 192;
+
+struct JitSeg {
+    uint32_t c0 = 0, c1 = 0;
+    std::vector<uint32_t> live_in;   // registers read before they are written here
+    std::vector<uint32_t> written;   // registers written here (each once)
+    uint32_t ck_base = 0;            // first checkpoint slot of live_in
+};
+
+std::vector<JitSeg> jit_segments(const RegTape& t, uint32_t* ck_total)
+{
+    std::vector<JitSeg> out;
+    uint32_t base = 0;
+    const uint32_t n = static_cast<uint32_t>(t.clauses.size());
+    std::vector<uint8_t> st(t.n_regs);
+    for (uint32_t c0 = 0; c0 < n; c0 += kJitSegClauses) {
+        JitSeg s;
+        s.c0 = c0;
+        s.c1 = std::min(n, c0 + kJitSegClauses);
+        s.ck_base = base;
+        std::fill(st.begin(), st.end(), 0);   // 0 untouched, 1 read first, 2 written
+        for (uint32_t c = s.c0; c < s.c1; ++c) {
+            const RegClause& cl = t.clauses[c];
+            auto read = [&](uint32_t kind, uint32_t r) {
+                if (kind != OPND_REG) return;
+                if (st[r] == 0) {
+                    st[r] = 1;
+                    s.live_in.push_back(r);
+                }
+            };
+            read(cl.kinds & 3, cl.a);
+            read(b_kind(cl), cl.b);
+            if (st[cl.out] != 2) {
+                if (std::find(s.written.begin(), s.written.end(), cl.out) == s.written.end()) {
+                    s.written.push_back(cl.out);
+                }
+                st[cl.out] = 2;
+            }
+        }
+        base += static_cast<uint32_t>(s.live_in.size());
+        out.push_back(std::move(s));
+    }
+    if (ck_total) *ck_total = base;
+    return out;
+}
+
+/// Operand of a clause inside a segment: the latest name of a register
+/// (a single-assignment name, or its live-in value), a literal or a free
+/// variable.
+std::string seg_operand(const RegTape& t, uint32_t kind, uint32_t idx,
+                        const std::vector<std::string>& name)
+{
+    if (kind == OPND_REG) return name[idx];
+    return operand(t, kind, idx);
+}
+
+/// Forward segment function: live-ins from R (and, with ckpt, stored to
+/// the checkpoint column Ci), the clauses in single assignment, the
+/// registers it writes back to R.
+std::string fseg_source(const RegTape& t, const JitSeg& sg, uint32_t k, bool ckpt)
+{
+    std::string s = "__device__ __noinline__ void fseg" + std::to_string(k) +
+                    "(float* __restrict__ R, float* __restrict__ Ci, unsigned m, "
+                    "const float* __restrict__ cp)\n{\n";
+    std::vector<std::string> name(t.n_regs);
+    for (size_t j = 0; j < sg.live_in.size(); ++j) {
+        const uint32_t r = sg.live_in[j];
+        name[r] = "v" + std::to_string(r);
+        s += "    const float " + name[r] + " = R[" + std::to_string(r) + "];\n";
+        if (ckpt) {
+            s += "    Ci[(size_t)" + std::to_string(sg.ck_base + j) + " * m] = " + name[r] + ";\n";
+        }
+    }
+    for (uint32_t c = sg.c0; c < sg.c1; ++c) {
+        const RegClause& cl = t.clauses[c];
+        const std::string a = seg_operand(t, cl.kinds & 3, cl.a, name);
+        const std::string b = seg_operand(t, b_kind(cl), cl.b, name);
+        const std::string e = expr(cl.op, a, b);
+        if (e.empty()) return std::string();
+        const std::string o = "s" + std::to_string(c);
+        s += "    const float " + o + " = " + e + ";\n";
+        name[cl.out] = o;
+    }
+    for (uint32_t r : sg.written) s += "    R[" + std::to_string(r) + "] = " + name[r] + ";\n";
+    s += "}\n";
+    return s;
+}
+
+/// Root operand after all segments (the register array or a literal).
+std::string root_from_R(const RegTape& t)
+{
+    if (t.root_kind == OPND_REG) return "R[" + std::to_string(t.root) + "]";
+    return operand(t, t.root_kind, t.root);
+}
+
+/// Value kernel of a long tape (same signature as values_source's).
+std::string values_source_segmented(const RegTape& t)
+{
+    const auto segs = jit_segments(t, nullptr);
+    std::string s = kPrelude;
+    for (uint32_t k = 0; k < segs.size(); ++k) {
+        const std::string f = fseg_source(t, segs[k], k, false);
+        if (f.empty()) return std::string();
+        s += f;
+    }
+    s += "extern \"C\" __global__ void __launch_bounds__(256)\n"
+         "lfb_tape_values(const float* __restrict__ X, const float* __restrict__ Y,\n"
+         "                const float* __restrict__ Z, float* __restrict__ out,\n"
+         "                unsigned long long n, const float* __restrict__ cp)\n{\n";
+    s += kHead;
+    s += "        float R[" + std::to_string(t.n_regs) + "];\n"
+         "        for (int r = 3; r < " + std::to_string(t.n_regs) + "; ++r) R[r] = 0.0f;\n"
+         "        R[0] = X[i]; R[1] = Y[i]; R[2] = Z[i];\n";
+    for (uint32_t k = 0; k < segs.size(); ++k) {
+        s += "        fseg" + std::to_string(k) + "(R, nullptr, 0u, cp);\n";
+    }
+    s += "        out[i] = " + root_from_R(t) + ";\n    }\n}\n";
+    return s;
+}
+
+/// Checkpointed reverse mode, forward kernel: f and the checkpoints.
+std::string ckpt_forward_source(const RegTape& t)
+{
+    const auto segs = jit_segments(t, nullptr);
+    std::string s = kPrelude;
+    for (uint32_t k = 0; k < segs.size(); ++k) {
+        const std::string f = fseg_source(t, segs[k], k, true);
+        if (f.empty()) return std::string();
+        s += f;
+    }
+    s += "extern \"C\" __global__ void __launch_bounds__(256)\n"
+         "lfb_tape_ckpt_fwd(const float* __restrict__ X, const float* __restrict__ Y,\n"
+         "                  const float* __restrict__ Z, float* __restrict__ C,\n"
+         "                  float* __restrict__ f, unsigned m, const float* __restrict__ cp)\n{\n"
+         "    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;\n"
+         "    if (i >= m) return;\n";
+    s += "    float R[" + std::to_string(t.n_regs) + "];\n"
+         "    for (int r = 3; r < " + std::to_string(t.n_regs) + "; ++r) R[r] = 0.0f;\n"
+         "    R[0] = X[i]; R[1] = Y[i]; R[2] = Z[i];\n";
+    for (uint32_t k = 0; k < segs.size(); ++k) {
+        s += "    fseg" + std::to_string(k) + "(R, C + i, m, cp);\n";
+    }
+    s += "    if (f) f[i] = " + root_from_R(t) + ";\n}\n";
+    return s;
+}
+
+/// Backward segment function: live-ins from the checkpoint, the clauses
+/// and their local partials recomputed, adjoints swept back; A holds the
+/// adjoint of every register at the segment's end on entry and at its
+/// start on return.
+std::string bseg_source(const RegTape& t, const JitSeg& sg, uint32_t k)
+{
+    std::string s = "__device__ __noinline__ void bseg" + std::to_string(k) +
+                    "(float* __restrict__ A, const float* __restrict__ Ci, unsigned m, "
+                    "const float* __restrict__ cp, float* Gv, int gv, int block_cv, int ok)\n{\n";
+    std::vector<std::string> name(t.n_regs);
+    for (size_t j = 0; j < sg.live_in.size(); ++j) {
+        const uint32_t r = sg.live_in[j];
+        name[r] = "v" + std::to_string(r);
+        s += "    const float " + name[r] + " = Ci[(size_t)" + std::to_string(sg.ck_base + j) +
+             " * m];\n";
+    }
+    // recompute: value and local partials of every clause
+    struct Ref {
+        uint32_t kind;      // OPND_REG / OPND_VAR / other
+        std::string adj;    // adjoint variable receiving the contribution
+        uint32_t var;       // variable index (OPND_VAR)
+    };
+    std::vector<Ref> ra(sg.c1 - sg.c0), rb(sg.c1 - sg.c0);
+    std::vector<uint8_t> is_written(t.n_regs, 0), is_live(t.n_regs, 0);
+    for (uint32_t r : sg.written) is_written[r] = 1;
+    for (uint32_t r : sg.live_in) is_live[r] = 1;
+    std::vector<std::string> adjname(t.n_regs);   // current adjoint variable of each register
+    for (uint32_t r : sg.live_in) adjname[r] = "gi" + std::to_string(r);
+    for (uint32_t c = sg.c0; c < sg.c1; ++c) {
+        const RegClause& cl = t.clauses[c];
+        std::string v, pa, pb, pre;
+        if (!partial_exprs(cl.op, &v, &pa, &pb, &pre)) return std::string();
+        if (cl.op == op::CONST_VAR) pa = "(block_cv ? 0.0f : 1.0f)";
+        // a min / max passes the adjoint to the chosen side: b gets 1 - pa
+        if (cl.op == op::MIN || cl.op == op::MAX) pb = "1.0f - pa" + std::to_string(c);
+        const uint32_t ka = cl.kinds & 3, kb = b_kind(cl);
+        const std::string c_ = std::to_string(c);
+        s += "    float s" + c_ + ", pa" + c_ + ", pb" + c_ + ";\n";
+        s += "    { const float a = " + seg_operand(t, ka, cl.a, name) + ", b = " +
+             seg_operand(t, kb, cl.b, name) + "; " + pre + "s" + c_ + " = " + v + "; pa" + c_ +
+             " = " + pa + "; pb" + c_ + " = " + pb + "; }\n";
+        const uint32_t i = c - sg.c0;
+        ra[i] = {ka, ka == OPND_REG ? adjname[cl.a] : std::string(),
+                 ka == OPND_VAR ? cl.a - t.n_const : 0u};
+        if (kb != 99u) {
+            rb[i] = {kb, kb == OPND_REG ? adjname[cl.b] : std::string(),
+                     kb == OPND_VAR ? cl.b - t.n_const : 0u};
+        } else {
+            rb[i] = {99u, std::string(), 0u};
+        }
+        name[cl.out] = "s" + c_;
+        adjname[cl.out] = "g" + c_;
+    }
+    // adjoint variables: clause results (the last definition of a register
+    // starts from the register's adjoint after the segment), live-ins (those
+    // not written here pass the adjoint after the segment through)
+    std::vector<uint8_t> last_def(sg.c1 - sg.c0, 0);
+    {
+        std::vector<uint8_t> seen(t.n_regs, 0);
+        for (uint32_t c = sg.c1; c-- > sg.c0;) {
+            const uint32_t o = t.clauses[c].out;
+            if (!seen[o]) {
+                seen[o] = 1;
+                last_def[c - sg.c0] = 1;
+            }
+        }
+    }
+    for (uint32_t c = sg.c0; c < sg.c1; ++c) {
+        const uint32_t o = t.clauses[c].out;
+        s += "    float g" + std::to_string(c) + " = " +
+             (last_def[c - sg.c0] ? "A[" + std::to_string(o) + "]" : std::string("0.0f")) + ";\n";
+    }
+    for (uint32_t r : sg.live_in) {
+        s += "    float gi" + std::to_string(r) + " = " +
+             (is_written[r] ? std::string("0.0f") : "A[" + std::to_string(r) + "]") + ";\n";
+    }
+    auto contrib = [&](const Ref& rf, const std::string& g) -> std::string {
+        if (rf.kind == OPND_REG) return "    " + rf.adj + " += " + g + ";\n";
+        if (rf.kind == OPND_VAR) {
+            return "    if (gv) lfb_add_var(Gv, " + std::to_string(rf.var) + ", ok ? " + g +
+                   " : 0.0f);\n";
+        }
+        return std::string();
+    };
+    for (uint32_t c = sg.c1; c-- > sg.c0;) {
+        const std::string c_ = std::to_string(c);
+        const uint32_t i = c - sg.c0;
+        s += contrib(ra[i], "g" + c_ + " * pa" + c_);
+        if (rb[i].kind != 99u) s += contrib(rb[i], "g" + c_ + " * pb" + c_);
+    }
+    for (uint32_t r : sg.live_in) s += "    A[" + std::to_string(r) + "] = gi" + std::to_string(r) + ";\n";
+    for (uint32_t r : sg.written) {
+        if (!is_live[r]) s += "    A[" + std::to_string(r) + "] = 0.0f;\n";
+    }
+    s += "}\n";
+    return s;
+}
+
+/// Checkpointed reverse mode, backward kernel (arguments as the backward
+/// kernel's, plus the checkpoints and the constant pool).
+std::string ckpt_backward_source(const RegTape& t)
+{
+    const auto segs = jit_segments(t, nullptr);
+    std::string s = kPrelude;
+    s += "__device__ __forceinline__ void lfb_add_var(float* Gv, unsigned k, float g)\n{\n"
+         "    for (int o = 16; o > 0; o >>= 1) g += __shfl_xor_sync(0xffffffffu, g, o);\n"
+         "    if ((threadIdx.x & 31) == 0 && g != 0.0f) atomicAdd(Gv + k, g);\n}\n";
+    for (uint32_t k = 0; k < segs.size(); ++k) {
+        const std::string b = bseg_source(t, segs[k], k);
+        if (b.empty()) return std::string();
+        s += b;
+    }
+    s += "extern \"C\" __global__ void __launch_bounds__(256)\n"
+         "lfb_tape_ckpt_bwd(const float* __restrict__ C, const float* __restrict__ seed,\n"
+         "                  float* __restrict__ gx, float* __restrict__ gy,\n"
+         "                  float* __restrict__ gz, float* __restrict__ gvars, unsigned m,\n"
+         "                  unsigned n_vars, int block_cv, const float* __restrict__ cp)\n{\n"
+         "    extern __shared__ float Gv[];\n"
+         "    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;\n"
+         "    const int ok = i < m;\n"
+         "    const int gv = gvars != nullptr;\n"
+         "    if (gv) {\n"
+         "        for (unsigned k = threadIdx.x; k < n_vars; k += blockDim.x) Gv[k] = 0.0f;\n"
+         "        __syncthreads();\n    }\n"
+         "    const float* const Ci = C + (ok ? i : 0);\n";
+    s += "    float A[" + std::to_string(t.n_regs) + "];\n"
+         "    for (int r = 0; r < " + std::to_string(t.n_regs) + "; ++r) A[r] = 0.0f;\n"
+         "    const float s0 = ok ? (seed ? seed[i] : 1.0f) : 0.0f;\n";
+    if (t.root_kind == OPND_REG) {
+        s += "    A[" + std::to_string(t.root) + "] = s0;\n";
+    } else if (t.root_kind == OPND_VAR) {
+        s += "    if (gv) lfb_add_var(Gv, " + std::to_string(t.root - t.n_const) + ", s0);\n";
+    }
+    for (uint32_t k = static_cast<uint32_t>(segs.size()); k-- > 0;) {
+        s += "    bseg" + std::to_string(k) + "(A, Ci, m, cp, Gv, gv, block_cv, ok);\n";
+    }
+    s += "    if (ok) {\n"
+         "        if (gx) gx[i] = A[0];\n        if (gy) gy[i] = A[1];\n        if (gz) gz[i] = A[2];\n"
+         "    }\n"
+         "    if (gv) {\n        __syncthreads();\n"
+         "        for (unsigned k = threadIdx.x; k < n_vars; k += blockDim.x) {\n"
+         "            if (Gv[k] != 0.0f) atomicAdd(gvars + k, Gv[k]);\n        }\n    }\n}\n";
+    return s;
+}
+
 /// Interval operand: registers are kept as Iv values; constants and free
 /// variables become degenerate intervals as the interpreter's fetch does.
 std::string iv_operand(const RegTape& t, uint32_t kind, uint32_t idx)
@@ -531,11 +840,19 @@ void* kernel(GpuTape& g, int k, const std::vector<uint32_t>* slots = nullptr)
     std::lock_guard<std::mutex> lock(g.mu);
     GpuTape::JitKernel& j = g.jit[k];
     if (j.state == 0) {
-        bool ok = api().ok && g.reg.clauses.size() <= (k == 4 ? kJitMaxIntervalClauses
-                                                                 : kJitMaxClauses);
+        const size_t n = g.reg.clauses.size();
+        bool ok = api().ok && n <= (k == 4 ? kJitMaxIntervalClauses
+                                    : (k == 0 || k >= 5) ? kJitMaxSegmentedClauses
+                                                         : kJitMaxClauses);
         if (ok) {
             switch (k) {
-                case 0: ok = build(g, 0, values_source(g.reg), "lfb_tape_values"); break;
+                case 0:
+                    ok = build(g, 0, n <= kJitMaxClauses ? values_source(g.reg)
+                                                         : values_source_segmented(g.reg),
+                               "lfb_tape_values");
+                    break;
+                case 5: ok = build(g, 5, ckpt_forward_source(g.reg), "lfb_tape_ckpt_fwd"); break;
+                case 6: ok = build(g, 6, ckpt_backward_source(g.reg), "lfb_tape_ckpt_bwd"); break;
                 case 1: ok = build(g, 1, derivs_source(g.reg), "lfb_tape_derivs"); break;
                 case 2: ok = build(g, 2, partials_source(g.reg, *slots), "lfb_tape_partials"); break;
                 case 3: ok = build(g, 3, backward_source(g.reg, *slots), "lfb_tape_backward"); break;
@@ -639,6 +956,43 @@ bool jit_backward(GpuTape& g, const uint32_t* slots, uint32_t m, const float* P,
     if (!fn) return false;
     if (m == 0) return true;
     void* args[] = {&P, &seed, &gx, &gy, &gz, &gvars, &m, &n_vars, &block_cv};
+    return launch_1d(fn, m, args, smem, s);
+}
+
+uint32_t jit_ckpt_prepare(GpuTape& g)
+{
+    if (!kernel(g, 5) || !kernel(g, 6)) return 0;
+    std::lock_guard<std::mutex> lock(g.mu);
+    if (!g.ckpt_floats) {
+        uint32_t total = 0;
+        jit_segments(g.reg, &total);
+        g.ckpt_floats = std::max<uint32_t>(total, 1);
+    }
+    return g.ckpt_floats;
+}
+
+bool jit_ckpt_forward(GpuTape& g, uint32_t m, const float* x, const float* y, const float* z,
+                      float* C, float* f, cudaStream_t s)
+{
+    void* fn = kernel(g, 5);
+    if (!fn) return false;
+    if (m == 0) return true;
+    const float* cp = g.d_cpool;
+    void* args[] = {&x, &y, &z, &C, &f, &m, &cp};
+    return launch_1d(fn, m, args, 0, s);
+}
+
+bool jit_ckpt_backward(GpuTape& g, uint32_t m, const float* C, const float* seed, float* gx,
+                       float* gy, float* gz, float* gvars, int block_cv, cudaStream_t s)
+{
+    uint32_t n_vars = g.reg.n_vars;
+    const unsigned smem = gvars ? n_vars * 4 : 0;
+    if (smem > 48 * 1024) return false;
+    void* fn = kernel(g, 6);
+    if (!fn) return false;
+    if (m == 0) return true;
+    const float* cp = g.d_cpool;
+    void* args[] = {&C, &seed, &gx, &gy, &gz, &gvars, &m, &n_vars, &block_cv, &cp};
     return launch_1d(fn, m, args, smem, s);
 }
 

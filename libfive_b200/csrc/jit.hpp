@@ -26,6 +26,11 @@ constexpr uint32_t kJitMaxClauses = 4096;
 /// clauses, 69 s for 1924), while the interval interpreter gives the same
 /// bounds and takes milliseconds for a height map's boxes.
 constexpr uint32_t kJitMaxIntervalClauses = 1024;
+/// Longer tapes are compiled in segments of a few hundred clauses (one
+/// function each, registers passed through local memory), whose compile time
+/// grows with the length: the value kernel and the checkpointed reverse mode
+/// take tapes up to this length.
+constexpr uint32_t kJitMaxSegmentedClauses = 65536;
 
 /// Values of the tape at n points through its compiled kernel (compiled on
 /// first use).  Returns false, with no error set, when the tape has no
@@ -67,6 +72,19 @@ bool jit_intervals(GpuTape& g, uint64_t n, const float* xlo, const float* xhi,
 /// and its compilation to a cubin, for checks that need no GPU.
 std::string jit_interval_source(const RegTape& t);
 bool jit_compile(const std::string& src, std::vector<char>* cubin, std::string* log);
+
+/// Checkpointed reverse mode (compiled in segments): the forward kernel
+/// writes f and, per point, the registers each segment reads from earlier
+/// segments (C[slot * m + i], jit_ckpt_prepare's count of slots); the
+/// backward kernel recomputes each segment from them and sweeps its
+/// adjoints back, with the products and sums of the partials / backward
+/// kernels.  jit_ckpt_prepare compiles both and returns the slot count, or 0
+/// when the tape has no compiled form.
+uint32_t jit_ckpt_prepare(GpuTape& g);
+bool jit_ckpt_forward(GpuTape& g, uint32_t m, const float* x, const float* y, const float* z,
+                      float* C, float* f, cudaStream_t s);
+bool jit_ckpt_backward(GpuTape& g, uint32_t m, const float* C, const float* seed, float* gx,
+                       float* gy, float* gz, float* gvars, int block_cv, cudaStream_t s);
 
 /// Releases a tape's compiled kernels (called when the tape is destroyed).
 void jit_release(GpuTape& g);

@@ -59,7 +59,9 @@ struct GpuTape {
         void* module = nullptr;
         void* function = nullptr;
     };
-    JitKernel jit[5];
+    // [5] / [6] checkpointed reverse mode, forward / backward
+    JitKernel jit[7];
+    uint32_t ckpt_floats = 0;   // checkpoint slots per point (0: not prepared)
 
     // The CUDA device that was current when the tape was made: its arrays
     // live there, so every call must run with that device current.

@@ -40,6 +40,11 @@ def shapes():
              + (y * 0.5).acos() + z.atan() + x ** 3 + y.nth_root(3) + z % 0.7
              + x.sqrt().nanfill(y) + x.compare(y)) - 0.5)
     out["trig"] = (trig, None)
+    # longer than the straight-line limit (4096 clauses): values and the
+    # reverse mode compile in segments; the free variables exercise the
+    # checkpointed backward pass's variable sums
+    long_, lvals = workloads.blended_spheres_vars(300, seed=6, stable=True)
+    out["long"] = (long_, lvals)
     return out
 
 
@@ -98,7 +103,7 @@ def points():
     return (np.concatenate([x, lx]), np.concatenate([y, ly]), np.concatenate([z, lz]))
 
 
-@pytest.mark.parametrize("name", ["spheres", "csg", "blend_vars", "misc", "trig"])
+@pytest.mark.parametrize("name", ["spheres", "csg", "blend_vars", "misc", "trig", "long"])
 def test_compiled_matches_interpreter(gpu, name, tmp_path):
     s, vals = shapes()[name]
     t = Tape(s, vals)
@@ -144,8 +149,8 @@ def test_variables_change_without_recompiling(gpu):
     assert np.array_equal(b.view(np.uint32), t2.values(*p).view(np.uint32))
 
 
-def test_long_tape_stays_interpreted(gpu):
-    # more clauses than the compiled kernels take (4096)
+def test_long_tape_compiles_in_segments(gpu):
     t = Tape(workloads.spheres_union(500, seed=2))
+    assert t.n_clauses > 4096
     t.values(*points())
-    assert ffi.load().lfb_tape_compiled(t.ptr) == 0
+    assert ffi.load().lfb_tape_compiled(t.ptr) == 1

@@ -51,12 +51,13 @@ def test_surface_points_lie_on_the_mesh():
     assert abs(np.mean(y < x) - 0.5) < 0.05
 
 
-def test_reverse_mode_bytes_follow_the_stored_partials():
-    # sqrt(x^2 + y^2) - 0.5: square, square and sqrt store one partial each,
-    # add and sub none: 24 B of coordinates and f traffic + 3 x 8 B
+def test_reverse_mode_ops_follow_the_tape():
+    # sqrt(x^2 + y^2) - 0.5: per clause twice its value weight (forward and
+    # local partials) and a multiply-add per operand: square 2 + 2 (x2),
+    # add 2 + 4, sqrt 2 + 2, sub 2 + 4
     import bench
     from libfive_b200.shape import X, Y
     shape = (X().square() + Y().square()).sqrt() - 0.5
-    assert bench.reverse_mode_bytes_per_point(shape) == (48, 3)
-    # min stores one (a choice), mul two
-    assert bench.reverse_mode_bytes_per_point(X().min(Y() * X()))[1] == 3
+    assert bench.reverse_mode_ops_per_point(shape) == 2 * 4 + 6 + 4 + 6
+    # library calls count 20 each
+    assert bench.reverse_mode_ops_per_point(X().sin()) == 2 * 20 + 2

@@ -657,7 +657,8 @@ std::string ckpt_forward_source(const RegTape& t)
 /// and their local partials recomputed, adjoints swept back; A holds the
 /// adjoint of every register at the segment's end on entry and at its
 /// start on return.
-std::string bseg_source(const RegTape& t, const JitSeg& sg, uint32_t k)
+std::string bseg_source(const RegTape& t, const JitSeg& sg, uint32_t k,
+                        std::vector<uint32_t>* vidx)
 {
     std::string s = "__device__ __noinline__ void bseg" + std::to_string(k) +
                     "(float* __restrict__ A, const float* __restrict__ Ci, unsigned m, "
@@ -729,12 +730,24 @@ std::string bseg_source(const RegTape& t, const JitSeg& sg, uint32_t k)
         s += "    float gi" + std::to_string(r) + " = " +
              (is_written[r] ? std::string("0.0f") : "A[" + std::to_string(r) + "]") + ";\n";
     }
+    // Variable adjoints: summed per thread over the segment, then over the
+    // warp 32 variables at a time (lfb_flush32) into the block's sums.
+    std::vector<uint32_t> seg_vars;
+    auto var_slot = [&](uint32_t v) {
+        auto it = std::find(seg_vars.begin(), seg_vars.end(), v);
+        if (it != seg_vars.end()) return static_cast<uint32_t>(it - seg_vars.begin());
+        seg_vars.push_back(v);
+        s += "    float va" + std::to_string(seg_vars.size() - 1) + " = 0.0f;\n";
+        return static_cast<uint32_t>(seg_vars.size() - 1);
+    };
+    for (uint32_t c = sg.c0; c < sg.c1; ++c) {
+        const uint32_t i = c - sg.c0;
+        if (ra[i].kind == OPND_VAR) var_slot(ra[i].var);
+        if (rb[i].kind == OPND_VAR) var_slot(rb[i].var);
+    }
     auto contrib = [&](const Ref& rf, const std::string& g) -> std::string {
         if (rf.kind == OPND_REG) return "    " + rf.adj + " += " + g + ";\n";
-        if (rf.kind == OPND_VAR) {
-            return "    if (gv) lfb_add_var(Gv, " + std::to_string(rf.var) + ", ok ? " + g +
-                   " : 0.0f);\n";
-        }
+        if (rf.kind == OPND_VAR) return "    va" + std::to_string(var_slot(rf.var)) + " += " + g + ";\n";
         return std::string();
     };
     for (uint32_t c = sg.c1; c-- > sg.c0;) {
@@ -742,6 +755,17 @@ std::string bseg_source(const RegTape& t, const JitSeg& sg, uint32_t k)
         const uint32_t i = c - sg.c0;
         s += contrib(ra[i], "g" + c_ + " * pa" + c_);
         if (rb[i].kind != 99u) s += contrib(rb[i], "g" + c_ + " * pb" + c_);
+    }
+    for (size_t g0 = 0; g0 < seg_vars.size(); g0 += 32) {
+        const size_t base = vidx->size();
+        s += "    if (gv) { float v[32] = {";
+        for (size_t j = 0; j < 32; ++j) {
+            const size_t q = g0 + j;
+            s += j ? ", " : "";
+            s += q < seg_vars.size() ? "ok ? va" + std::to_string(q) + " : 0.0f" : "0.0f";
+            vidx->push_back(q < seg_vars.size() ? seg_vars[q] : 0xffffu);
+        }
+        s += "}; lfb_flush32(v, Gv, " + std::to_string(base) + "u); }\n";
     }
     for (uint32_t r : sg.live_in) s += "    A[" + std::to_string(r) + "] = gi" + std::to_string(r) + ";\n";
     for (uint32_t r : sg.written) {
@@ -756,16 +780,42 @@ std::string bseg_source(const RegTape& t, const JitSeg& sg, uint32_t k)
 std::string ckpt_backward_source(const RegTape& t)
 {
     const auto segs = jit_segments(t, nullptr);
+    std::string body;
+    std::vector<uint32_t> vidx;
+    for (uint32_t k = 0; k < segs.size(); ++k) {
+        const std::string b = bseg_source(t, segs[k], k, &vidx);
+        if (b.empty()) return std::string();
+        body += b;
+    }
     std::string s = kPrelude;
     s += "__device__ __forceinline__ void lfb_add_var(float* Gv, unsigned k, float g)\n{\n"
          "    for (int o = 16; o > 0; o >>= 1) g += __shfl_xor_sync(0xffffffffu, g, o);\n"
          "    if ((threadIdx.x & 31) == 0 && g != 0.0f) atomicAdd(Gv + k, g);\n}\n";
-    for (uint32_t k = 0; k < segs.size(); ++k) {
-        const std::string b = bseg_source(t, segs[k], k);
-        if (b.empty()) return std::string();
-        s += b;
-    }
-    s += "extern \"C\" __global__ void __launch_bounds__(256)\n"
+    // variable of each flushed slot (0xffff: none)
+    s += "__device__ const unsigned short lfb_vidx[" + std::to_string(std::max<size_t>(vidx.size(), 1)) +
+         "] = {";
+    for (size_t j = 0; j < vidx.size(); ++j) s += (j ? "," : "") + std::to_string(vidx[j]);
+    if (vidx.empty()) s += "0";
+    s += "};\n";
+    // 32 per-thread sums -> lane l holds slot l's sum over the warp
+    // (recursive halving: 31 shuffles for 32 variables)
+    s += "__device__ __forceinline__ void lfb_flush32(float (&v)[32], float* Gv, unsigned base)\n{\n"
+         "    const unsigned lane = threadIdx.x & 31;\n"
+         "#pragma unroll\n"
+         "    for (int w = 16; w >= 1; w >>= 1) {\n"
+         "#pragma unroll\n"
+         "        for (int i = 0; i < w; ++i) {\n"
+         "            const bool up = lane & w;\n"
+         "            const float send = up ? v[i] : v[i + w];\n"
+         "            const float keep = up ? v[i + w] : v[i];\n"
+         "            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, w);\n"
+         "        }\n    }\n"
+         "    const unsigned k = lfb_vidx[base + lane];\n"
+         "    if (k != 0xffffu && v[0] != 0.0f) atomicAdd(Gv + k, v[0]);\n}\n";
+    s += body;
+    // at most 64 registers a thread: four blocks of 256 threads on an SM,
+    // enough warps to cover the instruction fetches of this long code
+    s += "extern \"C\" __global__ void __launch_bounds__(256, 4)\n"
          "lfb_tape_ckpt_bwd(const float* __restrict__ C, const float* __restrict__ seed,\n"
          "                  float* __restrict__ gx, float* __restrict__ gy,\n"
          "                  float* __restrict__ gz, float* __restrict__ gvars, unsigned m,\n"

@@ -606,7 +606,8 @@ def run_adjoint(args, world, rank, local):
     (256 blended spheres' centres and radii) and the 2^22 points, the points
     sampled area-uniformly from the mesh (64 voxels per unit) of a second
     seed's spheres.
-    One step = the forward values, the seed 2 f / N, and the reverse sweep."""
+    One step = lfb_eval_loss_grad: the forward pass (f and the checkpoints),
+    the seed 2 f / N and the reverse sweep."""
     import numpy as np
     import torch
     from libfive_b200 import workloads
@@ -633,12 +634,14 @@ def run_adjoint(args, world, rank, local):
     gv = torch.zeros(tape.n_vars, device="cuda")
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
 
+    loss = torch.zeros(1, device="cuda")
+
     def step():
+        # loss = mean f^2 and its gradients: one forward pass (f and the
+        # checkpoints), one backward pass with seed 2 f / n
         s = torch.cuda.current_stream().cuda_stream
-        tape.values(x, y, z, out=f, stream=s)
-        torch.mul(f, 2.0 / n, out=seed)
         gv.zero_()
-        tape.grad(x, y, z, seed=seed, f=f, gx=gx, gy=gy, gz=gz, gvars=gv, stream=s)
+        tape.loss_grad(x, y, z, f, gx, gy, gz, gvars=gv, loss=loss, stream=s)
 
     ms = _timed(step, args.steps, args.warmup, flush)
     ms_fwd = _timed(lambda: tape.values(x, y, z, out=f, stream=torch.cuda.current_stream().cuda_stream),

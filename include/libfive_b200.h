@@ -126,6 +126,18 @@ int lfb_eval_grad(lfb_tape t, uint64_t n, const float* x, const float* y,
 int lfb_tape_set_vars_device(lfb_tape t, const float* values, uint32_t n,
                              void* stream);
 
+/*  Loss and gradient in one call (new; the reference has no optimiser):
+ *  loss = mean_i f(p_i)^2 over n points, f[i] = f(p_i), and its gradients
+ *    gx/gy/gz[i] = 2 f(p_i) / n * df/dp_i     (any may be NULL)
+ *    gvars[k]   += sum_i 2 f(p_i) / n * df(p_i)/dvar_k   (NULL to skip)
+ *  *loss (NULL to skip) receives the loss as a float.  One forward pass
+ *  serves both f and the gradient (lfb_eval_grad with seed 2 f / n, without
+ *  a separate evaluation of f).  All arrays are device arrays: flags must
+ *  hold LFB_DEVICE_PTRS; work is ordered on `stream`. */
+int lfb_eval_loss_grad(lfb_tape t, uint64_t n, const float* x, const float* y,
+                       const float* z, float* f, float* gx, float* gy, float* gz,
+                       float* gvars, float* loss, void* stream, uint32_t flags);
+
 /*  Current values of the tape's free variables (lfb_tape_var_ids order) in
  *  a host array of len floats; after lfb_fit_adam_step this waits for the
  *  device and reads the values it wrote.  Counterpart of reading

@@ -691,6 +691,20 @@ int lfb_eval_grad(lfb_tape t, uint64_t n, const float* x, const float* y,
                      (flags & LFB_DEVICE_PTRS) != 0);
 }
 
+int lfb_eval_loss_grad(lfb_tape t, uint64_t n, const float* x, const float* y,
+                       const float* z, float* f, float* gx, float* gy, float* gz,
+                       float* gvars, float* loss, void* stream, uint32_t flags)
+{
+    clear_error();
+    if (!t) return set_error(LFB_E_INVALID, "null tape");
+    if (!(flags & LFB_DEVICE_PTRS)) {
+        return set_error(LFB_E_INVALID, "lfb_eval_loss_grad takes device arrays (LFB_DEVICE_PTRS)");
+    }
+    if (!t->g->on_current_device()) return LFB_E_INVALID;
+    return eval_loss_grad(*t->g, n, x, y, z, f, gx, gy, gz, gvars, loss,
+                          static_cast<cudaStream_t>(stream));
+}
+
 libfive_mesh* lfb_render_mesh(lfb_tape t, libfive_region3 R,
                               lfb_mesh_settings s, lfb_mesh_stats* stats)
 {

@@ -38,6 +38,11 @@ int eval_features_host(GpuTape& g, uint64_t n, const float* x, const float* y, c
 int eval_jacobian(GpuTape& g, uint64_t n, const float* x, const float* y,
                   const float* z, float* out, cudaStream_t s, bool device);
 
+/// lfb_eval_loss_grad (device arrays).
+int eval_loss_grad(GpuTape& g, uint64_t n, const float* x, const float* y, const float* z,
+                   float* f, float* gx, float* gy, float* gz, float* gvars, float* loss,
+                   cudaStream_t s);
+
 int eval_grad(GpuTape& g, uint64_t n, const float* x, const float* y,
               const float* z, const float* seed, float* f, float* gx,
               float* gy, float* gz, float* gvars, cudaStream_t s,

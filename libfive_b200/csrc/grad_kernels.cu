@@ -603,8 +603,10 @@ int eval_jacobian(GpuTape& g, uint64_t n, const float* x, const float* y, const 
 
 bool grad_prepare(GpuTape& g)
 {
+    // the checkpointed kernels, which grad_device takes when they compile;
+    // else the stored-partials kernels (m = 0: compile, no launch)
+    if (jit_ckpt_prepare(g)) return true;
     if (!ensure_pslots(g)) return false;
-    // m = 0: compile (or find that the tape has no compiled form), no launch
     const uint32_t* hs = g.h_pslot.data();
     jit_partials(g, hs, 0, nullptr, nullptr, nullptr, nullptr, nullptr, 0);
     jit_backward(g, hs, 0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0);
@@ -614,7 +616,106 @@ bool grad_prepare(GpuTape& g)
 bool grad_prepared(GpuTape& g)
 {
     std::lock_guard<std::mutex> lock(g.mu);
-    return g.pslot_ready && g.jit[2].state != 0 && g.jit[3].state != 0;
+    if (g.jit[5].state == 1 && g.jit[6].state == 1) return true;
+    return g.jit[5].state != 0 && g.jit[6].state != 0 && g.pslot_ready &&
+           g.jit[2].state != 0 && g.jit[3].state != 0;
+}
+
+namespace {
+
+/// sum of f^2 over the points, in FP64 (one atomic per block).
+__global__ void __launch_bounds__(256) k_sum_squares(const float* __restrict__ f, uint64_t n,
+                                                     double* out)
+{
+    __shared__ double part[8];
+    double acc = 0.0;
+    for (uint64_t i = blockIdx.x * 256ull + threadIdx.x; i < n; i += gridDim.x * 256ull) {
+        const double v = f[i];
+        acc += v * v;
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = 0.0;
+        for (int w = 0; w < 8; ++w) b += part[w];
+        atomicAdd(out, b);
+    }
+}
+
+__global__ void k_mean_to_float(const double* sum, uint64_t n, float* out)
+{
+    *out = static_cast<float>(*sum / static_cast<double>(n));
+}
+
+__global__ void k_scale(const float* __restrict__ a, float s, uint64_t n, float* __restrict__ out)
+{
+    for (uint64_t i = blockIdx.x * 256ull + threadIdx.x; i < n; i += gridDim.x * 256ull) {
+        out[i] = a[i] * s;
+    }
+}
+
+}  // namespace
+
+int eval_loss_grad(GpuTape& g, uint64_t n, const float* x, const float* y, const float* z,
+                   float* f, float* gx, float* gy, float* gz, float* gvars, float* loss,
+                   cudaStream_t s)
+{
+    if (!require_device()) return LFB_E_CUDA;
+    if (!x || !y || !z || !f) return set_error(LFB_E_INVALID, "lfb_eval_loss_grad: null argument");
+    if (n == 0) return set_error(LFB_E_INVALID, "lfb_eval_loss_grad: no points");
+    std::lock_guard<std::mutex> lock(global_mutex());
+    const float scale = static_cast<float>(2.0 / static_cast<double>(n));
+    const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256,
+                                                                     device_sm_count() * 8ull));
+    auto& st = grad_staging();
+    if (!st.out.reserve(sizeof(double))) return LFB_E_CUDA;
+    double* sum = st.out.as<double>();
+    if (const uint32_t ckf = jit_ckpt_prepare(g)) {
+        // one forward pass gives f and the checkpoints; the backward pass
+        // takes seed 2 f_i / n
+        const uint64_t per_point = 4ull * ckf;
+        const uint64_t cchunk = std::max<uint64_t>(kBlock, std::min<uint64_t>(
+            (4ull << 30) / per_point / kBlock * kBlock, uint64_t(1) << 22));
+        if (!st.partials.reserve(std::min(cchunk, n) * per_point)) return LFB_E_CUDA;
+        float* C = st.partials.as<float>();
+        const bool has_cv = tape_has_const_var(g);
+        for (uint64_t off = 0; off < n; off += cchunk) {
+            const uint32_t m = static_cast<uint32_t>(std::min(cchunk, n - off));
+            if (!jit_ckpt_forward(g, m, x + off, y + off, z + off, C, f + off, s)) {
+                return set_error(LFB_E_CUDA, "checkpointed gradient kernel launch failed");
+            }
+            float* ox = gx ? gx + off : nullptr;
+            float* oy = gy ? gy + off : nullptr;
+            float* oz = gz ? gz + off : nullptr;
+            bool ok = true;
+            if (!has_cv) {
+                ok = jit_ckpt_backward(g, m, C, f + off, ox, oy, oz, gvars, 0, s, scale);
+            } else {
+                ok = jit_ckpt_backward(g, m, C, f + off, ox, oy, oz, nullptr, 0, s, scale) &&
+                     (!gvars || jit_ckpt_backward(g, m, C, f + off, nullptr, nullptr, nullptr,
+                                                  gvars, 1, s, scale));
+            }
+            if (!ok) return set_error(LFB_E_CUDA, "checkpointed gradient kernel launch failed");
+        }
+    } else {
+        // without compiled kernels: values, then the gradient with seed 2 f / n
+        const int rc = eval_values_device(g, n, x, y, z, f, s);
+        if (rc) return rc;
+        if (!st.in.reserve(n * sizeof(float))) return LFB_E_CUDA;
+        float* seed = st.in.as<float>();
+        k_scale<<<blocks, 256, 0, s>>>(f, scale, n, seed);
+        note_launches(1);
+        const int rc2 = grad_device(g, n, x, y, z, seed, nullptr, gx, gy, gz, gvars, s);
+        if (rc2) return rc2;
+    }
+    if (loss) {
+        cudaMemsetAsync(sum, 0, sizeof(double), s);
+        k_sum_squares<<<blocks, 256, 0, s>>>(f, n, sum);
+        k_mean_to_float<<<1, 1, 0, s>>>(sum, n, loss);
+        note_launches(2);
+    }
+    return cuda_ok(cudaGetLastError(), "loss gradient") ? 0 : LFB_E_CUDA;
 }
 
 int eval_grad(GpuTape& g, uint64_t n, const float* x, const float* y, const float* z,

@@ -819,7 +819,8 @@ std::string ckpt_backward_source(const RegTape& t)
          "lfb_tape_ckpt_bwd(const float* __restrict__ C, const float* __restrict__ seed,\n"
          "                  float* __restrict__ gx, float* __restrict__ gy,\n"
          "                  float* __restrict__ gz, float* __restrict__ gvars, unsigned m,\n"
-         "                  unsigned n_vars, int block_cv, const float* __restrict__ cp)\n{\n"
+         "                  unsigned n_vars, int block_cv, const float* __restrict__ cp,\n"
+         "                  float sscale)\n{\n"
          "    extern __shared__ float Gv[];\n"
          "    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;\n"
          "    const int ok = i < m;\n"
@@ -830,7 +831,7 @@ std::string ckpt_backward_source(const RegTape& t)
          "    const float* const Ci = C + (ok ? i : 0);\n";
     s += "    float A[" + std::to_string(t.n_regs) + "];\n"
          "    for (int r = 0; r < " + std::to_string(t.n_regs) + "; ++r) A[r] = 0.0f;\n"
-         "    const float s0 = ok ? (seed ? seed[i] : 1.0f) : 0.0f;\n";
+         "    const float s0 = ok ? (seed ? seed[i] : 1.0f) * sscale : 0.0f;\n";
     if (t.root_kind == OPND_REG) {
         s += "    A[" + std::to_string(t.root) + "] = s0;\n";
     } else if (t.root_kind == OPND_VAR) {
@@ -1033,7 +1034,8 @@ bool jit_ckpt_forward(GpuTape& g, uint32_t m, const float* x, const float* y, co
 }
 
 bool jit_ckpt_backward(GpuTape& g, uint32_t m, const float* C, const float* seed, float* gx,
-                       float* gy, float* gz, float* gvars, int block_cv, cudaStream_t s)
+                       float* gy, float* gz, float* gvars, int block_cv, cudaStream_t s,
+                       float seed_scale)
 {
     uint32_t n_vars = g.reg.n_vars;
     const unsigned smem = gvars ? n_vars * 4 : 0;
@@ -1042,7 +1044,7 @@ bool jit_ckpt_backward(GpuTape& g, uint32_t m, const float* C, const float* seed
     if (!fn) return false;
     if (m == 0) return true;
     const float* cp = g.d_cpool;
-    void* args[] = {&C, &seed, &gx, &gy, &gz, &gvars, &m, &n_vars, &block_cv, &cp};
+    void* args[] = {&C, &seed, &gx, &gy, &gz, &gvars, &m, &n_vars, &block_cv, &cp, &seed_scale};
     return launch_1d(fn, m, args, smem, s);
 }
 

@@ -83,8 +83,10 @@ bool jit_compile(const std::string& src, std::vector<char>* cubin, std::string* 
 uint32_t jit_ckpt_prepare(GpuTape& g);
 bool jit_ckpt_forward(GpuTape& g, uint32_t m, const float* x, const float* y, const float* z,
                       float* C, float* f, cudaStream_t s);
+/// The seed of point i is seed[i] (1 when seed is null) times seed_scale.
 bool jit_ckpt_backward(GpuTape& g, uint32_t m, const float* C, const float* seed, float* gx,
-                       float* gy, float* gz, float* gvars, int block_cv, cudaStream_t s);
+                       float* gy, float* gz, float* gvars, int block_cv, cudaStream_t s,
+                       float seed_scale = 1.0f);
 
 /// Releases a tape's compiled kernels (called when the tape is destroyed).
 void jit_release(GpuTape& g);

@@ -148,6 +148,7 @@ SIGNATURES = [
     ("lfb_eval_derivs", ctypes.c_int, [tape_t, ctypes.c_uint64, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_uint32]),
     ("lfb_eval_intervals", ctypes.c_int, [tape_t, ctypes.c_uint64, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_uint32]),
     ("lfb_eval_features", ctypes.c_int, [tape_t, ctypes.c_uint64, vp, vp, vp, vp, vp, ctypes.c_uint32, vp]),
+    ("lfb_eval_loss_grad", ctypes.c_int, [tape_t, ctypes.c_uint64, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_uint32]),
     ("lfb_eval_jacobian", ctypes.c_int, [tape_t, ctypes.c_uint64, vp, vp, vp, vp, vp, ctypes.c_uint32]),
     ("lfb_eval_grad", ctypes.c_int, [tape_t, ctypes.c_uint64, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_uint32]),
     ("lfb_tape_get_vars", ctypes.c_int, [tape_t, fp, ctypes.c_uint32]),

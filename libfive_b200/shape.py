@@ -302,6 +302,16 @@ class Tape:
             stream, fl), "grad")
         return f, gx, gy, gz, gvars
 
+    def loss_grad(self, x, y, z, f, gx=None, gy=None, gz=None, gvars=None, loss=None,
+                  stream=None):
+        """loss = mean f^2 and its gradients in one call (CUDA tensors;
+        lfb_eval_loss_grad).  gvars accumulates; zero it first."""
+        ffi.check(_lib().lfb_eval_loss_grad(
+            self.ptr, len(x), _ptr(x)[0], _ptr(y)[0], _ptr(z)[0], _ptr(f)[0], _ptr(gx)[0],
+            _ptr(gy)[0], _ptr(gz)[0], _ptr(gvars)[0], _ptr(loss)[0], stream,
+            ffi.LFB_DEVICE_PTRS), "loss_grad")
+        return f, gx, gy, gz, gvars, loss
+
     def render_mesh(self, lower, upper, min_feature, max_err=1e-8, stats=False):
         region = ffi.Region3(*[ffi.Interval(a, b) for a, b in zip(lower, upper)])
         st = ffi.MeshStats()

@@ -229,3 +229,32 @@ def test_torch_autograd(gpu):
     want = (2 * ov.astype(np.float64)) @ jac
     scale = np.abs(2 * ov[:, None] * jac).sum(axis=0) + 1e-6
     assert np.all(np.abs(v.grad.cpu().numpy() - want) <= 1e-4 * scale)
+
+
+def test_loss_grad_equals_values_then_grad(gpu):
+    """lfb_eval_loss_grad (one forward pass for f and the gradient of
+    mean f^2) against lfb_eval_values then lfb_eval_grad with seed 2 f / n."""
+    torch = pytest.importorskip("torch")
+    s, vals = workloads.blended_spheres_vars(64, seed=3, stable=True)
+    tape = Tape(s, vals)
+    n = 100003
+    x, y, z = (torch.from_numpy(a).cuda() for a in workloads.uniform_points(n, seed=2, lo=-1.2, hi=1.2))
+    st = torch.cuda.current_stream().cuda_stream
+    f1 = torch.empty(n, device="cuda")
+    tape.values(x, y, z, out=f1, stream=st)
+    seed = f1 * (2.0 / n)
+    g1 = [torch.empty(n, device="cuda") for _ in range(3)]
+    gv1 = torch.zeros(tape.n_vars, device="cuda")
+    tape.grad(x, y, z, seed=seed, gx=g1[0], gy=g1[1], gz=g1[2], gvars=gv1, stream=st)
+    f2 = torch.empty(n, device="cuda")
+    g2 = [torch.empty(n, device="cuda") for _ in range(3)]
+    gv2 = torch.zeros(tape.n_vars, device="cuda")
+    loss = torch.zeros(1, device="cuda")
+    tape.loss_grad(x, y, z, f2, *g2, gvars=gv2, loss=loss, stream=st)
+    torch.cuda.synchronize()
+    assert torch.equal(f1, f2)
+    for a, b in zip(g1, g2):
+        assert torch.equal(a, b)
+    assert torch.allclose(gv1, gv2, rtol=1e-5, atol=1e-7)
+    want = (f1.double() ** 2).mean().item()
+    assert abs(loss.item() - want) <= 1e-6 * want

@@ -37,6 +37,12 @@ class Vec3(ctypes.Structure):
                 ("z", ctypes.c_float)]
 
 
+class MeshCoords(ctypes.Structure):
+    _fields_ = [("verts", ctypes.POINTER(Vec3)), ("vert_count", ctypes.c_uint32),
+                ("coord_indices", ctypes.POINTER(ctypes.c_int32)),
+                ("coord_index_count", ctypes.c_uint32)]
+
+
 class Tri(ctypes.Structure):
     _fields_ = [("a", ctypes.c_uint32), ("b", ctypes.c_uint32),
                 ("c", ctypes.c_uint32)]
@@ -124,7 +130,7 @@ SIGNATURES = [
     ("libfive_tree_save_slice", None, [tree_t, Region2, ctypes.c_float, ctypes.c_float, ctypes.c_char_p]),
     ("libfive_tree_render_mesh", ctypes.POINTER(Mesh), [tree_t, Region3, ctypes.c_float]),
     ("libfive_tree_render_mesh_st", ctypes.POINTER(Mesh), [tree_t, Region3, ctypes.c_float]),
-    ("libfive_tree_render_mesh_coords", vp, [tree_t, Region3, ctypes.c_float]),
+    ("libfive_tree_render_mesh_coords", ctypes.POINTER(MeshCoords), [tree_t, Region3, ctypes.c_float]),
     ("libfive_tree_save_mesh", ctypes.c_bool, [tree_t, Region3, ctypes.c_float, ctypes.c_char_p]),
     ("libfive_evaluator_save_mesh", ctypes.c_bool, [vp, Region3, ctypes.c_char_p]),
     ("libfive_tree_save_meshes", ctypes.c_bool, [ctypes.POINTER(tree_t), Region3, ctypes.c_float, ctypes.c_float, ctypes.c_char_p]),

@@ -164,3 +164,25 @@ def test_cone_renders(gpu):
     cone = (radius - 1).max(z.max(-1 - z))
     v, t, ov, ot = gpu_and_oracle(cone, (-10, -10, -10), (10, 10, 10), 0.1)
     assert same_mesh(v, t, ov, ot)
+
+
+def test_render_mesh_coords_matches_render_mesh(gpu, lib):
+    """libfive_tree_render_mesh_coords (libfive.cpp:354-395): the mesh's
+    vertices and, per triangle, its three vertex indices then -1."""
+    s = workloads.spheres_union(8, seed=2)
+    R = ffi.Region3(*[ffi.Interval(-1.5, 1.5)] * 3)
+    m = lib.libfive_tree_render_mesh(s.ptr, R, 10.0)
+    v, t = mesh_arrays(m)
+    mc = lib.libfive_tree_render_mesh_coords(s.ptr, R, 10.0)
+    assert mc
+    c = mc[0]
+    cv = np.ctypeslib.as_array(ctypes.cast(c.verts, ctypes.POINTER(ctypes.c_float)),
+                               shape=(c.vert_count * 3,)).reshape(-1, 3).copy()
+    ci = np.ctypeslib.as_array(c.coord_indices, shape=(c.coord_index_count,)).copy()
+    n_idx = c.coord_index_count
+    lib.libfive_mesh_coords_delete(mc)
+    assert n_idx == 4 * len(t) > 0
+    ci = ci.reshape(-1, 4)
+    assert np.all(ci[:, 3] == -1)
+    # the same mesh (vertex order may differ between two renders)
+    assert same_mesh(cv, ci[:, :3].astype(np.uint32), v, t)

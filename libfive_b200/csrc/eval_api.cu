@@ -28,6 +28,14 @@ int eval_values_device(GpuTape& g, uint64_t n, const float* x, const float* y,
 }
 
 namespace {
+// LFB_E_CUDA when an interpreter block gave up waiting for its clause copy
+// (its results were not written), else 0.
+int stage_status()
+{
+    if (!stage_fault_take()) return 0;
+    return set_error(LFB_E_CUDA, "interpreter: clause stream copy timed out");
+}
+
 struct Staging {
     DevBuf buf;
 };
@@ -57,10 +65,11 @@ int eval_values_host(GpuTape& g, uint64_t n, const float* x, const float* y,
     int rc = eval_values_device(g, n, d, d + n, d + 2 * n, d + 3 * n, s);
     if (rc) return rc;
     if (!cuda_ok(cudaMemcpyAsync(out, d + 3 * n, b, cudaMemcpyDeviceToHost, s), "copy") ||
+        !cuda_ok(stage_fault_fetch(s), "copy") ||
         !cuda_ok(cudaStreamSynchronize(s), "sync")) {
         return LFB_E_CUDA;
     }
-    return 0;
+    return stage_status();
 }
 
 int eval_derivs_device(GpuTape& g, uint64_t n, const float* x, const float* y,
@@ -111,7 +120,11 @@ int eval_derivs_host(GpuTape& g, uint64_t n, const float* x, const float* y,
             return LFB_E_CUDA;
         }
     }
-    return cuda_ok(cudaStreamSynchronize(s), "sync") ? 0 : LFB_E_CUDA;
+    if (!cuda_ok(stage_fault_fetch(s), "copy") ||
+        !cuda_ok(cudaStreamSynchronize(s), "sync")) {
+        return LFB_E_CUDA;
+    }
+    return stage_status();
 }
 
 int eval_intervals_device(GpuTape& g, uint64_t n, const float* xlo,
@@ -166,7 +179,11 @@ int eval_intervals_host(GpuTape& g, uint64_t n, const float* xlo,
         !cuda_ok(cudaMemcpyAsync(onan, dn, n, cudaMemcpyDeviceToHost, s), "copy")) {
         return LFB_E_CUDA;
     }
-    return cuda_ok(cudaStreamSynchronize(s), "sync") ? 0 : LFB_E_CUDA;
+    if (!cuda_ok(stage_fault_fetch(s), "copy") ||
+        !cuda_ok(cudaStreamSynchronize(s), "sync")) {
+        return LFB_E_CUDA;
+    }
+    return stage_status();
 }
 
 }  // namespace lfb

@@ -10,7 +10,10 @@
 //   ArrayEvaluator::values       (libfive/src/eval/eval_array.cpp:106-118)
 //   DerivArrayEvaluator::derivs  (libfive/src/eval/eval_deriv_array.cpp:101-117)
 //   IntervalEvaluator::eval      (libfive/src/eval/eval_interval.cpp:68-93)
-// which process at most 256 points per pass on one CPU thread.
+// which process at most 256 points per pass on one CPU thread.  The clause
+// stream reaches shared memory by bulk asynchronous copies (clause_stage.cuh);
+// the register planes follow the staging ring.
+#include "clause_stage.cuh"
 #include "eval_kernels.cuh"
 #include "runtime.hpp"
 
@@ -29,13 +32,15 @@ k_values(DevTape t, uint32_t n, const float* __restrict__ X,
          const float* __restrict__ Y, const float* __restrict__ Z,
          float* __restrict__ out)
 {
-    extern __shared__ float smem[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int B = blockDim.x * PTS;
     const int tid0 = threadIdx.x;
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * B;
+    ClauseStage stage(t, smem_raw, block_passes(n, B));
+    float* R = reinterpret_cast<float*>(smem_raw + stage_bytes());
+    const float* __restrict__ cp = t.cpool;
     for (uint64_t base = static_cast<uint64_t>(blockIdx.x) * B; base < n;
          base += stride) {
-        float* R = smem;
 #pragma unroll
         for (int p = 0; p < PTS; ++p) {
             const int tid = tid0 + p * blockDim.x;
@@ -45,31 +50,27 @@ k_values(DevTape t, uint32_t n, const float* __restrict__ X,
             R[1 * B + tid] = ok ? Y[i] : 0.0f;
             R[2 * B + tid] = ok ? Z[i] : 0.0f;
         }
-        const RegClause* __restrict__ cl = t.clauses;
-        for (uint32_t c = 0; c < t.n; ++c) {
-            const uint2 raw = __ldg(reinterpret_cast<const uint2*>(cl + c));
-            const uint8_t o = raw.x & 0xff;
-            const uint8_t kinds = (raw.x >> 8) & 0xff;
-            const uint16_t ro = raw.x >> 16;
-            const uint16_t ra = raw.y & 0xffff;
-            const uint16_t rb = raw.y >> 16;
+        const bool ok = stage.walk([&](uint8_t o, uint8_t kinds, uint16_t ro,
+                                       uint16_t ra, uint16_t rb) {
 #pragma unroll
             for (int p = 0; p < PTS; ++p) {
                 const int tid = tid0 + p * blockDim.x;
-                const float a = fetch_v(kinds & 3, ra, R, tid, B, t.cpool);
-                const float b = fetch_v((kinds >> 2) & 3, rb, R, tid, B, t.cpool);
+                const float a = fetch_v(kinds & 3, ra, R, tid, B, cp);
+                const float b = fetch_v((kinds >> 2) & 3, rb, R, tid, B, cp);
                 R[ro * B + tid] = dv_value(o, a, b);
             }
-        }
+        });
+        if (!ok) return;
 #pragma unroll
         for (int p = 0; p < PTS; ++p) {
             const int tid = tid0 + p * blockDim.x;
             const uint64_t i = base + tid;
             if (i < n) {
-                out[i] = fetch_v(t.root_kind, t.root, R, tid, B, t.cpool);
+                out[i] = fetch_v(t.root_kind, t.root, R, tid, B, cp);
             }
         }
     }
+    stage.finish();
 }
 
 __device__ __forceinline__ D4 fetch_d(uint8_t kind, uint16_t idx,
@@ -89,13 +90,15 @@ k_derivs(DevTape t, uint32_t n, const float* __restrict__ X,
          float* __restrict__ ov, float* __restrict__ odx,
          float* __restrict__ ody, float* __restrict__ odz)
 {
-    extern __shared__ float smem[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int B = blockDim.x;
     const int tid = threadIdx.x;
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * B;
+    ClauseStage stage(t, smem_raw, block_passes(n, B));
+    float* R = reinterpret_cast<float*>(smem_raw + stage_bytes());
+    const float* __restrict__ cp = t.cpool;
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * B + tid;
          i - tid < n; i += stride) {
-        float* R = smem;
         const bool ok = i < n;
         const float px = ok ? X[i] : 0.0f;
         const float py = ok ? Y[i] : 0.0f;
@@ -106,28 +109,24 @@ k_derivs(DevTape t, uint32_t n, const float* __restrict__ X,
         r1[0] = py; r1[B] = 0.0f; r1[2 * B] = 1.0f; r1[3 * B] = 0.0f;
         float* r2 = R + 2 * 4 * B + tid;
         r2[0] = pz; r2[B] = 0.0f; r2[2 * B] = 0.0f; r2[3 * B] = 1.0f;
-        const RegClause* __restrict__ cl = t.clauses;
-        for (uint32_t c = 0; c < t.n; ++c) {
-            const uint2 raw = __ldg(reinterpret_cast<const uint2*>(cl + c));
-            const uint8_t o = raw.x & 0xff;
-            const uint8_t kinds = (raw.x >> 8) & 0xff;
-            const uint16_t ro = raw.x >> 16;
-            const uint16_t ra = raw.y & 0xffff;
-            const uint16_t rb = raw.y >> 16;
-            const D4 a = fetch_d(kinds & 3, ra, R, tid, B, t.cpool);
-            const D4 b = fetch_d((kinds >> 2) & 3, rb, R, tid, B, t.cpool);
+        const bool live = stage.walk([&](uint8_t o, uint8_t kinds, uint16_t ro,
+                                         uint16_t ra, uint16_t rb) {
+            const D4 a = fetch_d(kinds & 3, ra, R, tid, B, cp);
+            const D4 b = fetch_d((kinds >> 2) & 3, rb, R, tid, B, cp);
             const D4 d = dv_deriv(o, a, b, false);
             float* r = R + ro * 4 * B + tid;
             r[0] = d.v; r[B] = d.dx; r[2 * B] = d.dy; r[3 * B] = d.dz;
-        }
+        });
+        if (!live) return;
         if (ok) {
-            const D4 d = fetch_d(t.root_kind, t.root, R, tid, B, t.cpool);
+            const D4 d = fetch_d(t.root_kind, t.root, R, tid, B, cp);
             ov[i] = d.v;
             if (odx) odx[i] = d.dx;
             if (ody) ody[i] = d.dy;
             if (odz) odz[i] = d.dz;
         }
     }
+    stage.finish();
 }
 
 __device__ __forceinline__ Iv fetch_i(uint8_t kind, uint16_t idx,
@@ -151,11 +150,13 @@ k_intervals(DevTape t, uint32_t n,
             float* __restrict__ olo, float* __restrict__ ohi,
             uint8_t* __restrict__ onan)
 {
-    extern __shared__ float smem[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int B = blockDim.x;
     const int tid = threadIdx.x;
-    float* R = smem;
-    uint8_t* N = reinterpret_cast<uint8_t*>(smem + t.n_regs * 2 * B);
+    ClauseStage stage(t, smem_raw, block_passes(n, B));
+    float* R = reinterpret_cast<float*>(smem_raw + stage_bytes());
+    uint8_t* N = reinterpret_cast<uint8_t*>(R + t.n_regs * 2 * B);
+    const float* __restrict__ cp = t.cpool;
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * B;
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * B + tid;
          i - tid < n; i += stride) {
@@ -169,32 +170,59 @@ k_intervals(DevTape t, uint32_t n,
             R[a * 2 * B + B + tid] = v.hi;
             N[a * B + tid] = v.nan;
         }
-        const RegClause* __restrict__ cl = t.clauses;
-        for (uint32_t c = 0; c < t.n; ++c) {
-            const uint2 raw = __ldg(reinterpret_cast<const uint2*>(cl + c));
-            const uint8_t o = raw.x & 0xff;
-            const uint8_t kinds = (raw.x >> 8) & 0xff;
-            const uint16_t ro = raw.x >> 16;
-            const uint16_t ra = raw.y & 0xffff;
-            const uint16_t rb = raw.y >> 16;
-            const Iv a = fetch_i(kinds & 3, ra, R, N, tid, B, t.cpool);
-            const Iv bb = fetch_i((kinds >> 2) & 3, rb, R, N, tid, B, t.cpool);
+        const bool live = stage.walk([&](uint8_t o, uint8_t kinds, uint16_t ro,
+                                         uint16_t ra, uint16_t rb) {
+            const Iv a = fetch_i(kinds & 3, ra, R, N, tid, B, cp);
+            const Iv bb = fetch_i((kinds >> 2) & 3, rb, R, N, tid, B, cp);
             const Iv r = iv_apply(o, a, bb);
             R[ro * 2 * B + tid] = r.lo;
             R[ro * 2 * B + B + tid] = r.hi;
             N[ro * B + tid] = r.nan;
-        }
+        });
+        if (!live) return;
         if (ok) {
-            const Iv r = fetch_i(t.root_kind, t.root, R, N, tid, B, t.cpool);
+            const Iv r = fetch_i(t.root_kind, t.root, R, N, tid, B, cp);
             olo[i] = r.lo;
             ohi[i] = r.hi;
             onan[i] = r.nan;
         }
     }
+    stage.finish();
 }
 
 ////////////////////////////////////////////////////////////////////////////////
 // Launchers
+
+static unsigned int* fault_pinned()
+{
+    static unsigned int* p = [] {
+        void* q = nullptr;
+        if (cudaHostAlloc(&q, sizeof(unsigned int), cudaHostAllocDefault) != cudaSuccess) {
+            return static_cast<unsigned int*>(nullptr);
+        }
+        *static_cast<unsigned int*>(q) = 0;
+        return static_cast<unsigned int*>(q);
+    }();
+    return p;
+}
+
+cudaError_t stage_fault_fetch(cudaStream_t s)
+{
+    unsigned int* p = fault_pinned();
+    if (!p) return cudaErrorMemoryAllocation;
+    return cudaMemcpyFromSymbolAsync(p, lfb_stage_fault, sizeof(unsigned int), 0,
+                                     cudaMemcpyDeviceToHost, s);
+}
+
+bool stage_fault_take()
+{
+    unsigned int* p = fault_pinned();
+    if (!p || *p == 0) return false;
+    *p = 0;
+    const unsigned int zero = 0;
+    cudaMemcpyToSymbol(lfb_stage_fault, &zero, sizeof(zero));
+    return true;
+}
 
 static int grid_for(uint64_t n, int block, int sm_count, int per_sm)
 {
@@ -221,8 +249,9 @@ cudaError_t launch_values(const DevTape& t, uint32_t n, const float* x,
     if (n == 0) return cudaSuccess;
     constexpr int PTS = 2;
     const int block = 128;
-    const size_t smem = static_cast<size_t>(t.n_regs) * block * PTS * sizeof(float);
-    if (smem > 200 * 1024) return cudaErrorInvalidConfiguration;
+    const size_t planes = static_cast<size_t>(t.n_regs) * block * PTS * sizeof(float);
+    if (planes > 200 * 1024) return cudaErrorInvalidConfiguration;
+    const size_t smem = stage_bytes() + planes;
     if (!raise_smem_limit(reinterpret_cast<const void*>(k_values<PTS>), smem)) {
         return cudaErrorInvalidValue;
     }
@@ -237,8 +266,9 @@ cudaError_t launch_derivs(const DevTape& t, uint32_t n, const float* x,
 {
     if (n == 0) return cudaSuccess;
     const int block = 128;
-    const size_t smem = static_cast<size_t>(t.n_regs) * block * 4 * sizeof(float);
-    if (smem > 200 * 1024) return cudaErrorInvalidConfiguration;
+    const size_t planes = static_cast<size_t>(t.n_regs) * block * 4 * sizeof(float);
+    if (planes > 200 * 1024) return cudaErrorInvalidConfiguration;
+    const size_t smem = stage_bytes() + planes;
     if (!raise_smem_limit(reinterpret_cast<const void*>(k_derivs), smem)) {
         return cudaErrorInvalidValue;
     }
@@ -255,8 +285,9 @@ cudaError_t launch_intervals(const DevTape& t, uint32_t n, const float* xlo,
 {
     if (n == 0) return cudaSuccess;
     const int block = 128;
-    const size_t smem = static_cast<size_t>(t.n_regs) * block * (2 * sizeof(float) + 1);
-    if (smem > 200 * 1024) return cudaErrorInvalidConfiguration;
+    const size_t planes = static_cast<size_t>(t.n_regs) * block * (2 * sizeof(float) + 1);
+    if (planes > 200 * 1024) return cudaErrorInvalidConfiguration;
+    const size_t smem = stage_bytes() + planes;
     if (!raise_smem_limit(reinterpret_cast<const void*>(k_intervals), smem)) {
         return cudaErrorInvalidValue;
     }

@@ -21,4 +21,11 @@ cudaError_t launch_intervals(const DevTape& t, uint32_t n, const float* xlo,
                              const float* zhi, float* olo, float* ohi,
                              uint8_t* onan, cudaStream_t s);
 
+// The interpreters' clause-copy timeout flag (clause_stage.cuh): fetch
+// enqueues a copy of the device flag to page-locked host memory on `s`;
+// after the stream has been synchronised, take() says whether it was set
+// and clears it.
+cudaError_t stage_fault_fetch(cudaStream_t s);
+bool stage_fault_take();
+
 }  // namespace lfb

@@ -194,7 +194,9 @@ std::shared_ptr<GpuTape> make_tape(const Tree& t)
         set_error(LFB_E_UNSUPPORTED, err);
         return nullptr;
     }
-    const size_t nc = std::max<size_t>(1, g->reg.clauses.size());
+    // an even clause count: the batched interpreters copy the tape to shared
+    // memory in 16-byte multiples
+    const size_t nc = std::max<size_t>(2, (g->reg.clauses.size() + 1) & ~size_t(1));
     const size_t np = std::max<size_t>(1, g->reg.cpool.size());
     if (!cuda_ok(cudaMalloc(&g->d_clauses, nc * sizeof(RegClause)), "tape alloc") ||
         !cuda_ok(cudaMalloc(&g->d_cpool, np * sizeof(float)), "tape alloc")) {

@@ -73,7 +73,7 @@ void libfive_mesh_coords_delete(libfive_mesh_coords* m)
 {
     if (!m) return;
     host_free(m->verts);
-    delete[] m->coord_indices;
+    host_free(m->coord_indices);
     delete m;
 }
 
@@ -316,24 +316,42 @@ static double min_feature_of(float res)
     return static_cast<double>(1 / res);
 }
 
+/// Renders into `mesh` (whose format says what comes back); false with the
+/// message printed on failure, as the reference's callers see a null mesh.
+static bool render_into(const std::shared_ptr<GpuTape>& g, libfive_region3 R,
+                        double min_feature, double max_err, const char* who,
+                        MeshOut& mesh)
+{
+    if (!g || render_dc_mesh(*g, R, min_feature, max_err, mesh, nullptr) != 0) {
+        std::string msg;
+        last_error(&msg);
+        std::fprintf(stderr, "%s: %s\n", who, msg.c_str());
+        return false;
+    }
+    return true;
+}
+
 static libfive_mesh* render_with(const std::shared_ptr<GpuTape>& g,
                                  libfive_region3 R, double min_feature,
                                  double max_err, const char* who)
 {
-    if (!g) {
-        std::string msg;
-        last_error(&msg);
-        std::fprintf(stderr, "%s: %s\n", who, msg.c_str());
-        return nullptr;
-    }
     MeshOut mesh;
-    if (render_dc_mesh(*g, R, min_feature, max_err, mesh, nullptr) != 0) {
-        std::string msg;
-        last_error(&msg);
-        std::fprintf(stderr, "%s: %s\n", who, msg.c_str());
-        return nullptr;
-    }
+    if (!render_into(g, R, min_feature, max_err, who, mesh)) return nullptr;
     return mesh.release();
+}
+
+/// Mesh::saveSTL of a freshly rendered mesh, the records packed on the
+/// device and streamed to the file (no file is created when the render
+/// fails, as in the reference, which renders before it opens the file).
+static bool save_with(const std::shared_ptr<GpuTape>& g, libfive_region3 R,
+                      double min_feature, double max_err, const char* path,
+                      const char* who)
+{
+    if (!path) return false;
+    MeshOut mesh;
+    mesh.format = MeshFormat::Stl;
+    mesh.stl_path = path;
+    return render_into(g, R, min_feature, max_err, who, mesh);
 }
 
 libfive_mesh* libfive_tree_render_mesh(libfive_tree tree, libfive_region3 R,
@@ -356,32 +374,30 @@ libfive_mesh_coords* libfive_tree_render_mesh_coords(libfive_tree tree,
                                                      libfive_region3 R,
                                                      float res)
 {
-    libfive_mesh* m = libfive_tree_render_mesh(tree, R, res);
-    if (!m) return nullptr;
-    auto out = new libfive_mesh_coords;
-    out->vert_count = m->vert_count;
-    out->verts = m->verts;
-    out->coord_index_count = 4 * m->tri_count;
-    out->coord_indices = new int32_t[out->coord_index_count];
-    for (uint32_t i = 0; i < m->tri_count; ++i) {
-        out->coord_indices[4 * i + 0] = static_cast<int32_t>(m->tris[i].a);
-        out->coord_indices[4 * i + 1] = static_cast<int32_t>(m->tris[i].b);
-        out->coord_indices[4 * i + 2] = static_cast<int32_t>(m->tris[i].c);
-        out->coord_indices[4 * i + 3] = -1;
+    if (!tree) return nullptr;
+    // the index list (a, b, c, -1 per triangle) is packed on the device
+    MeshOut mesh;
+    mesh.format = MeshFormat::Coords;
+    if (!render_into(cached_tape(N(tree)), R, min_feature_of(res), 1e-8,
+                     "libfive_tree_render_mesh_coords", mesh)) {
+        return nullptr;
     }
-    host_free(m->tris);
-    delete m;
+    auto out = new libfive_mesh_coords;
+    out->vert_count = mesh.vert_count;
+    out->verts = mesh.verts;
+    out->coord_index_count = 4 * mesh.tri_count;
+    out->coord_indices = mesh.coords;
+    mesh.verts = nullptr;
+    mesh.coords = nullptr;
     return out;
 }
 
 bool libfive_tree_save_mesh(libfive_tree tree, libfive_region3 R, float res,
                             const char* f)
 {
-    libfive_mesh* m = libfive_tree_render_mesh(tree, R, res);
-    if (!m) return false;
-    const bool ok = save_stl(f, {m});
-    libfive_mesh_delete(m);
-    return ok;
+    if (!tree) return false;
+    return save_with(cached_tape(N(tree)), R, min_feature_of(res), 1e-8, f,
+                     "libfive_tree_save_mesh");
 }
 
 bool libfive_tree_save_meshes(libfive_tree trees[], libfive_region3 R,
@@ -425,11 +441,7 @@ bool libfive_evaluator_save_mesh(libfive_evaluator ev, libfive_region3 R,
 {
     if (!ev) return false;
     // BRepSettings defaults (settings.hpp:34-43): min_feature 0.1, max_err 1e-8
-    auto m = render_with(ev->g, R, 0.1, 1e-8, "libfive_evaluator_save_mesh");
-    if (!m) return false;
-    const bool ok = save_stl(f, {m});
-    libfive_mesh_delete(m);
-    return ok;
+    return save_with(ev->g, R, 0.1, 1e-8, f, "libfive_evaluator_save_mesh");
 }
 
 ////////////////////////////////////////////////////////////////////////////////

@@ -2320,6 +2320,52 @@ __global__ void k_remap_tris(uint32_t* tris, uint32_t n, const uint32_t* scan)
     if (i < 3 * n) tris[i] = scan[tris[i]] + 1;
 }
 
+// Binary STL records (mesh.cpp:177-193): per triangle a zero normal, its
+// three vertices and a zero attribute word, 50 bytes, little-endian like
+// the host.  50-byte records are only 2-byte aligned, so a block packs its
+// kStlBlock records in shared memory as 16-bit words and writes them out as
+// one contiguous run of words.
+constexpr uint32_t kStlBlock = 128;
+constexpr uint32_t kStlWords = 25;
+
+__global__ void __launch_bounds__(kStlBlock)
+k_pack_stl(const float* __restrict__ verts, const uint32_t* __restrict__ tris, uint32_t n,
+           uint16_t* __restrict__ out)
+{
+    __shared__ uint16_t rec[kStlBlock * kStlWords];
+    const uint32_t first = blockIdx.x * kStlBlock;
+    const uint32_t i = first + threadIdx.x;
+    uint16_t* r = rec + threadIdx.x * kStlWords;
+    if (i < n) {
+        for (int k = 0; k < 6; ++k) r[k] = 0;
+        for (int v = 0; v < 3; ++v) {
+            const uint32_t id = tris[3 * static_cast<size_t>(i) + v];
+            for (int a = 0; a < 3; ++a) {
+                const uint32_t bits = __float_as_uint(verts[3 * static_cast<size_t>(id) + a]);
+                r[6 + 6 * v + 2 * a] = static_cast<uint16_t>(bits & 0xffff);
+                r[6 + 6 * v + 2 * a + 1] = static_cast<uint16_t>(bits >> 16);
+            }
+        }
+        r[24] = 0;
+    }
+    __syncthreads();
+    const uint32_t m = min(kStlBlock, n - first);
+    uint16_t* dst = out + static_cast<size_t>(first) * kStlWords;
+    for (uint32_t k = threadIdx.x; k < m * kStlWords; k += kStlBlock) dst[k] = rec[k];
+}
+
+// libfive_mesh_coords' index list (libfive.cpp:375-388): a, b, c, -1 per
+// triangle.
+__global__ void k_pack_coords(const uint32_t* __restrict__ tris, uint32_t n, int4* __restrict__ out)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const size_t t = 3 * static_cast<size_t>(i);
+        out[i] = make_int4(static_cast<int>(tris[t]), static_cast<int>(tris[t + 1]),
+                           static_cast<int>(tris[t + 2]), -1);
+    }
+}
+
 }  // namespace lfb
 
 ////////////////////////////////////////////////////////////////////////////////
@@ -2397,7 +2443,7 @@ enum BufKey {
     K_LIST_A, K_LIST_B, K_WIDE_S, K_WIDE_SN, K_WIDE_P, K_WIDE_LIVE, K_WIDE_NEW,
     K_WIDE_ST2, K_WIDE_L1, K_WIDE_WL, K_LEAF_RD, K_ORDER_K0, K_ORDER_K1,
     K_ORDER_V0, K_ORDER_V1, K_SORTTMP, K_PROF, K_GDEC, K_GLAST, K_FEATWS,
-    K_EDGES, K_GEDGES, K_RECGROUP, K_NREGS,
+    K_EDGES, K_GEDGES, K_RECGROUP, K_NREGS, K_STL, K_COORDS,
     K_LEVEL = 100,
 };
 
@@ -2555,6 +2601,7 @@ MeshOut::~MeshOut()
 {
     host_free(verts);
     host_free(tris);
+    host_free(coords);
 }
 
 libfive_mesh* MeshOut::release()
@@ -2639,6 +2686,76 @@ struct StageEvents {
         }
     }
 };
+
+/// Writes the STL file of a mesh whose vertices and triangles (indices from
+/// 1, vertex 0 the placeholder) are on the device: header and count, then
+/// the records, packed on the device kStlChunk triangles at a time into two
+/// alternating device buffers and copied into two page-locked halves, so
+/// that the file write of one chunk overlaps the packing and copy of the
+/// next.
+int stream_stl(Workspace& ws, const char* path, const float* verts, const uint32_t* tris,
+               uint32_t n_tri, cudaStream_t s, uint64_t& n_launch)
+{
+    constexpr uint32_t kStlChunk = 1u << 20;
+    const uint32_t chunk = std::min<uint32_t>(kStlChunk, std::max<uint32_t>(n_tri, 1));
+    const size_t chunk_bytes = static_cast<size_t>(chunk) * 2 * kStlWords;
+    uint16_t* dev = ws.get<uint16_t>(K_STL, 2 * chunk_bytes / 2);
+    if (!dev) return LFB_E_CUDA;
+    if (2 * chunk_bytes > ws.pinned_bytes) {
+        if (ws.pinned) cudaFreeHost(ws.pinned);
+        ws.pinned = nullptr;
+        ws.pinned_bytes = 0;
+        if (!cuda_ok(cudaMallocHost(&ws.pinned, 2 * chunk_bytes), "pinned staging")) {
+            return LFB_E_CUDA;
+        }
+        ws.pinned_bytes = 2 * chunk_bytes;
+    }
+    std::FILE* f = stl_begin(path, n_tri);
+    if (!f) return set_error(LFB_E_INVALID, std::string("could not open ") + path);
+    cudaEvent_t done[2];
+    if (!cuda_ok(cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming), "event") ||
+        !cuda_ok(cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming), "event")) {
+        std::fclose(f);
+        return LFB_E_CUDA;
+    }
+    int rc = 0;
+    const uint32_t n_chunks = (n_tri + chunk - 1) / chunk;
+    for (uint32_t k = 0; k <= n_chunks && rc == 0; ++k) {
+        if (k < n_chunks) {
+            const uint32_t first = k * chunk;
+            const uint32_t m = std::min(chunk, n_tri - first);
+            uint16_t* d = dev + (k & 1) * (chunk_bytes / 2);
+            char* h = static_cast<char*>(ws.pinned) + (k & 1) * chunk_bytes;
+            k_pack_stl<<<(m + kStlBlock - 1) / kStlBlock, kStlBlock, 0, s>>>(
+                verts, tris + 3 * static_cast<size_t>(first), m, d);
+            ++n_launch;
+            if (!cuda_ok(cudaGetLastError(), "STL kernel") ||
+                !cuda_ok(cudaMemcpyAsync(h, d, static_cast<size_t>(m) * 50,
+                                         cudaMemcpyDeviceToHost, s), "download") ||
+                !cuda_ok(cudaEventRecord(done[k & 1], s), "event")) {
+                rc = LFB_E_CUDA;
+            }
+        }
+        if (rc == 0 && k > 0) {
+            // the previous chunk: wait for its copy, then write it
+            const uint32_t p = k - 1;
+            const char* h = static_cast<const char*>(ws.pinned) + (p & 1) * chunk_bytes;
+            const size_t bytes = static_cast<size_t>(std::min(chunk, n_tri - p * chunk)) * 50;
+            if (!cuda_ok(cudaEventSynchronize(done[p & 1]), "download")) {
+                rc = LFB_E_CUDA;
+            } else if (std::fwrite(h, 1, bytes, f) != bytes) {
+                rc = set_error(LFB_E_INVALID, std::string("could not write ") + path);
+            }
+        }
+    }
+    cudaStreamSynchronize(s);
+    cudaEventDestroy(done[0]);
+    cudaEventDestroy(done[1]);
+    if (std::fclose(f) != 0 && rc == 0) {
+        rc = set_error(LFB_E_INVALID, std::string("could not write ") + path);
+    }
+    return rc;
+}
 
 /// One mesh in the context `ws` (held by the caller), on its stream; one
 /// attempt (render_in retries when a capacity estimate was too small).
@@ -3170,6 +3287,7 @@ int render_once(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_
     cudaMemcpyAsync(&root_type, o.lv[0].type, 1, cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
     const uint32_t n_keys = n_recs * 4;
+    bool stl_written = false;
     if (root_type == CELL_BRANCH && n_recs) {
         size_t task_cap = small ? 1024 : std::max<size_t>(1u << 16, static_cast<size_t>(n_recs) * 24);
         size_t tri_cap = small ? 1024 : std::max<size_t>(1u << 16, static_cast<size_t>(n_recs) * 16);
@@ -3232,22 +3350,57 @@ int render_once(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_
                 k_remap_tris<<<(3 * n_tri + 255) / 256, 256, 0, s>>>(tris, n_tri, vscan);
                 ++n_launch;
             }
+            if (out.format == MeshFormat::Stl) {
+                // records packed on the device, streamed to the file
+                out.tri_count = n_tri;
+                const int rc = stream_stl(ws, out.stl_path, verts, tris, n_tri, s, n_launch);
+                if (rc) return rc;
+                stl_written = true;
+                break;
+            }
             host_free(out.verts);
             out.verts = static_cast<libfive_vec3*>(
                 host_alloc((static_cast<size_t>(n_verts) + 1) * sizeof(libfive_vec3)));
-            out.tris = static_cast<libfive_tri*>(
-                host_alloc(static_cast<size_t>(n_tri) * sizeof(libfive_tri)));
-            if (!out.verts || !out.tris) return set_error(LFB_E_CAPACITY, "host allocation failed");
+            if (!out.verts) return set_error(LFB_E_CAPACITY, "host allocation failed");
             out.vert_count = n_verts + 1;
             out.tri_count = n_tri;
-            if (!download(ws, out.verts, verts, out.vert_count * sizeof(libfive_vec3), s) ||
-                !download(ws, out.tris, tris, static_cast<size_t>(n_tri) * sizeof(libfive_tri), s)) {
+            if (!download(ws, out.verts, verts, out.vert_count * sizeof(libfive_vec3), s)) {
+                return LFB_E_CUDA;
+            }
+            if (out.format == MeshFormat::Coords) {
+                int4* c = ws.get<int4>(K_COORDS, std::max<uint32_t>(n_tri, 1));
+                host_free(out.coords);
+                out.coords = static_cast<int32_t*>(host_alloc(static_cast<size_t>(n_tri) * 16));
+                if (!c) return LFB_E_CUDA;
+                if (!out.coords && n_tri) return set_error(LFB_E_CAPACITY, "host allocation failed");
+                if (n_tri) {
+                    k_pack_coords<<<(n_tri + 255) / 256, 256, 0, s>>>(tris, n_tri, c);
+                    ++n_launch;
+                    if (!download(ws, out.coords, c, static_cast<size_t>(n_tri) * 16, s)) {
+                        return LFB_E_CUDA;
+                    }
+                }
+                break;
+            }
+            out.tris = static_cast<libfive_tri*>(
+                host_alloc(static_cast<size_t>(n_tri) * sizeof(libfive_tri)));
+            if (!out.tris) return set_error(LFB_E_CAPACITY, "host allocation failed");
+            if (!download(ws, out.tris, tris, static_cast<size_t>(n_tri) * sizeof(libfive_tri), s)) {
                 return LFB_E_CUDA;
             }
             break;
         }
     }
 
+    if (out.format == MeshFormat::Stl && !stl_written) {
+        // no surface: the file holds the header and a zero count
+        std::FILE* f = stl_begin(out.stl_path, 0);
+        if (!f) return set_error(LFB_E_INVALID, std::string("could not open ") + out.stl_path);
+        const bool ok = std::ferror(f) == 0;
+        if (std::fclose(f) != 0 || !ok) {
+            return set_error(LFB_E_INVALID, std::string("could not write ") + out.stl_path);
+        }
+    }
     note_launches(n_launch);
     if (stats) {
         cudaEventRecord(ev[4], s);

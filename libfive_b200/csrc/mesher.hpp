@@ -1,6 +1,7 @@
 // Dual-contouring mesher driver (GPU) and STL writer.
 #pragma once
 #include <cstdint>
+#include <cstdio>
 #include <string>
 #include <vector>
 
@@ -10,13 +11,24 @@
 
 namespace lfb {
 
+/// What render_dc_mesh returns for the triangles: the indexed mesh
+/// (libfive_mesh), the vertices with 4 coordinate indices per triangle
+/// (a, b, c, -1: libfive_mesh_coords, libfive.cpp:354-395), or binary STL
+/// records (mesh.cpp:139-194) packed on the device and streamed to a file.
+enum class MeshFormat { Indexed, Coords, Stl };
+
 /// Mesh arrays in host memory from host_alloc (freed with host_free); the
 /// C API hands them to the caller's libfive_mesh without a copy.
 struct MeshOut {
     libfive_vec3* verts = nullptr;   // verts[0] is the dummy vertex
-    libfive_tri* tris = nullptr;     // indices start at 1
+    libfive_tri* tris = nullptr;     // indices start at 1 (Indexed only)
     uint32_t vert_count = 0;
     uint32_t tri_count = 0;
+    MeshFormat format = MeshFormat::Indexed;
+    int32_t* coords = nullptr;       // Coords: 4 * tri_count, host_alloc'd
+    const char* stl_path = nullptr;  // Stl: the file written (header, count,
+                                     // records) once the triangles are known;
+                                     // verts then holds the dummy vertex only
     MeshOut() = default;
     MeshOut(const MeshOut&) = delete;
     MeshOut& operator=(const MeshOut&) = delete;
@@ -65,5 +77,10 @@ int render_dc_meshes(MeshJob* jobs, size_t n, unsigned workers);
 /// uint32 triangle count, then per triangle a zero normal, three vertices
 /// and a zero attribute word.
 bool save_stl(const char* path, const std::vector<libfive_mesh*>& meshes);
+
+/// Opens `path` and writes the STL header and triangle count, with the
+/// reference's messages for a name without ".stl" and a failed open; null
+/// when the file cannot be opened.
+std::FILE* stl_begin(const char* path, uint32_t count);
 
 }  // namespace lfb

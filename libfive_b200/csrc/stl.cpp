@@ -9,9 +9,9 @@
 
 namespace lfb {
 
-bool save_stl(const char* path, const std::vector<libfive_mesh*>& meshes)
+std::FILE* stl_begin(const char* path, uint32_t count)
 {
-    if (!path) return false;
+    if (!path) return nullptr;
     const std::string name(path);
     if (name.size() < 4 ||
         (name.compare(name.size() - 4, 4, ".stl") != 0 &&
@@ -22,16 +22,23 @@ bool save_stl(const char* path, const std::vector<libfive_mesh*>& meshes)
     FILE* f = std::fopen(path, "wb");
     if (!f) {
         std::fprintf(stderr, "Mesh::saveSTL: could not open %s\n", path);
-        return false;
+        return nullptr;
     }
     char header[80];
     std::memset(header, ' ', sizeof(header));
     const char* text = "This is a binary STL exported from libfive.";
     std::memcpy(header, text, std::strlen(text));
     std::fwrite(header, 1, sizeof(header), f);
+    std::fwrite(&count, sizeof(count), 1, f);
+    return f;
+}
+
+bool save_stl(const char* path, const std::vector<libfive_mesh*>& meshes)
+{
     uint32_t count = 0;
     for (auto m : meshes) count += m->tri_count;
-    std::fwrite(&count, sizeof(count), 1, f);
+    FILE* f = stl_begin(path, count);
+    if (!f) return false;
     // Records are packed into one buffer by a few threads and written with
     // one call per mesh (a write per 50-byte record is the slow part of a
     // large file).

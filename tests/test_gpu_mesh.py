@@ -2,7 +2,6 @@
 the reference's mesh tests (libfive/test/mesh.cpp, api.cpp, xtree.cpp)."""
 import ctypes
 import os
-import tempfile
 
 import numpy as np
 import pytest
@@ -95,15 +94,60 @@ def test_edge_pairing_coarse(gpu):
     assert edge_pairs_ok(t)
 
 
-def test_save_mesh_stl(gpu, lib):
+STL_RECORD = np.dtype([("normal", "<f4", 3), ("v", "<f4", (3, 3)), ("attr", "<u2")])
+
+
+def read_stl(path):
+    """Binary STL (mesh.cpp:139-194): 80-byte header, uint32 count, 50-byte
+    records.  Returns (header, records)."""
+    data = open(path, "rb").read()
+    n = int.from_bytes(data[80:84], "little")
+    assert len(data) == 84 + 50 * n
+    return data[:80], np.frombuffer(data, STL_RECORD, count=n, offset=84)
+
+
+def stl_matches_mesh(recs, v, t):
+    """The records are the mesh's triangles (in any order), with zero
+    normals and attributes."""
+    assert not recs["normal"].any() and not recs["attr"].any()
+    flat = recs["v"].reshape(-1, 3)
+    idx = np.arange(len(flat), dtype=np.uint32).reshape(-1, 3)
+    return same_mesh(flat, idx, v, t)
+
+
+@pytest.mark.parametrize("res", [10.0, 300.0])
+def test_save_mesh_stl(gpu, lib, tmp_path, res):
+    # the records are packed on the device and streamed to the file in
+    # chunks of 2^20 triangles: res 300 (depth 10) writes two chunks
     s = workloads.sphere((0, 0, 0), 0.5)
-    with tempfile.TemporaryDirectory() as d:
-        path = os.path.join(d, "out.stl")
-        r = ffi.Region3(ffi.Interval(-1, 1), ffi.Interval(-1, 1), ffi.Interval(-1, 1))
-        assert lib.libfive_tree_save_mesh(s.ptr, r, 10.0, path.encode())
-        data = open(path, "rb").read()
-        n = int.from_bytes(data[80:84], "little")
-        assert len(data) == 84 + 50 * n and n > 0
+    path = str(tmp_path / "out.stl")
+    r = ffi.Region3(ffi.Interval(-1, 1), ffi.Interval(-1, 1), ffi.Interval(-1, 1))
+    assert lib.libfive_tree_save_mesh(s.ptr, r, res, path.encode())
+    header, recs = read_stl(path)
+    assert header.startswith(b"This is a binary STL exported from libfive.")
+    assert header.endswith(b" ")
+    v, t = mesh_arrays(lib.libfive_tree_render_mesh(s.ptr, r, res))
+    assert len(recs) == len(t) > 0
+    if res > 100:
+        assert len(t) > (1 << 20)
+    assert stl_matches_mesh(recs, v, t)
+
+
+def test_save_mesh_stl_empty_region(gpu, lib, tmp_path):
+    # no surface in the region: header and a zero count
+    s = workloads.sphere((5, 5, 5), 0.5)
+    path = str(tmp_path / "empty.stl")
+    r = ffi.Region3(ffi.Interval(-1, 1), ffi.Interval(-1, 1), ffi.Interval(-1, 1))
+    assert lib.libfive_tree_save_mesh(s.ptr, r, 10.0, path.encode())
+    _, recs = read_stl(path)
+    assert len(recs) == 0
+
+
+def test_save_mesh_unwritable_path(gpu, lib, tmp_path):
+    s = workloads.sphere((0, 0, 0), 0.5)
+    path = str(tmp_path / "no_such_dir" / "out.stl")
+    r = ffi.Region3(ffi.Interval(-1, 1), ffi.Interval(-1, 1), ffi.Interval(-1, 1))
+    assert not lib.libfive_tree_save_mesh(s.ptr, r, 10.0, path.encode())
 
 
 def _cube(h=1.5):

@@ -500,6 +500,42 @@ def run_batch(args, world, rank, local):
         torch.cuda.synchronize()
         timings[name] = rank_max((time.perf_counter() - t0) / args.steps)
         assert len(set(tris)) == 1
+
+    # The same comparison within each resolution class (one step each,
+    # after the warm-up above): small meshes leave the GPU idle between
+    # the host's per-level waits, large ones fill it alone.
+    by_res = {}
+    for res in sorted({r for _, _, r in specs}):
+        idx = [i for i, (_, _, r) in enumerate(specs) if r == res]
+        sub = [jobs[i] for i in idx]
+        m = len(sub)
+        s_tapes = (ffi.tape_t * m)(*[t.ptr for t, *_ in sub])
+        s_regions = (ffi.Region3 * m)(*[region] * m)
+        s_settings = (ffi.MeshSettings * m)(*[ffi.MeshSettings(mf, me) for _, _, _, mf, me in sub])
+        s_stats = (ffi.MeshStats * m)()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for t, _, _, mf, me in sub:
+            mm = lib.lfb_render_mesh(t.ptr, region, ffi.MeshSettings(mf, me), None)
+            if not mm:
+                raise RuntimeError("lfb_render_mesh failed: " + ffi.last_error()[1])
+            lib.libfive_mesh_delete(mm)
+        torch.cuda.synchronize()
+        t_loop = time.perf_counter() - t0
+        meshes = (ctypes.POINTER(ffi.Mesh) * m)()
+        t0 = time.perf_counter()
+        rc = lib.lfb_render_meshes(s_tapes, m, s_regions, s_settings, args.workers, meshes,
+                                   s_stats)
+        for mm in meshes:
+            if mm:
+                lib.libfive_mesh_delete(mm)
+        if rc != 0:
+            raise RuntimeError("lfb_render_meshes failed: " + ffi.last_error()[1])
+        torch.cuda.synchronize()
+        t_batch = time.perf_counter() - t0
+        t_loop, t_batch = rank_max(t_loop), rank_max(t_batch)
+        by_res[str(res)] = {"trees": m, "ms_loop": t_loop * 1e3, "ms_batch": t_batch * 1e3,
+                            "batch_over_loop": t_loop / t_batch}
     if rank == 0:
         n = len(jobs)
         print(json.dumps({
@@ -509,7 +545,8 @@ def run_batch(args, world, rank, local):
             "ms_per_step": timings["batch"] * 1e3, "higher_is_better": True,
             "loop_value": world * n / timings["loop"],
             "batch_over_loop": timings["loop"] / timings["batch"],
-            "triangles_per_step": tris[0], "dtype": "f32", "data": "synthetic",
+            "triangles_per_step": tris[0], "by_resolution": by_res,
+            "dtype": "f32", "data": "synthetic",
             "config": {"workload": "batch of %d random CSG trees, 8-4000 primitives, "
                                    "depth 8-11" % n, "workers": args.workers}}))
 

@@ -812,7 +812,9 @@ __host__ __device__ inline size_t group_smem_per_warp(uint32_t nregs_max)
     return (b + 15) / 16 * 16;
 }
 
-__global__ void __launch_bounds__(128)
+// 12 blocks of 4 warps per SM (40 registers): the kernel is latency-bound,
+// so resident warps are what it needs.
+__global__ void __launch_bounds__(128, 12)
 k_interval_group(GroupArgs A, int d)
 {
     extern __shared__ __align__(16) unsigned char gsm[];
@@ -2909,7 +2911,7 @@ int render_once(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_
 
     // Deep levels (many cells, short tapes) switch to one warp per sibling
     // group over register tapes; every level below stays in that mode.
-    const uint32_t group_warps = static_cast<uint32_t>(device_sm_count()) * 32;
+    const uint32_t group_warps = static_cast<uint32_t>(device_sm_count()) * 48;
     const uint32_t gdec_cap = std::max<uint32_t>(bt.n_choices, 1);
     uint8_t* gdec = ws.get<uint8_t>(K_GDEC, static_cast<size_t>(group_warps) * 8 * gdec_cap);
     uint8_t* glast = ws.get<uint8_t>(K_GLAST, static_cast<size_t>(group_warps) * 8 * kRenumberMax);

@@ -2,26 +2,32 @@
 //
 // The batched interpreters (k_values / k_derivs / k_intervals) walk one tape
 // with every thread of a block.  Instead of each warp fetching every clause
-// through the read-only cache, one thread per block copies the tape in
-// chunks of kStageClauses clauses into a two-slot ring in shared memory with
-// cp.async.bulk (completion counted on an mbarrier per slot), one chunk
-// ahead of the threads that read it.  Replaces the clause fetch of the
-// per-clause loops in ArrayEvaluator::values (libfive/src/eval/
+// through the read-only cache, one thread per block copies the tape into
+// shared memory with cp.async.bulk (completion counted on an mbarrier), and
+// every thread reads its clauses from there.  Replaces the clause fetch of
+// the per-clause loops in ArrayEvaluator::values (libfive/src/eval/
 // eval_array.cpp:112-114), DerivArrayEvaluator::derivs (eval_deriv_array.cpp:
 // 101-117) and IntervalEvaluator::eval (eval_interval.cpp:68-93).
 //
-// Layout in dynamic shared memory: [2 * kStageClauses clauses][2 mbarriers],
-// then the kernel's register planes (stage_bytes() from the start).
+// Two forms, by tape length:
+//  * resident (at most kResidentClauses clauses): the whole tape is copied
+//    once when the block starts and stays for all of the block's
+//    grid-stride passes; after the first wait no walk synchronises.
+//  * streamed (longer tapes): chunks of kStageClauses clauses go through a
+//    two-slot ring, one chunk ahead of the threads that read it.  Chunk j
+//    of a block's walk (counted over all of its passes) sits in slot j & 1
+//    and completes phase j >> 1 of that slot's mbarrier.  The copy of chunk
+//    j + 1 is issued when chunk j is about to be read; its slot last held
+//    chunk j - 1, which every thread finished before the block barrier that
+//    ends chunk j - 1.
 //
-// Chunk j of a block's walk (counted over all of its grid-stride passes)
-// sits in slot j & 1 and completes phase j >> 1 of that slot's mbarrier.
-// The copy of chunk j + 1 is issued when chunk j is about to be read; its
-// slot last held chunk j - 1, which every thread finished before the block
-// barrier that ends chunk j - 1.  Copies are tape-aligned (the tape's device
-// allocation is padded to an even clause count, so every copy is a multiple
-// of 16 bytes from a 16-byte aligned address).  Waits are bounded: a copy
-// that does not land within the limit sets lfb_stage_fault and the block
-// returns after waiting (again bounded) for its other copy in flight.
+// Layout in dynamic shared memory: the clause buffer (stage_bytes(n) -
+// 16 bytes), then 2 mbarriers, then the kernel's register planes.  Copies
+// are tape-aligned: the tape's device allocation is padded to an even clause
+// count, so every copy is a multiple of 16 bytes from a 16-byte aligned
+// address.  Waits are bounded: a copy that does not land within the limit
+// sets lfb_stage_fault and the block returns after waiting (again bounded)
+// for its other copy in flight.
 #pragma once
 #include <cstdint>
 
@@ -30,15 +36,19 @@
 namespace lfb {
 
 constexpr uint32_t kStageClauses = 512;
+constexpr uint32_t kResidentClauses = 2048;
 
 // Set (to 1) by a block whose clause copy did not complete in time (one
 // per translation unit that includes this header; the file that launches
 // the kernels reads and clears it).
 static __device__ unsigned int lfb_stage_fault = 0;
 
-__host__ __device__ constexpr size_t stage_bytes()
+/// Shared memory of the clause buffer and its mbarriers for a tape of n
+/// clauses (a multiple of 16 bytes).
+__host__ __device__ constexpr size_t stage_bytes(uint32_t n)
 {
-    return 2 * kStageClauses * sizeof(RegClause) + 2 * sizeof(uint64_t);
+    return (n <= kResidentClauses ? ((n + 1) & ~1u) : 2 * kStageClauses) * sizeof(RegClause) +
+           2 * sizeof(uint64_t);
 }
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p)
@@ -74,10 +84,12 @@ public:
     __device__ ClauseStage(const DevTape& t, void* smem, uint32_t passes)
         : src_(t.clauses), n_(t.n),
           ring_(static_cast<RegClause*>(smem)),
-          bar_(reinterpret_cast<uint64_t*>(static_cast<RegClause*>(smem) +
-                                            2 * kStageClauses)),
-          chunks_((t.n + kStageClauses - 1) / kStageClauses),
-          total_(chunks_ * passes), j_(0)
+          bar_(reinterpret_cast<uint64_t*>(static_cast<unsigned char*>(smem) +
+                                            stage_bytes(t.n) - 2 * sizeof(uint64_t))),
+          resident_(t.n <= kResidentClauses),
+          chunks_(t.n <= kResidentClauses ? (t.n ? 1 : 0)
+                                          : (t.n + kStageClauses - 1) / kStageClauses),
+          total_(resident_ ? chunks_ * (passes ? 1 : 0) : chunks_ * passes), j_(0)
     {
         if (threadIdx.x == 0) {
             for (int s = 0; s < 2; ++s) {
@@ -96,6 +108,19 @@ public:
     template <class F>
     __device__ __forceinline__ bool walk(F&& f)
     {
+        if (resident_) {
+            if (j_ < total_) {   // the first walk waits for the copy
+                const bool ok = mbar_wait_bounded(bar_, 0);
+                if (__syncthreads_or(!ok)) {
+                    give_up();
+                    return false;
+                }
+                j_ = total_;
+            }
+            const uint2* c = reinterpret_cast<const uint2*>(ring_);
+            for (uint32_t k = 0; k < n_; ++k) run(f, c[k]);
+            return true;
+        }
         for (uint32_t ck = 0; ck < chunks_; ++ck, ++j_) {
             if (threadIdx.x == 0 && j_ + 1 < total_) issue(j_ + 1);
             const bool ok = mbar_wait_bounded(bar_ + (j_ & 1), (j_ >> 1) & 1);
@@ -105,14 +130,7 @@ public:
             }
             const uint2* c = reinterpret_cast<const uint2*>(ring_ + (j_ & 1) * kStageClauses);
             const uint32_t m = min(kStageClauses, n_ - ck * kStageClauses);
-            for (uint32_t k = 0; k < m; ++k) {
-                const uint2 raw = c[k];
-                f(static_cast<uint8_t>(raw.x & 0xff),
-                  static_cast<uint8_t>((raw.x >> 8) & 0xff),
-                  static_cast<uint16_t>(raw.x >> 16),
-                  static_cast<uint16_t>(raw.y & 0xffff),
-                  static_cast<uint16_t>(raw.y >> 16));
-            }
+            for (uint32_t k = 0; k < m; ++k) run(f, c[k]);
             __syncthreads();
         }
         return true;
@@ -129,13 +147,24 @@ public:
     }
 
 private:
+    template <class F>
+    __device__ __forceinline__ static void run(F& f, const uint2 raw)
+    {
+        f(static_cast<uint8_t>(raw.x & 0xff),
+          static_cast<uint8_t>((raw.x >> 8) & 0xff),
+          static_cast<uint16_t>(raw.x >> 16),
+          static_cast<uint16_t>(raw.y & 0xffff),
+          static_cast<uint16_t>(raw.y >> 16));
+    }
+
     __device__ __forceinline__ void issue(uint32_t j)
     {
         const uint32_t ck = j % chunks_;
         const uint32_t first = ck * kStageClauses;
-        const uint32_t m = min(kStageClauses, n_ - first);
+        const uint32_t m = resident_ ? n_ : min(kStageClauses, n_ - first);
         const uint32_t bytes = ((m + 1) & ~1u) * static_cast<uint32_t>(sizeof(RegClause));
         uint64_t* bar = bar_ + (j & 1);
+        RegClause* dst = resident_ ? ring_ : ring_ + (j & 1) * kStageClauses;
         // the slot's previous contents were read through the generic proxy
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
@@ -143,8 +172,7 @@ private:
         asm volatile(
             "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes"
             " [%0], [%1], %2, [%3];"
-            :: "r"(smem_addr(ring_ + (j & 1) * kStageClauses)),
-               "l"(src_ + first), "r"(bytes), "r"(smem_addr(bar))
+            :: "r"(smem_addr(dst)), "l"(src_ + first), "r"(bytes), "r"(smem_addr(bar))
             : "memory");
     }
 
@@ -155,7 +183,7 @@ private:
         if (threadIdx.x == 0) {
             atomicExch(&lfb_stage_fault, 1u);
             const uint32_t nx = j_ + 1;
-            if (nx < total_) mbar_wait_bounded(bar_ + (nx & 1), (nx >> 1) & 1);
+            if (!resident_ && nx < total_) mbar_wait_bounded(bar_ + (nx & 1), (nx >> 1) & 1);
             mbar_wait_bounded(bar_ + (j_ & 1), (j_ >> 1) & 1);
         }
         __syncthreads();
@@ -165,6 +193,7 @@ private:
     uint32_t n_;
     RegClause* ring_;
     uint64_t* bar_;
+    bool resident_;
     uint32_t chunks_;
     uint32_t total_;
     uint32_t j_;

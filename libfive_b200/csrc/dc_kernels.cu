@@ -812,9 +812,7 @@ __host__ __device__ inline size_t group_smem_per_warp(uint32_t nregs_max)
     return (b + 15) / 16 * 16;
 }
 
-// 12 blocks of 4 warps per SM (40 registers): the kernel is latency-bound,
-// so resident warps are what it needs.
-__global__ void __launch_bounds__(128, 12)
+__global__ void __launch_bounds__(128)
 k_interval_group(GroupArgs A, int d)
 {
     extern __shared__ __align__(16) unsigned char gsm[];
@@ -2911,7 +2909,7 @@ int render_once(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_
 
     // Deep levels (many cells, short tapes) switch to one warp per sibling
     // group over register tapes; every level below stays in that mode.
-    const uint32_t group_warps = static_cast<uint32_t>(device_sm_count()) * 48;
+    const uint32_t group_warps = static_cast<uint32_t>(device_sm_count()) * 32;
     const uint32_t gdec_cap = std::max<uint32_t>(bt.n_choices, 1);
     uint8_t* gdec = ws.get<uint8_t>(K_GDEC, static_cast<size_t>(group_warps) * 8 * gdec_cap);
     uint8_t* glast = ws.get<uint8_t>(K_GLAST, static_cast<size_t>(group_warps) * 8 * kRenumberMax);
@@ -3549,6 +3547,17 @@ int render_dc_meshes(MeshJob* jobs, size_t n, unsigned workers)
                              j.want_stats ? &j.stats : nullptr, j.cancel);
             if (j.rc != 0) last_error(&j.err);
         }
+    }
+
+    // The side contexts give their scratch back, so that single-mesh calls
+    // (and other work on the device) after a batch find the memory free;
+    // context 0, which renders the large meshes, keeps its buffers for the
+    // next batch.
+    for (unsigned k = 1; k < workers; ++k) {
+        Workspace* w = stream_workspace(k);
+        std::lock_guard<std::mutex> lock(w->mu);
+        cudaStreamSynchronize(w->s);
+        w->bufs.clear();
     }
 
     clear_error();

@@ -37,7 +37,7 @@ k_values(DevTape t, uint32_t n, const float* __restrict__ X,
     const int tid0 = threadIdx.x;
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * B;
     ClauseStage stage(t, smem_raw, block_passes(n, B));
-    float* R = reinterpret_cast<float*>(smem_raw + stage_bytes());
+    float* R = reinterpret_cast<float*>(smem_raw + stage_bytes(t.n));
     const float* __restrict__ cp = t.cpool;
     for (uint64_t base = static_cast<uint64_t>(blockIdx.x) * B; base < n;
          base += stride) {
@@ -95,7 +95,7 @@ k_derivs(DevTape t, uint32_t n, const float* __restrict__ X,
     const int tid = threadIdx.x;
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * B;
     ClauseStage stage(t, smem_raw, block_passes(n, B));
-    float* R = reinterpret_cast<float*>(smem_raw + stage_bytes());
+    float* R = reinterpret_cast<float*>(smem_raw + stage_bytes(t.n));
     const float* __restrict__ cp = t.cpool;
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * B + tid;
          i - tid < n; i += stride) {
@@ -154,7 +154,7 @@ k_intervals(DevTape t, uint32_t n,
     const int B = blockDim.x;
     const int tid = threadIdx.x;
     ClauseStage stage(t, smem_raw, block_passes(n, B));
-    float* R = reinterpret_cast<float*>(smem_raw + stage_bytes());
+    float* R = reinterpret_cast<float*>(smem_raw + stage_bytes(t.n));
     uint8_t* N = reinterpret_cast<uint8_t*>(R + t.n_regs * 2 * B);
     const float* __restrict__ cp = t.cpool;
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * B;
@@ -251,7 +251,7 @@ cudaError_t launch_values(const DevTape& t, uint32_t n, const float* x,
     const int block = 128;
     const size_t planes = static_cast<size_t>(t.n_regs) * block * PTS * sizeof(float);
     if (planes > 200 * 1024) return cudaErrorInvalidConfiguration;
-    const size_t smem = stage_bytes() + planes;
+    const size_t smem = stage_bytes(t.n) + planes;
     if (!raise_smem_limit(reinterpret_cast<const void*>(k_values<PTS>), smem)) {
         return cudaErrorInvalidValue;
     }
@@ -268,7 +268,7 @@ cudaError_t launch_derivs(const DevTape& t, uint32_t n, const float* x,
     const int block = 128;
     const size_t planes = static_cast<size_t>(t.n_regs) * block * 4 * sizeof(float);
     if (planes > 200 * 1024) return cudaErrorInvalidConfiguration;
-    const size_t smem = stage_bytes() + planes;
+    const size_t smem = stage_bytes(t.n) + planes;
     if (!raise_smem_limit(reinterpret_cast<const void*>(k_derivs), smem)) {
         return cudaErrorInvalidValue;
     }
@@ -287,7 +287,7 @@ cudaError_t launch_intervals(const DevTape& t, uint32_t n, const float* xlo,
     const int block = 128;
     const size_t planes = static_cast<size_t>(t.n_regs) * block * (2 * sizeof(float) + 1);
     if (planes > 200 * 1024) return cudaErrorInvalidConfiguration;
-    const size_t smem = stage_bytes() + planes;
+    const size_t smem = stage_bytes(t.n) + planes;
     if (!raise_smem_limit(reinterpret_cast<const void*>(k_intervals), smem)) {
         return cudaErrorInvalidValue;
     }

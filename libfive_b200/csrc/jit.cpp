@@ -508,6 +508,10 @@ std::string backward_source(const RegTape& t, const std::vector<uint32_t>& slots
 // expressions as the partials / backward kernels', in the same order.
 
 constexpr uint32_t kJitSegClauses = 192;
+/// Threads per block of the checkpointed forward (40 registers: three
+/// blocks on an SM) and backward (64 registers: one block) kernels.
+constexpr unsigned kCkptFwdBlock = 512;
+constexpr unsigned kCkptBwdBlock = 1024;
 
 struct JitSeg {
     uint32_t c0 = 0, c1 = 0;
@@ -570,14 +574,15 @@ std::string fseg_source(const RegTape& t, const JitSeg& sg, uint32_t k, bool ckp
 {
     std::string s = "__device__ __noinline__ void fseg" + std::to_string(k) +
                     "(float* __restrict__ R, float* __restrict__ Ci, unsigned m, "
-                    "const float* __restrict__ cp)\n{\n";
+                    "const float* __restrict__ cp, int ok)\n{\n";
     std::vector<std::string> name(t.n_regs);
     for (size_t j = 0; j < sg.live_in.size(); ++j) {
         const uint32_t r = sg.live_in[j];
         name[r] = "v" + std::to_string(r);
         s += "    const float " + name[r] + " = R[" + std::to_string(r) + "];\n";
         if (ckpt) {
-            s += "    Ci[(size_t)" + std::to_string(sg.ck_base + j) + " * m] = " + name[r] + ";\n";
+            s += "    if (ok) Ci[(size_t)" + std::to_string(sg.ck_base + j) + " * m] = " + name[r] +
+                 ";\n";
         }
     }
     for (uint32_t c = sg.c0; c < sg.c1; ++c) {
@@ -621,7 +626,7 @@ std::string values_source_segmented(const RegTape& t)
          "        for (int r = 3; r < " + std::to_string(t.n_regs) + "; ++r) R[r] = 0.0f;\n"
          "        R[0] = X[i]; R[1] = Y[i]; R[2] = Z[i];\n";
     for (uint32_t k = 0; k < segs.size(); ++k) {
-        s += "        fseg" + std::to_string(k) + "(R, nullptr, 0u, cp);\n";
+        s += "        fseg" + std::to_string(k) + "(R, nullptr, 0u, cp, 0);\n";
     }
     s += "        out[i] = " + root_from_R(t) + ";\n    }\n}\n";
     return s;
@@ -637,19 +642,24 @@ std::string ckpt_forward_source(const RegTape& t)
         if (f.empty()) return std::string();
         s += f;
     }
-    s += "extern \"C\" __global__ void __launch_bounds__(256)\n"
+    // The segments are long straight-line code: a block barrier before
+    // each keeps the block's warps in the same segment, so that they share
+    // its instruction fetches (every thread runs every segment; those past
+    // the last point compute on point 0 and store nothing).
+    s += "extern \"C\" __global__ void __launch_bounds__(" + std::to_string(kCkptFwdBlock) + ")\n"
          "lfb_tape_ckpt_fwd(const float* __restrict__ X, const float* __restrict__ Y,\n"
          "                  const float* __restrict__ Z, float* __restrict__ C,\n"
          "                  float* __restrict__ f, unsigned m, const float* __restrict__ cp)\n{\n"
          "    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;\n"
-         "    if (i >= m) return;\n";
+         "    const int ok = i < m;\n"
+         "    const unsigned ii = ok ? i : 0u;\n";
     s += "    float R[" + std::to_string(t.n_regs) + "];\n"
          "    for (int r = 3; r < " + std::to_string(t.n_regs) + "; ++r) R[r] = 0.0f;\n"
-         "    R[0] = X[i]; R[1] = Y[i]; R[2] = Z[i];\n";
+         "    R[0] = X[ii]; R[1] = Y[ii]; R[2] = Z[ii];\n";
     for (uint32_t k = 0; k < segs.size(); ++k) {
-        s += "    fseg" + std::to_string(k) + "(R, C + i, m, cp);\n";
+        s += "    __syncthreads();\n    fseg" + std::to_string(k) + "(R, C + ii, m, cp, ok);\n";
     }
-    s += "    if (f) f[i] = " + root_from_R(t) + ";\n}\n";
+    s += "    if (ok && f) f[i] = " + root_from_R(t) + ";\n}\n";
     return s;
 }
 
@@ -813,9 +823,11 @@ std::string ckpt_backward_source(const RegTape& t)
          "    const unsigned k = lfb_vidx[base + lane];\n"
          "    if (k != 0xffffu && v[0] != 0.0f) atomicAdd(Gv + k, v[0]);\n}\n";
     s += body;
-    // at most 64 registers a thread: four blocks of 256 threads on an SM,
-    // enough warps to cover the instruction fetches of this long code
-    s += "extern \"C\" __global__ void __launch_bounds__(256, 4)\n"
+    // at most 64 registers a thread: one block of 1024 threads on an SM,
+    // with a block barrier before each segment, so that all of the SM's
+    // warps run the same segment and share its instruction fetches
+    s += "extern \"C\" __global__ void __launch_bounds__(" + std::to_string(kCkptBwdBlock) +
+         ", 1)\n"
          "lfb_tape_ckpt_bwd(const float* __restrict__ C, const float* __restrict__ seed,\n"
          "                  float* __restrict__ gx, float* __restrict__ gy,\n"
          "                  float* __restrict__ gz, float* __restrict__ gvars, unsigned m,\n"
@@ -838,7 +850,8 @@ std::string ckpt_backward_source(const RegTape& t)
         s += "    if (gv) lfb_add_var(Gv, " + std::to_string(t.root - t.n_const) + ", s0);\n";
     }
     for (uint32_t k = static_cast<uint32_t>(segs.size()); k-- > 0;) {
-        s += "    bseg" + std::to_string(k) + "(A, Ci, m, cp, Gv, gv, block_cv, ok);\n";
+        s += "    __syncthreads();\n    bseg" + std::to_string(k) +
+             "(A, Ci, m, cp, Gv, gv, block_cv, ok);\n";
     }
     s += "    if (ok) {\n"
          "        if (gx) gx[i] = A[0];\n        if (gy) gy[i] = A[1];\n        if (gz) gz[i] = A[2];\n"
@@ -915,10 +928,11 @@ void* kernel(GpuTape& g, int k, const std::vector<uint32_t>* slots = nullptr)
     return j.state == 1 ? j.function : nullptr;
 }
 
-bool launch_1d(void* fn, uint32_t m, void** args, unsigned smem, cudaStream_t s)
+bool launch_1d(void* fn, uint32_t m, void** args, unsigned smem, cudaStream_t s,
+               unsigned block = 256)
 {
-    const unsigned blocks = (m + 255) / 256;
-    if (api().launch(static_cast<CUfunction>(fn), blocks, 1, 1, 256, 1, 1, smem,
+    const unsigned blocks = (m + block - 1) / block;
+    if (api().launch(static_cast<CUfunction>(fn), blocks, 1, 1, block, 1, 1, smem,
                      reinterpret_cast<CUstream>(s), args, nullptr) != CUDA_SUCCESS) {
         return false;
     }
@@ -1030,7 +1044,7 @@ bool jit_ckpt_forward(GpuTape& g, uint32_t m, const float* x, const float* y, co
     if (m == 0) return true;
     const float* cp = g.d_cpool;
     void* args[] = {&x, &y, &z, &C, &f, &m, &cp};
-    return launch_1d(fn, m, args, 0, s);
+    return launch_1d(fn, m, args, 0, s, kCkptFwdBlock);
 }
 
 bool jit_ckpt_backward(GpuTape& g, uint32_t m, const float* C, const float* seed, float* gx,
@@ -1045,7 +1059,7 @@ bool jit_ckpt_backward(GpuTape& g, uint32_t m, const float* C, const float* seed
     if (m == 0) return true;
     const float* cp = g.d_cpool;
     void* args[] = {&C, &seed, &gx, &gy, &gz, &gvars, &m, &n_vars, &block_cv, &cp, &seed_scale};
-    return launch_1d(fn, m, args, smem, s);
+    return launch_1d(fn, m, args, smem, s, kCkptBwdBlock);
 }
 
 bool jit_compile(const std::string& src, std::vector<char>* cubin, std::string* log)

@@ -215,4 +215,135 @@ inline void build_dc_tables(DcTables& t)
     }
 }
 
+////////////////////////////////////////////////////////////////////////////////
+// Quadtree tables (MarchingTable<2>, DCTree<2>::cornersAreManifold), built
+// the same way: the four base cases of marching squares (marching.cpp:
+// 66-96) closed under the 90-degree rotation of the square, directed edges
+// numbered in order of first appearance.  Corner i of a square cell is at
+// (i & 1 ? upper.x : lower.x, i & 2 ? upper.y : lower.y).
+
+struct DcTables2 {
+    int8_t v[16][2][4][2];   // v[mask][patch][k] = {filled, empty}, -1 terminated
+    int8_t e[4][4];          // directed edge id (0..7) of a corner pair, -1 otherwise
+    int8_t p[16][8];         // patch containing a directed edge, -1 otherwise
+    uint8_t manifold[16];
+    uint8_t npatch[16];
+    uint8_t nedge[16][2];
+};
+
+namespace dc_tables_detail {
+
+// +90 degrees about the square's centre: (x, y) -> (-y, x)
+inline int rotate_vertex2(int v)
+{
+    const int x = (v & 1) ? 1 : -1, y = (v & 2) ? 1 : -1;
+    return (-y > 0 ? 1 : 0) | (x > 0 ? 2 : 0);
+}
+
+inline int rotate_mask2(int mask)
+{
+    int out = 0;
+    for (int i = 0; i < 4; ++i) {
+        if (mask & (1 << i)) out |= 1 << rotate_vertex2(i);
+    }
+    return out;
+}
+
+/// The contraction test of corners_manifold on the square's four edges.
+inline bool corners_manifold2(int index)
+{
+    int f[4];
+    for (int i = 0; i < 4; ++i) f[i] = (index >> i) & 1;
+    int edges[4][2] = {{0, 1}, {0, 2}, {1, 3}, {2, 3}};
+    int ne = 4;
+    for (;;) {
+        int hit = -1;
+        for (int k = 0; k < ne; ++k) {
+            if (f[edges[k][0]] == f[edges[k][1]]) { hit = k; break; }
+        }
+        if (hit < 0) break;
+        const int a = edges[hit][0], b = edges[hit][1];
+        int m = 0;
+        for (int k = 0; k < ne; ++k) {
+            const int e0 = edges[k][0] == a ? b : edges[k][0];
+            const int e1 = edges[k][1] == a ? b : edges[k][1];
+            if (e0 != e1) {
+                edges[m][0] = e0;
+                edges[m][1] = e1;
+                ++m;
+            }
+        }
+        ne = m;
+    }
+    int distinct = 0;
+    for (int k = 0; k < ne; ++k) {
+        const int lo = edges[k][0] < edges[k][1] ? edges[k][0] : edges[k][1];
+        const int hi = edges[k][0] < edges[k][1] ? edges[k][1] : edges[k][0];
+        bool seen = false;
+        for (int q = 0; q < k; ++q) {
+            const int lo2 = edges[q][0] < edges[q][1] ? edges[q][0] : edges[q][1];
+            const int hi2 = edges[q][0] < edges[q][1] ? edges[q][1] : edges[q][0];
+            if (lo == lo2 && hi == hi2) { seen = true; break; }
+        }
+        if (!seen) ++distinct;
+    }
+    return distinct <= 1;
+}
+
+}  // namespace dc_tables_detail
+
+inline void build_dc_tables2(DcTables2& t)
+{
+    using namespace dc_tables_detail;
+    std::memset(t.v, -1, sizeof(t.v));
+    std::memset(t.e, -1, sizeof(t.e));
+    std::memset(t.p, -1, sizeof(t.p));
+    // {mask, patch, k, filled corner, empty corner}
+    static const int base[][5] = {
+        {1, 0, 0, 0, 1}, {1, 0, 1, 0, 2},
+        {3, 0, 0, 1, 3}, {3, 0, 1, 0, 2},
+        {9, 0, 0, 0, 1}, {9, 0, 1, 0, 2}, {9, 1, 0, 3, 2}, {9, 1, 1, 3, 1},
+        {7, 0, 0, 1, 3}, {7, 0, 1, 2, 3},
+    };
+    for (const auto& b : base) {
+        t.v[b[0]][b[1]][b[2]][0] = static_cast<int8_t>(b[3]);
+        t.v[b[0]][b[1]][b[2]][1] = static_cast<int8_t>(b[4]);
+    }
+    bool changed[16];
+    for (int i = 0; i < 16; ++i) changed[i] = t.v[i][0][0][0] != -1;
+    bool any = true;
+    while (any) {
+        any = false;
+        for (int i = 0; i < 16; ++i) {
+            if (!changed[i]) continue;
+            changed[i] = false;
+            const int j = rotate_mask2(i);
+            if (t.v[j][0][0][0] != -1) continue;
+            changed[j] = true;
+            any = true;
+            for (int p = 0; p < 2 && t.v[i][p][0][0] != -1; ++p) {
+                for (int e = 0; e < 4 && t.v[i][p][e][0] != -1; ++e) {
+                    t.v[j][p][e][0] = static_cast<int8_t>(rotate_vertex2(t.v[i][p][e][0]));
+                    t.v[j][p][e][1] = static_cast<int8_t>(rotate_vertex2(t.v[i][p][e][1]));
+                }
+            }
+        }
+    }
+    int next = 0;
+    for (int i = 0; i < 16; ++i) {
+        t.npatch[i] = 0;
+        t.nedge[i][0] = t.nedge[i][1] = 0;
+        for (int p = 0; p < 2 && t.v[i][p][0][0] != -1; ++p) {
+            t.npatch[i] = static_cast<uint8_t>(p + 1);
+            for (int e = 0; e < 4 && t.v[i][p][e][0] != -1; ++e) {
+                t.nedge[i][p] = static_cast<uint8_t>(e + 1);
+                int8_t& id = t.e[t.v[i][p][e][0]][t.v[i][p][e][1]];
+                if (id == -1) id = static_cast<int8_t>(next++);
+                t.p[i][id] = static_cast<int8_t>(p);
+            }
+        }
+        t.manifold[i] = corners_manifold2(i) ? 1 : 0;
+    }
+}
+
 }  // namespace lfb

@@ -239,6 +239,16 @@ double ora_qef_vertex(const double ata[6], const double atb[3], double btb,
     for (int i = 0; i < 4; ++i) q.mass[i] = mass[i];
     return lfb::qef_vertex(q, v, rank);
 }
+/// The quadtree form: q = {ata xx, xy, yy, atb x, y, btb, mass x, y, count}.
+double ora_qef2_vertex(const double q9[9], double v[2], int* rank)
+{
+    lfb::Qef2 q;
+    for (int i = 0; i < 3; ++i) q.ata[i] = q9[i];
+    for (int i = 0; i < 2; ++i) q.atb[i] = q9[3 + i];
+    q.btb = q9[5];
+    for (int i = 0; i < 3; ++i) q.mass[i] = q9[6 + i];
+    return lfb::qef2_vertex(q, v, rank);
+}
 }
 
 // The mesher's constant tables (dc_tables.hpp), for checks against the

@@ -73,3 +73,25 @@ def hausdorff(v1, t1, v2, t2):
     da, _ = cKDTree(b).query(a)
     db, _ = cKDTree(a).query(b)
     return float(max(da.max(), db.max()))
+
+
+def canonical_contours(contours):
+    """Contours as a sorted list of tuples of float32 bit patterns: closed
+    contours (first point == last) lose the repeated point and are rotated
+    to start at their smallest point, so that the segment order in which
+    they were welded does not matter."""
+    out = []
+    for c in contours:
+        c = np.asarray(c, np.float32).reshape(-1, 2)
+        bits = [tuple(p) for p in c.view(np.uint32).tolist()]
+        if len(bits) > 1 and bits[0] == bits[-1]:
+            bits = bits[:-1]
+            k = min(range(len(bits)), key=lambda i: bits[i])
+            bits = bits[k:] + bits[:k]
+            bits.append(bits[0])
+        out.append(tuple(bits))
+    return sorted(out)
+
+
+def same_contours(a, b):
+    return canonical_contours(a) == canonical_contours(b)

@@ -45,6 +45,13 @@ def load():
             _lib.ora_time_mesh.argtypes = [vp] + [ctypes.c_float] * 6 + [
                 ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, vp,
                 ctypes.POINTER(ctypes.c_uint32)]
+        _lib.ora_render_contours.restype = ctypes.c_int
+        _lib.ora_render_contours.argtypes = [vp] + [ctypes.c_double] * 7 + [
+            ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(vp),
+            ctypes.POINTER(ctypes.c_uint32)]
+        _lib.ora_dc_tables2.argtypes = [vp]
+        _lib.ora_weld.restype = ctypes.c_uint32
+        _lib.ora_weld.argtypes = [vp, ctypes.c_uint32, vp, vp]
         _lib.ora_libm_mode.argtypes = [ctypes.c_int]
         _lib.ora_libm_table.argtypes = [vp, vp, ctypes.c_uint64]
         _lib.ora_libm_take.restype = ctypes.c_uint64
@@ -166,3 +173,52 @@ def render_heightmap(tape, lower, upper, res, workers=8):
     norm = np.zeros((h, w), np.uint32)
     load().ora_render_heightmap(tape.h, _p(lo), _p(hi), _p(r), workers, _p(depth), _p(norm))
     return depth, norm
+
+
+def render_contours(tape, lo, hi, z, min_feature, max_err=1e-8):
+    """Contours::render restated: (list of [n, 2] float32 point arrays, depth)."""
+    lib = load()
+    pp, cp = ctypes.c_void_p(), ctypes.c_void_p()
+    npt, nc = ctypes.c_uint32(), ctypes.c_uint32()
+    depth = lib.ora_render_contours(tape.h, lo[0], lo[1], hi[0], hi[1], z, min_feature, max_err,
+                                    ctypes.byref(pp), ctypes.byref(npt), ctypes.byref(cp),
+                                    ctypes.byref(nc))
+    pts = np.ctypeslib.as_array(ctypes.cast(pp, ctypes.POINTER(ctypes.c_float)),
+                                shape=(max(npt.value, 1) * 2,)).reshape(-1, 2)[:npt.value].copy()
+    counts = np.ctypeslib.as_array(ctypes.cast(cp, ctypes.POINTER(ctypes.c_uint32)),
+                                   shape=(max(nc.value, 1),))[:nc.value].copy()
+    lib.ora_free(pp)
+    lib.ora_free(cp)
+    out, k = [], 0
+    for c in counts:
+        out.append(pts[k:k + c])
+        k += c
+    return out, depth
+
+
+def dc_tables2():
+    """DcTables2 as numpy arrays (v, e, p, manifold, npatch, nedge)."""
+    raw = np.zeros(16 * 2 * 4 * 2 + 16 + 16 * 8 + 16 + 16 + 32, np.int8)
+    load().ora_dc_tables2(raw.ctypes.data)
+    o = 0
+    v = raw[o:o + 256].reshape(16, 2, 4, 2); o += 256
+    e = raw[o:o + 16].reshape(4, 4); o += 16
+    p = raw[o:o + 128].reshape(16, 8); o += 128
+    manifold = raw[o:o + 16].view(np.uint8); o += 16
+    npatch = raw[o:o + 16].view(np.uint8); o += 16
+    nedge = raw[o:o + 32].view(np.uint8).reshape(16, 2)
+    return v, e, p, manifold, npatch, nedge
+
+
+def weld(segs):
+    """Contours::collect's welding of directed segments [(a, b), ...]:
+    lists of vertex ids."""
+    segs = np.ascontiguousarray(segs, np.uint32).reshape(-1, 2)
+    out = np.zeros(2 * len(segs) + 1, np.uint32)
+    counts = np.zeros(len(segs) + 1, np.uint32)
+    n = load().ora_weld(segs.ctypes.data, len(segs), out.ctypes.data, counts.ctypes.data)
+    res, k = [], 0
+    for c in counts[:n]:
+        res.append(out[k:k + c].tolist())
+        k += c
+    return res

@@ -217,6 +217,14 @@ libfive_mesh* lfb_render_mesh(lfb_tape t, libfive_region3 R,
                               lfb_mesh_settings settings,
                               lfb_mesh_stats* stats);
 
+/* Contours::render (contours.cpp:25-49) on the GPU: the contours of the
+ * slice z of the tape over the region R, with BRepSettings' min_feature and
+ * max_err (libfive_tree_render_slice uses 1 / res and 1e-8).  Freed with
+ * libfive_contours_delete; NULL on failure (lfb_last_error says why).  A
+ * closed contour repeats its first point at its end. */
+libfive_contours* lfb_render_slice(lfb_tape t, libfive_region2 R, float z,
+                                   double min_feature, double max_err);
+
 /* Heightmap::render (heightmap.cpp:247-296) on the GPU over the Voxels
  * region (voxels.cpp:16-44) of lower / upper / res (per-axis voxels per
  * unit; 0 gives one sample).  dims receives {cols, rows, z samples}; when

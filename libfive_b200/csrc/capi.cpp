@@ -13,6 +13,7 @@
 #include "libfive.h"
 #include "libfive_b200.h"
 #include "heightmap.hpp"
+#include "contours.hpp"
 #include "mesher.hpp"
 #include "eval_api.hpp"
 #include "runtime.hpp"
@@ -255,27 +256,108 @@ libfive_vec3 libfive_tree_eval_d(libfive_tree t, libfive_vec3 p)
 ////////////////////////////////////////////////////////////////////////////////
 // Outside the evaluate-and-mesh path
 
-libfive_contours* libfive_tree_render_slice(libfive_tree, libfive_region2,
-                                            float, float)
+static double min_feature_of(float res);
+
+/// Contours::render for the slice calls (libfive.cpp:233-304): the GPU
+/// contourer with BRepSettings' max_err (1e-8) and min_feature = 1 / res;
+/// false, with the message printed, on failure.
+static bool render_slice(const std::shared_ptr<GpuTape>& g, libfive_region2 R, float z,
+                         double min_feature, double max_err, ContoursOut& cs, const char* who)
 {
-    std::fprintf(stderr, "libfive_tree_render_slice: 2D contouring is not "
-                         "provided by libfive_b200\n");
-    return nullptr;
+    const double lo[2] = {R.X.lower, R.Y.lower}, hi[2] = {R.X.upper, R.Y.upper};
+    if (!g || render_contours(*g, lo, hi, z, min_feature, max_err, cs) != 0) {
+        std::string msg;
+        last_error(&msg);
+        std::fprintf(stderr, "%s: %s\n", who, msg.c_str());
+        return false;
+    }
+    return true;
 }
 
-libfive_contours3* libfive_tree_render_slice3(libfive_tree, libfive_region2,
-                                              float, float)
+/// The contours as the reference's C structs (arrays from new[], freed by
+/// libfive_contours_delete / libfive_contours3_delete).
+static libfive_contours* contours_struct(const ContoursOut& cs)
 {
-    std::fprintf(stderr, "libfive_tree_render_slice3: 2D contouring is not "
-                         "provided by libfive_b200\n");
-    return nullptr;
+    auto out = new libfive_contours;
+    out->count = static_cast<uint32_t>(cs.counts.size());
+    out->cs = new libfive_contour[out->count];
+    size_t k = 0;
+    for (uint32_t i = 0; i < out->count; ++i) {
+        out->cs[i].count = cs.counts[i];
+        out->cs[i].pts = new libfive_vec2[cs.counts[i]];
+        for (uint32_t j = 0; j < cs.counts[i]; ++j, ++k) {
+            out->cs[i].pts[j] = {cs.pts[2 * k], cs.pts[2 * k + 1]};
+        }
+    }
+    return out;
 }
 
-void libfive_tree_save_slice(libfive_tree, libfive_region2, float, float,
-                             const char*)
+static libfive_contours3* contours3_struct(const ContoursOut& cs, float z)
 {
-    std::fprintf(stderr, "libfive_tree_save_slice: 2D contouring is not "
-                         "provided by libfive_b200\n");
+    auto out = new libfive_contours3;
+    out->count = static_cast<uint32_t>(cs.counts.size());
+    out->cs = new libfive_contour3[out->count];
+    size_t k = 0;
+    for (uint32_t i = 0; i < out->count; ++i) {
+        out->cs[i].count = cs.counts[i];
+        out->cs[i].pts = new libfive_vec3[cs.counts[i]];
+        for (uint32_t j = 0; j < cs.counts[i]; ++j, ++k) {
+            out->cs[i].pts[j] = {cs.pts[2 * k], cs.pts[2 * k + 1], z};
+        }
+    }
+    return out;
+}
+
+libfive_contours* libfive_tree_render_slice(libfive_tree tree, libfive_region2 R,
+                                            float z, float res)
+{
+    if (!tree) return nullptr;
+    ContoursOut cs;
+    if (!render_slice(cached_tape(N(tree)), R, z, min_feature_of(res), 1e-8, cs,
+                      "libfive_tree_render_slice")) {
+        return nullptr;
+    }
+    return contours_struct(cs);
+}
+
+libfive_contours3* libfive_tree_render_slice3(libfive_tree tree, libfive_region2 R,
+                                              float z, float res)
+{
+    if (!tree) return nullptr;
+    ContoursOut cs;
+    if (!render_slice(cached_tape(N(tree)), R, z, min_feature_of(res), 1e-8, cs,
+                      "libfive_tree_render_slice3")) {
+        return nullptr;
+    }
+    // each 2D point gets z as its third coordinate (libfive.cpp:289-293)
+    return contours3_struct(cs, z);
+}
+
+void libfive_tree_save_slice(libfive_tree tree, libfive_region2 R, float z, float res,
+                             const char* f)
+{
+    if (!tree || !f) return;
+    ContoursOut cs;
+    if (!render_slice(cached_tape(N(tree)), R, z, min_feature_of(res), 1e-8, cs,
+                      "libfive_tree_save_slice")) {
+        return;
+    }
+    const double lo[2] = {R.X.lower, R.Y.lower}, hi[2] = {R.X.upper, R.Y.upper};
+    save_svg(f, cs, lo, hi);
+}
+
+libfive_contours* lfb_render_slice(lfb_tape t, libfive_region2 R, float z,
+                                   double min_feature, double max_err)
+{
+    auto g = tape_of(t);
+    ContoursOut cs;
+    if (!g) {
+        set_error(LFB_E_INVALID, "null tape");
+        return nullptr;
+    }
+    const double lo[2] = {R.X.lower, R.Y.lower}, hi[2] = {R.X.upper, R.Y.upper};
+    if (render_contours(*g, lo, hi, z, min_feature, max_err, cs) != 0) return nullptr;
+    return contours_struct(cs);
 }
 
 libfive_pixels* libfive_tree_render_pixels(libfive_tree tree, libfive_region2 R,

@@ -1,10 +1,12 @@
 #include <algorithm>
+#include <cctype>
 #include <cstdio>
 #include <cstring>
 #include <string>
 #include <thread>
 #include <vector>
 
+#include "contours.hpp"
 #include "mesher.hpp"
 
 namespace lfb {
@@ -71,6 +73,53 @@ bool save_stl(const char* path, const std::vector<libfive_mesh*>& meshes)
     const bool ok = std::ferror(f) == 0;
     std::fclose(f);
     return ok;
+}
+
+/// Contours::saveSVG (contours.cpp:51-116): one path per contour, y
+/// flipped into the bounding box, "Z" closing a contour whose last point
+/// repeats its first; numbers in the stream's default format (%g).
+bool save_svg(const char* path, const ContoursOut& cs, const double lo[2], const double hi[2])
+{
+    const std::string name(path);
+    const auto ends_with = [&](const char* suf) {
+        const size_t n = std::strlen(suf);
+        if (name.size() < n) return false;
+        for (size_t k = 0; k < n; ++k) {
+            const char a = name[name.size() - n + k];
+            if (std::tolower(static_cast<unsigned char>(a)) != suf[k]) return false;
+        }
+        return true;
+    };
+    if (!ends_with(".svg")) {
+        std::fprintf(stderr, "Contours::saveSVG: filename \"%s\" does not end in .svg\n", path);
+    }
+    FILE* f = std::fopen(path, "w");
+    if (!f) {
+        std::printf("Contours::saveSVG: could not open %s\n", path);
+        return false;
+    }
+    std::fprintf(f,
+                 "<?xml version=\"1.0\" encoding=\"UTF-8\" standalone=\"no\"?>\n"
+                 "<svg xmlns=\"http://www.w3.org/2000/svg\" version=\"1.1\"\n"
+                 " width=\"%g\" height=\"%g\" id=\"libfive\">\n",
+                 hi[0] - lo[0], hi[1] - lo[1]);
+    size_t k = 0;
+    for (uint32_t n : cs.counts) {
+        const float* p = cs.pts.data() + 2 * k;
+        k += n;
+        std::fprintf(f, "<path d=\"");
+        const bool closed = n > 0 && p[0] == p[2 * (n - 1)] && p[1] == p[2 * (n - 1) + 1];
+        const uint32_t end = closed ? n - 1 : n;
+        for (uint32_t j = 0; j < end; ++j) {
+            std::fprintf(f, "%s %g %g ", j == 0 ? "M" : "L", static_cast<double>(p[2 * j]) - lo[0],
+                         hi[1] - static_cast<double>(p[2 * j + 1]));
+        }
+        if (closed) std::fprintf(f, "Z");
+        std::fprintf(f, "\"\nfill=\"none\" stroke=\"black\" stroke-width=\"0.01\"/>");
+    }
+    std::fprintf(f, "\n</svg>");
+    const bool ok = std::ferror(f) == 0;
+    return std::fclose(f) == 0 && ok;
 }
 
 }  // namespace lfb

@@ -48,6 +48,14 @@ class Tri(ctypes.Structure):
                 ("c", ctypes.c_uint32)]
 
 
+class Contour(ctypes.Structure):
+    _fields_ = [("pts", ctypes.c_void_p), ("count", ctypes.c_uint32)]
+
+
+class Contours(ctypes.Structure):
+    _fields_ = [("cs", ctypes.POINTER(Contour)), ("count", ctypes.c_uint32)]
+
+
 class Mesh(ctypes.Structure):
     _fields_ = [("verts", ctypes.POINTER(Vec3)), ("tris", ctypes.POINTER(Tri)),
                 ("tri_count", ctypes.c_uint32), ("vert_count", ctypes.c_uint32)]
@@ -125,8 +133,8 @@ SIGNATURES = [
     ("libfive_tree_optimized", tree_t, [tree_t]),
     ("libfive_tree_print", ctypes.c_void_p, [tree_t]),
     ("libfive_free_str", None, [ctypes.c_void_p]),
-    ("libfive_tree_render_slice", vp, [tree_t, Region2, ctypes.c_float, ctypes.c_float]),
-    ("libfive_tree_render_slice3", vp, [tree_t, Region2, ctypes.c_float, ctypes.c_float]),
+    ("libfive_tree_render_slice", ctypes.POINTER(Contours), [tree_t, Region2, ctypes.c_float, ctypes.c_float]),
+    ("libfive_tree_render_slice3", ctypes.POINTER(Contours), [tree_t, Region2, ctypes.c_float, ctypes.c_float]),
     ("libfive_tree_save_slice", None, [tree_t, Region2, ctypes.c_float, ctypes.c_float, ctypes.c_char_p]),
     ("libfive_tree_render_mesh", ctypes.POINTER(Mesh), [tree_t, Region3, ctypes.c_float]),
     ("libfive_tree_render_mesh_st", ctypes.POINTER(Mesh), [tree_t, Region3, ctypes.c_float]),
@@ -165,6 +173,8 @@ SIGNATURES = [
                                          ctypes.POINTER(ctypes.c_uint64), vp, vp, AdamSettings,
                                          ctypes.c_uint32, vp, vp]),
     ("lfb_render_mesh", ctypes.POINTER(Mesh), [tape_t, Region3, MeshSettings, ctypes.POINTER(MeshStats)]),
+    ("lfb_render_slice", ctypes.POINTER(Contours), [tape_t, Region2, ctypes.c_float, ctypes.c_double,
+                                                    ctypes.c_double]),
     ("lfb_render_heightmap", ctypes.c_int, [tape_t, fp, fp, fp, u32p, fp, u32p]),
     ("lfb_render_meshes", ctypes.c_int, [ctypes.POINTER(tape_t), ctypes.c_uint32,
                                          ctypes.POINTER(Region3), ctypes.POINTER(MeshSettings),

@@ -169,6 +169,21 @@ class Shape:
                                                filename.encode())
 
 
+def contour_arrays(cs_p, dim=2, delete=True):
+    """Copies a libfive_contours* (dim 2) or libfive_contours3* (dim 3) into
+    a list of float32 [n, dim] arrays."""
+    out = []
+    cs = cs_p[0]
+    for i in range(cs.count):
+        c = cs.cs[i]
+        a = np.ctypeslib.as_array(ctypes.cast(c.pts, ctypes.POINTER(ctypes.c_float)),
+                                  shape=(c.count * dim,)).reshape(c.count, dim).copy()
+        out.append(a)
+    if delete:
+        (_lib().libfive_contours_delete if dim == 2 else _lib().libfive_contours3_delete)(cs_p)
+    return out
+
+
 def mesh_arrays(mesh_p, delete=True):
     """Copies a libfive_mesh* into numpy (verts float32 [N,3], tris uint32 [M,3])."""
     m = mesh_p[0]
@@ -322,6 +337,17 @@ class Tape:
             raise RuntimeError("lfb_render_mesh failed: %s" % ffi.last_error()[1])
         v, t = mesh_arrays(m)
         return (v, t, st) if stats else (v, t)
+
+
+def render_slice(tape, lower, upper, z, min_feature, max_err=1e-8):
+    """Contours of the slice z of a Tape over [lower, upper] (2D): a list of
+    float32 [n, 2] point arrays, closed contours repeating their first
+    point."""
+    region = ffi.Region2(*[ffi.Interval(a, b) for a, b in zip(lower, upper)])
+    cs = _lib().lfb_render_slice(tape.ptr, region, z, min_feature, max_err)
+    if not cs:
+        raise RuntimeError("lfb_render_slice failed: %s" % ffi.last_error()[1])
+    return contour_arrays(cs)
 
 
 def render_heightmap(tape, lower, upper, res, normals=True):

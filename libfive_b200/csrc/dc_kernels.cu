@@ -2421,11 +2421,22 @@ Workspace& default_workspace()
 /// Context k of the concurrent batch path, created on first use with its
 /// own non-blocking stream (so that batched meshes overlap each other and
 /// never wait on unrelated default-stream work).
+struct StreamPool {
+    std::mutex mu;
+    std::vector<Workspace*> pool;
+};
+
+StreamPool& stream_pool()
+{
+    static StreamPool* p = new StreamPool;   // never destroyed, like the contexts
+    return *p;
+}
+
 Workspace* stream_workspace(unsigned k)
 {
-    static std::mutex mu;
-    static std::vector<Workspace*> pool;
-    std::lock_guard<std::mutex> lock(mu);
+    auto& sp = stream_pool();
+    std::lock_guard<std::mutex> lock(sp.mu);
+    auto& pool = sp.pool;
     while (pool.size() <= k) {
         auto* w = new Workspace;
         if (!cuda_ok(cudaStreamCreateWithFlags(&w->s, cudaStreamNonBlocking), "stream")) {
@@ -3454,7 +3465,27 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
     if (!require_device()) return LFB_E_CUDA;
     Workspace& ws = default_workspace();
     std::lock_guard<std::mutex> lock(ws.mu);
-    return render_in(ws, g, R, min_feature, max_err, out, stats, cancel);
+    take_device_oom();
+    int rc = render_in(ws, g, R, min_feature, max_err, out, stats, cancel);
+    if (rc == LFB_E_CUDA && take_device_oom()) {
+        // The device ran out of memory: idle batch contexts give their
+        // scratch back, this context starts from empty buffers, and the
+        // mesh is rendered once more.
+        cudaStreamSynchronize(ws.s);
+        cudaGetLastError();
+        {
+            auto& sp = stream_pool();
+            std::lock_guard<std::mutex> plock(sp.mu);
+            for (Workspace* w : sp.pool) {
+                std::unique_lock<std::mutex> wl(w->mu, std::try_to_lock);
+                if (wl.owns_lock()) w->bufs.clear();
+            }
+        }
+        ws.bufs.clear();
+        clear_error();
+        rc = render_in(ws, g, R, min_feature, max_err, out, stats, cancel);
+    }
+    return rc;
 }
 
 int render_dc_meshes(MeshJob* jobs, size_t n, unsigned workers)

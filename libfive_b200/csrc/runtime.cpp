@@ -11,6 +11,11 @@
 
 namespace lfb {
 
+// Set when a scratch allocation found the device out of memory (not an
+// injected failure); read and cleared by take_device_oom.
+thread_local bool t_device_oom = false;
+
+
 static thread_local int t_code = 0;
 static thread_local std::string t_msg;
 
@@ -270,6 +275,13 @@ DebugHooks& debug_hooks()
     return h;
 }
 
+bool take_device_oom()
+{
+    const bool r = t_device_oom;
+    t_device_oom = false;
+    return r;
+}
+
 bool debug_alloc_allowed()
 {
     auto& h = debug_hooks().fail_alloc_after;
@@ -294,7 +306,9 @@ bool DevBuf::reserve(size_t n)
     bytes = 0;
     const size_t want = std::max<size_t>(n, 256);
     if (!debug_alloc_allowed()) return false;
-    if (!cuda_ok(cudaMalloc(&ptr, want), "scratch alloc")) {
+    const cudaError_t e = cudaMalloc(&ptr, want);
+    if (e == cudaErrorMemoryAllocation) t_device_oom = true;
+    if (!cuda_ok(e, "scratch alloc")) {
         return false;
     }
     bytes = want;

@@ -100,6 +100,9 @@ struct DebugHooks {
 DebugHooks& debug_hooks();
 /// False when the allocation-failure hook says this allocation must fail.
 bool debug_alloc_allowed();
+/// Whether a scratch allocation of this thread ran the device out of memory
+/// since the last call (injected failures do not count); clears the flag.
+bool take_device_oom();
 
 /// Growable device buffer.
 struct DevBuf {

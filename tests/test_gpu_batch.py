@@ -69,7 +69,8 @@ def test_batch_empty_and_errors(gpu):
     lib = ffi.load()
     assert lib.lfb_render_meshes(None, 0, None, None, 0, None, None) == 0
     n = 2
-    tapes = (ffi.tape_t * n)(Tape(workloads.spheres_union(4, seed=1)).ptr, None)
+    keep = Tape(workloads.spheres_union(4, seed=1))   # alive for the call
+    tapes = (ffi.tape_t * n)(keep.ptr, None)
     regions = (ffi.Region3 * n)()
     settings = (ffi.MeshSettings * n)()
     meshes = (ffi.ctypes.POINTER(ffi.Mesh) * n)()

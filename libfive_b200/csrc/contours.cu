@@ -982,6 +982,11 @@ int render_contours(GpuTape& g, const double lo[2], const double hi[2], double z
         // quadtree build, level by level
         for (int d = 0; d < L; ++d) {
             const uint32_t n = t.lv[d].n;
+            if (n == 0) {
+                // every cell was decided above: the deeper levels are empty
+                if (!alloc_level(d + 1, 0)) return LFB_E_CUDA;
+                continue;
+            }
             if (!b_out_tape.reserve(static_cast<size_t>(n) * sizeof(TapeRef)) ||
                 !b_flags.reserve(static_cast<size_t>(n + 1) * 4) ||
                 !b_scan.reserve(static_cast<size_t>(n + 1) * 4)) {

@@ -3580,17 +3580,6 @@ int render_dc_meshes(MeshJob* jobs, size_t n, unsigned workers)
         }
     }
 
-    // The side contexts give their scratch back, so that single-mesh calls
-    // (and other work on the device) after a batch find the memory free;
-    // context 0, which renders the large meshes, keeps its buffers for the
-    // next batch.
-    for (unsigned k = 1; k < workers; ++k) {
-        Workspace* w = stream_workspace(k);
-        std::lock_guard<std::mutex> lock(w->mu);
-        cudaStreamSynchronize(w->s);
-        w->bufs.clear();
-    }
-
     clear_error();
     for (size_t i = 0; i < n; ++i) {
         const MeshJob& j = jobs[i];

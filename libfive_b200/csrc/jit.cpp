@@ -508,10 +508,9 @@ std::string backward_source(const RegTape& t, const std::vector<uint32_t>& slots
 // expressions as the partials / backward kernels', in the same order.
 
 constexpr uint32_t kJitSegClauses = 192;
-/// Threads per block of the checkpointed forward (40 registers: three
-/// blocks on an SM) and backward (64 registers: one block) kernels.
-constexpr unsigned kCkptFwdBlock = 512;
-constexpr unsigned kCkptBwdBlock = 1024;
+/// Threads per block of the checkpointed forward and backward kernels.
+constexpr unsigned kCkptFwdBlock = 256;
+constexpr unsigned kCkptBwdBlock = 256;
 
 struct JitSeg {
     uint32_t c0 = 0, c1 = 0;
@@ -642,10 +641,6 @@ std::string ckpt_forward_source(const RegTape& t)
         if (f.empty()) return std::string();
         s += f;
     }
-    // The segments are long straight-line code: a block barrier before
-    // each keeps the block's warps in the same segment, so that they share
-    // its instruction fetches (every thread runs every segment; those past
-    // the last point compute on point 0 and store nothing).
     s += "extern \"C\" __global__ void __launch_bounds__(" + std::to_string(kCkptFwdBlock) + ")\n"
          "lfb_tape_ckpt_fwd(const float* __restrict__ X, const float* __restrict__ Y,\n"
          "                  const float* __restrict__ Z, float* __restrict__ C,\n"
@@ -657,7 +652,7 @@ std::string ckpt_forward_source(const RegTape& t)
          "    for (int r = 3; r < " + std::to_string(t.n_regs) + "; ++r) R[r] = 0.0f;\n"
          "    R[0] = X[ii]; R[1] = Y[ii]; R[2] = Z[ii];\n";
     for (uint32_t k = 0; k < segs.size(); ++k) {
-        s += "    __syncthreads();\n    fseg" + std::to_string(k) + "(R, C + ii, m, cp, ok);\n";
+        s += "    fseg" + std::to_string(k) + "(R, C + ii, m, cp, ok);\n";
     }
     s += "    if (ok && f) f[i] = " + root_from_R(t) + ";\n}\n";
     return s;
@@ -823,11 +818,12 @@ std::string ckpt_backward_source(const RegTape& t)
          "    const unsigned k = lfb_vidx[base + lane];\n"
          "    if (k != 0xffffu && v[0] != 0.0f) atomicAdd(Gv + k, v[0]);\n}\n";
     s += body;
-    // at most 64 registers a thread: one block of 1024 threads on an SM,
-    // with a block barrier before each segment, so that all of the SM's
-    // warps run the same segment and share its instruction fetches
+    // at most 64 registers a thread: four blocks of 256 threads on an SM.
+    // (One 1024-thread block with a barrier before each segment, so that
+    // an SM's warps share a segment's instruction fetches, was measured
+    // slower: the barriers cost more than the fetch stalls they saved.)
     s += "extern \"C\" __global__ void __launch_bounds__(" + std::to_string(kCkptBwdBlock) +
-         ", 1)\n"
+         ", 4)\n"
          "lfb_tape_ckpt_bwd(const float* __restrict__ C, const float* __restrict__ seed,\n"
          "                  float* __restrict__ gx, float* __restrict__ gy,\n"
          "                  float* __restrict__ gz, float* __restrict__ gvars, unsigned m,\n"
@@ -850,8 +846,7 @@ std::string ckpt_backward_source(const RegTape& t)
         s += "    if (gv) lfb_add_var(Gv, " + std::to_string(t.root - t.n_const) + ", s0);\n";
     }
     for (uint32_t k = static_cast<uint32_t>(segs.size()); k-- > 0;) {
-        s += "    __syncthreads();\n    bseg" + std::to_string(k) +
-             "(A, Ci, m, cp, Gv, gv, block_cv, ok);\n";
+        s += "    bseg" + std::to_string(k) + "(A, Ci, m, cp, Gv, gv, block_cv, ok);\n";
     }
     s += "    if (ok) {\n"
          "        if (gx) gx[i] = A[0];\n        if (gy) gy[i] = A[1];\n        if (gz) gz[i] = A[2];\n"

@@ -488,8 +488,10 @@ def run_batch(args, world, rank, local):
                 lib.libfive_mesh_delete(m)
         if rc != 0:
             raise RuntimeError("lfb_render_meshes failed: " + ffi.last_error()[1])
+        inflight[0] = sum(st.ms_total for st in b_stats)
         return sum(st.triangles for st in b_stats)
 
+    inflight = [0.0]
     timings = {}
     for name, fn in (("loop", loop), ("batch", batch)):
         for _ in range(args.warmup):
@@ -546,6 +548,7 @@ def run_batch(args, world, rank, local):
             "loop_value": world * n / timings["loop"],
             "batch_over_loop": timings["loop"] / timings["batch"],
             "triangles_per_step": tris[0], "by_resolution": by_res,
+            "mean_meshes_in_flight": inflight[0] / (timings["batch"] * 1e3),
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": "batch of %d random CSG trees, 8-4000 primitives, "
                                    "depth 8-11" % n, "workers": args.workers}}))

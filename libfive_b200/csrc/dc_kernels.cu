@@ -2390,6 +2390,10 @@ namespace {
 /// keyed by purpose, the stream its work runs on and download()'s
 /// page-locked staging buffer.  A context serves one mesh at a time (its
 /// mutex) and keeps its buffers from call to call.
+/// Freed scratch the device's memory pool keeps across synchronisations
+/// (for the next mesh of any context) before it returns memory to the driver.
+constexpr uint64_t kPoolKeepBytes = uint64_t(32) << 30;
+
 struct Workspace {
     std::mutex mu;
     cudaStream_t s = 0;
@@ -2405,6 +2409,12 @@ struct Workspace {
     T* get(int key, size_t count)
     {
         DevBuf& b = bufs[key];
+        if (!b.ordered) {
+            // scratch lives in the device's memory pool, allocated in this
+            // context's stream order
+            b.ordered = true;
+            b.stream = s;
+        }
         if (!b.reserve(std::max<size_t>(count, 1) * sizeof(T))) return nullptr;
         return b.as<T>();
     }
@@ -3463,6 +3473,7 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
                    const volatile int32_t* cancel)
 {
     if (!require_device()) return LFB_E_CUDA;
+    keep_pool_memory(kPoolKeepBytes);
     Workspace& ws = default_workspace();
     std::lock_guard<std::mutex> lock(ws.mu);
     take_device_oom();
@@ -3491,6 +3502,7 @@ int render_dc_mesh(GpuTape& g, const libfive_region3& R, double min_feature,
 int render_dc_meshes(MeshJob* jobs, size_t n, unsigned workers)
 {
     if (!require_device()) return LFB_E_CUDA;
+    keep_pool_memory(kPoolKeepBytes);
     if (n == 0) return 0;
     for (size_t i = 0; i < n; ++i) {
         if (!jobs[i].g) return set_error(LFB_E_INVALID, "null tape in a mesh batch");
@@ -3531,6 +3543,11 @@ int render_dc_meshes(MeshJob* jobs, size_t n, unsigned workers)
             j.rc = render_in(*ws, *j.g, j.R, j.min_feature, j.max_err, j.out,
                              j.want_stats ? &j.stats : nullptr, j.cancel);
             if (j.rc != 0) last_error(&j.err);
+            // The context's scratch goes back to the device's memory pool
+            // (stream-ordered frees), where the other contexts' next meshes
+            // find it: memory in use follows the meshes in flight, not each
+            // context's largest mesh so far.
+            ws->bufs.clear();
         }
     };
     auto work = [&](unsigned k) {

@@ -266,7 +266,25 @@ void invalidate_cached(const Node* root)
 
 DevBuf::~DevBuf()
 {
-    if (ptr) cudaFree(ptr);
+    if (!ptr) return;
+    if (ordered) cudaFreeAsync(ptr, stream);
+    else cudaFree(ptr);
+}
+
+void keep_pool_memory(uint64_t bytes)
+{
+    static std::mutex mu;
+    static uint64_t done = 0;   // one bit per device
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return;
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev < 64 && ((done >> dev) & 1)) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &bytes);
+    }
+    cudaGetLastError();
+    if (dev < 64) done |= 1ull << dev;
 }
 
 DebugHooks& debug_hooks()
@@ -301,12 +319,15 @@ bool debug_alloc_allowed()
 bool DevBuf::reserve(size_t n)
 {
     if (n <= bytes) return true;
-    if (ptr) cudaFree(ptr);
+    if (ptr) {
+        if (ordered) cudaFreeAsync(ptr, stream);
+        else cudaFree(ptr);
+    }
     ptr = nullptr;
     bytes = 0;
     const size_t want = std::max<size_t>(n, 256);
     if (!debug_alloc_allowed()) return false;
-    const cudaError_t e = cudaMalloc(&ptr, want);
+    const cudaError_t e = ordered ? cudaMallocAsync(&ptr, want, stream) : cudaMalloc(&ptr, want);
     if (e == cudaErrorMemoryAllocation) t_device_oom = true;
     if (!cuda_ok(e, "scratch alloc")) {
         return false;

@@ -104,14 +104,26 @@ bool debug_alloc_allowed();
 /// since the last call (injected failures do not count); clears the flag.
 bool take_device_oom();
 
-/// Growable device buffer.
+/// Growable device buffer.  With `ordered` set, it is allocated and freed
+/// in stream order on `stream` (cudaMallocAsync / cudaFreeAsync from the
+/// device's memory pool): no device-wide synchronisation, and memory a
+/// buffer gives back is reused by the other streams' buffers.
 struct DevBuf {
     void* ptr = nullptr;
     size_t bytes = 0;
+    cudaStream_t stream = nullptr;
+    bool ordered = false;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
     ~DevBuf();
     bool reserve(size_t n);
     template <class T> T* as() const { return static_cast<T*>(ptr); }
 };
+
+/// Keeps up to `bytes` of freed memory cached in the current device's
+/// default memory pool across synchronisations (once per device).
+void keep_pool_memory(uint64_t bytes);
 
 /// Lets `fn` (a __global__ function) be launched with `bytes` of dynamic
 /// shared memory on the current device.  The limit only ever rises, under a

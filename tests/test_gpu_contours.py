@@ -78,8 +78,9 @@ def test_slice3_carries_z(gpu, lib):
     c2 = contour_arrays(lib.libfive_tree_render_slice(s.ptr, R, 0.25, 20.0))
     c3 = contour_arrays(lib.libfive_tree_render_slice3(s.ptr, R, 0.25, 20.0), dim=3)
     assert len(c2) == len(c3) >= 1
-    for a, b in zip(c2, c3):
-        assert np.array_equal(b[:, :2], a)
+    # two renders: the same contours, each possibly starting elsewhere
+    assert same_contours([b[:, :2] for b in c3], c2)
+    for b in c3:
         assert np.all(b[:, 2] == np.float32(0.25))
 
 

@@ -2393,6 +2393,8 @@ namespace {
 /// Freed scratch the device's memory pool keeps across synchronisations
 /// (for the next mesh of any context) before it returns memory to the driver.
 constexpr uint64_t kPoolKeepBytes = uint64_t(32) << 30;
+/// Scratch a batch context keeps between its meshes.
+constexpr size_t kContextKeepBytes = size_t(4) << 30;
 
 struct Workspace {
     std::mutex mu;
@@ -3543,11 +3545,14 @@ int render_dc_meshes(MeshJob* jobs, size_t n, unsigned workers)
             j.rc = render_in(*ws, *j.g, j.R, j.min_feature, j.max_err, j.out,
                              j.want_stats ? &j.stats : nullptr, j.cancel);
             if (j.rc != 0) last_error(&j.err);
-            // The context's scratch goes back to the device's memory pool
-            // (stream-ordered frees), where the other contexts' next meshes
-            // find it: memory in use follows the meshes in flight, not each
-            // context's largest mesh so far.
-            ws->bufs.clear();
+            // A context that holds much scratch gives it back to the
+            // device's memory pool (stream-ordered frees), where the other
+            // contexts' next meshes find it: memory in use follows the
+            // meshes in flight rather than each context's largest mesh so
+            // far.  Small scratch stays, so small meshes reuse it.
+            size_t held = 0;
+            for (const auto& kv : ws->bufs) held += kv.second.bytes;
+            if (held > kContextKeepBytes) ws->bufs.clear();
         }
     };
     auto work = [&](unsigned k) {

@@ -66,7 +66,7 @@ def parse():
                         "depths are for profiling captures")
     p.add_argument("--workload", default="csg2000",
                    choices=["csg2000", "batch", "eval", "adjoint", "heightmap", "fit",
-                            "spheres64"],
+                            "spheres64", "slice"],
                    help="batch: many trees of mixed size and depth, meshed "
                         "one after another and through lfb_render_meshes")
     p.add_argument("--trees", type=int, default=512, help="batch workload: tree count")
@@ -985,11 +985,53 @@ def run_heightmap(args, world, rank, local):
         print(json.dumps(line))
 
 
+def run_slice(args, world, rank, local):
+    """2D contours: the benchmark's 2000-primitive CSG (seed 2 + rank) cut at
+    z = 0 over [-1.5,1.5]^2 with min_feature 3/4096 (a depth-12 quadtree),
+    max_err 1e-8, contours downloaded and welded on the host every step.
+    The CPU line is the oracle's restatement of Contours::render on one
+    core, once, on the same slice; `matches_oracle` compares the contours
+    point for point as cyclic sequences."""
+    import torch
+    from libfive_b200.shape import Tape, render_slice
+    torch.cuda.set_device(local)
+    shape = build_shape(SEED_BASE + rank)
+    tape = Tape(shape)
+    lo, hi, z, mf = (-1.5, -1.5), (1.5, 1.5), 0.0, 3.0 / 4096
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    out = {}
+    ms = _timed(lambda: out.update(c=render_slice(tape, lo, hi, z, mf, MAX_ERR)), args.steps,
+                args.warmup, flush)
+    ms = rank_max(ms)
+    cs = out["c"]
+    pts = int(sum(len(c) for c in cs))
+    line = {
+        "metric": "slices/s", "value": world * 1e3 / ms, "unit": "slices/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+        "contours": len(cs), "points": pts,
+        "config": {"workload": "2000-primitive CSG slice z = 0, depth-12 quadtree",
+                   "clauses": tape.n_clauses}}
+    if rank == 0 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from mesh_compare import same_contours
+        from oracle_ffi import OracleTape, render_contours
+        t0 = time.perf_counter()
+        want, _ = render_contours(OracleTape(shape), lo, hi, z, mf, MAX_ERR)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": 1.0 / dt, "unit": "slices/s", "cores": 1,
+                                "kind": "port", "sample": "the same slice, once"}
+        line["matches_oracle"] = bool(same_contours(cs, want))
+    if rank == 0:
+        print(json.dumps(line))
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
     aux = {"batch": run_batch, "eval": run_eval, "adjoint": run_adjoint,
-           "heightmap": run_heightmap, "fit": run_fit, "spheres64": run_spheres_mesh}
+           "heightmap": run_heightmap, "fit": run_fit, "spheres64": run_spheres_mesh,
+           "slice": run_slice}
     if args.workload in aux:
         global _AUX_PG
         _AUX_PG = aux_group(world, local)

@@ -408,7 +408,8 @@ def run_ours(args, world, rank, local):
                      "triangles": stats.triangles, "vertices": stats.vertices,
                      "leaf_records": stats.leaves_ambiguous},
             "roofline": {
-                "kernel": "k_leaf_groups",
+                "kernel": "leaf stage: k_leaf_groups (corners, edge search; 82 % of the "
+                          "stage) + k_leaf_qef + k_edge_rank + k_leaf_vertices",
                 "bound": "fp32",
                 "achieved": achieved, "peak": peak, "unit": "G lane-ops/s",
                 "frac": achieved / peak,
@@ -418,7 +419,8 @@ def run_ours(args, world, rank, local):
                 "clause_evals_per_launch": (evals_v + evals_g) / args.steps,
                 "kernel_ms_per_launch": leaf_ms / args.steps,
                 "traffic": traffic,
-                "traffic_source": ("ncu capture of this kernel on this workload "
+                "traffic_source": ("ncu capture of k_leaf_groups, the stage's dominant "
+                                   "kernel, on this workload "
                                    "(profiles/k_leaf_groups_csg2000_depth10_dram.md)"
                                    if traffic is not None else None),
             },

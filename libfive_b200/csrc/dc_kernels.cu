@@ -3529,10 +3529,12 @@ int render_dc_meshes(MeshJob* jobs, size_t n, unsigned workers)
     workers = std::max(1u, std::min<unsigned>(workers, static_cast<unsigned>(
                                                            std::min<size_t>(n, 16))));
     // Large meshes (tape length x 4^depth above kBigCost) fill the GPU on
-    // their own and need the most scratch memory: worker 0 renders them one
-    // after another while the other workers render the small ones side by
-    // side; worker 0 joins them when the large ones are done.
-    constexpr double kBigCost = 2e9;
+    // their own: run side by side they only compete for SMs, L2 and memory
+    // (measured slower than one after another).  So context 0 renders them
+    // first, one after another and alone; then all contexts render the
+    // small meshes side by side, whose per-level host waits leave the GPU
+    // idle.
+    constexpr double kBigCost = 1e9;
     std::vector<size_t> big, small;
     for (size_t i : order) (cost[i] >= kBigCost && workers > 1 ? big : small).push_back(i);
     std::atomic<size_t> next_big{0}, next_small{0};
@@ -3555,12 +3557,18 @@ int render_dc_meshes(MeshJob* jobs, size_t n, unsigned workers)
             if (held > kContextKeepBytes) ws->bufs.clear();
         }
     };
+    if (!big.empty()) {
+        Workspace* ws = stream_workspace(0);
+        if (ws) {
+            std::lock_guard<std::mutex> lock(ws->mu);
+            run_queue(ws, big, next_big);
+        }
+    }
     auto work = [&](unsigned k) {
         cudaSetDevice(dev);
         Workspace* ws = stream_workspace(k);
         if (!ws) return;
         std::lock_guard<std::mutex> lock(ws->mu);
-        if (k == 0) run_queue(ws, big, next_big);
         run_queue(ws, small, next_small);
     };
     std::vector<std::thread> pool;

@@ -2393,8 +2393,6 @@ namespace {
 /// Freed scratch the device's memory pool keeps across synchronisations
 /// (for the next mesh of any context) before it returns memory to the driver.
 constexpr uint64_t kPoolKeepBytes = uint64_t(32) << 30;
-/// Scratch a batch context keeps between its meshes.
-constexpr size_t kContextKeepBytes = size_t(4) << 30;
 
 struct Workspace {
     std::mutex mu;
@@ -3529,12 +3527,10 @@ int render_dc_meshes(MeshJob* jobs, size_t n, unsigned workers)
     workers = std::max(1u, std::min<unsigned>(workers, static_cast<unsigned>(
                                                            std::min<size_t>(n, 16))));
     // Large meshes (tape length x 4^depth above kBigCost) fill the GPU on
-    // their own: run side by side they only compete for SMs, L2 and memory
-    // (measured slower than one after another).  So context 0 renders them
-    // first, one after another and alone; then all contexts render the
-    // small meshes side by side, whose per-level host waits leave the GPU
-    // idle.
-    constexpr double kBigCost = 1e9;
+    // their own and need the most scratch memory: worker 0 renders them one
+    // after another while the other workers render the small ones side by
+    // side; worker 0 joins them when the large ones are done.
+    constexpr double kBigCost = 2e9;
     std::vector<size_t> big, small;
     for (size_t i : order) (cost[i] >= kBigCost && workers > 1 ? big : small).push_back(i);
     std::atomic<size_t> next_big{0}, next_small{0};
@@ -3547,28 +3543,14 @@ int render_dc_meshes(MeshJob* jobs, size_t n, unsigned workers)
             j.rc = render_in(*ws, *j.g, j.R, j.min_feature, j.max_err, j.out,
                              j.want_stats ? &j.stats : nullptr, j.cancel);
             if (j.rc != 0) last_error(&j.err);
-            // A context that holds much scratch gives it back to the
-            // device's memory pool (stream-ordered frees), where the other
-            // contexts' next meshes find it: memory in use follows the
-            // meshes in flight rather than each context's largest mesh so
-            // far.  Small scratch stays, so small meshes reuse it.
-            size_t held = 0;
-            for (const auto& kv : ws->bufs) held += kv.second.bytes;
-            if (held > kContextKeepBytes) ws->bufs.clear();
         }
     };
-    if (!big.empty()) {
-        Workspace* ws = stream_workspace(0);
-        if (ws) {
-            std::lock_guard<std::mutex> lock(ws->mu);
-            run_queue(ws, big, next_big);
-        }
-    }
     auto work = [&](unsigned k) {
         cudaSetDevice(dev);
         Workspace* ws = stream_workspace(k);
         if (!ws) return;
         std::lock_guard<std::mutex> lock(ws->mu);
+        if (k == 0) run_queue(ws, big, next_big);
         run_queue(ws, small, next_small);
     };
     std::vector<std::thread> pool;

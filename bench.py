@@ -419,8 +419,8 @@ def run_ours(args, world, rank, local):
                 "clause_evals_per_launch": (evals_v + evals_g) / args.steps,
                 "kernel_ms_per_launch": leaf_ms / args.steps,
                 "traffic": traffic,
-                "traffic_source": ("ncu capture of k_leaf_groups, the stage's dominant "
-                                   "kernel, on this workload "
+                "traffic_source": ("ncu capture of the leaf stage's four kernels on this "
+                                   "workload, dram__bytes_read.sum + dram__bytes_write.sum "
                                    "(profiles/k_leaf_groups_csg2000_depth10_dram.md)"
                                    if traffic is not None else None),
             },

@@ -796,7 +796,7 @@ struct GroupArgs {
     RegClause* arena;
     unsigned long long* arena_top;
     uint64_t arena_cap;
-    uint8_t* dec;                  // [warps][dec_cap][8] min/max decisions
+    uint8_t* dec;                  // [warps][8][dec_cap] min/max decisions
     uint32_t dec_cap;
     uint8_t* lastuse;              // [warps][8][kRenumberMax] renumbering flags
     uint32_t nregs_max;            // register file size (this depth's largest group tape)
@@ -812,7 +812,7 @@ __host__ __device__ inline size_t group_smem_per_warp(uint32_t nregs_max)
     return (b + 15) / 16 * 16;
 }
 
-__global__ void __launch_bounds__(128, 8)
+__global__ void __launch_bounds__(128)
 k_interval_group(GroupArgs A, int d)
 {
     extern __shared__ __align__(16) unsigned char gsm[];
@@ -829,9 +829,7 @@ k_interval_group(GroupArgs A, int d)
     uint8_t* Nn = reinterpret_cast<uint8_t*>(reinterpret_cast<uint32_t*>(
                       reinterpret_cast<uint16_t*>(Hi + nr * 8) + nr * 8) + 8 * 13);
     const uint32_t gw = blockIdx.x * wpb + warp;
-    // decisions interleaved by lane ([choice][8 cells]): the eight cells'
-    // bytes of one choice share a sector
-    uint8_t* dec = A.dec + static_cast<size_t>(gw) * 8 * A.dec_cap + (lane & 7);
+    uint8_t* dec = A.dec + (static_cast<size_t>(gw) * 8 + (lane & 7)) * A.dec_cap;
     uint8_t* lastuse = A.lastuse + (static_cast<size_t>(gw) * 8 + (lane & 7)) * kRenumberMax;
     const Octree& o = A.o;
     const LevelView& lv = o.lv[d];
@@ -865,15 +863,8 @@ k_interval_group(GroupArgs A, int d)
         // (IntervalEvaluator::push, eval_interval.cpp:116-167).
         bool changed = false;
         uint32_t ch = 0;
-        // the clause stream is read two clauses ahead of the one evaluated,
-        // so that its load latency overlaps the evaluation
-        const uint2* cl2 = reinterpret_cast<const uint2*>(cl);
-        uint2 nx0 = T.len > 0 ? __ldg(cl2) : make_uint2(0, 0);
-        uint2 nx1 = T.len > 1 ? __ldg(cl2 + 1) : make_uint2(0, 0);
         for (uint32_t c = 0; c < T.len; ++c) {
-            const uint2 raw = nx0;
-            nx0 = nx1;
-            if (c + 2 < T.len) nx1 = __ldg(cl2 + c + 2);
+            const uint2 raw = __ldg(reinterpret_cast<const uint2*>(cl + c));
             const uint8_t o_ = raw.x & 0xff;
             const uint32_t kinds = (raw.x >> 8) & 0xff;
             const uint32_t ro = raw.x >> 16;
@@ -885,7 +876,7 @@ k_interval_group(GroupArgs A, int d)
                 if (a.lo > b.hi) keep = (o_ == op::MAX) ? 1 : 2;
                 else if (b.lo > a.hi) keep = (o_ == op::MAX) ? 2 : 1;
                 changed |= keep != 0;
-                if (ch < A.dec_cap) dec[static_cast<size_t>(ch) * 8] = keep;
+                if (ch < A.dec_cap) dec[ch] = keep;
                 ++ch;
             }
             Lo[ro * 8 + lane] = r.lo;
@@ -924,16 +915,13 @@ k_interval_group(GroupArgs A, int d)
                     break;
                 }
             }
-            const uint2* cb = reinterpret_cast<const uint2*>(cl);
-            uint2 pv = T.len > 0 ? __ldg(cb + T.len - 1) : make_uint2(0, 0);
             for (int64_t c = static_cast<int64_t>(T.len) - 1; c >= 0; --c) {
-                const uint2 raw = pv;
-                if (c > 0) pv = __ldg(cb + c - 1);
+                const uint2 raw = __ldg(reinterpret_cast<const uint2*>(cl + c));
                 const uint8_t o_ = raw.x & 0xff;
                 const uint32_t kinds = (raw.x >> 8) & 0xff;
                 const uint32_t ro = raw.x >> 16;
                 uint8_t keep = 0;
-                if (o_ == op::MIN || o_ == op::MAX) keep = dec[static_cast<size_t>(--chi) * 8];
+                if (o_ == op::MIN || o_ == op::MAX) keep = dec[--chi];
                 if (!Nn[ro * 8 + lane]) continue;
                 Nn[ro * 8 + lane] = 0;
                 uint2 outc = raw;

@@ -3024,16 +3024,26 @@ int render_once(Workspace& ws, GpuTape& g, const libfive_region3& R, double min_
                 if (!ws.get<WideEntry>(out_key, tops[1] + tops[1] / 4 + 1024)) return LFB_E_CUDA;
             }
             if (st & ST_ARENA_OVERFLOW) {
+                // The arena keeps its contents (the tapes of the levels
+                // above): a larger buffer in the same stream order, the
+                // used part copied over, the old one freed after the copy.
                 const uint64_t new_cap = tops[0] + tops[0] / 4 + (1u << 20);
+                DevBuf& b = ws.bufs[K_ARENA];
                 RegClause* bigger = nullptr;
-                if (!cuda_ok(cudaMalloc(&bigger, new_cap * sizeof(RegClause)), "arena grow")) {
-                    return LFB_E_CUDA;
-                }
+                const cudaError_t e =
+                    b.ordered ? cudaMallocAsync(reinterpret_cast<void**>(&bigger),
+                                                new_cap * sizeof(RegClause), b.stream)
+                              : cudaMalloc(&bigger, new_cap * sizeof(RegClause));
+                if (e == cudaErrorMemoryAllocation) note_device_oom();
+                if (!cuda_ok(e, "arena grow")) return LFB_E_CUDA;
                 cudaMemcpyAsync(bigger, arena, arena_before * sizeof(RegClause),
                                 cudaMemcpyDeviceToDevice, s);
-                DevBuf& b = ws.bufs[K_ARENA];
-                cudaStreamSynchronize(s);
-                cudaFree(b.ptr);
+                if (b.ordered) {
+                    cudaFreeAsync(b.ptr, b.stream);
+                } else {
+                    cudaStreamSynchronize(s);
+                    cudaFree(b.ptr);
+                }
                 b.ptr = bigger;
                 b.bytes = new_cap * sizeof(RegClause);
                 arena = bigger;

@@ -293,6 +293,8 @@ DebugHooks& debug_hooks()
     return h;
 }
 
+void note_device_oom() { t_device_oom = true; }
+
 bool take_device_oom()
 {
     const bool r = t_device_oom;

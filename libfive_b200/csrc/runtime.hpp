@@ -103,6 +103,8 @@ bool debug_alloc_allowed();
 /// Whether a scratch allocation of this thread ran the device out of memory
 /// since the last call (injected failures do not count); clears the flag.
 bool take_device_oom();
+/// Records that an allocation outside DevBuf found the device out of memory.
+void note_device_oom();
 
 /// Growable device buffer.  With `ordered` set, it is allocated and freed
 /// in stream order on `stream` (cudaMallocAsync / cudaFreeAsync from the

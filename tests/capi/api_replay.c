@@ -144,6 +144,37 @@ int main(int argc, char** argv)
         libfive_tree_delete(d);
     }
 
+    /* libfive_tree_render_slice (api.cpp:75-105): x^2 + y^2 - 1 cut at z = 0,
+     * one contour, every point at radius^2 in (0.99, 1.01) */
+    {
+        libfive_tree x = libfive_tree_x(), y = libfive_tree_y();
+        libfive_tree x2 = libfive_tree_unary(op("square"), x);
+        libfive_tree y2 = libfive_tree_unary(op("square"), y);
+        libfive_tree r = libfive_tree_binary(op("add"), x2, y2);
+        libfive_tree one = libfive_tree_const(1.0f);
+        libfive_tree d = libfive_tree_binary(op("sub"), r, one);
+        libfive_region2 R = {{-2, 2}, {-2, 2}};
+        libfive_contours* cs = libfive_tree_render_slice(d, R, 0, 10);
+        CHECK(cs != NULL);
+        if (cs) {
+            CHECK(cs->count == 1);
+            if (cs->count == 1) {
+                CHECK(cs->cs[0].count > 0);
+                float rmin = 2, rmax = 0;
+                for (uint32_t i = 0; i < cs->cs[0].count; ++i) {
+                    const libfive_vec2 v = cs->cs[0].pts[i];
+                    const float q = v.x * v.x + v.y * v.y;
+                    rmin = q < rmin ? q : rmin;
+                    rmax = q > rmax ? q : rmax;
+                }
+                CHECK(rmin > 0.99f && rmax < 1.01f);
+            }
+            libfive_contours_delete(cs);
+        }
+        libfive_tree ts[7] = {x, y, x2, y2, r, one, d};
+        for (int i = 0; i < 7; ++i) libfive_tree_delete(ts[i]);
+    }
+
     /* invalid opcodes and arguments give NULL */
     {
         CHECK(libfive_tree_nullary(op("min")) == NULL);

@@ -593,6 +593,7 @@ struct QCollapseArgs {
     QTree t;
     int d;
     DevTape bt;                // the unpruned tape
+    const RegClause* arena;    // the unpruned and pruned tapes
     QLeaf* recs;
     uint32_t* rec_top;
     uint32_t rec_cap;
@@ -671,22 +672,30 @@ __global__ void k_q_collapse(QCollapseArgs A)
         bool inside = true;
         for (int a = 0; a < 2; ++a) inside = inside && v[a] >= lo[a] - 1e-6 && v[a] <= hi[a] + 1e-6;
         if (!(err < A.max_err && inside)) continue;
-        // value at the vertex (the base tape gives the same value as any
-        // pruned tape valid there)
+        // Value at the vertex with a tape valid there (Tape::getBase,
+        // tape.cpp:188-209): every valid tape gives the same value, so the
+        // shortest is taken: the one pruned over this cell's box (its
+        // children's) when the vertex lies in that box, else the unpruned.
+        const float vx = static_cast<float>(v[0]), vy = static_cast<float>(v[1]);
+        const bool in_cell = vx >= static_cast<float>(lo[0]) && vx <= static_cast<float>(hi[0]) &&
+                             vy >= static_cast<float>(lo[1]) && vy <= static_cast<float>(hi[1]);
+        const TapeRef tr = in_cell ? nx.tape[c0] : root_tape_ref(A.bt);
+        const RegClause* cl = A.arena + tr.off;
+        const uint32_t rk = tr.root >> 16, rr = tr.root & 0xffff;
         float* R = A.regs;
         const uint32_t T = A.T;
-        R[0 * T + tid] = static_cast<float>(v[0]);
-        R[1 * T + tid] = static_cast<float>(v[1]);
+        R[0 * T + tid] = vx;
+        R[1 * T + tid] = vy;
         R[2 * T + tid] = A.t.perp;
-        const DevTape& bt = A.bt;
-        for (uint32_t c = 0; c < bt.n; ++c) {
-            const RegClause k = bt.clauses[c];
+        const float* cp = A.bt.cpool;
+        for (uint32_t c = 0; c < tr.len; ++c) {
+            const RegClause k = cl[c];
             const uint8_t ka = k.kinds & 3, kb = (k.kinds >> 2) & 3;
-            const float a = ka == OPND_REG ? R[k.a * T + tid] : __ldg(bt.cpool + k.a);
-            const float b = kb == OPND_REG ? R[k.b * T + tid] : __ldg(bt.cpool + k.b);
+            const float a = ka == OPND_REG ? R[k.a * T + tid] : __ldg(cp + k.a);
+            const float b = kb == OPND_REG ? R[k.b * T + tid] : __ldg(cp + k.b);
             R[k.out * T + tid] = dv_value(k.op, a, b);
         }
-        const float value = bt.root_kind == OPND_REG ? R[bt.root * T + tid] : __ldg(bt.cpool + bt.root);
+        const float value = rk == OPND_REG ? R[rr * T + tid] : __ldg(cp + rr);
         if (!(fabsf(value) < A.max_err)) continue;
         const uint32_t rec = atomicAdd(A.rec_top, 1u);
         if (rec >= A.rec_cap) {
@@ -1028,7 +1037,7 @@ int render_contours(GpuTape& g, const double lo[2], const double hi[2], double z
         }
         // collapse, bottom-up
         for (int d = L - 1; d >= 0; --d) {
-            QCollapseArgs C{t, d, bt, b_recs.as<QLeaf>(), rec_top, rec_cap, max_err,
+            QCollapseArgs C{t, d, bt, arena, b_recs.as<QLeaf>(), rec_top, rec_cap, max_err,
                             b_cregs.as<float>(), T, status};
             k_q_collapse<<<T / 256, 256, 0, s>>>(C);
             note_launches(1);

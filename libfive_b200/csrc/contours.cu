@@ -106,41 +106,16 @@ struct QIntervalArgs {
     uint32_t* status;
 };
 
-constexpr uint32_t kQBlock = 256;
-
-/// Bytes of shared memory of k_q_interval<true>: per thread and tape
-/// register the interval (2 floats), its NaN flag and a liveness flag.
-__host__ __device__ constexpr size_t q_interval_smem(uint32_t nregs)
-{
-    return static_cast<size_t>(nregs) * kQBlock * 10;
-}
-
-/// One thread per cell.  With SMEM the register file and the liveness flags
-/// are in shared memory ([register][thread]); otherwise (tapes with too many
-/// registers) in the global scratch of the arguments.  Every clause reads
-/// registers the previous clauses wrote, so the register file's latency is
-/// on the critical path of a long tape.
-template <bool SMEM>
-__global__ void __launch_bounds__(kQBlock)
+__global__ void __launch_bounds__(256)
 k_q_interval(QIntervalArgs A)
 {
-    extern __shared__ __align__(16) unsigned char qsm[];
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t T = A.T;
     const QLevel& lv = A.t.lv[A.d];
     const float* cp = A.bt.cpool;
-    const uint32_t nregs = max(A.bt.n_regs, 3u);
-    // register r of this thread: element r * stride + col
-    const uint32_t stride = SMEM ? kQBlock : T;
-    const uint32_t col = SMEM ? threadIdx.x : tid;
-    float* const Rlo = SMEM ? reinterpret_cast<float*>(qsm) : A.rlo;
-    float* const Rhi = SMEM ? Rlo + static_cast<size_t>(nregs) * kQBlock : A.rhi;
-    uint8_t* const Rnan = SMEM ? reinterpret_cast<uint8_t*>(Rhi + static_cast<size_t>(nregs) * kQBlock)
-                               : A.rnan;
-    uint8_t* const Live = SMEM ? Rnan + static_cast<size_t>(nregs) * kQBlock : A.live;
     auto fetch = [&](uint32_t kind, uint32_t idx) -> Iv {
         if (kind == OPND_REG) {
-            return {Rlo[idx * stride + col], Rhi[idx * stride + col], Rnan[idx * stride + col] != 0};
+            return {A.rlo[idx * T + tid], A.rhi[idx * T + tid], A.rnan[idx * T + tid] != 0};
         }
         const float v = __ldg(cp + idx);
         return iv_make(v, v);
@@ -155,9 +130,9 @@ k_q_interval(QIntervalArgs A)
                           iv_make(static_cast<float>(lo[1]), static_cast<float>(hi[1])),
                           iv_make(A.t.perp, A.t.perp)};
         for (int a = 0; a < 3; ++a) {
-            Rlo[a * stride + col] = in[a].lo;
-            Rhi[a * stride + col] = in[a].hi;
-            Rnan[a * stride + col] = in[a].nan;
+            A.rlo[a * T + tid] = in[a].lo;
+            A.rhi[a * T + tid] = in[a].hi;
+            A.rnan[a * T + tid] = in[a].nan;
         }
         // Forward pass, recording the push decision of every min/max
         // (IntervalEvaluator::push, eval_interval.cpp:116-167).
@@ -179,9 +154,9 @@ k_q_interval(QIntervalArgs A)
                 if (ch < A.dec_cap) A.dec[static_cast<size_t>(ch) * T + tid] = keep;
                 ++ch;
             }
-            Rlo[ro * stride + col] = r.lo;
-            Rhi[ro * stride + col] = r.hi;
-            Rnan[ro * stride + col] = r.nan;
+            A.rlo[ro * T + tid] = r.lo;
+            A.rhi[ro * T + tid] = r.hi;
+            A.rnan[ro * T + tid] = r.nan;
         }
         const Iv root = fetch(rk, rr);
         const uint8_t state = iv_state(root);
@@ -197,8 +172,8 @@ k_q_interval(QIntervalArgs A)
         // clauses from the back (they stay in evaluation order).
         uint32_t kept = 0;
         for (int pass = 0; pass < 2; ++pass) {
-            for (uint32_t r = 0; r < tr.nregs; ++r) Live[r * stride + col] = 0;
-            if (rk == OPND_REG) Live[rr * stride + col] = 1;
+            for (uint32_t r = 0; r < tr.nregs; ++r) A.live[r * T + tid] = 0;
+            if (rk == OPND_REG) A.live[rr * T + tid] = 1;
             uint32_t pos = kept;
             uint32_t chi = ch;
             unsigned long long off = 0;
@@ -216,23 +191,23 @@ k_q_interval(QIntervalArgs A)
                 const uint32_t ro = raw.x >> 16;
                 uint8_t keep = 0;
                 if (o == op::MIN || o == op::MAX) keep = A.dec[static_cast<size_t>(--chi) * T + tid];
-                if (!Live[ro * stride + col]) continue;
-                Live[ro * stride + col] = 0;
+                if (!A.live[ro * T + tid]) continue;
+                A.live[ro * T + tid] = 0;
                 uint2 outc = raw;
                 bool emit = true;
                 if (keep) {
                     const uint32_t k = keep == 1 ? (kinds & 3) : ((kinds >> 2) & 3);
                     const uint32_t src = keep == 1 ? (raw.y & 0xffff) : (raw.y >> 16);
                     if (k == OPND_REG) {
-                        Live[src * stride + col] = 1;
+                        A.live[src * T + tid] = 1;
                         emit = src != ro;
                     }
                     outc.x = OP_COPY | (k << 8) | (ro << 16);
                     outc.y = src;
                 } else {
-                    if ((kinds & 3) == OPND_REG) Live[(raw.y & 0xffff) * stride + col] = 1;
+                    if ((kinds & 3) == OPND_REG) A.live[(raw.y & 0xffff) * T + tid] = 1;
                     if (dev_is_binary(o) && ((kinds >> 2) & 3) == OPND_REG) {
-                        Live[(raw.y >> 16) * stride + col] = 1;
+                        A.live[(raw.y >> 16) * T + tid] = 1;
                     }
                 }
                 if (!emit) continue;
@@ -628,13 +603,8 @@ struct QCollapseArgs {
     uint32_t* status;
 };
 
-/// With SMEM the vertex evaluation's register file is in shared memory
-/// ([register][thread]), else in the global scratch of the arguments.
-template <bool SMEM>
-__global__ void __launch_bounds__(kQBlock)
-k_q_collapse(QCollapseArgs A)
+__global__ void k_q_collapse(QCollapseArgs A)
 {
-    extern __shared__ __align__(16) unsigned char csm[];
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     const QLevel& lv = A.t.lv[A.d];
     const QLevel& nx = A.t.lv[A.d + 1];
@@ -712,21 +682,20 @@ k_q_collapse(QCollapseArgs A)
         const TapeRef tr = in_cell ? nx.tape[c0] : root_tape_ref(A.bt);
         const RegClause* cl = A.arena + tr.off;
         const uint32_t rk = tr.root >> 16, rr = tr.root & 0xffff;
-        float* R = SMEM ? reinterpret_cast<float*>(csm) : A.regs;
-        const uint32_t T = SMEM ? kQBlock : A.T;
-        const uint32_t me = SMEM ? threadIdx.x : tid;
-        R[0 * T + me] = vx;
-        R[1 * T + me] = vy;
-        R[2 * T + me] = A.t.perp;
+        float* R = A.regs;
+        const uint32_t T = A.T;
+        R[0 * T + tid] = vx;
+        R[1 * T + tid] = vy;
+        R[2 * T + tid] = A.t.perp;
         const float* cp = A.bt.cpool;
         for (uint32_t c = 0; c < tr.len; ++c) {
             const RegClause k = cl[c];
             const uint8_t ka = k.kinds & 3, kb = (k.kinds >> 2) & 3;
-            const float a = ka == OPND_REG ? R[k.a * T + me] : __ldg(cp + k.a);
-            const float b = kb == OPND_REG ? R[k.b * T + me] : __ldg(cp + k.b);
-            R[k.out * T + me] = dv_value(k.op, a, b);
+            const float a = ka == OPND_REG ? R[k.a * T + tid] : __ldg(cp + k.a);
+            const float b = kb == OPND_REG ? R[k.b * T + tid] : __ldg(cp + k.b);
+            R[k.out * T + tid] = dv_value(k.op, a, b);
         }
-        const float value = rk == OPND_REG ? R[rr * T + me] : __ldg(cp + rr);
+        const float value = rk == OPND_REG ? R[rr * T + tid] : __ldg(cp + rr);
         if (!(fabsf(value) < A.max_err)) continue;
         const uint32_t rec = atomicAdd(A.rec_top, 1u);
         if (rec >= A.rec_cap) {
@@ -1035,13 +1004,7 @@ int render_contours(GpuTape& g, const double lo[2], const double hi[2], double z
             QIntervalArgs A{t, d, bt, arena, arena_top, arena_cap, b_out_tape.as<TapeRef>(),
                             b_rlo.as<float>(), b_rhi.as<float>(), b_rnan.as<uint8_t>(),
                             b_live.as<uint8_t>(), b_dec.as<uint8_t>(), dec_cap, T, status};
-            const size_t qsm = q_interval_smem(nregs);
-            if (qsm <= 200 * 1024 &&
-                raise_smem_limit(reinterpret_cast<const void*>(k_q_interval<true>), qsm)) {
-                k_q_interval<true><<<T / kQBlock, kQBlock, qsm, s>>>(A);
-            } else {
-                k_q_interval<false><<<T / kQBlock, kQBlock, 0, s>>>(A);
-            }
+            k_q_interval<<<T / 256, 256, 0, s>>>(A);
             k_q_branch_flags<<<(n + 255) / 256, 256, 0, s>>>(t.lv[d].type, n, b_flags.as<uint32_t>());
             note_launches(2);
             // exclusive scan of the branch flags on the host (quadtree
@@ -1076,13 +1039,7 @@ int render_contours(GpuTape& g, const double lo[2], const double hi[2], double z
         for (int d = L - 1; d >= 0; --d) {
             QCollapseArgs C{t, d, bt, arena, b_recs.as<QLeaf>(), rec_top, rec_cap, max_err,
                             b_cregs.as<float>(), T, status};
-            const size_t csm = static_cast<size_t>(nregs) * kQBlock * sizeof(float);
-            if (csm <= 200 * 1024 &&
-                raise_smem_limit(reinterpret_cast<const void*>(k_q_collapse<true>), csm)) {
-                k_q_collapse<true><<<T / kQBlock, kQBlock, csm, s>>>(C);
-            } else {
-                k_q_collapse<false><<<T / kQBlock, kQBlock, 0, s>>>(C);
-            }
+            k_q_collapse<<<T / 256, 256, 0, s>>>(C);
             note_launches(1);
         }
         uint32_t st = 0;

@@ -329,18 +329,20 @@ k_grad_backward(DevTape t, const uint32_t* __restrict__ pslot, uint32_t m,
                                        : make_float2(p0, 0.0f);
             }
             if (blocked) pd = make_float2(0.0f, 0.0f);
-            const float ga = adj * pd.x;
+            // register adjoints accumulate with one fused multiply-add per
+            // operand, as the compiled backward kernels do
             if (ka == OPND_REG) {
-                A[(ra * PTS + k) * B + tid] += ga;
+                float* aa = A + (ra * PTS + k) * B + tid;
+                *aa = __fmaf_rn(adj, pd.x, *aa);
             } else {
-                va += ga;
+                va += adj * pd.x;
             }
             if (binary) {
-                const float gb = adj * pd.y;
                 if (kb == OPND_REG) {
-                    A[(rb * PTS + k) * B + tid] += gb;
+                    float* ab = A + (rb * PTS + k) * B + tid;
+                    *ab = __fmaf_rn(adj, pd.y, *ab);
                 } else {
-                    vb += gb;
+                    vb += adj * pd.y;
                 }
             }
         }

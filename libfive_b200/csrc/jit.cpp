@@ -436,10 +436,15 @@ std::string backward_source(const RegTape& t, const std::vector<uint32_t>& slots
     } else if (t.root_kind == OPND_VAR) {
         s += "    if (gv) lfb_add_var(Gv, " + std::to_string(t.root - t.n_const) + ", s0);\n";
     }
-    auto contribution = [&](uint32_t kind, uint32_t idx, const std::string& g) {
-        if (kind == OPND_REG) return "a" + std::to_string(idx) + " += " + g + "; ";
+    // register adjoints: one fused multiply-add per operand (as the
+    // interpreter); variable adjoints: the product, summed per warp
+    auto contribution = [&](uint32_t kind, uint32_t idx, const std::string& pd) {
+        if (kind == OPND_REG) {
+            const std::string a = "a" + std::to_string(idx);
+            return a + " = __fmaf_rn(adj, " + pd + ", " + a + "); ";
+        }
         if (kind == OPND_VAR) {
-            return "if (gv) lfb_add_var(Gv, " + std::to_string(idx - t.n_const) + ", " + g +
+            return "if (gv) lfb_add_var(Gv, " + std::to_string(idx - t.n_const) + ", adj * " + pd +
                    "); ";
         }
         return std::string();
@@ -476,8 +481,8 @@ std::string backward_source(const RegTape& t, const std::vector<uint32_t>& slots
                      " * m] : 0.0f; ";
             }
         }
-        s += contribution(ka, cl.a, "adj * " + pdx);
-        if (binary) s += contribution(kb, cl.b, "adj * " + pdy);
+        s += contribution(ka, cl.a, pdx);
+        if (binary) s += contribution(kb, cl.b, pdy);
         s += "}\n";
     }
     s += "    if (ok) {\n"
@@ -750,16 +755,22 @@ std::string bseg_source(const RegTape& t, const JitSeg& sg, uint32_t k,
         if (ra[i].kind == OPND_VAR) var_slot(ra[i].var);
         if (rb[i].kind == OPND_VAR) var_slot(rb[i].var);
     }
-    auto contrib = [&](const Ref& rf, const std::string& g) -> std::string {
-        if (rf.kind == OPND_REG) return "    " + rf.adj + " += " + g + ";\n";
-        if (rf.kind == OPND_VAR) return "    va" + std::to_string(var_slot(rf.var)) + " += " + g + ";\n";
+    // register adjoints: one fused multiply-add per operand (as the
+    // interpreter); variable sums: product then sum
+    auto contrib = [&](const Ref& rf, const std::string& g, const std::string& p) -> std::string {
+        if (rf.kind == OPND_REG) {
+            return "    " + rf.adj + " = __fmaf_rn(" + g + ", " + p + ", " + rf.adj + ");\n";
+        }
+        if (rf.kind == OPND_VAR) {
+            return "    va" + std::to_string(var_slot(rf.var)) + " += " + g + " * " + p + ";\n";
+        }
         return std::string();
     };
     for (uint32_t c = sg.c1; c-- > sg.c0;) {
         const std::string c_ = std::to_string(c);
         const uint32_t i = c - sg.c0;
-        s += contrib(ra[i], "g" + c_ + " * pa" + c_);
-        if (rb[i].kind != 99u) s += contrib(rb[i], "g" + c_ + " * pb" + c_);
+        s += contrib(ra[i], "g" + c_, "pa" + c_);
+        if (rb[i].kind != 99u) s += contrib(rb[i], "g" + c_, "pb" + c_);
     }
     for (size_t g0 = 0; g0 < seg_vars.size(); g0 += 32) {
         const size_t base = vidx->size();

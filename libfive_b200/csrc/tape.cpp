@@ -10,20 +10,22 @@ namespace lfb {
 
 bool build_slot_tape(const Tree& root_, SlotTape& out, std::string* err)
 {
-    const Tree root = root_.optimized();
-    const auto flat = root.walk();
+    const Tree root = root_.optimized();   // flattened: no remap / apply left
+    std::vector<uint32_t> kid_pos;
+    const auto flat = root.walk(&kid_pos);
 
     // Slot ids count down from flat.size() so that the root lands on 1
-    // (deck.cpp:24-58); slot 0 is the reference's placeholder.
-    FlatMap<const Node*, uint32_t, PtrHash> slot(flat.size() + 4);
-    slot[nullptr] = 0;
-    // walk() lists every child before its parents, so operands always
-    // have a slot by the time they are read.
-    auto slot_of = [&slot](const Node* n) { return *slot.find(n); };
-    uint32_t id = static_cast<uint32_t>(flat.size());
+    // (deck.cpp:24-58); slot 0 is the reference's placeholder.  The node at
+    // position j of the walk takes slot flat.size() - j.
+    const uint32_t n_flat = static_cast<uint32_t>(flat.size());
+    uint32_t id = n_flat;
     std::vector<SlotClause> rev;
     rev.reserve(flat.size());
-    for (const Node* m : flat) {
+    const Node* axes[3] = {Tree::X().get(), Tree::Y().get(), Tree::Z().get()};
+    uint32_t axis_slot[3] = {0, 0, 0};
+    for (uint32_t j = 0; j < n_flat; ++j) {
+        const Node* m = flat[j];
+        auto slot_of_kid = [&](int i) { return n_flat - kid_pos[2 * j + i]; };
         switch (m->kind) {
             case Kind::Constant:
                 out.constants.push_back({id, m->value});
@@ -38,34 +40,35 @@ bool build_slot_tape(const Tree& root_, SlotTape& out, std::string* err)
                 }
                 break;
             case Kind::Unary:
-                rev.push_back({m->op, id, slot_of(m->kid[0]), 0});
+                rev.push_back({m->op, id, slot_of_kid(0), 0});
                 break;
             case Kind::Binary:
-                rev.push_back({m->op, id, slot_of(m->kid[0]),
-                               slot_of(m->kid[1])});
+                rev.push_back({m->op, id, slot_of_kid(0), slot_of_kid(1)});
                 break;
             default:
                 if (err) *err = "tree contains an unsupported node";
                 return false;
         }
-        slot[m] = id--;
+        for (int a = 0; a < 3; ++a) {
+            if (m == axes[a]) axis_slot[a] = id;
+        }
+        --id;
     }
     out.clauses.assign(rev.rbegin(), rev.rend());
 
-    const Node* axes[3] = {Tree::X().get(), Tree::Y().get(), Tree::Z().get()};
-    for (auto a : axes) {
-        if (!slot.find(a)) {
-            const uint32_t next = static_cast<uint32_t>(slot.size());
-            slot[a] = next;
-        }
+    // Axes that the tree does not use take the next free slots, in x, y, z
+    // order.
+    uint32_t next = n_flat + 1;
+    for (int a = 0; a < 3; ++a) {
+        if (!axis_slot[a]) axis_slot[a] = next++;
     }
-    out.num_clauses = static_cast<uint32_t>(slot.size() - 1);
-    out.X = slot_of(axes[0]);
-    out.Y = slot_of(axes[1]);
-    out.Z = slot_of(axes[2]);
+    out.num_clauses = next - 1;
+    out.X = axis_slot[0];
+    out.Y = axis_slot[1];
+    out.Z = axis_slot[2];
     std::sort(out.vars.begin(), out.vars.end(),
               [](const auto& a, const auto& b) { return a.first < b.first; });
-    out.root = slot_of(root.get());
+    out.root = 1;   // the walk ends at the root
     return true;
 }
 

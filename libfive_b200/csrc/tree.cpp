@@ -462,36 +462,77 @@ std::vector<const Node*> Tree::walk() const
     if (p->flags & Node::HAS_REMAP) {
         return flatten().walk();
     }
+    return walk(nullptr);
+}
+
+std::vector<const Node*> Tree::walk(std::vector<uint32_t>* kid_pos) const
+{
+    // Pass 1 gives every distinct node a dense index (one hash lookup per
+    // edge of the DAG) and counts its parents; pass 2 emits a node once all
+    // its parents are out, through the dense arrays alone, and reversing
+    // that order puts every child before its parents (tree.cpp:530-594).
     static std::atomic<size_t> count_hint{1024};   // capacity hint, as in optimized()
-    FlatMap<const Node*, unsigned, PtrHash> count(count_hint.load(std::memory_order_relaxed));
-    std::vector<const Node*> todo{p};
+    FlatMap<const Node*, uint32_t, PtrHash> index(count_hint.load(std::memory_order_relaxed));
+    std::vector<const Node*> nodes{p};
+    std::vector<uint32_t> parents{0};
+    std::vector<uint32_t> kids{UINT32_MAX, UINT32_MAX};   // 2 per index
+    nodes.reserve(count_hint.load(std::memory_order_relaxed) + 1);
+    index.emplace(p, 0u);
     auto nkids = [](const Node* n) {
         return n->kind == Kind::Unary ? 1 : n->kind == Kind::Binary ? 2 : 0;
     };
+    std::vector<uint32_t> todo{0};
     while (!todo.empty()) {
-        const Node* n = todo.back();
+        const uint32_t ni = todo.back();
         todo.pop_back();
+        const Node* n = nodes[ni];
         for (int i = 0; i < nkids(n); ++i) {
-            if (count[n->kid[i]]++ == 0) {
-                todo.push_back(n->kid[i]);
+            const auto r = index.emplace(n->kid[i], static_cast<uint32_t>(nodes.size()));
+            const uint32_t ki = *r.first;
+            if (r.second) {
+                nodes.push_back(n->kid[i]);
+                parents.push_back(0);
+                kids.push_back(UINT32_MAX);
+                kids.push_back(UINT32_MAX);
+                todo.push_back(ki);
+            }
+            kids[2 * ni + i] = ki;
+            ++parents[ki];
+        }
+    }
+    const size_t total = nodes.size();
+    std::vector<uint32_t> order;   // indices, root first
+    order.reserve(total);
+    todo.push_back(0);
+    while (!todo.empty()) {
+        const uint32_t ni = todo.back();
+        todo.pop_back();
+        order.push_back(ni);
+        for (int i = 0; i < 2; ++i) {
+            const uint32_t ki = kids[2 * ni + i];
+            if (ki != UINT32_MAX && --parents[ki] == 0) {
+                todo.push_back(ki);
             }
         }
     }
-    std::vector<const Node*> flat;
-    flat.reserve(count.size() + 1);
-    todo.push_back(p);
-    while (!todo.empty()) {
-        const Node* n = todo.back();
-        todo.pop_back();
-        flat.push_back(n);
-        for (int i = 0; i < nkids(n); ++i) {
-            if (--*count.find(n->kid[i]) == 0) {
-                todo.push_back(n->kid[i]);
+    count_hint.store(std::max<size_t>(1024, total), std::memory_order_relaxed);
+    std::vector<const Node*> flat(total);
+    std::vector<uint32_t> pos(kid_pos ? total : 0);
+    for (size_t j = 0; j < total; ++j) {
+        const uint32_t ni = order[total - 1 - j];
+        flat[j] = nodes[ni];
+        if (kid_pos) pos[ni] = static_cast<uint32_t>(j);
+    }
+    if (kid_pos) {
+        kid_pos->assign(2 * total, UINT32_MAX);
+        for (size_t j = 0; j < total; ++j) {
+            const uint32_t ni = order[total - 1 - j];
+            for (int i = 0; i < 2; ++i) {
+                const uint32_t ki = kids[2 * ni + i];
+                if (ki != UINT32_MAX) (*kid_pos)[2 * j + i] = pos[ki];
             }
         }
     }
-    count_hint.store(std::max<size_t>(1024, count.size()), std::memory_order_relaxed);
-    std::reverse(flat.begin(), flat.end());
     return flat;
 }
 
@@ -621,6 +662,90 @@ Key key_of(const Node* n)
     return k;
 }
 
+/// The optimizer's table of canonical nodes: one reference to each, keyed by
+/// the node's structure (key_of).  Slots are bare node pointers (8 bytes,
+/// against 64 for a (Key, Tree) pair) probed through a dense one-byte tag
+/// array, so that the table of a model of some 10^4-10^5 nodes stays in the
+/// host's L2 cache; a slot's node is read only when its tag matches.
+class CanonSet {
+public:
+    explicit CanonSet(size_t expected)
+    {
+        size_t cap = 16;
+        while (cap < 2 * expected) cap <<= 1;
+        reset(cap);
+    }
+    ~CanonSet()
+    {
+        for (size_t i = 0; i < slots_.size(); ++i) {
+            if (tags_[i]) Tree::reclaim(slots_[i]);
+        }
+    }
+    CanonSet(const CanonSet&) = delete;
+    CanonSet& operator=(const CanonSet&) = delete;
+
+    size_t size() const { return count_; }
+
+    /// The stored node structurally equal to n; when there is none, n itself,
+    /// stored without taking a reference (*inserted = true: the caller hands
+    /// the table one).
+    const Node* intern(const Node* n, bool* inserted)
+    {
+        if ((count_ + 1) * 2 > slots_.size()) grow();
+        const Key k = key_of(n);
+        const uint64_t h = static_cast<uint64_t>(KeyHash()(k)) * 0x9e3779b97f4a7c15ull;
+        const uint8_t t = static_cast<uint8_t>((h >> 8) | 1);
+        size_t i = static_cast<size_t>(h >> shift_) & mask_;
+        while (tags_[i]) {
+            if (tags_[i] == t && (slots_[i] == n || key_of(slots_[i]) == k)) {
+                *inserted = false;
+                return slots_[i];
+            }
+            i = (i + 1) & mask_;
+        }
+        tags_[i] = t;
+        slots_[i] = n;
+        ++count_;
+        *inserted = true;
+        return n;
+    }
+
+private:
+    void reset(size_t cap)
+    {
+        slots_.assign(cap, nullptr);
+        tags_.assign(cap, 0);
+        mask_ = cap - 1;
+        shift_ = 64;
+        for (size_t c = cap; c > 1; c >>= 1) --shift_;
+        count_ = 0;
+    }
+    void grow()
+    {
+        std::vector<const Node*> old_slots;
+        std::vector<uint8_t> old_tags;
+        old_slots.swap(slots_);
+        old_tags.swap(tags_);
+        reset(old_slots.size() * 2);
+        for (size_t i = 0; i < old_slots.size(); ++i) {
+            if (!old_tags[i]) continue;
+            const uint64_t h = static_cast<uint64_t>(KeyHash()(key_of(old_slots[i]))) *
+                               0x9e3779b97f4a7c15ull;
+            size_t j = static_cast<size_t>(h >> shift_) & mask_;
+            while (tags_[j]) j = (j + 1) & mask_;
+            tags_[j] = old_tags[i];
+            slots_[j] = old_slots[i];
+            ++count_;
+        }
+    }
+
+    std::vector<const Node*> slots_;
+    std::vector<uint8_t> tags_;
+    size_t mask_ = 0;
+    unsigned shift_ = 64;
+    size_t count_ = 0;
+};
+
 /// Orders trees the way the reference orders them by address: here by the
 /// creation serial number.
 bool serial_less(const Node* a, const Node* b)
@@ -646,18 +771,18 @@ Tree Tree::optimized() const
     // Sized from the previous call (a capacity hint only: trees built
     // repeatedly from the same kind of model skip the rehashing).
     static std::atomic<size_t> canon_hint{1024};
-    FlatMap<Key, Tree, KeyHash> canonical(canon_hint.load(std::memory_order_relaxed));
+    CanonSet canonical(canon_hint.load(std::memory_order_relaxed));
     auto uniq_new = [&canonical](Tree&& t) -> const Node* {
-        const Key k = key_of(t.p);
-        return canonical.emplace(k, std::move(t)).first->p;
+        bool inserted = false;
+        const Node* c = canonical.intern(t.get(), &inserted);
+        if (inserted) t.release();   // the table keeps t's reference
+        return c;
     };
     auto uniq_old = [&canonical](const Node* n) -> const Node* {
-        const Key k = key_of(n);
-        if (Tree* found = canonical.find(k)) {
-            return found->p;
-        }
-        canonical.emplace(k, Tree(n));
-        return n;
+        bool inserted = false;
+        const Node* c = canonical.intern(n, &inserted);
+        if (inserted) Tree(n).release();   // one new reference, for the table
+        return c;
     };
     // The constant 1 is created on first use, like the reference's static
     // (tree.cpp:251-254); its creation serial orders it among affine terms,

@@ -75,6 +75,11 @@ public:
 
     /// Leaves-to-root topological order of the (flattened) DAG.
     std::vector<const Node*> walk() const;
+    /// The same order, and for the node at position i the positions of its
+    /// operands in (*kid_pos)[2 i] and [2 i + 1] (UINT32_MAX where it has
+    /// fewer), for passes that would otherwise look every operand up.  The
+    /// tree must not need flattening (no remap / apply nodes).
+    std::vector<const Node*> walk(std::vector<uint32_t>* kid_pos) const;
     size_t size() const;
 
     bool is_valid() const { return p && p->kind != Kind::Invalid; }

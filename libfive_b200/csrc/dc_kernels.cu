@@ -966,11 +966,7 @@ k_interval_group(GroupArgs A, int d)
 
 struct EdgeSlot {
     double t0[3], t1[3];   // current search bracket: inside, outside
-    Qef q;
     float g0[4], g1[4];    // gradient + value at t0 / t1
-    int32_t rank;
-    uint8_t lat;           // lattice edge id
-    uint8_t exists;        // received at least one sample
     uint8_t amb[2];        // tied min/max at t0 / t1
 };
 
@@ -982,8 +978,9 @@ struct LeafWarpShared {
     int32_t rec[8];
 };
 
-/// Per-warp state kept in global memory (L1-cached): edge brackets / QEFs
-/// and the feature evaluator's scratch, one slice per resident warp.
+/// Per-warp state kept in global memory (L1-cached): edge brackets, the
+/// gradients at their final ends and the feature evaluator's scratch, one
+/// slice per resident warp.
 struct LeafWarpScratch {
     FeatureScratch fs;
     EdgeSlot e[54];
@@ -1029,12 +1026,6 @@ __device__ __forceinline__ LeafOp* leaf_ops(uint32_t off)
     return reinterpret_cast<LeafOp*>(rf_smem + off);
 }
 
-/// Values of the tape at four points per lane (point k of this lane in
-/// component k).  Tapes of at most kLeafOps clauses were decoded into the
-/// warp's buffer when the group started; longer ones are decoded chunk by
-/// chunk here.  With TIES, bit k of *amb reports a min / max with equal
-/// arguments at point k (ArrayEvaluator::getAmbiguous, eval_array.cpp:
-/// 197-217).
 /// dv_value on four points (a float4 per operand), the value rules of
 /// dev_point.cuh; the rare opcodes out of line.
 __device__ __forceinline__ float4 dv_value4f(uint8_t o, const float4& a, const float4& b)
@@ -1392,9 +1383,6 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
             pt_pos(f0 ? p0 : p1, a);
             pt_pos(f0 ? p1 : p0, b);
             for (int k = 0; k < 3; ++k) { es.t0[k] = a[k]; es.t1[k] = b[k]; }
-            es.lat = static_cast<uint8_t>(e);
-            es.exists = 0;
-            qef_zero(es.q);
         }
         __syncwarp();
         if (lane == 0) S->nslots = static_cast<uint8_t>(first_slot + __popc(m));

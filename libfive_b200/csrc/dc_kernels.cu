@@ -1167,6 +1167,11 @@ __global__ void __launch_bounds__(256, 3)
 k_leaf_groups(LeafArgs A, uint32_t n_groups)
 {
     extern __shared__ __align__(16) unsigned char lsmem[];
+    // The edge search's sample fractions j / 15, divided once per block
+    // (the same correctly rounded quotients as dividing at every sample).
+    __shared__ double frac_tab[16];
+    if (threadIdx.x < 16) frac_tab[threadIdx.x] = threadIdx.x / (16 - 1.0);
+    __syncthreads();
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int wpb = blockDim.x >> 5;
@@ -1402,7 +1407,7 @@ k_leaf_groups(LeafArgs A, uint32_t n_groups)
     // sub-batch k is sample 1 + p % 14 of edge base + p / 14.  Most groups
     // have nine crossing edges, one pass per round.
     auto sample = [&](int slot, int j, double q[3]) {
-        const double frac = j / (16 - 1.0);
+        const double frac = frac_tab[j];
         const EdgeSlot& es = W->e[slot];
         for (int k = 0; k < 3; ++k) q[k] = es.t0[k] * (1 - frac) + es.t1[k] * frac;
     };

@@ -421,7 +421,9 @@ def run_ours(args, world, rank, local):
                 "traffic": traffic,
                 "traffic_source": ("ncu capture of the leaf stage's four kernels on this "
                                    "workload, dram__bytes_read.sum + dram__bytes_write.sum "
-                                   "(profiles/k_leaf_groups_csg2000_depth10_dram.md)"
+                                   "(profiles/k_leaf_groups_csg2000_depth10_dram.md), taken "
+                                   "before the edge-slot cleanup of k_leaf_groups: an upper "
+                                   "bound for this build"
                                    if traffic is not None else None),
             },
             "stages_ms": {"interval": stats.ms_interval, "leaf": stats.ms_leaf,

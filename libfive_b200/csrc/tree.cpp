@@ -956,21 +956,24 @@ Tree Tree::optimized() const
         } else if (task.type == Task::UP) {
             --depth;
             const Node* d = task.t;
-            const Node* self = uniq_old(d);
+            // The reference enters d in the table before replacing it when
+            // an operand changed (tree.cpp:776-789); that entry can never be
+            // found again (no node built later has d's old operands, which
+            // only ever come out of this pass changed), so it is skipped.
+            const Node* self = nullptr;
             if (d->kind == Kind::Unary) {
                 const Node* a = out.back();
                 out.pop_back();
-                if (a != d->kid[0]) {
-                    self = uniq_new(unary_n(d->op, a));
-                }
+                self = a != d->kid[0] ? uniq_new(unary_n(d->op, a)) : uniq_old(d);
             } else if (d->kind == Kind::Binary) {
                 const Node* a = out.back();
                 out.pop_back();
                 const Node* b = out.back();
                 out.pop_back();
-                if (a != d->kid[0] || b != d->kid[1]) {
-                    self = uniq_new(binary_n(d->op, a, b));
-                }
+                self = (a != d->kid[0] || b != d->kid[1]) ? uniq_new(binary_n(d->op, a, b))
+                                                          : uniq_old(d);
+            } else {
+                self = uniq_old(d);
             }
             deliver(self, task.scale);
         } else if (task.type == Task::UP_AFFINE) {

@@ -15,7 +15,56 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from libfive_b200 import workloads  # noqa: E402
-from libfive_b200.shape import X, Y, Z, slot_tape  # noqa: E402
+from libfive_b200.shape import Shape, X, Y, Z, slot_tape  # noqa: E402
+
+UNARY = ("square", "sqrt", "neg", "abs", "sin", "cos", "tan", "asin", "acos", "atan",
+         "exp", "log", "const-var")
+BINARY = ("add", "mul", "min", "max", "sub", "div", "atan2", "pow", "nth-root", "mod",
+          "nanfill", "compare")
+
+
+def random_dag(seed, n_nodes):
+    """A seeded random expression DAG over every unary and binary opcode:
+    operands drawn from all earlier nodes (so subtrees are shared), from a
+    small set of repeated constants (0, 1, -1, 2: the optimizer's folding
+    and affine cases) or from three free variables; every node is then
+    folded into one root by min / max / add / sub / mul, and some trees are
+    remapped.  Returns (shape, variables in creation order)."""
+    rng = workloads.SplitMix64(seed)
+    vs = [Shape.var() for _ in range(3)]
+    pool = [X(), Y(), Z()]
+
+    def operand():
+        k = rng.below(10)
+        if k == 0:
+            return Shape.constant((0.0, 1.0, -1.0, 2.0)[rng.below(4)])
+        if k == 1:
+            return Shape.constant(rng.uniform(-2, 2))
+        if k == 2:
+            return vs[rng.below(3)]
+        return pool[rng.below(len(pool))]
+
+    for _ in range(n_nodes):
+        k = rng.below(10)
+        if k == 0:
+            node = Shape.constant(rng.uniform(-2, 2))
+        elif k <= 3:
+            node = Shape.new(UNARY[rng.below(len(UNARY))], pool[rng.below(len(pool))])
+        else:
+            node = Shape.new(BINARY[rng.below(len(BINARY))], operand(), operand())
+        pool.append(node)
+    level = pool[3:]
+    while len(level) > 1:
+        nxt = [Shape.new(("min", "max", "add", "sub", "mul")[rng.below(5)], level[i], level[i + 1])
+               for i in range(0, len(level) - 1, 2)]
+        if len(level) % 2:
+            nxt.append(level[-1])
+        level = nxt
+    root = level[0]
+    if rng.below(4) == 0:
+        x, y, z = X(), Y(), Z()
+        root = root.remap(x + y * 0.5, y.square() - 1, z * 2 + x)
+    return root, vs
 
 
 def trees():
@@ -32,6 +81,8 @@ def trees():
     x, y, z = X(), Y(), Z()
     out["affine"] = ((((x * 2 + y * 3 - z / 4) * (x - 1) * (y + 2)).max(-(x + x + x))
                       .min(z * 0.5 - x * 0.5)) / (y.square() + 1), [])
+    for s in range(40):
+        out["dag%d" % s] = random_dag(600 + s, 20 + 10 * s)
     return out
 
 

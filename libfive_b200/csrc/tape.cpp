@@ -2,9 +2,6 @@
 
 #include <algorithm>
 #include <queue>
-#include <unordered_map>
-
-#include "flat_map.hpp"
 
 namespace lfb {
 

@@ -423,7 +423,7 @@ def run_ours(args, world, rank, local):
                                    "workload, dram__bytes_read.sum + dram__bytes_write.sum "
                                    "(profiles/k_leaf_groups_csg2000_depth10_dram.md), taken "
                                    "before the edge-slot cleanup of k_leaf_groups: an upper "
-                                   "bound for this build"
+                                   "bound for the current kernels"
                                    if traffic is not None else None),
             },
             "stages_ms": {"interval": stats.ms_interval, "leaf": stats.ms_leaf,

@@ -710,6 +710,28 @@ public:
         return n;
     }
 
+    /// The stored constant whose key is v's (every NaN one key, +0 and -0
+    /// one key), or null: lets a caller skip building a constant node that
+    /// intern() would only find already present.
+    const Node* find_constant(float v) const
+    {
+        Key k{};
+        if (std::isnan(v)) {
+            k.tag = 1;
+        } else {
+            k.tag = 2;
+            k.value = v;
+        }
+        const uint64_t h = static_cast<uint64_t>(KeyHash()(k)) * 0x9e3779b97f4a7c15ull;
+        const uint8_t t = static_cast<uint8_t>((h >> 8) | 1);
+        size_t i = static_cast<size_t>(h >> shift_) & mask_;
+        while (tags_[i]) {
+            if (tags_[i] == t && key_of(slots_[i]) == k) return slots_[i];
+            i = (i + 1) & mask_;
+        }
+        return nullptr;
+    }
+
 private:
     void reset(size_t cap)
     {
@@ -777,6 +799,13 @@ Tree Tree::optimized() const
         const Node* c = canonical.intern(t.get(), &inserted);
         if (inserted) t.release();   // the table keeps t's reference
         return c;
+    };
+    // uniq_new(constant(v)) without building the node when the table
+    // already holds an equal constant (the skipped node would only have
+    // taken a creation serial, which orders nothing that survives).
+    auto uniq_const = [&canonical, &uniq_new](float v) -> const Node* {
+        if (const Node* c = canonical.find_constant(v)) return c;
+        return uniq_new(constant(v));
     };
     auto uniq_old = [&canonical](const Node* n) -> const Node* {
         bool inserted = false;
@@ -1028,15 +1057,15 @@ Tree Tree::optimized() const
                     }
                     if (mult != 1) {
                         if (t == ONE()) {
-                            t = uniq_new(constant(mult));
+                            t = uniq_const(mult);
                         } else {
                             t = uniq_new(binary_n(op::MUL, t,
-                                                  uniq_new(constant(mult))));
+                                                  uniq_const(mult)));
                         }
                     }
                     acc = acc ? uniq_new(binary_n(op::ADD, acc, t)) : t;
                 }
-                return acc ? acc : uniq_new(constant(0.0f));
+                return acc ? acc : uniq_const(0.0f);
             };
             const Node* P = collapse(pos);
             const Node* N = collapse(neg);

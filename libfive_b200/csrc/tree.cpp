@@ -134,9 +134,11 @@ Tree Tree::make(Kind k, int o, float value, const Node* a, const Node* b,
         if (kk) kk->refs.fetch_add(1, std::memory_order_relaxed);
     }
     n->flags = compute_flags(k, o, n->kid);
-    n->serial = g_serial.fetch_add(1);
-    n->refs.store(0);
-    return Tree(n, true, false);
+    n->serial = g_serial.fetch_add(1, std::memory_order_relaxed);
+    // The node is not shared yet: its one reference (the returned handle's)
+    // needs no read-modify-write.
+    n->refs.store(1, std::memory_order_relaxed);
+    return Tree(n, false, false);
 }
 
 Tree Tree::constant(double v)
